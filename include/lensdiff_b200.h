@@ -1,0 +1,265 @@
+/*
+ * lensdiff_b200.h — C ABI of the B200 (sm_100a) LensDiff diffraction path.
+ *
+ * The library replaces one call of the LensDiff OpenFX plugin:
+ *
+ *     bool RunLensDiffCuda(const LensDiffRenderRequest& request,
+ *                          const LensDiffParams& params,
+ *                          LensDiffPsfBankCache& cache,
+ *                          std::string* error);
+ *
+ * declared at source/src/cuda/LensDiffCuda.h:7-10 and called from
+ * source/src/LensDiff.cpp:3833.  The structs below are plain-old-data mirrors
+ * of the reference's request and parameter types (source/src/core/
+ * LensDiffTypes.h:94-208); enum values keep the reference's declaration order
+ * (LensDiffTypes.h:14-91) so a field can be copied with a cast.  No torch or
+ * CUDA type appears in a signature: device pointers and the stream travel as
+ * `void*`.
+ *
+ * Every entry point returns an ld_status_code.  On failure `status->stage`
+ * holds a short stage string in the reference's style
+ * ("missing-source-or-destination-cuda-buffer", ...).  The library never falls
+ * back to a CPU path.
+ */
+#ifndef LENSDIFF_B200_H
+#define LENSDIFF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LD_ABI_VERSION 1
+#define LD_MAX_WAVELENGTHS 64   /* reference caps at 9 (LensDiffTypes.h:12) */
+#define LD_NOLL_COUNT 23        /* Noll index j = 0..22; j = 0 unused      */
+#define LD_STAGE_LEN 128
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum {
+    LD_OK = 0,
+    LD_ERR_ARG = 1,         /* malformed request or parameter             */
+    LD_ERR_OOM = 2,         /* device allocation failed                   */
+    LD_ERR_BUDGET = 3,      /* request does not fit the HBM budget        */
+    LD_ERR_TIMEOUT = 4,     /* a bounded device wait ran out              */
+    LD_ERR_CUDA = 5,        /* a CUDA runtime / launch error              */
+    LD_ERR_UNSUPPORTED = 6  /* valid reference setting not on this path   */
+} ld_status_code;
+
+/* ---- enums (values mirror LensDiffTypes.h:14-91) ------------------------ */
+enum { LD_EXTRACT_MAXRGB = 0, LD_EXTRACT_LUMA = 1 };
+enum {
+    LD_APERTURE_CIRCLE = 0, LD_APERTURE_POLYGON = 1, LD_APERTURE_STAR = 2,
+    LD_APERTURE_SPIRAL = 3, LD_APERTURE_CUSTOM = 4, LD_APERTURE_HEXAGON = 5,
+    LD_APERTURE_SQUAREGRID = 6, LD_APERTURE_SNOWFLAKE = 7
+};
+enum { LD_APOD_FLAT = 0, LD_APOD_COSINE = 1, LD_APOD_GAUSSIAN = 2 };
+enum { LD_SPECTRAL_MONO = 0, LD_SPECTRAL_TRISTIMULUS = 1, LD_SPECTRAL_5 = 2, LD_SPECTRAL_9 = 3 };
+enum { LD_STYLE_NATURAL = 0, LD_STYLE_CYANMAGENTA = 1, LD_STYLE_WARMCOOL = 2 };
+enum { LD_LOOK_PHYSICAL = 0, LD_LOOK_SPLIT = 1 };
+enum { LD_ENERGY_PRESERVE = 0, LD_ENERGY_AUGMENT = 1 };
+enum { LD_DEBUG_FINAL = 0 };  /* other LensDiffDebugView values: UNSUPPORTED */
+enum { LD_TRANSFER_LINEAR = 0, LD_TRANSFER_DAVINCI_INTERMEDIATE = 1 };
+enum { LD_PHASE_OFF = 0, LD_PHASE_ENABLED = 1 };
+
+/* ---- extensions (not in the reference) ---------------------------------- */
+enum {
+    LD_RGB_FROM_CALLER = 0,  /* natural/style matrices supplied by the caller
+                                (the plugin computes them with its own
+                                BuildLensDiffSpectrumConfig, LensDiffSpectrum.cpp:380) */
+    LD_RGB_GAUSSIAN = 1      /* Gaussian RGB responses: rgb_gauss_center/sigma */
+};
+enum {
+    LD_FFT_OWN_FP32 = 0,     /* hand-written FP32 Stockham chain ("plain")   */
+    LD_FFT_OWN_CHOSEN = 1,   /* hand-written chain, FP16 tile-scaled spectra */
+    LD_FFT_CUFFT = 2         /* same chain with cuFFT transforms (comparator) */
+};
+
+/* ---- request (mirrors LensDiffRenderRequest, LensDiffTypes.h:94-126) ---- */
+typedef struct {
+    int32_t x1, y1, x2, y2;
+} ld_rect;
+
+typedef struct {
+    void* data;              /* DEVICE pointer to float RGBA rows           */
+    int64_t row_bytes;
+    ld_rect bounds;
+    int32_t origin_x, origin_y;
+    int32_t components;      /* must be 4                                   */
+    int32_t bytes_per_component; /* must be 4                               */
+} ld_image_view;
+
+typedef struct {
+    ld_rect render_window;
+    ld_rect frame_bounds;
+    ld_image_view src;
+    ld_image_view dst;
+    int32_t frame_short_side_px;
+    int32_t host_enabled_cuda_render;
+    void* cuda_stream;       /* cudaStream_t of the host                    */
+} ld_render_request;
+
+/* ---- parameters (mirrors LensDiffParams, LensDiffTypes.h:128-208) ------- */
+typedef struct {
+    int32_t extraction_mode;
+    int32_t aperture_mode;
+    int32_t apodization_mode;
+    int32_t spectral_mode;
+    int32_t spectrum_style;
+    int32_t look_mode;
+    int32_t energy_mode;
+    int32_t debug_view;
+    int32_t input_transfer;
+    int32_t resolution_aware;
+
+    double threshold;
+    double softness_stops;
+    double point_emphasis;
+    double core_preserve;
+
+    int32_t blade_count;
+    int32_t vane_count;
+    double roundness;
+    double rotation_deg;
+    double central_obstruction;
+    double vane_thickness;
+    double diffraction_scale_px;   /* percent of the optics short side      */
+    int32_t pupil_resolution;
+    int32_t frame_short_side_px;
+    double max_kernel_radius_px;   /* percent of the optics short side      */
+
+    int32_t phase_mode;
+    int32_t chromatic_affects_luma;
+    double phase_defocus;          /* Noll 4  */
+    double phase_astigmatism0;     /* Noll 6  */
+    double phase_astigmatism45;    /* Noll 5  */
+    double phase_coma_x;           /* Noll 8  */
+    double phase_coma_y;           /* Noll 7  */
+    double phase_spherical;        /* Noll 11 */
+    double phase_trefoil_x;        /* Noll 10 */
+    double phase_trefoil_y;        /* Noll 9  */
+    double phase_secondary_astigmatism0;  /* Noll 12 */
+    double phase_secondary_astigmatism45; /* Noll 13 */
+    double phase_quadrafoil0;      /* Noll 14 */
+    double phase_quadrafoil45;     /* Noll 15 */
+    double phase_secondary_coma_x; /* Noll 16 */
+    double phase_secondary_coma_y; /* Noll 17 */
+    double pupil_decenter_x;
+    double pupil_decenter_y;
+
+    double phase_field_strength;
+    double phase_field_edge_bias;
+    double phase_field_defocus;
+    double phase_field_astig_radial;
+    double phase_field_astig_tangential;
+    double phase_field_coma_radial;
+    double phase_field_coma_tangential;
+    double phase_field_spherical;
+    double phase_field_trefoil_radial;
+    double phase_field_trefoil_tangential;
+    double phase_field_secondary_astig_radial;
+    double phase_field_secondary_astig_tangential;
+    double phase_field_quadrafoil_radial;
+    double phase_field_quadrafoil_tangential;
+    double phase_field_secondary_coma_radial;
+    double phase_field_secondary_coma_tangential;
+
+    double spectrum_force;
+    double spectrum_saturation;
+    double chromatic_focus;
+    double chromatic_spread;
+    double creative_fringe;
+    double scatter_amount;
+    double scatter_radius;
+
+    double effect_gain;
+    double core_compensation;
+    double anisotropy_emphasis;
+    double core_gain;
+    double structure_gain;
+    double core_shoulder;
+    double structure_shoulder;
+
+    /* ---- extensions; all-zero keeps the reference's behaviour ---------- */
+    int32_t wavelength_count;      /* 0: the spectral_mode's wavelengths    */
+    float wavelengths_nm[LD_MAX_WAVELENGTHS];
+    int32_t rgb_mode;              /* LD_RGB_FROM_CALLER / LD_RGB_GAUSSIAN   */
+    int32_t field_grid;            /* 0: reference 3x3 when field phase on   */
+    float natural_matrix[3 * LD_MAX_WAVELENGTHS]; /* row-major 3 x count     */
+    float style_matrix[3 * LD_MAX_WAVELENGTHS];
+    float rgb_gauss_center_nm[3];  /* R, G, B                                */
+    float rgb_gauss_sigma_nm;
+    double noll[LD_NOLL_COUNT];    /* added to the named terms; j=2,3,18..22 */
+    int32_t fft_form;              /* LD_FFT_OWN_FP32 / _CHOSEN / _CUFFT      */
+    int32_t reserved[7];
+} ld_params;
+
+typedef struct {
+    int32_t code;                  /* ld_status_code                          */
+    char stage[LD_STAGE_LEN];      /* reference-style stage string            */
+    int32_t bank_rebuilt;          /* 1 if this call rebuilt the PSF bank     */
+    int32_t spectra_rebuilt;       /* 1 if the kernel spectra were rebuilt    */
+    int32_t pupil_size;            /* N_p                                     */
+    int32_t raw_psf_size;          /* S                                       */
+    int32_t max_kernel_radius;     /* R_max                                   */
+    int32_t support_radius;        /* max adaptive support radius (export)    */
+    int32_t grid_requested_w, grid_requested_h;  /* W+K-1, H+K-1              */
+    int32_t grid_used_w, grid_used_h;            /* smooth FFT grid used      */
+    int32_t wavelength_count;
+    int32_t kernel_launches;       /* kernels this call launched              */
+} ld_status;
+
+typedef struct ld_ctx ld_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+/* Creates a context on `device`.  hbm_budget_bytes = 0 means no budget. */
+int ld_create(ld_ctx** out, int device, size_t hbm_budget_bytes);
+void ld_destroy(ld_ctx* ctx);
+int ld_abi_version(void);
+/* Device bytes the context holds (work buffers + caches). */
+size_t ld_device_bytes(const ld_ctx* ctx);
+/* Drops the cached PSF banks and kernel spectra. */
+void ld_clear_caches(ld_ctx* ctx);
+
+/* ---- the drop-in render (replaces RunLensDiffCuda, LensDiffCuda.h:7-10) -- */
+/* Enqueues the whole frame on request->cuda_stream; no host synchronisation
+ * except the one-time first-zero calibration per (pupil size, PSF size). */
+int ld_render(ld_ctx* ctx, const ld_render_request* request,
+              const ld_params* params, ld_status* status);
+
+/* ---- PSF bank (EnsureLensDiffPsfBank, LensDiffCpuReference.h:62-63) ----- */
+/* Builds (or finds cached) the bank for `params` on `stream`. */
+int ld_build_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream,
+                      ld_status* status);
+
+/* Copies the bank's `full` kernels to HOST memory: for wavelength i,
+ * sizes[i] = 2*radius_i+1 and a sizes[i]^2 row-major kernel is written at
+ * kernels_out + offsets[i].  `capacity` is the float count of kernels_out.
+ * Synchronises `stream`. */
+int ld_export_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream,
+                       float* wavelengths_out, int32_t* sizes, int64_t* offsets,
+                       float* kernels_out, int64_t capacity, ld_status* status);
+
+/* Writes the normalised, fft-shifted raw PSF (S x S floats, DEVICE pointer)
+ * of wavelength `wavelength_index`, as BuildLensDiffShiftedRawPsf does
+ * (LensDiffCpuReference.cpp:831-859, chromatic focus applied as at :1720-1728). */
+int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index,
+               float* psf_out_device, void* stream, ld_status* status);
+
+/* Resolved sizes of the path for `params` (N_p, S, R_max, wavelength count). */
+int ld_resolve_sizes(const ld_params* params, int32_t* pupil_size,
+                     int32_t* raw_psf_size, int32_t* max_kernel_radius,
+                     int32_t* wavelength_count);
+
+/* Fills a 3 x count natural matrix of Gaussian RGB responses (row-normalised
+ * to unit sum), the weighting used for wavelength sets the reference cannot
+ * express (more than 9 bins). */
+int ld_gaussian_rgb_matrix(const float* wavelengths_nm, int32_t count,
+                           const float* center_nm, float sigma_nm,
+                           float* matrix_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LENSDIFF_B200_H */
