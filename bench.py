@@ -1,0 +1,406 @@
+"""Benchmark of the LensDiff diffraction path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl own|reference]
+                    [--workload uhd31|hd16|small3] [--bank cold|warm]
+
+A step renders one frame of the workload through the path: with --bank cold
+(the default, the headline) every frame changes the defocus coefficient by
+1e-6 waves, so the 31-wavelength PSF bank and the kernel spectra are rebuilt
+on every frame; --bank warm keeps them cached.  Inputs (a 3840x2160 RGBA f32
+frame, ~133 MB, plus >1 GB of spectra) are larger than the 126 MB L2.
+
+value  frames/s over the whole job: frames of all ranks / max-over-ranks
+       device time (CUDA events on the rendering stream), inputs resident.
+e2e    the same metric through the public entry point with host buffers:
+       each step copies the frame from pinned host memory, renders, and
+       copies the result back (both copies inside the timed region).
+
+Multi-GPU: the path does not shard inside a frame; each rank renders its own
+frames (replicas), timing is the max over ranks.
+
+--impl reference times the reference's own CPU implementation (built from its
+sources into oracle/_ref/libldref.so) on this machine's host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "uhd31": "workload_uhd31",
+    "hd16": "workload_hd",
+    "small3": "workload_small",
+}
+METRIC = "UHD frames/s (31-wavelength PSF bank, FFT convolution, composite)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="own", choices=["own", "reference"])
+    ap.add_argument("--workload", default="uhd31", choices=sorted(WORKLOADS))
+    ap.add_argument("--bank", default="cold", choices=["cold", "warm"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+# reference CPU timing (oracle/_ref: the reference's own CPU code)
+# ---------------------------------------------------------------------------
+def _ref_unit(args):
+    """One unit of the reference's per-frame work for one wavelength: one bin
+    convolution of the full frame driver with a kernel of the bank's size
+    (convolveScalar, LensDiffCpuReference.cpp:1167-1193) plus one raw PSF of
+    the bank (buildShiftedRawPsf, :831-859).  Returns seconds."""
+    w, h, k, np_, s = args
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    from oracle import ref_lib as R
+
+    rng = np.random.default_rng(7)
+    d = np.zeros((h, w), np.float32)
+    d[rng.integers(0, h, 64), rng.integers(0, w, 64)] = 10.0
+    ker = np.ones((k, k), np.float32) / float(k * k)
+    pupil = np.ones((np_, np_), np.float32)
+    t = time.perf_counter()
+    R.convolve_scalar(d, ker)
+    R.raw_psf_from(pupil, None, s)
+    return time.perf_counter() - t
+
+
+def reference_units(w, h, k, np_, s, workers):
+    """Runs `workers` units in parallel (spawned processes); returns their times."""
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+        return pool.map(_ref_unit, [(w, h, k, np_, s)] * workers)
+
+
+def cpu_baseline(w, h, k, np_, s, bins, workers):
+    times = reference_units(w, h, k, np_, s, workers)
+    t = max(times)
+    value = workers / (bins * t)  # frames/s: each frame needs `bins` units
+    return {
+        "value": value,
+        "unit": "frames/s",
+        "cores": workers,
+        "kind": "reference",
+        "sample": (f"{workers} processes x 1 unit = reference convolveScalar of the {w}x{h} driver with a "
+                   f"{k}x{k} kernel + reference buildShiftedRawPsf {np_}->{s}; a frame is {bins} units "
+                   f"(one per wavelength, effect kernel only); unit time {t:.2f} s"),
+    }
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from lensdiff_b200 import synthetic as S
+    from oracle import ref_lib as R
+    from oracle import ld_oracle as O
+
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libldref.so not built (reference sources absent)"}))
+        return
+    p, frame = getattr(S, WORKLOADS[args.workload])()
+    np_, s, rmax = O.resolve_sizes(p)
+    bins = len(O.wavelengths(p))
+    h, w = frame.shape[:2]
+    workers = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        reference_units(w, h, 2 * rmax + 1, np_, s, 1)
+    t0 = time.perf_counter()
+    step_times = []
+    for _ in range(args.steps):
+        ts = time.perf_counter()
+        reference_units(w, h, 2 * rmax + 1, np_, s, workers)
+        step_times.append(time.perf_counter() - ts)
+    total = time.perf_counter() - t0
+    frames = args.steps * workers / bins
+    value = frames / total
+    ms = total * 1000.0 / args.steps
+    line = {
+        "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "frame": [w, h], "wavelengths": bins, "pupil": np_, "psf": s,
+                   "max_kernel_radius": rmax},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "frames/s", "cores": workers, "kind": "reference",
+                         "sample": (f"each step: {workers} spawned processes, each one reference bin convolution "
+                                    f"({w}x{h}, kernel {2 * rmax + 1}^2) + one reference raw PSF ({np_}->{s}); "
+                                    f"{bins} such units per frame")},
+        "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler
+# ---------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sms, maxs, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sms.append(float(parts[1]))
+                    maxs = max(maxs, float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        if not sms:
+            return None
+        sms.sort()
+        return {"sm_mhz": sms[len(sms) // 2], "sm_max_mhz": maxs, "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per launch of the frame-chain kernels
+# ---------------------------------------------------------------------------
+def algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, out_pixels):
+    """Bytes each frame kernel must move with this algorithm (complex = 8 B):
+    frame_rows reads the RGBA source and writes the H x (Px/2+1) row spectra;
+    frame_cols reads them and the kernel spectra (Py x (Px/2+1) each) and writes
+    H x (Px/2+1) per output; frame_inverse reads those, re-reads the source for
+    the composite and writes the RGBA output."""
+    Px, Py = grid
+    bins = Px // 2 + 1
+    row_spec = 8 * H * bins
+    return {
+        "frame_rows": 16 * W * H + n_drv * row_spec,
+        "frame_cols": n_drv * row_spec + n_ker * 8 * Py * bins + n_out * row_spec,
+        "frame_inverse": n_out * row_spec + 16 * W * H + 16 * out_pixels,
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    ws, rank, local = dist_env()
+    import numpy as np
+    import torch
+
+    pool_ctx = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+    from lensdiff_b200 import synthetic as S
+    from lensdiff_b200.backend import LensDiffPsfBankCache, image_request
+
+    p, frame = getattr(S, WORKLOADS[args.workload])(seed=1003 + rank)
+    H, W = frame.shape[:2]
+    dev = torch.device("cuda", local)
+    cache = LensDiffPsfBankCache(local)
+    stream = torch.cuda.Stream(device=dev)
+    src = torch.from_numpy(frame).to(dev)
+    dst = torch.empty_like(src)
+    req = image_request(src, dst, stream, frame_short_side=p.frameShortSidePx)
+    counter = [0]
+
+    def params_for_step():
+        counter[0] += 1
+        if args.bank == "cold":
+            return p.copy(phaseDefocus=p.phaseDefocus + 1e-6 * counter[0])
+        return p
+
+    launches_per_frame = [0]
+
+    def step():
+        st = cache.render(req, params_for_step())
+        if not st.ok:
+            raise RuntimeError(f"render failed: {st}")
+        launches_per_frame[0] = st.kernel_launches
+        return st
+
+    with torch.cuda.stream(stream):
+        st0 = step()
+        for _ in range(max(0, args.warmup - 1)):
+            step()
+    torch.cuda.synchronize(dev)
+
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    cache.set_profiling(True)
+    cache.profile_collect()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(stream):
+        evs[0].record(stream)
+        for i in range(args.steps):
+            step()
+            evs[i + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    if ws > 1:
+        torch.distributed.barrier()
+    stage = cache.profile_collect()
+    cache.set_profiling(False)
+    clk = clocks.stop()
+    per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    total_ms = evs[0].elapsed_time(evs[-1])
+    t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+    if ws > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = ws * args.steps / (total_ms / 1000.0)
+    ps = sorted(per_step)
+    p50 = ps[len(ps) // 2]
+    p99 = ps[min(len(ps) - 1, int(math.ceil(0.99 * len(ps))) - 1)]
+
+    # ---- end to end through the public entry point with host buffers -----
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.from_numpy(frame).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                src.copy_(host_in, non_blocking=True)
+                step()
+                host_out.copy_(dst, non_blocking=True)
+            torch.cuda.synchronize(dev)
+            if ws > 1:
+                torch.distributed.barrier()
+            ev0.record(stream)
+            for _ in range(args.steps):
+                src.copy_(host_in, non_blocking=True)
+                step()
+                host_out.copy_(dst, non_blocking=True)
+            ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        e_ms = torch.tensor([ev0.elapsed_time(ev1)], device=dev, dtype=torch.float64)
+        if ws > 1:
+            torch.distributed.all_reduce(e_ms, op=torch.distributed.ReduceOp.MAX)
+        nbytes = frame.nbytes
+        e2e = {"value": ws * args.steps / (float(e_ms.item()) / 1000.0), "unit": "frames/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+
+    # ---- roofline of the dominant kernel ----------------------------------
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+        peak_src = "measured"
+    grid = st0.grid_used
+    spectral = int(p.spectralMode) != 0
+    n_drv = 1 if spectral else 3
+    n_ker = 3 if spectral else 1
+    n_out = 3
+    alg = algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, W * H)
+    dominant = max(stage, key=lambda k: stage[k][0])
+    dom_ms, dom_n = stage[dominant]
+    roofline = None
+    if dominant in alg and dom_n:
+        per_launch_ms = dom_ms / dom_n
+        achieved = alg[dominant] / (per_launch_ms / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_src, "traffic": None,
+                    "algorithmic_bytes_per_launch": alg[dominant], "launch_ms": per_launch_ms}
+    else:
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": None, "peak": peak, "unit": "GB/s",
+                    "frac": None, "peak_source": peak_src, "traffic": None}
+    stage_ms = {k: round(v[0] / max(1, args.steps), 4) for k, v in stage.items() if v[1]}
+
+    # ---- CPU baseline (rank 0, N=1) ----------------------------------------
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import ref_lib as R
+
+        if R.available():
+            cpu = cpu_baseline(W, H, 2 * st0.max_kernel_radius + 1, st0.pupil_size, st0.raw_psf_size,
+                               st0.wavelength_count, os.cpu_count() or 1)
+        else:
+            cpu = {"value": None, "unit": "frames/s", "cores": 0, "kind": "reference",
+                   "sample": "oracle/_ref/libldref.so not built"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "p50_ms": p50, "p99_ms": p99,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator; no public dataset exists)",
+            "config": {"workload": args.workload, "frame": [W, H], "wavelengths": st0.wavelength_count,
+                       "pupil": st0.pupil_size, "psf": st0.raw_psf_size,
+                       "max_kernel_radius": st0.max_kernel_radius, "bank": args.bank,
+                       "grid_requested": list(st0.grid_requested), "grid_used": list(st0.grid_used),
+                       "fft_form": "own_fp32", "parallelism": f"replicas x{ws}",
+                       "l2": "inputs larger than L2 (frame 133 MB + spectra > 1 GB)"},
+            "gpu_launches": launches_per_frame[0] * args.steps,
+            "stage_ms_per_frame": stage_ms,
+            "roofline": roofline,
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    cache.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -222,6 +222,21 @@ size_t ld_device_bytes(const ld_ctx* ctx);
 /* Drops the cached PSF banks and kernel spectra. */
 void ld_clear_caches(ld_ctx* ctx);
 
+/* ---- stage timing (CUDA events on the launching stream) ---------------- */
+/* Stage ids reported by ld_profile_collect. */
+enum {
+    LD_STAGE_PSF_ROWS = 0, LD_STAGE_PSF_COLS, LD_STAGE_RESAMPLE, LD_STAGE_SHAPE_STATS,
+    LD_STAGE_SUPPORT, LD_STAGE_CROP_SUM, LD_STAGE_COMBINE, LD_STAGE_KSPEC_ROWS,
+    LD_STAGE_KSPEC_COLS, LD_STAGE_FRAME_ROWS, LD_STAGE_FRAME_COLS, LD_STAGE_FRAME_INVERSE,
+    LD_STAGE_COUNT
+};
+/* When enabled, every kernel launch of ld_render / ld_build_psf_bank is
+ * bracketed by a pair of CUDA events on its stream. */
+int ld_set_profiling(ld_ctx* ctx, int enable);
+/* Synchronises the recorded events and writes, per stage id, the summed
+ * device milliseconds and the launch count since the last collect; resets. */
+int ld_profile_collect(ld_ctx* ctx, double* ms_per_stage, int32_t* launches_per_stage, int32_t count);
+
 /* ---- the drop-in render (replaces RunLensDiffCuda, LensDiffCuda.h:7-10) -- */
 /* Enqueues the whole frame on request->cuda_stream; no host synchronisation
  * except the one-time first-zero calibration per (pupil size, PSF size). */

@@ -301,7 +301,12 @@ EXPORTED_SYMBOLS = [
     "ld_raw_psf",
     "ld_resolve_sizes",
     "ld_gaussian_rgb_matrix",
+    "ld_set_profiling",
+    "ld_profile_collect",
 ]
+
+STAGE_NAMES = ["psf_rows", "psf_cols", "resample", "shape_stats", "support", "crop_sum", "combine",
+               "kspec_rows", "kspec_cols", "frame_rows", "frame_cols", "frame_inverse"]
 
 
 def lib() -> ctypes.CDLL:
@@ -345,6 +350,10 @@ def lib() -> ctypes.CDLL:
     L.ld_gaussian_rgb_matrix.argtypes = [ctypes.POINTER(c_f32), c_i32, ctypes.POINTER(c_f32),
                                          c_f32, ctypes.POINTER(c_f32)]
     L.ld_gaussian_rgb_matrix.restype = ctypes.c_int
+    L.ld_set_profiling.argtypes = [vp, ctypes.c_int]
+    L.ld_set_profiling.restype = ctypes.c_int
+    L.ld_profile_collect.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_i32), c_i32]
+    L.ld_profile_collect.restype = ctypes.c_int
     if L.ld_abi_version() != 1:
         raise RuntimeError("liblensdiff_b200.so ABI version mismatch")
     _LIB = L

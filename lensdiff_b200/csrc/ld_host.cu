@@ -1,0 +1,1068 @@
+// ld_host.cu — host orchestration and the C ABI (include/lensdiff_b200.h).
+//
+// ld_render replaces RunLensDiffCuda (reference source/src/cuda/LensDiffCuda.h:7-10,
+// implemented at LensDiffCuda.cu:4642-7587).  The sequence per frame is
+//   [bank miss]    pupil/|FFT|^2 window -> lambda-rescale -> shaping -> crop
+//   [spectra miss] weighted combination -> kernel spectra on the FFT grid
+//   frame          forward rows (+extraction) -> columns (+multiply) ->
+//                  inverse rows (+spectral map +composite)
+// all enqueued on the caller's stream.  The only host synchronisation is the
+// one-time first-zero calibration per (pupil size, PSF size), the analogue of
+// the reference's process-wide GetLensDiffReferenceRawPsfCached
+// (LensDiffCpuReference.cpp:2018-2038).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/lensdiff_b200.h"
+#include "ld_internal.h"
+
+using namespace ld;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// device memory
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct BankEntry {
+    bool valid = false;
+    std::string key;
+    int B = 0, np = 0, S = 0, R = 0, K = 0;
+    int win_stride = 0;
+    std::vector<float> wavelengths;
+    DevBuf canvas, ring_round, ring_ceil, ring_peak, scalars, wl;
+    PsfBankArgs args{};
+};
+
+struct SpectraEntry {
+    bool valid = false;
+    std::string key;
+    DevBuf spectra;
+    GridGeom g{};
+    int n_ker = 0;
+};
+
+}  // namespace
+
+struct ld_ctx {
+    int device = 0;
+    size_t budget = 0;
+    size_t held = 0;
+    bool configured = false;
+    std::mutex mu;
+    std::map<int, DevBuf> twiddles;
+    std::map<std::pair<int, int>, float> r0_cache;
+    std::map<int, DevBuf> ring_counts;  // by R
+    BankEntry bank;
+    SpectraEntry spectra;
+    // work buffers, grown on demand
+    DevBuf rows, win, combine_out, kspec_rows, frameA, frameB, scratch, calib, calib_psf;
+    int launches = 0;
+    // stage timing
+    bool profiling = false;
+    std::vector<cudaEvent_t> event_pool;
+    size_t events_used = 0;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+struct Fail {
+    int code;
+    std::string stage;
+};
+
+void set_status(ld_status* st, int code, const std::string& stage) {
+    if (!st) return;
+    st->code = code;
+    std::strncpy(st->stage, stage.c_str(), LD_STAGE_LEN - 1);
+    st->stage[LD_STAGE_LEN - 1] = '\0';
+}
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Fail{LD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+void check_launch(const char* what) { check_cuda(cudaGetLastError(), what); }
+
+void free_buf(ld_ctx* c, DevBuf& b) {
+    if (b.p) {
+        cudaFree(b.p);
+        c->held -= b.bytes;
+    }
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+void* ensure(ld_ctx* c, DevBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return b.p;
+    const size_t old = b.bytes;
+    if (c->budget && c->held - old + bytes > c->budget)
+        throw Fail{LD_ERR_BUDGET, "hbm-budget-exceeded"};
+    free_buf(c, b);
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        throw Fail{LD_ERR_OOM, "device-allocation-failed"};
+    }
+    b.p = p;
+    b.bytes = bytes;
+    c->held += bytes;
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// stage timing
+// ---------------------------------------------------------------------------
+cudaEvent_t next_event(ld_ctx* c) {
+    if (c->events_used == c->event_pool.size()) {
+        cudaEvent_t e;
+        check_cuda(cudaEventCreate(&e), "event-create");
+        c->event_pool.push_back(e);
+    }
+    return c->event_pool[c->events_used++];
+}
+
+// Runs `launch` bracketed by events when profiling is on.
+template <class F>
+void staged(ld_ctx* c, int stage, cudaStream_t s, F launch) {
+    if (!c->profiling) {
+        launch();
+        ++c->launches;
+        return;
+    }
+    cudaEvent_t a = next_event(c), b = next_event(c);
+    cudaEventRecord(a, s);
+    launch();
+    cudaEventRecord(b, s);
+    c->marks.push_back({stage, {a, b}});
+    ++c->launches;
+}
+
+// ---------------------------------------------------------------------------
+// FFT plans and twiddles
+// ---------------------------------------------------------------------------
+bool factor_plan(int n, FftPlan* plan) {
+    int m = n;
+    int k = 0;
+    std::vector<int> r;
+    while (m % 8 == 0 && m > 8) {
+        r.push_back(8);
+        m /= 8;
+    }
+    while (m % 5 == 0) {
+        r.push_back(5);
+        m /= 5;
+    }
+    while (m % 3 == 0) {
+        r.push_back(3);
+        m /= 3;
+    }
+    while (m % 8 == 0) {
+        r.push_back(8);
+        m /= 8;
+    }
+    if (m % 4 == 0) {
+        r.push_back(4);
+        m /= 4;
+    }
+    if (m % 2 == 0) {
+        r.push_back(2);
+        m /= 2;
+    }
+    if (m != 1 || r.size() > static_cast<size_t>(kMaxStages)) return false;
+    // large radices first
+    std::sort(r.begin(), r.end(), [](int a, int b) { return a > b; });
+    plan->n = n;
+    plan->nstages = static_cast<int>(r.size());
+    for (int v : r) plan->radix[k++] = v;
+    return true;
+}
+
+bool smooth(int n) {
+    if (n <= 0) return false;
+    for (int p : {2, 3, 5})
+        while (n % p == 0) n /= p;
+    return n == 1;
+}
+
+int next_smooth(int n, bool even) {
+    int m = std::max(n, 2);
+    while (!(smooth(m) && (!even || (m % 2 == 0)))) ++m;
+    return m;
+}
+
+const float2* twiddles(ld_ctx* c, int n) {
+    auto it = c->twiddles.find(n);
+    if (it != c->twiddles.end()) return static_cast<const float2*>(it->second.p);
+    std::vector<float2> h(static_cast<size_t>(n));
+    for (int k = 0; k < n; ++k) {
+        const double a = -2.0 * M_PI * static_cast<double>(k) / static_cast<double>(n);
+        h[static_cast<size_t>(k)] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
+    }
+    DevBuf b;
+    ensure(c, b, h.size() * sizeof(float2));
+    check_cuda(cudaMemcpy(b.p, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice), "twiddle-upload");
+    c->twiddles[n] = b;
+    return static_cast<const float2*>(b.p);
+}
+
+FftPlan make_plan(ld_ctx* c, int n) {
+    FftPlan p{};
+    if (!factor_plan(n, &p)) throw Fail{LD_ERR_UNSUPPORTED, "fft-length-not-5-smooth"};
+    p.tw = twiddles(c, n);
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// parameter resolution (reference float/double expressions)
+// ---------------------------------------------------------------------------
+constexpr float kPiRef = 3.14159265358979323846f;  // kPi, LensDiffCpuReference.cpp:25
+
+int optics_short_side(const ld_params& p) {  // LensDiffTypes.h:302-305
+    return p.resolution_aware ? 2160 : std::max(1, p.frame_short_side_px);
+}
+double percent_to_px(double pct, int side) {  // LensDiffTypes.h:312-314
+    return std::max(0.0, pct) * 0.01 * static_cast<double>(std::max(1, side));
+}
+int max_kernel_radius(const ld_params& p) {  // LensDiffTypes.h:316-320 + CpuReference.cpp:1710
+    const int r = std::max(0, static_cast<int>(std::ceil(percent_to_px(p.max_kernel_radius_px, optics_short_side(p)))));
+    return std::max(4, r);
+}
+int pupil_size(const ld_params& p) { return std::min(std::max(p.pupil_resolution, 64), 1024); }
+int raw_psf_size(int np, int rmax) {  // chooseRawPsfSize, CpuReference.cpp:112-115
+    return std::min(std::max(std::max(np * 2, std::max(512, rmax * 4)), 128), 16384);
+}
+
+bool is_mono(const ld_params& p) { return p.spectral_mode == LD_SPECTRAL_MONO; }
+
+std::vector<float> wavelengths_of(const ld_params& p) {  // CpuReference.cpp:1602-1614
+    if (!is_mono(p) && p.wavelength_count > 0) {
+        return std::vector<float>(p.wavelengths_nm, p.wavelengths_nm + p.wavelength_count);
+    }
+    switch (p.spectral_mode) {
+        case LD_SPECTRAL_9: return {420.f, 450.f, 480.f, 510.f, 540.f, 570.f, 600.f, 630.f, 660.f};
+        case LD_SPECTRAL_5: return {440.f, 490.f, 540.f, 590.f, 640.f};
+        case LD_SPECTRAL_TRISTIMULUS: return {460.f, 550.f, 610.f};
+        default: return {550.f};
+    }
+}
+
+bool has_field_phase(const ld_params& p) {  // LensDiffPhase.cpp:40-57
+    if (p.phase_mode != LD_PHASE_ENABLED || std::abs(p.phase_field_strength) <= 1e-6) return false;
+    const double v[] = {p.phase_field_defocus, p.phase_field_astig_radial, p.phase_field_astig_tangential,
+                        p.phase_field_coma_radial, p.phase_field_coma_tangential, p.phase_field_spherical,
+                        p.phase_field_trefoil_radial, p.phase_field_trefoil_tangential,
+                        p.phase_field_secondary_astig_radial, p.phase_field_secondary_astig_tangential,
+                        p.phase_field_quadrafoil_radial, p.phase_field_quadrafoil_tangential,
+                        p.phase_field_secondary_coma_radial, p.phase_field_secondary_coma_tangential};
+    for (double x : v)
+        if (std::abs(x) > 1e-6) return true;
+    return false;
+}
+
+// Noll-indexed coefficients for one wavelength: the named terms
+// (LensDiffPhase.cpp:199-212) with the chromatic defocus offset
+// (CpuReference.cpp:1721-1726) plus the extension vector.
+PhaseCoeffs phase_for_wavelength(const ld_params& p, float wavelength) {
+    PhaseCoeffs pc{};
+    const float off = (wavelength - 550.0f) / 110.0f;
+    const double defocus = p.phase_defocus + p.chromatic_focus * static_cast<double>(off);
+    const bool enabled = p.phase_mode == LD_PHASE_ENABLED || std::abs(defocus) > 1e-6;
+    double c[LD_NOLL_COUNT] = {0};
+    c[4] = defocus;
+    c[5] = p.phase_astigmatism45;
+    c[6] = p.phase_astigmatism0;
+    c[7] = p.phase_coma_y;
+    c[8] = p.phase_coma_x;
+    c[9] = p.phase_trefoil_y;
+    c[10] = p.phase_trefoil_x;
+    c[11] = p.phase_spherical;
+    c[12] = p.phase_secondary_astigmatism0;
+    c[13] = p.phase_secondary_astigmatism45;
+    c[14] = p.phase_quadrafoil0;
+    c[15] = p.phase_quadrafoil45;
+    c[16] = p.phase_secondary_coma_x;
+    c[17] = p.phase_secondary_coma_y;
+    bool nonflat = std::abs(p.pupil_decenter_x) > 1e-6 || std::abs(p.pupil_decenter_y) > 1e-6;
+    for (int j = 1; j < LD_NOLL_COUNT; ++j) {
+        c[j] += p.noll[j];
+        if (std::abs(c[j]) > 1e-6) nonflat = true;
+    }
+    pc.enabled = (enabled && nonflat) ? 1 : 0;
+    for (int j = 0; j < LD_NOLL_COUNT; ++j) pc.c[j] = static_cast<float>(c[j]);
+    return pc;
+}
+
+PupilParams pupil_params(const ld_params& p, bool circle_reference) {
+    PupilParams pp{};
+    pp.size = pupil_size(p);
+    if (circle_reference) {  // GetLensDiffReferenceRawPsfCached, CpuReference.cpp:2028-2033
+        pp.mode = 0;
+        pp.sides = 6;
+        pp.apod = 0;
+        pp.roundness = 1.0f;
+        pp.phase_cs = 1.0f;
+        return pp;
+    }
+    pp.mode = p.aperture_mode;
+    pp.sides = p.aperture_mode == LD_APERTURE_HEXAGON ? 6 : std::max(3, p.blade_count);
+    if (pp.mode == LD_APERTURE_HEXAGON) pp.mode = LD_APERTURE_POLYGON;
+    pp.apod = p.apodization_mode;
+    pp.roundness = static_cast<float>(std::min(std::max(p.roundness, 0.0), 1.0));
+    pp.rotation = static_cast<float>(p.rotation_deg * static_cast<double>(kPiRef) / 180.0);
+    pp.obstruction = static_cast<float>(std::max(0.0, std::min(0.95, p.central_obstruction))) * 0.86f;
+    const float thick = static_cast<float>(std::max(0.0, p.vane_thickness));
+    pp.vane_half = thick * 0.86f;
+    pp.vanes = (p.vane_count <= 0 || thick <= 0.0f) ? 0 : std::max(1, p.vane_count);
+    for (int i = 0; i < pp.vanes; ++i) {  // blockedByVanes, CpuReference.cpp:477-479
+        const float ang = pp.rotation + static_cast<float>(i) * kPiRef / static_cast<float>(pp.vanes);
+        pp.vane_cs[i] = std::cos(ang);
+        pp.vane_sn[i] = std::sin(ang);
+    }
+    pp.decx = static_cast<float>(p.pupil_decenter_x);
+    pp.decy = static_cast<float>(p.pupil_decenter_y);
+    pp.phase_cs = std::cos(-pp.rotation);  // LensDiffPhase.cpp:225-226
+    pp.phase_sn = std::sin(-pp.rotation);
+    return pp;
+}
+
+std::string append_bytes(std::string s, const void* p, size_t n) {
+    s.append(static_cast<const char*>(p), n);
+    return s;
+}
+
+// Identity of a PSF bank: every parameter the bank depends on
+// (MakeLensDiffPsfBankKey, CpuReference.cpp:1836-1875, plus the extensions).
+std::string bank_key(const ld_params& p, const std::vector<float>& wl) {
+    std::string k;
+    const int ints[] = {p.aperture_mode, p.apodization_mode, p.blade_count, p.vane_count, pupil_size(p),
+                        optics_short_side(p), p.phase_mode};
+    const double dbl[] = {p.roundness, p.rotation_deg, p.central_obstruction, p.vane_thickness,
+                          p.max_kernel_radius_px, p.diffraction_scale_px, p.anisotropy_emphasis,
+                          p.phase_defocus, p.phase_astigmatism0, p.phase_astigmatism45, p.phase_coma_x,
+                          p.phase_coma_y, p.phase_spherical, p.phase_trefoil_x, p.phase_trefoil_y,
+                          p.phase_secondary_astigmatism0, p.phase_secondary_astigmatism45,
+                          p.phase_quadrafoil0, p.phase_quadrafoil45, p.phase_secondary_coma_x,
+                          p.phase_secondary_coma_y, p.pupil_decenter_x, p.pupil_decenter_y,
+                          p.chromatic_focus, p.chromatic_spread};
+    k = append_bytes(k, ints, sizeof(ints));
+    k = append_bytes(k, dbl, sizeof(dbl));
+    k = append_bytes(k, p.noll, sizeof(p.noll));
+    k = append_bytes(k, wl.data(), wl.size() * sizeof(float));
+    return k;
+}
+
+void validate_params(const ld_params& p) {
+    if (p.debug_view != LD_DEBUG_FINAL) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-debug-view"};
+    if (p.look_mode != LD_LOOK_PHYSICAL) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-look-mode-split"};
+    if (p.energy_mode != LD_ENERGY_AUGMENT) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-energy-mode-preserve"};
+    if (p.input_transfer != LD_TRANSFER_LINEAR) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-input-transfer"};
+    if (p.resolution_aware) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-resolution-aware"};
+    if (p.aperture_mode != LD_APERTURE_CIRCLE && p.aperture_mode != LD_APERTURE_POLYGON &&
+        p.aperture_mode != LD_APERTURE_HEXAGON)
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-aperture-mode"};
+    if (p.apodization_mode < 0 || p.apodization_mode > 2) throw Fail{LD_ERR_ARG, "invalid-apodization-mode"};
+    if (p.spectral_mode < 0 || p.spectral_mode > 3) throw Fail{LD_ERR_ARG, "invalid-spectral-mode"};
+    if (has_field_phase(p)) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-field-phase"};
+    if (p.scatter_amount > 1e-6 && percent_to_px(p.scatter_radius, optics_short_side(p)) > 0.25)
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-scatter"};
+    if (percent_to_px(p.creative_fringe, optics_short_side(p)) > 1e-6)
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-creative-fringe"};
+    if (p.wavelength_count < 0 || p.wavelength_count > LD_MAX_WAVELENGTHS)
+        throw Fail{LD_ERR_ARG, "invalid-wavelength-count"};
+    if (p.vane_count > kMaxVanes) throw Fail{LD_ERR_UNSUPPORTED, "too-many-vanes"};
+    if (p.fft_form != LD_FFT_OWN_FP32) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-fft-form"};
+}
+
+size_t align256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
+
+// ---------------------------------------------------------------------------
+// first-zero calibration of the clear circle (one host sync per (N_p, S))
+// ---------------------------------------------------------------------------
+float first_zero(ld_ctx* c, int np, int S, cudaStream_t s) {
+    auto key = std::make_pair(np, S);
+    auto it = c->r0_cache.find(key);
+    if (it != c->r0_cache.end()) return it->second;
+    ld_params cp{};
+    cp.pupil_resolution = np;
+    PsfBankArgs a{};
+    a.pupil = pupil_params(cp, true);
+    a.B = 1;
+    a.S = S;
+    a.half = S / 2;
+    a.off = std::max(0, (S - np) / 2);
+    a.win_stride = S;
+    a.plan_s = make_plan(c, S);
+    WavelengthInfo wi{};
+    wi.win_x0 = 0;
+    wi.win_n = S;
+    const size_t rings = static_cast<size_t>(S / 2 + 1);
+    // scratch layout, each part 256-byte aligned: wavelength info | scalars |
+    // ring sums + profile (3 * rings doubles) | counts | total | r0
+    const size_t o_sc = align256(sizeof(WavelengthInfo));
+    const size_t o_sums = o_sc + align256(sizeof(PsfScalars));
+    const size_t o_cnt = o_sums + align256(rings * 3 * sizeof(double));
+    const size_t o_tot = o_cnt + align256(rings * sizeof(int));
+    const size_t o_r0 = o_tot + 256;
+    char* cal = static_cast<char*>(ensure(c, c->calib, o_r0 + 256));
+    WavelengthInfo* dwl = reinterpret_cast<WavelengthInfo*>(cal);
+    PsfScalars* dsc = reinterpret_cast<PsfScalars*>(cal + o_sc);
+    double* sums = reinterpret_cast<double*>(cal + o_sums);
+    int* counts = reinterpret_cast<int*>(cal + o_cnt);
+    double* total = reinterpret_cast<double*>(cal + o_tot);
+    float* r0d = reinterpret_cast<float*>(cal + o_r0);
+    a.wl = dwl;
+    a.scalars = dsc;
+    a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(np) * S * sizeof(float2)));
+    a.win = static_cast<float*>(ensure(c, c->calib_psf, static_cast<size_t>(S) * S * sizeof(float)));
+    check_cuda(cudaMemcpyAsync(dwl, &wi, sizeof(wi), cudaMemcpyHostToDevice, s), "calib-upload");
+    check_cuda(cudaMemsetAsync(dsc, 0, sizeof(PsfScalars), s), "calib-memset");
+    check_cuda(cudaMemsetAsync(cal + o_sums, 0, o_r0 + 256 - o_sums, s), "calib-memset");
+    launch_psf_rows(a, s);
+    launch_psf_cols(a, s);
+    launch_first_zero(a.win, S, sums, counts, total, r0d, s);
+    check_launch("first-zero-calibration");
+    float r0 = 0.0f;
+    check_cuda(cudaMemcpyAsync(&r0, r0d, sizeof(float), cudaMemcpyDeviceToHost, s), "calib-readback");
+    check_cuda(cudaStreamSynchronize(s), "calib-sync");
+    c->launches += 5;
+    c->r0_cache[key] = r0;
+    return r0;
+}
+
+// ---------------------------------------------------------------------------
+// PSF bank
+// ---------------------------------------------------------------------------
+void fill_wavelength_infos(const ld_params& p, const std::vector<float>& wl, float r0, int S, int R,
+                           std::vector<WavelengthInfo>* out, int* win_stride) {
+    const float r0f = std::max(1.0f, r0);
+    const double diff_px = percent_to_px(p.diffraction_scale_px, optics_short_side(p));
+    const float scale_base = static_cast<float>(std::max(1.0, diff_px)) / r0f;  // CpuReference.cpp:1715
+    const float rc = (S % 2 == 0) ? static_cast<float>(S) * 0.5f : static_cast<float>(S - 1) * 0.5f;
+    *win_stride = 0;
+    out->clear();
+    for (float w : wl) {
+        WavelengthInfo wi{};
+        wi.phase = phase_for_wavelength(p, w);
+        const float off = (w - 550.0f) / 110.0f;
+        const float chrom = std::max(0.25f, 1.0f + static_cast<float>(p.chromatic_spread) * off);
+        const float scale = scale_base * (w / 550.0f) * chrom;  // CpuReference.cpp:1729-1730
+        const float inv = 1.0f / std::max(scale, 0.05f);        // :1071
+        wi.inv_scale = inv;
+        if (inv <= 1.0f) {
+            wi.taps = 0;
+            wi.step = 0.0f;
+        } else {  // :343-344
+            wi.taps = std::min(std::max(static_cast<int>(std::ceil(inv)), 2), 6);
+            wi.step = inv / static_cast<float>(wi.taps);
+        }
+        const double reach = static_cast<double>(R) * inv + (inv > 1.0f ? 0.5 * inv : 0.0);
+        int lo = static_cast<int>(std::floor(rc - reach)) - 2;
+        int hi = static_cast<int>(std::ceil(rc + reach)) + 3;
+        lo = std::max(0, lo);
+        hi = std::min(S, hi);
+        wi.win_x0 = lo;
+        wi.win_n = std::max(1, hi - lo);
+        *win_stride = std::max(*win_stride, wi.win_n);
+        out->push_back(wi);
+    }
+}
+
+const int* ring_counts(ld_ctx* c, int R) {
+    auto it = c->ring_counts.find(R);
+    if (it != c->ring_counts.end()) return static_cast<const int*>(it->second.p);
+    const int K = 2 * R + 1;
+    std::vector<int> cnt(static_cast<size_t>(R + 1), 0);
+    const float kc = static_cast<float>(K - 1) * 0.5f;
+    for (int y = 0; y < K; ++y)
+        for (int x = 0; x < K; ++x) {
+            const float dx = static_cast<float>(x) - kc, dy = static_cast<float>(y) - kc;
+            const int r = std::min(R, static_cast<int>(std::round(std::sqrt(dx * dx + dy * dy))));
+            cnt[static_cast<size_t>(r)] += 1;
+        }
+    DevBuf b;
+    ensure(c, b, cnt.size() * sizeof(int));
+    check_cuda(cudaMemcpy(b.p, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice), "ring-count-upload");
+    c->ring_counts[R] = b;
+    return static_cast<const int*>(b.p);
+}
+
+BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebuilt) {
+    const std::vector<float> wl = wavelengths_of(p);
+    const std::string key = bank_key(p, wl);
+    *rebuilt = false;
+    if (c->bank.valid && c->bank.key == key) return c->bank;
+    BankEntry& b = c->bank;
+    b.valid = false;
+    const int np = pupil_size(p);
+    const int R = max_kernel_radius(p);
+    const int S = raw_psf_size(np, R);
+    const int K = 2 * R + 1;
+    const int B = static_cast<int>(wl.size());
+    if (B > kMaxBins) throw Fail{LD_ERR_ARG, "too-many-wavelengths"};
+    const float r0 = first_zero(c, np, S, s);
+    std::vector<WavelengthInfo> infos;
+    int win_stride = 0;
+    fill_wavelength_infos(p, wl, r0, S, R, &infos, &win_stride);
+
+    PsfBankArgs& a = b.args;
+    a = PsfBankArgs{};
+    a.pupil = pupil_params(p, false);
+    a.B = B;
+    a.S = S;
+    a.half = S / 2;
+    a.off = std::max(0, (S - np) / 2);
+    a.win_stride = win_stride;
+    a.raw_center = (S % 2 == 0) ? static_cast<float>(S) * 0.5f : static_cast<float>(S - 1) * 0.5f;
+    a.R = R;
+    a.K = K;
+    a.gain = 1.0f + std::max(0.0f, static_cast<float>(p.anisotropy_emphasis)) * 4.0f;  // :1127
+    a.plan_s = make_plan(c, S);
+    a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(B) * np * win_stride * sizeof(float2)));
+    a.win = static_cast<float*>(ensure(c, c->win, static_cast<size_t>(B) * win_stride * win_stride * sizeof(float)));
+    a.canvas = static_cast<float*>(ensure(c, b.canvas, static_cast<size_t>(B) * K * K * sizeof(float)));
+    const size_t ringn = static_cast<size_t>(B) * (R + 1);
+    a.ring_round = static_cast<double*>(ensure(c, b.ring_round, ringn * sizeof(double)));
+    a.ring_ceil = static_cast<double*>(ensure(c, b.ring_ceil, ringn * sizeof(double)));
+    a.ring_peak = static_cast<unsigned int*>(ensure(c, b.ring_peak, ringn * sizeof(unsigned int)));
+    a.scalars = static_cast<PsfScalars*>(ensure(c, b.scalars, static_cast<size_t>(B) * sizeof(PsfScalars)));
+    WavelengthInfo* dwl = static_cast<WavelengthInfo*>(ensure(c, b.wl, static_cast<size_t>(B) * sizeof(WavelengthInfo)));
+    a.wl = dwl;
+    a.count_round = ring_counts(c, R);
+    a.want_energy = 0;
+    check_cuda(cudaMemcpyAsync(dwl, infos.data(), infos.size() * sizeof(WavelengthInfo), cudaMemcpyHostToDevice, s),
+               "bank-upload");
+    check_cuda(cudaMemsetAsync(a.ring_round, 0, ringn * sizeof(double), s), "bank-memset");
+    check_cuda(cudaMemsetAsync(a.ring_ceil, 0, ringn * sizeof(double), s), "bank-memset");
+    check_cuda(cudaMemsetAsync(a.ring_peak, 0, ringn * sizeof(unsigned int), s), "bank-memset");
+    check_cuda(cudaMemsetAsync(a.scalars, 0, static_cast<size_t>(B) * sizeof(PsfScalars), s), "bank-memset");
+    staged(c, LD_STAGE_PSF_ROWS, s, [&] { launch_psf_rows(a, s); });
+    staged(c, LD_STAGE_PSF_COLS, s, [&] { launch_psf_cols(a, s); });
+    staged(c, LD_STAGE_RESAMPLE, s, [&] { launch_resample(a, s); });
+    staged(c, LD_STAGE_SHAPE_STATS, s, [&] { launch_shape_stats(a, s); });
+    staged(c, LD_STAGE_SUPPORT, s, [&] { launch_support(a, s); });
+    staged(c, LD_STAGE_CROP_SUM, s, [&] { launch_crop_sum(a, s); });
+    check_launch("psf-bank");
+    b.B = B;
+    b.np = np;
+    b.S = S;
+    b.R = R;
+    b.K = K;
+    b.win_stride = win_stride;
+    b.wavelengths = wl;
+    b.key = key;
+    b.valid = true;
+    c->spectra.valid = false;
+    *rebuilt = true;
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// spectral -> RGB combination (MapLensDiffSpectralBins, LensDiffSpectrum.cpp:462-497)
+// ---------------------------------------------------------------------------
+struct Combination {
+    int mono = 0;
+    int n_drv = 1, n_ker = 3, n_out = 3;
+    int luma_lock = 0;
+    float saturation = 1.0f;
+    float coef[4][kMaxBins] = {};
+};
+
+void gaussian_matrix(const float* wl, int n, const float* center, float sigma, float* m) {
+    for (int c = 0; c < 3; ++c) {
+        double sum = 0.0;
+        for (int b = 0; b < n; ++b) {
+            const double t = (static_cast<double>(wl[b]) - center[c]) / sigma;
+            sum += std::exp(-0.5 * t * t);
+        }
+        for (int b = 0; b < n; ++b) {
+            const double t = (static_cast<double>(wl[b]) - center[c]) / sigma;
+            m[c * n + b] = static_cast<float>(std::exp(-0.5 * t * t) / (sum > 0.0 ? sum : 1.0));
+        }
+    }
+}
+
+Combination make_combination(const ld_params& p, const std::vector<float>& wl) {
+    Combination cb;
+    const int B = static_cast<int>(wl.size());
+    if (is_mono(p)) {  // convolveRgba, CpuReference.cpp:1195-1217
+        cb.mono = 1;
+        cb.n_drv = 3;
+        cb.n_ker = 1;
+        cb.n_out = 3;
+        cb.coef[0][0] = 1.0f;
+        return cb;
+    }
+    std::vector<float> nat(static_cast<size_t>(3 * B)), sty(static_cast<size_t>(3 * B));
+    if (B <= 1) {  // mulMatrix with binCount <= 1 replicates the bin (LensDiffSpectrum.cpp:365-367)
+        for (int c = 0; c < 3; ++c) nat[c] = sty[c] = 1.0f;
+    } else if (p.rgb_mode == LD_RGB_GAUSSIAN) {
+        gaussian_matrix(wl.data(), B, p.rgb_gauss_center_nm, p.rgb_gauss_sigma_nm, nat.data());
+        sty = nat;
+    } else {
+        for (int i = 0; i < 3 * B; ++i) {
+            nat[static_cast<size_t>(i)] = p.natural_matrix[i];
+            sty[static_cast<size_t>(i)] = p.style_matrix[i];
+        }
+        bool any = false;
+        for (float v : nat) any |= v != 0.0f;
+        if (!any) throw Fail{LD_ERR_ARG, "missing-spectral-matrix"};
+    }
+    const float force = std::min(std::max(static_cast<float>(p.spectrum_force), 0.0f), 1.0f);
+    cb.saturation = static_cast<float>(std::max(0.0, p.spectrum_saturation));
+    const float lw[3] = {0.2126f, 0.7152f, 0.0722f};
+    bool lock_identity = true;
+    for (int b = 0; b < B; ++b) {
+        float ln = 0.0f, lm = 0.0f;
+        for (int c = 0; c < 3; ++c) {
+            const float n = nat[static_cast<size_t>(c * B + b)];
+            const float m = n * (1.0f - force) + sty[static_cast<size_t>(c * B + b)] * force;
+            cb.coef[c][b] = m;
+            if (m < 0.0f) lock_identity = false;
+            ln += lw[c] * n;
+            lm += lw[c] * m;
+        }
+        cb.coef[3][b] = ln;
+        if (std::abs(ln - lm) > 1e-6f * std::max(1.0f, std::abs(ln))) lock_identity = false;
+    }
+    cb.luma_lock = (!p.chromatic_affects_luma && !lock_identity) ? 1 : 0;
+    cb.n_ker = cb.luma_lock ? 4 : 3;
+    cb.n_out = cb.n_ker;
+    cb.n_drv = 1;
+    return cb;
+}
+
+std::string spectra_key(const BankEntry& b, const Combination& cb, const GridGeom& g) {
+    std::string k = b.key;
+    k = append_bytes(k, &cb.n_ker, sizeof(int));
+    k = append_bytes(k, cb.coef, sizeof(cb.coef));
+    k = append_bytes(k, &g.Px, sizeof(int));
+    k = append_bytes(k, &g.Py, sizeof(int));
+    return k;
+}
+
+GridGeom make_geometry(ld_ctx* c, int W, int H, int K, int* req_w, int* req_h) {
+    GridGeom g{};
+    *req_w = W + K - 1;
+    *req_h = H + K - 1;
+    g.Px = next_smooth(*req_w, true);
+    g.Py = next_smooth(*req_h, false);
+    g.M = g.Px / 2;
+    if (g.M > 6912 || g.Py > 6912) throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-fft-grid"};
+    g.Pw = ((g.M + 1 + kColTile - 1) / kColTile) * kColTile;
+    g.tiles = g.Pw / kColTile;
+    g.plan_m = make_plan(c, g.M);
+    g.plan_py = make_plan(c, g.Py);
+    g.tw_px = twiddles(c, g.Px);
+    return g;
+}
+
+SpectraEntry& ensure_spectra(ld_ctx* c, BankEntry& b, const Combination& cb, const GridGeom& g, cudaStream_t s,
+                             bool* rebuilt) {
+    const std::string key = spectra_key(b, cb, g);
+    *rebuilt = false;
+    SpectraEntry& e = c->spectra;
+    if (e.valid && e.key == key) return e;
+    e.valid = false;
+    CombineArgs ca{};
+    ca.bank = b.args;
+    ca.n_ker = cb.n_ker;
+    std::memcpy(ca.coef, cb.coef, sizeof(ca.coef));
+    const size_t kk = static_cast<size_t>(b.K) * b.K;
+    ca.out = static_cast<float*>(ensure(c, c->combine_out, cb.n_ker * kk * sizeof(float)));
+    staged(c, LD_STAGE_COMBINE, s, [&] { launch_combine(ca, s); });
+    KernelSpectraArgs ka{};
+    ka.g = g;
+    ka.n_ker = cb.n_ker;
+    ka.R = b.R;
+    ka.K = b.K;
+    ka.canvas = ca.out;
+    ka.rows = static_cast<float2*>(ensure(c, c->kspec_rows, static_cast<size_t>(cb.n_ker) * b.K * g.Pw * sizeof(float2)));
+    ka.spectra = static_cast<float2*>(
+        ensure(c, e.spectra, static_cast<size_t>(cb.n_ker) * g.tiles * g.Py * kColTile * sizeof(float2)));
+    ka.scale = static_cast<float>(1.0 / (static_cast<double>(g.M) * static_cast<double>(g.Py)));
+    staged(c, LD_STAGE_KSPEC_ROWS, s, [&] { launch_kspec_rows(ka, s); });
+    staged(c, LD_STAGE_KSPEC_COLS, s, [&] { launch_kspec_cols(ka, s); });
+    check_launch("kernel-spectra");
+    e.g = g;
+    e.n_ker = cb.n_ker;
+    e.key = key;
+    e.valid = true;
+    *rebuilt = true;
+    return e;
+}
+
+void fill_sizes(ld_status* st, const ld_params& p) {
+    if (!st) return;
+    st->pupil_size = pupil_size(p);
+    st->max_kernel_radius = max_kernel_radius(p);
+    st->raw_psf_size = raw_psf_size(st->pupil_size, st->max_kernel_radius);
+    st->wavelength_count = static_cast<int>(wavelengths_of(p).size());
+}
+
+SelectionParams selection_params(const ld_params& p) {  // CpuReference.cpp:1221-1223, :2096
+    SelectionParams s{};
+    const float soft = static_cast<float>(std::max(0.01, p.softness_stops));
+    const float thr = static_cast<float>(p.threshold);
+    s.luma = p.extraction_mode == LD_EXTRACT_LUMA;
+    s.thr_stops = thr;
+    s.edge0 = thr - soft * 0.5f;
+    s.edge1 = thr + soft * 0.5f;
+    s.thr_linear = 0.18f * std::pow(2.0f, thr);
+    s.point_emphasis = static_cast<float>(p.point_emphasis);
+    s.rscale = 1.0f - static_cast<float>(std::min(std::max(p.core_preserve, 0.0), 1.0));
+    return s;
+}
+
+int run_guarded(ld_ctx* ctx, ld_status* st, const std::function<void()>& fn);
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int ld_abi_version(void) { return LD_ABI_VERSION; }
+
+int ld_create(ld_ctx** out, int device, size_t hbm_budget_bytes) {
+    if (!out) return LD_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return LD_ERR_CUDA;
+    }
+    ld_ctx* c = new ld_ctx();
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    {
+        DeviceGuard g(device);
+        configure_kernels();
+        if (cudaGetLastError() != cudaSuccess) {
+            delete c;
+            return LD_ERR_CUDA;
+        }
+    }
+    c->configured = true;
+    *out = c;
+    return LD_OK;
+}
+
+void ld_destroy(ld_ctx* c) {
+    if (!c) return;
+    DeviceGuard g(c->device);
+    for (auto& kv : c->twiddles) free_buf(c, kv.second);
+    for (auto& kv : c->ring_counts) free_buf(c, kv.second);
+    DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,
+                      &c->frameB, &c->scratch, &c->calib,       &c->calib_psf};
+    for (DevBuf* b : bufs) free_buf(c, *b);
+    for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+    DevBuf* bb[] = {&c->bank.canvas, &c->bank.ring_round, &c->bank.ring_ceil, &c->bank.ring_peak,
+                    &c->bank.scalars, &c->bank.wl,        &c->spectra.spectra};
+    for (DevBuf* b : bb) free_buf(c, *b);
+    delete c;
+}
+
+size_t ld_device_bytes(const ld_ctx* c) { return c ? c->held : 0; }
+
+int ld_set_profiling(ld_ctx* c, int enable) {
+    if (!c) return LD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->profiling = enable != 0;
+    return LD_OK;
+}
+
+int ld_profile_collect(ld_ctx* c, double* ms, int32_t* launches, int32_t count) {
+    if (!c || count < 0) return LD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    DeviceGuard g(c->device);
+    for (int i = 0; i < count; ++i) {
+        if (ms) ms[i] = 0.0;
+        if (launches) launches[i] = 0;
+    }
+    int rc = LD_OK;
+    for (auto& m : c->marks) {
+        if (cudaEventSynchronize(m.second.second) != cudaSuccess) {
+            rc = LD_ERR_CUDA;
+            continue;
+        }
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, m.second.first, m.second.second);
+        if (m.first < count) {
+            if (ms) ms[m.first] += t;
+            if (launches) launches[m.first] += 1;
+        }
+    }
+    c->marks.clear();
+    c->events_used = 0;
+    return rc;
+}
+
+void ld_clear_caches(ld_ctx* c) {
+    if (!c) return;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->bank.valid = false;
+    c->spectra.valid = false;
+}
+
+int ld_resolve_sizes(const ld_params* p, int32_t* np, int32_t* S, int32_t* R, int32_t* B) {
+    if (!p) return LD_ERR_ARG;
+    const int n = pupil_size(*p), r = max_kernel_radius(*p);
+    if (np) *np = n;
+    if (R) *R = r;
+    if (S) *S = raw_psf_size(n, r);
+    if (B) *B = static_cast<int32_t>(wavelengths_of(*p).size());
+    return LD_OK;
+}
+
+int ld_gaussian_rgb_matrix(const float* wl, int32_t count, const float* center, float sigma, float* out) {
+    if (!wl || !center || !out || count <= 0 || count > LD_MAX_WAVELENGTHS || !(sigma > 0.0f)) return LD_ERR_ARG;
+    gaussian_matrix(wl, count, center, sigma, out);
+    return LD_OK;
+}
+
+int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params, ld_status* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (!ctx || !rq || !params) {
+        set_status(st, LD_ERR_ARG, "null-argument");
+        return LD_ERR_ARG;
+    }
+    // LensDiffCuda.cu:4646-4657
+    if (!rq->host_enabled_cuda_render || rq->cuda_stream == nullptr) {
+        set_status(st, LD_ERR_ARG, "cuda-render-not-enabled-by-host");
+        return LD_ERR_ARG;
+    }
+    if (rq->src.data == nullptr || rq->dst.data == nullptr) {
+        set_status(st, LD_ERR_ARG, "missing-source-or-destination-cuda-buffer");
+        return LD_ERR_ARG;
+    }
+    return run_guarded(ctx, st, [&]() {
+        const ld_params& p = *params;
+        cudaStream_t s = static_cast<cudaStream_t>(rq->cuda_stream);
+        const int W = rq->src.bounds.x2 - rq->src.bounds.x1;
+        const int H = rq->src.bounds.y2 - rq->src.bounds.y1;
+        if (W <= 0 || H <= 0) throw Fail{LD_ERR_ARG, "invalid-source-bounds"};
+        if (rq->src.components != 4 || rq->src.bytes_per_component != 4 || rq->dst.components != 4 ||
+            rq->dst.bytes_per_component != 4)
+            throw Fail{LD_ERR_ARG, "unsupported-pixel-format"};
+        validate_params(p);
+        fill_sizes(st, p);
+        ctx->launches = 0;
+        bool bank_rebuilt = false, spectra_rebuilt = false;
+        BankEntry& bank = ensure_bank(ctx, p, s, &bank_rebuilt);
+        const Combination cb = make_combination(p, bank.wavelengths);
+        int rw = 0, rh = 0;
+        const GridGeom g = make_geometry(ctx, W, H, bank.K, &rw, &rh);
+        SpectraEntry& sp = ensure_spectra(ctx, bank, cb, g, s, &spectra_rebuilt);
+
+        FrameArgs fa{};
+        fa.g = g;
+        fa.sel = selection_params(p);
+        fa.W = W;
+        fa.H = H;
+        fa.src = static_cast<const unsigned char*>(rq->src.data);
+        fa.src_pitch = rq->src.row_bytes;
+        fa.dst = static_cast<unsigned char*>(rq->dst.data);
+        fa.dst_pitch = rq->dst.row_bytes;
+        fa.src_x1 = rq->src.bounds.x1;
+        fa.src_y1 = rq->src.bounds.y1;
+        fa.dst_x1 = rq->dst.bounds.x1;
+        fa.dst_y1 = rq->dst.bounds.y1;
+        // intersectRect(renderWindow, dst.bounds), CpuReference.cpp:116-125, :2235
+        fa.out_x1 = std::max(rq->render_window.x1, rq->dst.bounds.x1);
+        fa.out_y1 = std::max(rq->render_window.y1, rq->dst.bounds.y1);
+        fa.out_x2 = std::max(fa.out_x1, std::min(rq->render_window.x2, rq->dst.bounds.x2));
+        fa.out_y2 = std::max(fa.out_y1, std::min(rq->render_window.y2, rq->dst.bounds.y2));
+        fa.n_drv = cb.n_drv;
+        fa.n_out = cb.n_out;
+        fa.n_ker = cb.n_ker;
+        fa.mono = cb.mono;
+        fa.saturation = cb.saturation;
+        fa.luma_lock = cb.luma_lock;
+        // Augment: effect gain and core compensation (CpuReference.cpp:2104-2109)
+        fa.effect_gain = static_cast<float>(std::max(0.0, p.effect_gain));
+        fa.core_comp = static_cast<float>(std::max(0.0, p.core_compensation));
+        const float protect = std::max(0.2f, static_cast<float>(std::min(std::max(p.core_preserve, 0.0), 1.0)));
+        fa.max_sub = fa.sel.rscale > 1e-6f ? (1.0f - protect) / fa.sel.rscale : 0.0f;
+        fa.A = static_cast<float2*>(ensure(ctx, ctx->frameA, static_cast<size_t>(cb.n_drv) * H * g.Pw * sizeof(float2)));
+        fa.Bout = static_cast<float2*>(ensure(ctx, ctx->frameB, static_cast<size_t>(cb.n_out) * H * g.Pw * sizeof(float2)));
+        fa.spectra = static_cast<const float2*>(sp.spectra.p);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+        fa.col_grid = std::min(g.tiles, sms * column_pass_blocks_per_sm(g.Py));
+        fa.scratch = static_cast<float2*>(
+            ensure(ctx, ctx->scratch, static_cast<size_t>(fa.col_grid) * g.Py * kColTile * sizeof(float2)));
+        staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
+        staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
+        staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse(fa, s); });
+        check_launch("frame-chain");
+        if (st) {
+            st->bank_rebuilt = bank_rebuilt;
+            st->spectra_rebuilt = spectra_rebuilt;
+            st->grid_requested_w = rw;
+            st->grid_requested_h = rh;
+            st->grid_used_w = g.Px;
+            st->grid_used_h = g.Py;
+            st->kernel_launches = ctx->launches;
+        }
+    });
+}
+
+int ld_build_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream, ld_status* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (!ctx || !params) {
+        set_status(st, LD_ERR_ARG, "null-argument");
+        return LD_ERR_ARG;
+    }
+    return run_guarded(ctx, st, [&]() {
+        validate_params(*params);
+        fill_sizes(st, *params);
+        bool rebuilt = false;
+        ensure_bank(ctx, *params, static_cast<cudaStream_t>(stream), &rebuilt);
+        if (st) st->bank_rebuilt = rebuilt;
+    });
+}
+
+int ld_export_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream, float* wl_out, int32_t* sizes,
+                       int64_t* offsets, float* kernels_out, int64_t capacity, ld_status* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (!ctx || !params || !sizes || !offsets || !kernels_out) {
+        set_status(st, LD_ERR_ARG, "null-argument");
+        return LD_ERR_ARG;
+    }
+    return run_guarded(ctx, st, [&]() {
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        validate_params(*params);
+        fill_sizes(st, *params);
+        bool rebuilt = false;
+        BankEntry& b = ensure_bank(ctx, *params, s, &rebuilt);
+        std::vector<PsfScalars> sc(static_cast<size_t>(b.B));
+        check_cuda(cudaMemcpyAsync(sc.data(), b.args.scalars, sc.size() * sizeof(PsfScalars), cudaMemcpyDeviceToHost, s),
+                   "export-readback");
+        check_cuda(cudaStreamSynchronize(s), "export-sync");
+        int64_t total = 0;
+        int support = 4;
+        for (int i = 0; i < b.B; ++i) {
+            const int side = 2 * sc[static_cast<size_t>(i)].radius + 1;
+            sizes[i] = side;
+            offsets[i] = total;
+            total += static_cast<int64_t>(side) * side;
+            support = std::max(support, sc[static_cast<size_t>(i)].radius);
+            if (wl_out) wl_out[i] = b.wavelengths[static_cast<size_t>(i)];
+        }
+        if (total > capacity) throw Fail{LD_ERR_ARG, "export-capacity-too-small"};
+        DevBuf off;
+        DevBuf out;
+        ensure(ctx, off, static_cast<size_t>(b.B) * sizeof(int64_t));
+        ensure(ctx, out, static_cast<size_t>(total) * sizeof(float));
+        check_cuda(cudaMemcpyAsync(off.p, offsets, static_cast<size_t>(b.B) * sizeof(int64_t), cudaMemcpyHostToDevice, s),
+                   "export-upload");
+        launch_export(b.args, static_cast<const int64_t*>(off.p), static_cast<float*>(out.p), s);
+        check_launch("export");
+        check_cuda(cudaMemcpyAsync(kernels_out, out.p, static_cast<size_t>(total) * sizeof(float), cudaMemcpyDeviceToHost, s),
+                   "export-download");
+        check_cuda(cudaStreamSynchronize(s), "export-sync");
+        free_buf(ctx, off);
+        free_buf(ctx, out);
+        if (st) {
+            st->bank_rebuilt = rebuilt;
+            st->support_radius = support;
+        }
+    });
+}
+
+int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float* psf_out, void* stream,
+               ld_status* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (!ctx || !params || !psf_out) {
+        set_status(st, LD_ERR_ARG, "null-argument");
+        return LD_ERR_ARG;
+    }
+    return run_guarded(ctx, st, [&]() {
+        const ld_params& p = *params;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (p.aperture_mode != LD_APERTURE_CIRCLE && p.aperture_mode != LD_APERTURE_POLYGON &&
+            p.aperture_mode != LD_APERTURE_HEXAGON)
+            throw Fail{LD_ERR_UNSUPPORTED, "unsupported-aperture-mode"};
+        fill_sizes(st, p);
+        const std::vector<float> wl = wavelengths_of(p);
+        if (wavelength_index < 0 || wavelength_index >= static_cast<int>(wl.size()))
+            throw Fail{LD_ERR_ARG, "invalid-wavelength-index"};
+        const int np = pupil_size(p), R = max_kernel_radius(p), S = raw_psf_size(np, R);
+        PsfBankArgs a{};
+        a.pupil = pupil_params(p, false);
+        a.B = 1;
+        a.S = S;
+        a.half = S / 2;
+        a.off = std::max(0, (S - np) / 2);
+        a.win_stride = S;
+        a.plan_s = make_plan(ctx, S);
+        WavelengthInfo wi{};
+        wi.phase = phase_for_wavelength(p, wl[static_cast<size_t>(wavelength_index)]);
+        wi.win_x0 = 0;
+        wi.win_n = S;
+        char* cal = static_cast<char*>(ensure(ctx, ctx->calib, 2 * align256(sizeof(WavelengthInfo) + sizeof(PsfScalars))));
+        WavelengthInfo* dwl = reinterpret_cast<WavelengthInfo*>(cal);
+        PsfScalars* dsc = reinterpret_cast<PsfScalars*>(cal + align256(sizeof(WavelengthInfo)));
+        a.wl = dwl;
+        a.scalars = dsc;
+        a.want_energy = 1;
+        a.rows = static_cast<float2*>(ensure(ctx, ctx->rows, static_cast<size_t>(np) * S * sizeof(float2)));
+        a.win = psf_out;
+        check_cuda(cudaMemcpyAsync(dwl, &wi, sizeof(wi), cudaMemcpyHostToDevice, s), "rawpsf-upload");
+        check_cuda(cudaMemsetAsync(dsc, 0, sizeof(PsfScalars), s), "rawpsf-memset");
+        launch_psf_rows(a, s);
+        launch_psf_cols(a, s);
+        launch_normalize_psf(psf_out, S * S, dsc, s);
+        check_launch("raw-psf");
+        // the upload above reads `wi` from the stack: finish before returning
+        check_cuda(cudaStreamSynchronize(s), "rawpsf-sync");
+    });
+}
+
+}  // extern "C"
+
+namespace {
+int run_guarded(ld_ctx* ctx, ld_status* st, const std::function<void()>& fn) {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        fn();
+    } catch (const Fail& f) {
+        set_status(st, f.code, f.stage);
+        return f.code;
+    } catch (const std::exception& e) {
+        set_status(st, LD_ERR_CUDA, e.what());
+        return LD_ERR_CUDA;
+    }
+    set_status(st, LD_OK, "ok");
+    return LD_OK;
+}
+}  // namespace

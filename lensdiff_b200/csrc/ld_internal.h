@@ -1,0 +1,156 @@
+// ld_internal.h — argument blocks and launchers shared by the host
+// orchestration (ld_host.cu) and the kernels (ld_psf.cu, ld_frame.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ld_fft.cuh"
+#include "ld_optics.cuh"
+
+namespace ld {
+
+constexpr int kMaxBins = 64;  // LD_MAX_WAVELENGTHS
+constexpr int kColTile = 4;   // interleaved columns per column-pass CTA
+
+// ---- PSF bank -----------------------------------------------------------------
+// Per-wavelength constants, computed on the host with the reference's float
+// expressions (LensDiffCpuReference.cpp:1720-1731, :1069-1071, :343-345).
+struct WavelengthInfo {
+    PhaseCoeffs phase;
+    float inv_scale;   // 1 / max(scaleFactor, 0.05f)
+    int taps;          // box-filter taps (0: plain bilinear)
+    float step;        // footprint / taps
+    int win_x0;        // window origin in shifted PSF coordinates
+    int win_n;         // window side (<= S)
+};
+
+struct PsfScalars {      // per wavelength, FP64 sums of the shaping chain
+    double s1;           // sum of resampled values
+    double s2;           // sum of the azimuthal-mean kernel (unnormalised)
+    double s3;           // sum of the shaped kernel (unnormalised)
+    double s4;           // sum of the cropped, tapered, normalised kernel
+    double energy;       // sum of |F|^2 over the computed window (raw PSF export)
+    unsigned int peak;   // max shaped value (float bits)
+    int radius;          // adaptive support radius
+    float extent, fade, start;  // taper constants
+};
+
+struct PsfBankArgs {
+    PupilParams pupil;
+    const WavelengthInfo* wl;    // [B]
+    int B;
+    int S;                       // raw PSF size
+    int half;                    // S / 2 (integer)
+    int off;                     // (S - N_p) / 2
+    int win_stride;              // max window side over wavelengths
+    float raw_center;            // shiftedSpectrumCenterCoordinate(S)
+    int R;                       // R_max
+    int K;                       // 2 R_max + 1
+    float gain;                  // 1 + 4 max(0, anisotropy)
+    FftPlan plan_s;              // length S
+    float2* rows;                // [B][N_p][win_stride] row-pass output
+    float* win;                  // [B][win_stride][win_stride] |F|^2 windows
+    float* canvas;               // [B][K][K] resampled kernels
+    double* ring_round;          // [B][R+1] sums by round(r)
+    double* ring_ceil;           // [B][R+1] sums by ceil(r)
+    unsigned int* ring_peak;     // [B][R+1] max by ceil(r) (float bits)
+    const int* count_round;      // [R+1] pixel counts by round(r)
+    PsfScalars* scalars;         // [B]
+    int want_energy;
+};
+
+void launch_psf_rows(const PsfBankArgs& a, cudaStream_t s);
+void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s);
+void launch_resample(const PsfBankArgs& a, cudaStream_t s);
+void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s);
+void launch_support(const PsfBankArgs& a, cudaStream_t s);
+void launch_crop_sum(const PsfBankArgs& a, cudaStream_t s);
+
+// Combination of the per-wavelength final kernels into n_ker output kernels:
+// out[k][i] = sum_b coef[k][b] * final_b[i].
+struct CombineArgs {
+    PsfBankArgs bank;
+    int n_ker;
+    float coef[4][kMaxBins];
+    float* out;                  // [n_ker][K][K]
+};
+void launch_combine(const CombineArgs& a, cudaStream_t s);
+
+// Packs each wavelength's final (cropped) kernel back to back at offsets[b].
+void launch_export(const PsfBankArgs& a, const int64_t* offsets_dev, float* out, cudaStream_t s);
+
+// Radial profile of a full S x S intensity and the first-minimum scan
+// (LensDiffCpuReference.cpp:865-955).
+void launch_first_zero(const float* psf, int S, double* ring_sums, int* ring_counts, double* total,
+                       float* r0_out, cudaStream_t s);
+
+// Shifted full raw PSF export: window covers all of S x S; writes psf / energy.
+void launch_normalize_psf(float* psf, int n, const PsfScalars* sc, cudaStream_t s);
+
+// ---- kernel spectra and frame chain ------------------------------------------------
+struct GridGeom {
+    int Px, Py;        // FFT grid
+    int M;             // Px / 2
+    int Pw;            // padded row width in complex (multiple of kColTile, > M)
+    int tiles;         // Pw / kColTile
+    FftPlan plan_m;    // length M (real rows via half-length complex)
+    FftPlan plan_py;   // length Py (columns)
+    const float2* tw_px;  // exp(-2 pi i k / Px), k < Px
+};
+
+struct KernelSpectraArgs {
+    GridGeom g;
+    int n_ker;
+    int R, K;
+    const float* canvas;  // [n_ker][K][K]
+    float2* rows;         // [n_ker][K][Pw]
+    float2* spectra;      // [n_ker][tiles][Py][kColTile]
+    float scale;          // 1 / (M * Py)
+};
+void launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s);
+void launch_kspec_cols(const KernelSpectraArgs& a, cudaStream_t s);
+
+struct SelectionParams {
+    int luma;              // extraction mode
+    float thr_stops;       // threshold in stops
+    float edge0, edge1;    // smoothstep edges in stops
+    float thr_linear;      // 0.18 * 2^threshold
+    float point_emphasis;
+    float rscale;          // 1 - corePreserve
+};
+
+struct FrameArgs {
+    GridGeom g;
+    SelectionParams sel;
+    int W, H;
+    const unsigned char* src;  // device, row-major float RGBA
+    int64_t src_pitch;
+    unsigned char* dst;
+    int64_t dst_pitch;
+    int src_x1, src_y1;        // src bounds origin
+    int dst_x1, dst_y1;        // dst bounds origin
+    int out_x1, out_y1, out_x2, out_y2;  // render window intersect dst bounds
+    int n_drv;                 // 1 (spectral scalar driver) or 3 (Mono RGB)
+    int n_out;                 // 3 or 4 (4th: luma-lock target)
+    int n_ker;                 // kernels (1 for Mono)
+    float2* A;                 // [n_drv][H][Pw]
+    float2* Bout;              // [n_out][H][Pw]
+    const float2* spectra;     // [n_ker][tiles][Py][kColTile]
+    float2* scratch;           // [grid][Py][kColTile]
+    int col_grid;              // persistent CTAs of the column pass
+    // epilogue
+    int mono;
+    float saturation;
+    int luma_lock;
+    float effect_gain, core_comp, max_sub;
+};
+void launch_frame_rows(const FrameArgs& a, cudaStream_t s);
+void launch_frame_cols(const FrameArgs& a, cudaStream_t s);
+void launch_frame_inverse(const FrameArgs& a, cudaStream_t s);
+
+// shared-memory opt-in for every kernel instantiation (once per device)
+void configure_kernels();
+int column_pass_blocks_per_sm(int Py);
+
+}  // namespace ld

@@ -1,0 +1,651 @@
+// ld_psf.cu — PSF-bank kernels: pupil -> |FFT|^2 window -> lambda-rescale ->
+// kernel shaping -> adaptive crop/taper -> weighted combination.
+//
+// Reference stages (LensDiffCpuReference.cpp):
+//   buildShiftedRawPsf      :831-859   -> psf_rows_kernel + psf_cols_kernel
+//   makeResampledKernel     :1060-1086 -> resample_kernel
+//   azimuthalMeanKernel / reshapeAnisotropy / estimateAdaptiveSupportRadius
+//                           :1088-1135, :984-1031 -> shape_stats_kernel, support_kernel
+//   cropKernelToRadius + applySupportBoundaryTaper :1038-1058, :957-982
+//                           -> crop_sum_kernel (normaliser) and combine_kernel
+//   estimateFirstMinimumRadius :865-955 -> profile_kernel + first_zero_scan_kernel
+//
+// All wavelengths of a bank run in the same launches (blockIdx.y / .z is the
+// wavelength).  No stage returns to the host.
+#include "ld_internal.h"
+
+namespace ld {
+namespace {
+
+constexpr int kTile = 32;       // canvas tile side for the per-pixel kernels
+constexpr int kRingSpan = 64;   // ring indices one 32x32 tile can touch
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of one double; result valid in thread 0.
+__device__ double block_sum(double v) {
+    __shared__ double part[32];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane2 = tid & 31, warp2 = tid >> 5;
+    (void)lane;
+    (void)warp;
+    v = warp_sum(v);
+    const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+    __syncthreads();
+    if (lane2 == 0) part[warp2] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (warp2 == 0) {
+        r = lane2 < nwarps ? part[lane2] : 0.0;
+        r = warp_sum(r);
+    }
+    return r;
+}
+
+// ---- raw PSF: row pass ---------------------------------------------------------
+// grid (N_p, B).  Row y of the pupil raster, embedded at (S-N_p)/2 of a length-S
+// row; the pupil field is generated in the first stage's load, the window
+// columns are written by the last stage.
+template <int T, int NMAX>
+__global__ void __launch_bounds__(T) psf_rows_kernel(PsfBankArgs a) {
+    extern __shared__ float2 smem[];
+    __shared__ PhaseCoeffs pc;
+    const int y = blockIdx.x;
+    const int b = blockIdx.y;
+    const WavelengthInfo* w = a.wl + b;
+    if (threadIdx.x == 0) pc = w->phase;
+    __syncthreads();
+    const int np = a.pupil.size;
+    const int off = a.off;
+    smem_fill<T, 1>(smem, a.S, [&](int idx, int) -> float2 {
+        const int x = idx - off;
+        if (x < 0 || x >= np) return make_float2(0.0f, 0.0f);
+        return pupil_field(a.pupil, pc, x, y);
+    });
+    fft_run<T, 1, NMAX, false>(a.plan_s, smem);
+    const int wn = w->win_n;
+    const int wx0 = w->win_x0;
+    const int S = a.S;
+    float2* out = a.rows + (static_cast<size_t>(b) * np + y) * a.win_stride;
+    for (int wx = threadIdx.x; wx < wn; wx += T) {
+        int u = wx0 + wx + a.half;  // shifted column X -> unshifted (X + S/2) mod S
+        if (u >= S) u -= S;
+        out[wx] = smem[u];
+    }
+}
+
+// ---- raw PSF: column pass + |.|^2 + fftshift window -----------------------------
+// grid (ceil(win/C), B).  Columns X0..X0+C of the window; the N_p non-zero rows
+// are read in the first stage, |F|^2 of the window rows written by the last.
+template <int T, int C, int NMAX>
+__global__ void __launch_bounds__(T) psf_cols_kernel(PsfBankArgs a) {
+    extern __shared__ float2 smem[];
+    const int b = blockIdx.y;
+    const WavelengthInfo* w = a.wl + b;
+    const int wn = w->win_n;
+    const int X0 = blockIdx.x * C;
+    if (X0 >= wn) return;
+    const int np = a.pupil.size;
+    const int off = a.off;
+    const int stride = a.win_stride;
+    const float2* in = a.rows + static_cast<size_t>(b) * np * stride;
+    float* outw = a.win + static_cast<size_t>(b) * stride * stride;
+    smem_fill<T, C>(smem, a.S, [&](int idx, int col) -> float2 {
+        const int g = idx - off;
+        const int X = X0 + col;
+        if (g < 0 || g >= np || X >= wn) return make_float2(0.0f, 0.0f);
+        return in[static_cast<size_t>(g) * stride + X];
+    });
+    fft_run<T, C, NMAX, false>(a.plan_s, smem);
+    const int S = a.S;
+    const int wy0 = w->win_x0;
+    double esum = 0.0;
+    for (int i = threadIdx.x; i < wn * C; i += T) {
+        const int wy = i / C, col = i % C;
+        const int X = X0 + col;
+        if (X >= wn) continue;
+        int v = wy0 + wy + a.half;  // shifted row Y -> unshifted (Y + S/2) mod S
+        if (v >= S) v -= S;
+        const float2 f = smem[v * C + col];
+        const float I = f.x * f.x + f.y * f.y;
+        outw[static_cast<size_t>(wy) * stride + X] = I;
+        esum += I;
+    }
+    if (a.want_energy) {
+        const double tot = block_sum(esum);
+        if (threadIdx.x == 0) atomicAdd(&a.scalars[b].energy, tot);
+    }
+}
+
+// ---- lambda-rescale -----------------------------------------------------------------
+struct Window {
+    const float* p;
+    int stride, x0, n, S;
+};
+
+// sampleSquareBilinear (LensDiffCpuReference.cpp:316-336) reading the |F|^2
+// window; the window covers every pixel the kernel touches.
+__device__ __forceinline__ float sample_bilinear(const Window& w, float x, float y) {
+    const float lim = static_cast<float>(w.S - 1);
+    if (x < 0.0f || y < 0.0f || x > lim || y > lim) return 0.0f;
+    const int x0 = static_cast<int>(floorf(x));
+    const int y0 = static_cast<int>(floorf(y));
+    const int x1 = min(x0 + 1, w.S - 1);
+    const int y1 = min(y0 + 1, w.S - 1);
+    const float tx = x - static_cast<float>(x0);
+    const float ty = y - static_cast<float>(y0);
+    const int hi = w.n - 1;
+    const int ax0 = min(max(x0 - w.x0, 0), hi), ax1 = min(max(x1 - w.x0, 0), hi);
+    const int ay0 = min(max(y0 - w.x0, 0), hi), ay1 = min(max(y1 - w.x0, 0), hi);
+    const float v00 = w.p[static_cast<size_t>(ay0) * w.stride + ax0];
+    const float v10 = w.p[static_cast<size_t>(ay0) * w.stride + ax1];
+    const float v01 = w.p[static_cast<size_t>(ay1) * w.stride + ax0];
+    const float v11 = w.p[static_cast<size_t>(ay1) * w.stride + ax1];
+    const float vx0 = v00 + (v10 - v00) * tx;
+    const float vx1 = v01 + (v11 - v01) * tx;
+    return vx0 + (vx1 - vx0) * ty;
+}
+
+// sampleSquareFiltered (LensDiffCpuReference.cpp:338-353)
+__device__ __forceinline__ float sample_filtered(const Window& w, float x, float y, float footprint, int taps,
+                                                 float step) {
+    if (taps == 0) return sample_bilinear(w, x, y);
+    float sum = 0.0f;
+    for (int ty = 0; ty < taps; ++ty) {
+        const float oy = (static_cast<float>(ty) + 0.5f) * step - footprint * 0.5f;
+        for (int tx = 0; tx < taps; ++tx) {
+            const float ox = (static_cast<float>(tx) + 0.5f) * step - footprint * 0.5f;
+            sum += sample_bilinear(w, x + ox, y + oy);
+        }
+    }
+    return sum / static_cast<float>(taps * taps);
+}
+
+// First ring index a 32x32 tile can touch, for a centre at (c, c) and ring
+// indices clamped to `cap`: every pixel of the tile has a ring index in
+// [base, base + kRingSpan).
+__device__ __forceinline__ int tile_ring_base(int tx0, int ty0, int c, int cap) {
+    const int dx = tx0 > c ? tx0 - c : (tx0 + kTile - 1 < c ? c - (tx0 + kTile - 1) : 0);
+    const int dy = ty0 > c ? ty0 - c : (ty0 + kTile - 1 < c ? c - (ty0 + kTile - 1) : 0);
+    const float r = sqrtf(static_cast<float>(dx * dx + dy * dy));
+    return min(cap, max(0, static_cast<int>(r) - 1));
+}
+
+// grid (ceil(K/32), ceil(K/32), B), block (32, 8).
+__global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
+    __shared__ double ring[kRingSpan];
+    const int b = blockIdx.z;
+    const WavelengthInfo* wi = a.wl + b;
+    const int K = a.K, R = a.R;
+    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
+    const int tid = threadIdx.x + threadIdx.y * 32;
+    const int rbase = tile_ring_base(tx0, ty0, R, R);
+    for (int i = tid; i < kRingSpan; i += 256) ring[i] = 0.0;
+    __syncthreads();
+    Window w{a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride, a.win_stride, wi->win_x0, wi->win_n, a.S};
+    const float kc = static_cast<float>(K - 1) * 0.5f;
+    const float inv = wi->inv_scale;
+    const float rc = a.raw_center;
+    float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
+    double lsum = 0.0;
+    const int x = tx0 + threadIdx.x;
+#pragma unroll
+    for (int i = 0; i < kTile / 8; ++i) {
+        const int y = ty0 + threadIdx.y + 8 * i;
+        if (x < K && y < K) {
+            const float dx = static_cast<float>(x) - kc;
+            const float dy = static_cast<float>(y) - kc;
+            const float sx = rc + dx * inv;
+            const float sy = rc + dy * inv;
+            const float v = sample_filtered(w, sx, sy, inv, wi->taps, wi->step);
+            canvas[static_cast<size_t>(y) * K + x] = v;
+            lsum += v;
+            const int r = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy))));
+            atomicAdd(&ring[r - rbase], static_cast<double>(v));
+        }
+    }
+    __syncthreads();
+    double* gring = a.ring_round + static_cast<size_t>(b) * (R + 1);
+    for (int i = tid; i < kRingSpan; i += 256) {
+        if (ring[i] != 0.0 && rbase + i <= R) atomicAdd(&gring[rbase + i], ring[i]);
+    }
+    const double tot = block_sum(lsum);
+    if (tid == 0) atomicAdd(&a.scalars[b].s1, tot);
+}
+
+// Sum over rings of the unnormalised azimuthal mean, i.e. the normaliser of
+// azimuthalMeanKernel: sum_r count[r] * (ring[r] / s1) / count[r].
+__device__ double mean_kernel_sum(const PsfBankArgs& a, int b, double s1) {
+    const double* ring = a.ring_round + static_cast<size_t>(b) * (a.R + 1);
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nth = blockDim.x * blockDim.y;
+    double acc = 0.0;
+    for (int r = tid; r <= a.R; r += nth) {
+        const int c = max(1, a.count_round[r]);
+        acc += static_cast<double>(a.count_round[r]) * ((ring[r] / s1) / c);
+    }
+    __shared__ double s2_shared;
+    const double t = block_sum(acc);
+    if (tid == 0) s2_shared = t;
+    __syncthreads();
+    return s2_shared;
+}
+
+struct ShapeCtx {
+    const float* canvas;
+    const double* ring;
+    const int* count;
+    float inv_s1;     // 1 / s1
+    double s1, s2;
+    float gain;
+    int R, K;
+    float kc;
+};
+
+// reshapeAnisotropy value of one canvas pixel (unnormalised shaped kernel),
+// from the resampled value and its ring mean (LensDiffCpuReference.cpp:1088-1135).
+__device__ __forceinline__ float shaped_value(const ShapeCtx& c, int x, int y, float dx, float dy) {
+    const float base = c.canvas[static_cast<size_t>(y) * c.K + x] * c.inv_s1;
+    const int r = min(c.R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy))));
+    const float mean = static_cast<float>(((c.ring[r] / c.s1) / max(1, c.count[r])) / c.s2);
+    return fmaxf(0.0f, mean + (base - mean) * c.gain);
+}
+
+__device__ __forceinline__ ShapeCtx make_shape_ctx(const PsfBankArgs& a, int b, double s2) {
+    ShapeCtx c;
+    c.canvas = a.canvas + static_cast<size_t>(b) * a.K * a.K;
+    c.ring = a.ring_round + static_cast<size_t>(b) * (a.R + 1);
+    c.count = a.count_round;
+    c.s1 = a.scalars[b].s1;
+    c.inv_s1 = static_cast<float>(1.0 / c.s1);
+    c.s2 = s2;
+    c.gain = a.gain;
+    c.R = a.R;
+    c.K = a.K;
+    c.kc = static_cast<float>(a.K - 1) * 0.5f;
+    return c;
+}
+
+// grid (ceil(K/32), ceil(K/32), B): shaped kernel sums, ring energy/peak by
+// ceil(r) (estimateAdaptiveSupportRadius, LensDiffCpuReference.cpp:984-1007).
+__global__ void __launch_bounds__(256) shape_stats_kernel(PsfBankArgs a) {
+    __shared__ double ring_e[kRingSpan];
+    __shared__ unsigned int ring_p[kRingSpan];
+    const int b = blockIdx.z;
+    const int tid = threadIdx.x + threadIdx.y * 32;
+    const double s1 = a.scalars[b].s1;
+    const double s2 = mean_kernel_sum(a, b, s1);
+    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) a.scalars[b].s2 = s2;
+    const ShapeCtx c = make_shape_ctx(a, b, s2);
+    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
+    const int rbase = tile_ring_base(tx0, ty0, a.R, a.R);
+    for (int i = tid; i < kRingSpan; i += 256) {
+        ring_e[i] = 0.0;
+        ring_p[i] = 0u;
+    }
+    __syncthreads();
+    double lsum = 0.0;
+    unsigned int lpeak = 0u;
+    const int x = tx0 + threadIdx.x;
+#pragma unroll
+    for (int i = 0; i < kTile / 8; ++i) {
+        const int y = ty0 + threadIdx.y + 8 * i;
+        if (x < a.K && y < a.K) {
+            const float dx = static_cast<float>(x) - c.kc;
+            const float dy = static_cast<float>(y) - c.kc;
+            const float v = shaped_value(c, x, y, dx, dy);
+            lsum += v;
+            const unsigned int bits = __float_as_uint(v);
+            lpeak = max(lpeak, bits);
+            const int r = min(a.R, static_cast<int>(ceilf(sqrtf(dx * dx + dy * dy))));
+            atomicAdd(&ring_e[r - rbase], static_cast<double>(v));
+            atomicMax(&ring_p[r - rbase], bits);
+        }
+    }
+    __syncthreads();
+    const size_t ro = static_cast<size_t>(b) * (a.R + 1);
+    for (int i = tid; i < kRingSpan; i += 256) {
+        if (rbase + i <= a.R) {
+            if (ring_e[i] != 0.0) atomicAdd(&a.ring_ceil[ro + rbase + i], ring_e[i]);
+            if (ring_p[i] != 0u) atomicMax(&a.ring_peak[ro + rbase + i], ring_p[i]);
+        }
+    }
+    // block max of the peak
+    for (int o = 16; o > 0; o >>= 1) lpeak = max(lpeak, __shfl_xor_sync(0xffffffffu, lpeak, o));
+    if ((tid & 31) == 0 && lpeak != 0u) atomicMax(&a.scalars[b].peak, lpeak);
+    const double tot = block_sum(lsum);
+    if (tid == 0) atomicAdd(&a.scalars[b].s3, tot);
+}
+
+// grid (B), block 32: adaptive support radius and taper constants
+// (estimateAdaptiveSupportRadius :1009-1030, paddedAdaptiveSupportRadius
+// :1033-1036, cropKernelToRadius :1039, applySupportBoundaryTaper :962-965).
+__global__ void support_kernel(PsfBankArgs a) {
+    const int b = blockIdx.x;
+    if (threadIdx.x != 0) return;
+    PsfScalars& sc = a.scalars[b];
+    const int R = a.R;
+    const int radius_max = min(R, a.K / 2);
+    const double* e = a.ring_ceil + static_cast<size_t>(b) * (R + 1);
+    const unsigned int* pk = a.ring_peak + static_cast<size_t>(b) * (R + 1);
+    const double total = sc.s3;
+    const float peak = __uint_as_float(sc.peak);
+    int est = max(4, radius_max);
+    // thresholds apply to the normalised kernel: total 1, peak = peak / total
+    const bool degenerate = !(total > 0.0) || (static_cast<double>(peak) / total <= 1e-6);
+    if (!degenerate) {
+        // outsidePeak (suffix maxima of the ring peaks) written in place, then
+        // the first ring where captured energy and the remaining peak both pass.
+        double cum = 0.0;
+        float run = 0.0f;
+        unsigned int* pw = a.ring_peak + static_cast<size_t>(b) * (R + 1);
+        for (int r = radius_max; r >= 0; --r) {
+            run = fmaxf(run, __uint_as_float(pk[r]));
+            pw[r] = __float_as_uint(run);
+        }
+        const double thr_cap = static_cast<double>(0.9999f);
+        const float thr_peak = peak * 2e-4f;
+        for (int r = 0; r <= radius_max; ++r) {
+            cum += e[r];
+            const double captured = cum / total;
+            const float remaining = (r + 1 <= radius_max) ? __uint_as_float(pw[r + 1]) : 0.0f;
+            if (captured >= thr_cap && remaining <= thr_peak) {
+                est = max(4, r + 1);
+                break;
+            }
+        }
+    }
+    const int pad = max(6, min(24, static_cast<int>(ceilf(static_cast<float>(max(1, est)) * 0.05f))));
+    int rho = min(max(est + pad, 4), max(4, R));
+    rho = min(max(rho, 1), a.K / 2);
+    sc.radius = rho;
+    const float extent = fmaxf(1.0f, static_cast<float>(rho));
+    const float fade = fmaxf(6.0f, fminf(24.0f, extent * 0.04f));
+    sc.extent = extent;
+    sc.fade = fade;
+    sc.start = fmaxf(0.0f, extent - fade);
+}
+
+// grid (ceil(K/32), ceil(K/32), B): s4 = sum of taper * normalised shaped kernel
+// over the crop box (the normaliser of cropKernelToRadius).
+__global__ void __launch_bounds__(256) crop_sum_kernel(PsfBankArgs a) {
+    const int b = blockIdx.z;
+    const PsfScalars& sc = a.scalars[b];
+    const ShapeCtx c = make_shape_ctx(a, b, sc.s2);
+    const float inv_s3 = static_cast<float>(1.0 / sc.s3);
+    const int rho = sc.radius;
+    const int x = blockIdx.x * kTile + threadIdx.x;
+    double lsum = 0.0;
+#pragma unroll
+    for (int i = 0; i < kTile / 8; ++i) {
+        const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
+        if (x < a.K && y < a.K) {
+            const int ix = x - a.R, iy = y - a.R;
+            if (abs(ix) <= rho && abs(iy) <= rho) {
+                const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
+                const float v = shaped_value(c, x, y, static_cast<float>(x) - c.kc, static_cast<float>(y) - c.kc) * inv_s3;
+                const float wgt = taper_weight(sqrtf(dx * dx + dy * dy), sc.extent, sc.fade, sc.start);
+                lsum += static_cast<double>(v * wgt);
+            }
+        }
+    }
+    const double tot = block_sum(lsum);
+    if (threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(&a.scalars[b].s4, tot);
+}
+
+// Final kernel value of wavelength b at canvas pixel (x, y), 0 outside its crop.
+__device__ __forceinline__ float final_value(const PsfBankArgs& a, int b, int x, int y) {
+    const PsfScalars& sc = a.scalars[b];
+    const int ix = x - a.R, iy = y - a.R;
+    if (abs(ix) > sc.radius || abs(iy) > sc.radius) return 0.0f;
+    const ShapeCtx c = make_shape_ctx(a, b, sc.s2);
+    const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
+    const float v = shaped_value(c, x, y, static_cast<float>(x) - c.kc, static_cast<float>(y) - c.kc) *
+                    static_cast<float>(1.0 / sc.s3);
+    const float wgt = taper_weight(sqrtf(dx * dx + dy * dy), sc.extent, sc.fade, sc.start);
+    return (v * wgt) * static_cast<float>(1.0 / sc.s4);
+}
+
+// grid (ceil(K/32), ceil(K/32)), block (32, 8).
+__global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
+    const int x = blockIdx.x * kTile + threadIdx.x;
+    const int K = a.bank.K;
+#pragma unroll 1
+    for (int i = 0; i < kTile / 8; ++i) {
+        const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
+        if (x >= K || y >= K) continue;
+        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (int b = 0; b < a.bank.B; ++b) {
+            const float v = final_value(a.bank, b, x, y);
+            if (v != 0.0f) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (k < a.n_ker) acc[k] += a.coef[k][b] * v;
+            }
+        }
+        for (int k = 0; k < a.n_ker; ++k) a.out[(static_cast<size_t>(k) * K + y) * K + x] = acc[k];
+    }
+}
+
+// grid (ceil(K/32), ceil(K/32), B): final kernels packed at offsets[b].
+__global__ void __launch_bounds__(256) export_kernel(PsfBankArgs a, const int64_t* offsets, float* out) {
+    const int b = blockIdx.z;
+    const int rho = a.scalars[b].radius;
+    const int side = 2 * rho + 1;
+    const int x = blockIdx.x * kTile + threadIdx.x;
+    for (int i = 0; i < kTile / 8; ++i) {
+        const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
+        if (x >= a.K || y >= a.K) continue;
+        const int ix = x - a.R + rho, iy = y - a.R + rho;
+        if (ix < 0 || iy < 0 || ix >= side || iy >= side) continue;
+        out[offsets[b] + static_cast<int64_t>(iy) * side + ix] = final_value(a, b, x, y);
+    }
+}
+
+// ---- first-minimum calibration ------------------------------------------------------
+// grid (ceil(S/32), ceil(S/32)), block (32, 8): sums and counts of the shifted
+// intensity by round(r) around shiftedSpectrumCenterCoordinate.
+__global__ void __launch_bounds__(256) profile_kernel(const float* psf, int S, double* sums, int* counts,
+                                                      double* total) {
+    __shared__ double rs[kRingSpan];
+    __shared__ int rc[kRingSpan];
+    const int tid = threadIdx.x + threadIdx.y * 32;
+    const float c = (S & 1) == 0 ? static_cast<float>(S) * 0.5f : static_cast<float>(S - 1) * 0.5f;
+    const int ci = static_cast<int>(c);
+    const int rmax = S / 2;
+    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
+    const int rbase = tile_ring_base(tx0, ty0, ci, rmax);
+    for (int i = tid; i < kRingSpan; i += 256) {
+        rs[i] = 0.0;
+        rc[i] = 0;
+    }
+    __syncthreads();
+    double lsum = 0.0;
+    const int x = tx0 + threadIdx.x;
+    for (int i = 0; i < kTile / 8; ++i) {
+        const int y = ty0 + threadIdx.y + 8 * i;
+        if (x < S && y < S) {
+            const float dx = static_cast<float>(x) - c;
+            const float dy = static_cast<float>(y) - c;
+            const int r = min(rmax, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy))));
+            const float v = psf[static_cast<size_t>(y) * S + x];
+            lsum += v;
+            atomicAdd(&rs[r - rbase], static_cast<double>(v));
+            atomicAdd(&rc[r - rbase], 1);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < kRingSpan; i += 256) {
+        if (rc[i] != 0 && rbase + i <= rmax) {
+            atomicAdd(&sums[rbase + i], rs[i]);
+            atomicAdd(&counts[rbase + i], rc[i]);
+        }
+    }
+    const double tot = block_sum(lsum);
+    if (tid == 0) atomicAdd(total, tot);
+}
+
+__device__ float refine_parabolic(double l, double c, double r) {
+    const double den = l - 2.0 * c + r;
+    if (fabs(den) < 1e-6) return 0.0f;
+    return static_cast<float>(fmin(fmax(0.5 * (l - r) / den, -0.5), 0.5));
+}
+
+// One thread: radialMeanProfile normalised by the total, [1,2,1]/4 smoothing,
+// first local minimum after >= 2 descents with parabolic refinement, fallback
+// argmin over [1, max(4, S/8)] (LensDiffCpuReference.cpp:897-955).
+__global__ void first_zero_scan_kernel(const double* sums, const int* counts, const double* total, int S,
+                                       double* prof, float* r0) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n = S / 2 + 1;
+    const double t = *total > 0.0 ? *total : 1.0;
+    for (int r = 0; r < n; ++r) prof[r] = (sums[r] / t) / max(1, counts[r]);
+    if (n < 4) {
+        *r0 = 1.0f;
+        return;
+    }
+    double* sm = prof + n;
+    for (int i = 0; i < n; ++i) {
+        const double left = prof[i == 0 ? 0 : i - 1];
+        const double right = prof[i + 1 < n ? i + 1 : i];
+        sm[i] = (left + 2.0 * prof[i] + right) * 0.25;
+    }
+    int best = 1;
+    double bestv = sm[1];
+    int desc = sm[1] < sm[0] ? 1 : 0;
+    for (int i = 2; i + 1 < n; ++i) {
+        if (sm[i] <= sm[i - 1]) {
+            desc += 1;
+            if (sm[i] < bestv) {
+                bestv = sm[i];
+                best = i;
+            }
+            continue;
+        }
+        if (desc >= 2 && best > 0 && best + 1 < n) {
+            *r0 = fmaxf(1.0f, static_cast<float>(best) + refine_parabolic(sm[best - 1], sm[best], sm[best + 1]));
+            return;
+        }
+        best = i;
+        bestv = sm[i];
+        desc = 0;
+    }
+    const int limit = max(2, min(n - 1, max(4, S / 8)));
+    best = 1;
+    bestv = sm[1];
+    for (int i = 2; i <= limit; ++i) {
+        if (sm[i] < bestv) {
+            bestv = sm[i];
+            best = i;
+        }
+    }
+    if (best > 0 && best + 1 < n)
+        *r0 = fmaxf(1.0f, static_cast<float>(best) + refine_parabolic(sm[best - 1], sm[best], sm[best + 1]));
+    else
+        *r0 = static_cast<float>(best);
+}
+
+__global__ void normalize_psf_kernel(float* psf, int64_t n, const PsfScalars* sc) {
+    const double e = sc->energy;
+    const float inv = e > 0.0 ? static_cast<float>(1.0 / e) : 1.0f;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        psf[i] *= inv;
+}
+
+// ---- launch helpers ---------------------------------------------------------------
+template <int T, int NMAX>
+void rows_launch(const PsfBankArgs& a, cudaStream_t s) {
+    dim3 grid(a.pupil.size, a.B);
+    psf_rows_kernel<T, NMAX><<<grid, T, a.S * sizeof(float2), s>>>(a);
+}
+
+template <int T, int C, int NMAX>
+void cols_launch(const PsfBankArgs& a, cudaStream_t s) {
+    dim3 grid((a.win_stride + C - 1) / C, a.B);
+    psf_cols_kernel<T, C, NMAX><<<grid, T, static_cast<size_t>(a.S) * C * sizeof(float2), s>>>(a);
+}
+
+}  // namespace
+
+void launch_psf_rows(const PsfBankArgs& a, cudaStream_t s) {
+    if (a.S <= 1024) rows_launch<64, 1024>(a, s);
+    else if (a.S <= 2048) rows_launch<128, 2048>(a, s);
+    else if (a.S <= 4096) rows_launch<256, 4096>(a, s);
+    else if (a.S <= 8192) rows_launch<512, 8192>(a, s);
+    else rows_launch<1024, 16384>(a, s);
+}
+
+void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s) {
+    if (a.S <= 1024) cols_launch<256, 4, 1024>(a, s);
+    else if (a.S <= 2048) cols_launch<512, 4, 2048>(a, s);
+    else if (a.S <= 4096) cols_launch<1024, 4, 4096>(a, s);
+    else if (a.S <= 8192) cols_launch<1024, 2, 8192>(a, s);
+    else cols_launch<1024, 1, 16384>(a, s);
+}
+
+static dim3 canvas_grid(const PsfBankArgs& a, int z) {
+    return dim3((a.K + kTile - 1) / kTile, (a.K + kTile - 1) / kTile, z);
+}
+
+void launch_resample(const PsfBankArgs& a, cudaStream_t s) {
+    resample_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
+}
+
+void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s) {
+    shape_stats_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
+}
+
+void launch_support(const PsfBankArgs& a, cudaStream_t s) { support_kernel<<<a.B, 32, 0, s>>>(a); }
+
+void launch_crop_sum(const PsfBankArgs& a, cudaStream_t s) {
+    crop_sum_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
+}
+
+void launch_combine(const CombineArgs& a, cudaStream_t s) {
+    combine_kernel<<<canvas_grid(a.bank, 1), dim3(32, 8), 0, s>>>(a);
+}
+
+void launch_export(const PsfBankArgs& a, const int64_t* offsets_dev, float* out, cudaStream_t s) {
+    export_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a, offsets_dev, out);
+}
+
+void launch_first_zero(const float* psf, int S, double* ring_sums, int* ring_counts, double* total, float* r0_out,
+                       cudaStream_t s) {
+    dim3 grid((S + kTile - 1) / kTile, (S + kTile - 1) / kTile);
+    profile_kernel<<<grid, dim3(32, 8), 0, s>>>(psf, S, ring_sums, ring_counts, total);
+    // profile scratch follows the ring sums: 2 * (S/2 + 1) doubles
+    first_zero_scan_kernel<<<1, 32, 0, s>>>(ring_sums, ring_counts, total, S, ring_sums + (S / 2 + 1), r0_out);
+}
+
+void launch_normalize_psf(float* psf, int n, const PsfScalars* sc, cudaStream_t s) {
+    normalize_psf_kernel<<<592, 256, 0, s>>>(psf, static_cast<int64_t>(n), sc);
+}
+
+namespace {
+template <class Kern>
+void opt_in(Kern k, size_t bytes) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+}  // namespace
+
+void configure_psf_kernels() {
+    opt_in(psf_rows_kernel<64, 1024>, 1024 * 8);
+    opt_in(psf_rows_kernel<128, 2048>, 2048 * 8);
+    opt_in(psf_rows_kernel<256, 4096>, 4096 * 8);
+    opt_in(psf_rows_kernel<512, 8192>, 8192 * 8);
+    opt_in(psf_rows_kernel<1024, 16384>, 16384 * 8);
+    opt_in(psf_cols_kernel<256, 4, 1024>, 1024 * 4 * 8);
+    opt_in(psf_cols_kernel<512, 4, 2048>, 2048 * 4 * 8);
+    opt_in(psf_cols_kernel<1024, 4, 4096>, 4096 * 4 * 8);
+    opt_in(psf_cols_kernel<1024, 2, 8192>, 8192 * 2 * 8);
+    opt_in(psf_cols_kernel<1024, 1, 16384>, 16384 * 8);
+}
+
+}  // namespace ld
