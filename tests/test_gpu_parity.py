@@ -42,8 +42,19 @@ def _oracle_matrices(p):
     return np.array(p.naturalMatrix, np.float64), np.array(p.styleMatrix, np.float64)
 
 
+_STREAM = []
+
+
+def side_stream():
+    """A non-default stream: like the plugin host, the path requires a real
+    cudaStream (handle 0 is rejected as at LensDiffCuda.cu:4646-4651)."""
+    if not _STREAM:
+        _STREAM.append(torch.cuda.Stream())
+    return _STREAM[0]
+
+
 def render_gpu(cache, p, src, src_origin=(0, 0), dst_shape=None, dst_origin=None, render_window=None):
-    stream = torch.cuda.current_stream()
+    stream = side_stream()
     s = torch.from_numpy(np.ascontiguousarray(src, np.float32)).cuda()
     if dst_shape is None:
         dst_shape = src.shape
@@ -122,6 +133,7 @@ def test_render_matches_reference_fixture(cache, name):
     p, src, dst, _, _, _ = golden_case(name)
     p = with_matrices(p)
     out, st = render_gpu(cache, p, src)
+    torch.cuda.synchronize()
     assert st.ok, st
     assert rel_err(out, dst, dst[..., :3].max()) < OUT_TOL
     eff_ref = dst[..., :3] - src[..., :3]
@@ -203,9 +215,13 @@ def test_error_behaviour_mirrors_reference(cache):
     p = with_matrices(small_lens())
     src = torch.zeros(32, 32, 4, device="cuda")
     dst = torch.zeros(32, 32, 4, device="cuda")
-    stream = torch.cuda.current_stream()
+    stream = side_stream()
     req = image_request(src, dst, stream, frame_short_side=144)
     req.hostEnabledCudaRender = False
+    err = []
+    assert not run_lensdiff_cuda(req, p, cache, err)
+    assert err == ["cuda-render-not-enabled-by-host"]
+    req = image_request(src, dst, 0, frame_short_side=144)
     err = []
     assert not run_lensdiff_cuda(req, p, cache, err)
     assert err == ["cuda-render-not-enabled-by-host"]
@@ -215,6 +231,8 @@ def test_error_behaviour_mirrors_reference(cache):
     assert not run_lensdiff_cuda(req, p, cache, err)
     assert err == ["missing-source-or-destination-cuda-buffer"]
     req = image_request(src, dst, stream, frame_short_side=144)
+    st = cache.render(req, p.copy(debugView=3))
+    assert st.code == 6 and "debug" in st.stage
     st = cache.render(req, p.copy(lookMode=LensDiffLookMode.Split))
     assert st.code == 6 and "split" in st.stage
     st = cache.render(req, p)
