@@ -221,6 +221,10 @@ int ld_abi_version(void);
 size_t ld_device_bytes(const ld_ctx* ctx);
 /* Drops the cached PSF banks and kernel spectra. */
 void ld_clear_caches(ld_ctx* ctx);
+/* Reads and clears the context's device error word (synchronising the
+ * device): LD_OK if no kernel reported a problem since the last check,
+ * LD_ERR_TIMEOUT if a bounded device wait (bulk-copy barrier) gave up. */
+int ld_check_device_errors(ld_ctx* ctx, int32_t* error_word);
 
 /* ---- stage timing (CUDA events on the launching stream) ---------------- */
 /* Stage ids reported by ld_profile_collect. */
@@ -228,7 +232,7 @@ enum {
     LD_STAGE_PSF_ROWS = 0, LD_STAGE_PSF_COLS, LD_STAGE_RESAMPLE, LD_STAGE_SHAPE_STATS,
     LD_STAGE_SUPPORT, LD_STAGE_CROP_SUM, LD_STAGE_COMBINE, LD_STAGE_KSPEC_ROWS,
     LD_STAGE_KSPEC_COLS, LD_STAGE_FRAME_ROWS, LD_STAGE_FRAME_COLS, LD_STAGE_FRAME_INVERSE,
-    LD_STAGE_COUNT
+    LD_STAGE_PUPIL, LD_STAGE_COUNT
 };
 /* When enabled, every kernel launch of ld_render / ld_build_psf_bank is
  * bracketed by a pair of CUDA events on its stream. */

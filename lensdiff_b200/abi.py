@@ -295,6 +295,7 @@ EXPORTED_SYMBOLS = [
     "ld_abi_version",
     "ld_device_bytes",
     "ld_clear_caches",
+    "ld_check_device_errors",
     "ld_render",
     "ld_build_psf_bank",
     "ld_export_psf_bank",
@@ -306,7 +307,7 @@ EXPORTED_SYMBOLS = [
 ]
 
 STAGE_NAMES = ["psf_rows", "psf_cols", "resample", "shape_stats", "support", "crop_sum", "combine",
-               "kspec_rows", "kspec_cols", "frame_rows", "frame_cols", "frame_inverse"]
+               "kspec_rows", "kspec_cols", "frame_rows", "frame_cols", "frame_inverse", "pupil"]
 
 
 def lib() -> ctypes.CDLL:
@@ -350,6 +351,8 @@ def lib() -> ctypes.CDLL:
     L.ld_gaussian_rgb_matrix.argtypes = [ctypes.POINTER(c_f32), c_i32, ctypes.POINTER(c_f32),
                                          c_f32, ctypes.POINTER(c_f32)]
     L.ld_gaussian_rgb_matrix.restype = ctypes.c_int
+    L.ld_check_device_errors.argtypes = [vp, ctypes.POINTER(c_i32)]
+    L.ld_check_device_errors.restype = ctypes.c_int
     L.ld_set_profiling.argtypes = [vp, ctypes.c_int]
     L.ld_set_profiling.restype = ctypes.c_int
     L.ld_profile_collect.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_i32), c_i32]

@@ -140,6 +140,12 @@ class LensDiffPsfBankCache:
     def clear(self) -> None:
         self._lib.ld_clear_caches(self._h)
 
+    def check_device_errors(self) -> int:
+        """Reads and clears the device error word (0: no kernel gave up a wait)."""
+        w = ctypes.c_int32()
+        self._lib.ld_check_device_errors(self._h, ctypes.byref(w))
+        return int(w.value)
+
     def set_profiling(self, enable: bool) -> None:
         self._lib.ld_set_profiling(self._h, 1 if enable else 0)
 

@@ -67,7 +67,9 @@ struct ld_ctx {
     BankEntry bank;
     SpectraEntry spectra;
     // work buffers, grown on demand
-    DevBuf rows, win, combine_out, kspec_rows, frameA, frameB, scratch, calib, calib_psf;
+    DevBuf rows, win, combine_out, kspec_rows, frameA, frameB, calib, calib_psf, pupil_pre;
+    DevBuf err_word;    // device int: nonzero after a bounded wait gave up
+    int* err = nullptr;
     int launches = 0;
     // stage timing
     bool profiling = false;
@@ -200,7 +202,8 @@ bool factor_plan(int n, FftPlan* plan) {
     std::sort(r.begin(), r.end(), [](int a, int b) { return a > b; });
     plan->n = n;
     plan->nstages = static_cast<int>(r.size());
-    for (int v : r) plan->radix[k++] = v;
+    plan->codes = 0ull;
+    for (int v : r) plan->codes |= static_cast<unsigned long long>(v) << (4 * k++);
     return true;
 }
 
@@ -402,6 +405,33 @@ void validate_params(const ld_params& p) {
 
 size_t align256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
 
+// Fills the pupil part of a bank argument block and launches the per-bank
+// pupil pre-pass (amplitude, the λ-independent phase, the defocus term).
+// Only pupil rows whose pixel centres lie within the outer radius of the
+// (decentred) aperture can be non-zero; the row passes skip the others.
+void setup_pupil(ld_ctx* c, PsfBankArgs& a, const ld_params& p, bool circle, cudaStream_t s) {
+    a.pupil = pupil_params(p, circle);
+    a.base_phase = circle ? PhaseCoeffs{} : phase_for_wavelength(p, 550.0f);
+    a.base_phase.c[4] = 0.0f;  // defocus is carried per wavelength
+    const int n = a.pupil.size;
+    int lo = n, hi = 0;
+    for (int y = 0; y < n; ++y) {
+        const float ny = ((static_cast<float>(y) + 0.5f) / static_cast<float>(n) - 0.5f) * 2.0f;
+        if (std::abs(ny - a.pupil.decy) <= 0.8601f) {
+            lo = std::min(lo, y);
+            hi = std::max(hi, y + 1);
+        }
+    }
+    if (hi <= lo) {
+        lo = 0;
+        hi = 1;
+    }
+    a.row_lo = lo;
+    a.row_n = hi - lo;
+    a.pupil_pre = static_cast<float4*>(ensure(c, c->pupil_pre, static_cast<size_t>(n) * n * sizeof(float4)));
+    staged(c, LD_STAGE_PUPIL, s, [&] { launch_pupil_pre(a, s); });
+}
+
 // ---------------------------------------------------------------------------
 // first-zero calibration of the clear circle (one host sync per (N_p, S))
 // ---------------------------------------------------------------------------
@@ -412,7 +442,7 @@ float first_zero(ld_ctx* c, int np, int S, cudaStream_t s) {
     ld_params cp{};
     cp.pupil_resolution = np;
     PsfBankArgs a{};
-    a.pupil = pupil_params(cp, true);
+    setup_pupil(c, a, cp, true, s);
     a.B = 1;
     a.S = S;
     a.half = S / 2;
@@ -439,7 +469,7 @@ float first_zero(ld_ctx* c, int np, int S, cudaStream_t s) {
     float* r0d = reinterpret_cast<float*>(cal + o_r0);
     a.wl = dwl;
     a.scalars = dsc;
-    a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(np) * S * sizeof(float2)));
+    a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(a.row_n) * S * sizeof(float2)));
     a.win = static_cast<float*>(ensure(c, c->calib_psf, static_cast<size_t>(S) * S * sizeof(float)));
     check_cuda(cudaMemcpyAsync(dwl, &wi, sizeof(wi), cudaMemcpyHostToDevice, s), "calib-upload");
     check_cuda(cudaMemsetAsync(dsc, 0, sizeof(PsfScalars), s), "calib-memset");
@@ -533,7 +563,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
 
     PsfBankArgs& a = b.args;
     a = PsfBankArgs{};
-    a.pupil = pupil_params(p, false);
+    setup_pupil(c, a, p, false, s);
     a.B = B;
     a.S = S;
     a.half = S / 2;
@@ -544,7 +574,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     a.K = K;
     a.gain = 1.0f + std::max(0.0f, static_cast<float>(p.anisotropy_emphasis)) * 4.0f;  // :1127
     a.plan_s = make_plan(c, S);
-    a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(B) * np * win_stride * sizeof(float2)));
+    a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(B) * a.row_n * win_stride * sizeof(float2)));
     a.win = static_cast<float*>(ensure(c, c->win, static_cast<size_t>(B) * win_stride * win_stride * sizeof(float)));
     a.canvas = static_cast<float*>(ensure(c, b.canvas, static_cast<size_t>(B) * K * K * sizeof(float)));
     const size_t ringn = static_cast<size_t>(B) * (R + 1);
@@ -667,20 +697,45 @@ std::string spectra_key(const BankEntry& b, const Combination& cb, const GridGeo
     return k;
 }
 
-GridGeom make_geometry(ld_ctx* c, int W, int H, int K, int* req_w, int* req_h) {
+constexpr size_t kSmemBudget = 227 * 1024;
+
+// Smallest 5-smooth grid covering the linear convolution, both sides even (the
+// rows are real transforms of length Px = 2M; the column tiles are 16-byte
+// multiples for the bulk copies).  Column tiles are two spectrum columns wide
+// unless the column pass's shared-memory working set would not fit.
+GridGeom make_geometry(ld_ctx* c, int W, int H, int K, int n_drv, int* req_w, int* req_h) {
     GridGeom g{};
     *req_w = W + K - 1;
     *req_h = H + K - 1;
     g.Px = next_smooth(*req_w, true);
-    g.Py = next_smooth(*req_h, false);
+    g.Py = next_smooth(*req_h, true);
     g.M = g.Px / 2;
     if (g.M > 6912 || g.Py > 6912) throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-fft-grid"};
-    g.Pw = ((g.M + 1 + kColTile - 1) / kColTile) * kColTile;
-    g.tiles = g.Pw / kColTile;
+    const int Hp = H + (H & 1);
+    const int Kp = K + (K & 1);
+    g.ct = 0;
+    for (int ct : {2, 1}) {
+        g.ct = ct;
+        FrameArgs probe{};
+        probe.g = g;
+        probe.Hp = Hp;
+        probe.n_drv = n_drv;
+        if (frame_cols_smem(probe) <= kSmemBudget && kspec_cols_smem(g, Kp) <= kSmemBudget) break;
+        g.ct = 0;
+    }
+    if (g.ct == 0) throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-column-pass"};
+    g.Pw = ((g.M + 1 + g.ct - 1) / g.ct) * g.ct;
+    g.tiles = g.Pw / g.ct;
     g.plan_m = make_plan(c, g.M);
     g.plan_py = make_plan(c, g.Py);
     g.tw_px = twiddles(c, g.Px);
     return g;
+}
+
+int sm_count(int device) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return sms;
 }
 
 SpectraEntry& ensure_spectra(ld_ctx* c, BankEntry& b, const Combination& cb, const GridGeom& g, cudaStream_t s,
@@ -702,11 +757,15 @@ SpectraEntry& ensure_spectra(ld_ctx* c, BankEntry& b, const Combination& cb, con
     ka.n_ker = cb.n_ker;
     ka.R = b.R;
     ka.K = b.K;
+    ka.Kp = b.K + (b.K & 1);
     ka.canvas = ca.out;
-    ka.rows = static_cast<float2*>(ensure(c, c->kspec_rows, static_cast<size_t>(cb.n_ker) * b.K * g.Pw * sizeof(float2)));
+    ka.rows = static_cast<float2*>(
+        ensure(c, c->kspec_rows, static_cast<size_t>(cb.n_ker) * g.tiles * ka.Kp * g.ct * sizeof(float2)));
     ka.spectra = static_cast<float2*>(
-        ensure(c, e.spectra, static_cast<size_t>(cb.n_ker) * g.tiles * g.Py * kColTile * sizeof(float2)));
+        ensure(c, e.spectra, static_cast<size_t>(cb.n_ker) * g.tiles * g.Py * g.ct * sizeof(float2)));
     ka.scale = static_cast<float>(1.0 / (static_cast<double>(g.M) * static_cast<double>(g.Py)));
+    ka.grid = std::min(cb.n_ker * g.tiles, sm_count(c->device));
+    ka.err = c->err;
     staged(c, LD_STAGE_KSPEC_ROWS, s, [&] { launch_kspec_rows(ka, s); });
     staged(c, LD_STAGE_KSPEC_COLS, s, [&] { launch_kspec_cols(ka, s); });
     check_launch("kernel-spectra");
@@ -765,7 +824,16 @@ int ld_create(ld_ctx** out, int device, size_t hbm_budget_bytes) {
     {
         DeviceGuard g(device);
         configure_kernels();
-        if (cudaGetLastError() != cudaSuccess) {
+        bool ok = cudaGetLastError() == cudaSuccess;
+        if (ok) {
+            try {
+                c->err = static_cast<int*>(ensure(c, c->err_word, sizeof(int)));
+                ok = cudaMemset(c->err, 0, sizeof(int)) == cudaSuccess;
+            } catch (const Fail&) {
+                ok = false;
+            }
+        }
+        if (!ok) {
             delete c;
             return LD_ERR_CUDA;
         }
@@ -775,13 +843,24 @@ int ld_create(ld_ctx** out, int device, size_t hbm_budget_bytes) {
     return LD_OK;
 }
 
+int ld_check_device_errors(ld_ctx* c, int32_t* error_word) {
+    if (!c) return LD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    DeviceGuard g(c->device);
+    int v = 0;
+    if (cudaMemcpy(&v, c->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return LD_ERR_CUDA;
+    if (v != 0 && cudaMemset(c->err, 0, sizeof(int)) != cudaSuccess) return LD_ERR_CUDA;
+    if (error_word) *error_word = v;
+    return v == 0 ? LD_OK : LD_ERR_TIMEOUT;
+}
+
 void ld_destroy(ld_ctx* c) {
     if (!c) return;
     DeviceGuard g(c->device);
     for (auto& kv : c->twiddles) free_buf(c, kv.second);
     for (auto& kv : c->ring_counts) free_buf(c, kv.second);
-    DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,
-                      &c->frameB, &c->scratch, &c->calib,       &c->calib_psf};
+    DevBuf* bufs[] = {&c->rows,   &c->win,  &c->combine_out, &c->kspec_rows, &c->frameA,
+                      &c->frameB, &c->calib, &c->calib_psf,  &c->err_word, &c->pupil_pre};
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
     DevBuf* bb[] = {&c->bank.canvas, &c->bank.ring_round, &c->bank.ring_ceil, &c->bank.ring_peak,
@@ -879,7 +958,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         BankEntry& bank = ensure_bank(ctx, p, s, &bank_rebuilt);
         const Combination cb = make_combination(p, bank.wavelengths);
         int rw = 0, rh = 0;
-        const GridGeom g = make_geometry(ctx, W, H, bank.K, &rw, &rh);
+        const GridGeom g = make_geometry(ctx, W, H, bank.K, cb.n_drv, &rw, &rh);
         SpectraEntry& sp = ensure_spectra(ctx, bank, cb, g, s, &spectra_rebuilt);
 
         FrameArgs fa{};
@@ -911,14 +990,14 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         fa.core_comp = static_cast<float>(std::max(0.0, p.core_compensation));
         const float protect = std::max(0.2f, static_cast<float>(std::min(std::max(p.core_preserve, 0.0), 1.0)));
         fa.max_sub = fa.sel.rscale > 1e-6f ? (1.0f - protect) / fa.sel.rscale : 0.0f;
-        fa.A = static_cast<float2*>(ensure(ctx, ctx->frameA, static_cast<size_t>(cb.n_drv) * H * g.Pw * sizeof(float2)));
-        fa.Bout = static_cast<float2*>(ensure(ctx, ctx->frameB, static_cast<size_t>(cb.n_out) * H * g.Pw * sizeof(float2)));
+        fa.Hp = H + (H & 1);
+        fa.A = static_cast<float2*>(
+            ensure(ctx, ctx->frameA, static_cast<size_t>(cb.n_drv) * g.tiles * fa.Hp * g.ct * sizeof(float2)));
+        fa.Bout = static_cast<float2*>(
+            ensure(ctx, ctx->frameB, static_cast<size_t>(cb.n_out) * g.tiles * H * g.ct * sizeof(float2)));
         fa.spectra = static_cast<const float2*>(sp.spectra.p);
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        fa.col_grid = std::min(g.tiles, sms * column_pass_blocks_per_sm(g.Py));
-        fa.scratch = static_cast<float2*>(
-            ensure(ctx, ctx->scratch, static_cast<size_t>(fa.col_grid) * g.Py * kColTile * sizeof(float2)));
+        fa.col_grid = std::min(g.tiles, sm_count(ctx->device));  // one persistent CTA per SM
+        fa.err = ctx->err;
         staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
         staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
         staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse(fa, s); });
@@ -1017,7 +1096,7 @@ int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float
             throw Fail{LD_ERR_ARG, "invalid-wavelength-index"};
         const int np = pupil_size(p), R = max_kernel_radius(p), S = raw_psf_size(np, R);
         PsfBankArgs a{};
-        a.pupil = pupil_params(p, false);
+        setup_pupil(ctx, a, p, false, s);
         a.B = 1;
         a.S = S;
         a.half = S / 2;
@@ -1034,7 +1113,7 @@ int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float
         a.wl = dwl;
         a.scalars = dsc;
         a.want_energy = 1;
-        a.rows = static_cast<float2*>(ensure(ctx, ctx->rows, static_cast<size_t>(np) * S * sizeof(float2)));
+        a.rows = static_cast<float2*>(ensure(ctx, ctx->rows, static_cast<size_t>(a.row_n) * S * sizeof(float2)));
         a.win = psf_out;
         check_cuda(cudaMemcpyAsync(dwl, &wi, sizeof(wi), cudaMemcpyHostToDevice, s), "rawpsf-upload");
         check_cuda(cudaMemsetAsync(dsc, 0, sizeof(PsfScalars), s), "rawpsf-memset");

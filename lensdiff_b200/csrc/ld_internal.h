@@ -38,6 +38,9 @@ struct PsfScalars {      // per wavelength, FP64 sums of the shaping chain
 
 struct PsfBankArgs {
     PupilParams pupil;
+    PhaseCoeffs base_phase;      // every coefficient but defocus (λ independent)
+    float4* pupil_pre;           // [N_p][N_p]: amplitude, phi0, z4, phase valid
+    int row_lo, row_n;           // pupil rows that can be non-zero
     const WavelengthInfo* wl;    // [B]
     int B;
     int S;                       // raw PSF size
@@ -60,6 +63,7 @@ struct PsfBankArgs {
     int want_energy;
 };
 
+void launch_pupil_pre(const PsfBankArgs& a, cudaStream_t s);
 void launch_psf_rows(const PsfBankArgs& a, cudaStream_t s);
 void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s);
 void launch_resample(const PsfBankArgs& a, cudaStream_t s);
@@ -89,11 +93,19 @@ void launch_first_zero(const float* psf, int S, double* ring_sums, int* ring_cou
 void launch_normalize_psf(float* psf, int n, const PsfScalars* sc, cudaStream_t s);
 
 // ---- kernel spectra and frame chain ------------------------------------------------
+// Column tiles are `ct` (2, or 1 for very tall grids) adjacent spectrum columns.
+// Every array the column pass touches is stored tile-major so that one tile is
+// one contiguous block that a single bulk copy moves:
+//   A  [n_drv][tiles][Hp][ct]   forward row spectra (Hp = H rounded up to even)
+//   B  [n_out][tiles][H][ct]    column-pass outputs
+//   KR [n_ker][tiles][Kp][ct]   kernel row spectra (Kp = K rounded up to even)
+//   KS [n_ker][tiles][Py][ct]   kernel spectra, scaled by 1 / (M * Py)
 struct GridGeom {
     int Px, Py;        // FFT grid
     int M;             // Px / 2
-    int Pw;            // padded row width in complex (multiple of kColTile, > M)
-    int tiles;         // Pw / kColTile
+    int ct;            // column tile width
+    int Pw;            // padded bins per row (multiple of ct, > M)
+    int tiles;         // Pw / ct
     FftPlan plan_m;    // length M (real rows via half-length complex)
     FftPlan plan_py;   // length Py (columns)
     const float2* tw_px;  // exp(-2 pi i k / Px), k < Px
@@ -102,14 +114,17 @@ struct GridGeom {
 struct KernelSpectraArgs {
     GridGeom g;
     int n_ker;
-    int R, K;
+    int R, K, Kp;
     const float* canvas;  // [n_ker][K][K]
-    float2* rows;         // [n_ker][K][Pw]
-    float2* spectra;      // [n_ker][tiles][Py][kColTile]
+    float2* rows;         // KR
+    float2* spectra;      // KS
     float scale;          // 1 / (M * Py)
+    int grid;             // persistent CTAs of the column pass
+    int* err;             // device error word
 };
 void launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s);
 void launch_kspec_cols(const KernelSpectraArgs& a, cudaStream_t s);
+size_t kspec_cols_smem(const GridGeom& g, int Kp);
 
 struct SelectionParams {
     int luma;              // extraction mode
@@ -123,7 +138,7 @@ struct SelectionParams {
 struct FrameArgs {
     GridGeom g;
     SelectionParams sel;
-    int W, H;
+    int W, H, Hp;
     const unsigned char* src;  // device, row-major float RGBA
     int64_t src_pitch;
     unsigned char* dst;
@@ -134,11 +149,11 @@ struct FrameArgs {
     int n_drv;                 // 1 (spectral scalar driver) or 3 (Mono RGB)
     int n_out;                 // 3 or 4 (4th: luma-lock target)
     int n_ker;                 // kernels (1 for Mono)
-    float2* A;                 // [n_drv][H][Pw]
-    float2* Bout;              // [n_out][H][Pw]
-    const float2* spectra;     // [n_ker][tiles][Py][kColTile]
-    float2* scratch;           // [grid][Py][kColTile]
+    float2* A;
+    float2* Bout;
+    const float2* spectra;
     int col_grid;              // persistent CTAs of the column pass
+    int* err;                  // device error word
     // epilogue
     int mono;
     float saturation;
@@ -148,9 +163,10 @@ struct FrameArgs {
 void launch_frame_rows(const FrameArgs& a, cudaStream_t s);
 void launch_frame_cols(const FrameArgs& a, cudaStream_t s);
 void launch_frame_inverse(const FrameArgs& a, cudaStream_t s);
+size_t frame_cols_smem(const FrameArgs& a);
+int frame_cols_threads(int Py);
 
 // shared-memory opt-in for every kernel instantiation (once per device)
 void configure_kernels();
-int column_pass_blocks_per_sm(int Py);
 
 }  // namespace ld

@@ -131,6 +131,38 @@ __device__ __forceinline__ float pupil_phase(const PupilParams& p, const PhaseCo
     return v;
 }
 
+// The phase of one pupil pixel split as phi = phi0 + c4 * z4: phi0 collects
+// every term but defocus, z4 is the defocus polynomial.  Only defocus varies
+// across the wavelengths of a bank (the chromatic focus offset,
+// LensDiffCpuReference.cpp:1721-1723), so phi0 and z4 are computed once per
+// bank.  `valid` is 0 outside the phase support (radius > outer or r^2 > 1).
+__device__ __forceinline__ void pupil_phase_split(const PupilParams& p, const PhaseCoeffs& c, int x, int y,
+                                                  float* phi0, float* z4, float* valid) {
+    PhaseCoeffs c0 = c;
+    c0.enabled = 1;
+    const float c4 = c0.c[4];
+    c0.c[4] = 0.0f;
+    *phi0 = pupil_phase(p, c0, x, y);
+    c0 = PhaseCoeffs{};
+    c0.enabled = 1;
+    c0.c[4] = 1.0f;
+    *z4 = pupil_phase(p, c0, x, y);
+    (void)c4;
+    // the support test of pupil_phase, repeated
+    const float nx = pupil_coord(x, p.size);
+    const float ny = pupil_coord(y, p.size);
+    const float radius = sqrtf(nx * nx + ny * ny);
+    bool ok = radius <= kOuterRadius;
+    if (ok) {
+        const float rx = nx * p.phase_cs - ny * p.phase_sn;
+        const float ry = nx * p.phase_sn + ny * p.phase_cs;
+        const float sx = rx / kOuterRadius - p.decx;
+        const float sy = ry / kOuterRadius - p.decy;
+        ok = sx * sx + sy * sy <= 1.0f;
+    }
+    *valid = ok ? 1.0f : 0.0f;
+}
+
 // Pupil field sample A * exp(i 2 pi phi) (LensDiffCpuReference.cpp:838-848).
 __device__ __forceinline__ float2 pupil_field(const PupilParams& p, const PhaseCoeffs& c, int x, int y) {
     const float a = pupil_amplitude(p, x, y);

@@ -2,16 +2,21 @@
 // kernel shaping -> adaptive crop/taper -> weighted combination.
 //
 // Reference stages (LensDiffCpuReference.cpp):
+//   buildPupilAmplitude / BuildLensDiffPupilPhaseWaves :758-829
+//                           -> pupil_pre_kernel (once per bank)
 //   buildShiftedRawPsf      :831-859   -> psf_rows_kernel + psf_cols_kernel
 //   makeResampledKernel     :1060-1086 -> resample_kernel
 //   azimuthalMeanKernel / reshapeAnisotropy / estimateAdaptiveSupportRadius
 //                           :1088-1135, :984-1031 -> shape_stats_kernel, support_kernel
 //   cropKernelToRadius + applySupportBoundaryTaper :1038-1058, :957-982
-//                           -> crop_sum_kernel (normaliser) and combine_kernel
+//                           -> crop_sum_kernel, combine_kernel
 //   estimateFirstMinimumRadius :865-955 -> profile_kernel + first_zero_scan_kernel
 //
 // All wavelengths of a bank run in the same launches (blockIdx.y / .z is the
-// wavelength).  No stage returns to the host.
+// wavelength).  No stage returns to the host.  The canvas of a wavelength is
+// overwritten stage by stage: resampled value -> shaped value (shape_stats) ->
+// shaped * taper inside the crop box, 0 outside (crop_sum); the final,
+// normalised kernel is that value / (s3 * s4).
 #include "ld_internal.h"
 
 namespace ld {
@@ -29,50 +34,91 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Block-wide sum of one double; result valid in thread 0.
 __device__ double block_sum(double v) {
     __shared__ double part[32];
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-    const int lane2 = tid & 31, warp2 = tid >> 5;
-    (void)lane;
-    (void)warp;
+    const int lane = tid & 31, warp = tid >> 5;
     v = warp_sum(v);
     const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
     __syncthreads();
-    if (lane2 == 0) part[warp2] = v;
+    if (lane == 0) part[warp] = v;
     __syncthreads();
     double r = 0.0;
-    if (warp2 == 0) {
-        r = lane2 < nwarps ? part[lane2] : 0.0;
+    if (warp == 0) {
+        r = lane < nwarps ? part[lane] : 0.0;
         r = warp_sum(r);
     }
     return r;
 }
 
+// Warp-segmented reduction over runs of equal `slot` in consecutive lanes
+// (slot < 0: inactive lane).  Returns true on the last lane of each run, whose
+// `v` then holds the run's sum (MAX=false) or maximum (MAX=true).  Along a
+// canvas row the ring index of consecutive pixels changes slowly, so a warp
+// of 32 pixels collapses to a few runs and one shared-memory atomic each.
+template <bool MAX>
+__device__ __forceinline__ bool warp_run_reduce(int slot, float& v) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int prev = __shfl_up_sync(full, slot, 1);
+    const int nxt = __shfl_down_sync(full, slot, 1);
+    const bool head = lane == 0 || prev != slot;
+    const unsigned heads = __ballot_sync(full, head);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const float o = __shfl_up_sync(full, v, d);
+        if (lane >= d) {
+            // lane-d is in this run iff no run starts in (lane-d, lane]
+            const unsigned long long span = ((2ull << lane) - 1ull) ^ ((2ull << (lane - d)) - 1ull);
+            if ((static_cast<unsigned long long>(heads) & span) == 0ull) v = MAX ? fmaxf(v, o) : v + o;
+        }
+    }
+    const bool tail = lane == 31 || nxt != slot;
+    return tail && slot >= 0;
+}
+
+// ---- pupil, once per bank --------------------------------------------------------
+__global__ void __launch_bounds__(256) pupil_pre_kernel(PsfBankArgs a) {
+    const int n = a.pupil.size;
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= n * n) return;
+    const int x = i % n, y = i / n;
+    const float amp = pupil_amplitude(a.pupil, x, y);
+    float phi0 = 0.0f, z4 = 0.0f, valid = 0.0f;
+    if (amp > 0.0f) pupil_phase_split(a.pupil, a.base_phase, x, y, &phi0, &z4, &valid);
+    a.pupil_pre[i] = make_float4(amp, phi0, z4, valid);
+}
+
 // ---- raw PSF: row pass ---------------------------------------------------------
-// grid (N_p, B).  Row y of the pupil raster, embedded at (S-N_p)/2 of a length-S
-// row; the pupil field is generated in the first stage's load, the window
-// columns are written by the last stage.
+// grid (row_n, B).  Pupil row y = row_lo + blockIdx.x, embedded at (S-N_p)/2 of
+// a length-S row; the field A exp(i 2 pi phi) is generated in the fill, the
+// window columns are written by the drain.
 template <int T, int NMAX>
 __global__ void __launch_bounds__(T) psf_rows_kernel(PsfBankArgs a) {
     extern __shared__ float2 smem[];
-    __shared__ PhaseCoeffs pc;
-    const int y = blockIdx.x;
+    const int yr = blockIdx.x;
+    const int y = a.row_lo + yr;
     const int b = blockIdx.y;
     const WavelengthInfo* w = a.wl + b;
-    if (threadIdx.x == 0) pc = w->phase;
-    __syncthreads();
     const int np = a.pupil.size;
     const int off = a.off;
-    smem_fill<T, 1>(smem, a.S, [&](int idx, int) -> float2 {
+    const int enabled = w->phase.enabled;
+    const float c4 = w->phase.c[4];
+    const float4* pre = a.pupil_pre + static_cast<size_t>(y) * np;
+    smem_fill<T, 1>(smem, a.S, [=](int idx, int) -> float2 {
         const int x = idx - off;
         if (x < 0 || x >= np) return make_float2(0.0f, 0.0f);
-        return pupil_field(a.pupil, pc, x, y);
+        const float4 q = pre[x];
+        if (q.x <= 0.0f) return make_float2(0.0f, 0.0f);
+        const float ph = (enabled && q.w != 0.0f) ? q.y + c4 * q.z : 0.0f;
+        if (ph == 0.0f) return make_float2(q.x, 0.0f);
+        float sn, cs;
+        sincosf(ph * 2.0f * kPiF, &sn, &cs);
+        return make_float2(q.x * cs, q.x * sn);
     });
     fft_run<T, 1, NMAX, false>(a.plan_s, smem);
     const int wn = w->win_n;
     const int wx0 = w->win_x0;
     const int S = a.S;
-    float2* out = a.rows + (static_cast<size_t>(b) * np + y) * a.win_stride;
+    float2* out = a.rows + (static_cast<size_t>(b) * a.row_n + yr) * a.win_stride;
     for (int wx = threadIdx.x; wx < wn; wx += T) {
         int u = wx0 + wx + a.half;  // shifted column X -> unshifted (X + S/2) mod S
         if (u >= S) u -= S;
@@ -81,8 +127,8 @@ __global__ void __launch_bounds__(T) psf_rows_kernel(PsfBankArgs a) {
 }
 
 // ---- raw PSF: column pass + |.|^2 + fftshift window -----------------------------
-// grid (ceil(win/C), B).  Columns X0..X0+C of the window; the N_p non-zero rows
-// are read in the first stage, |F|^2 of the window rows written by the last.
+// grid (ceil(win/C), B).  Columns X0..X0+C of the window; only the pupil rows
+// that can be non-zero are read, |F|^2 of the window rows is written.
 template <int T, int C, int NMAX>
 __global__ void __launch_bounds__(T) psf_cols_kernel(PsfBankArgs a) {
     extern __shared__ float2 smem[];
@@ -91,15 +137,15 @@ __global__ void __launch_bounds__(T) psf_cols_kernel(PsfBankArgs a) {
     const int wn = w->win_n;
     const int X0 = blockIdx.x * C;
     if (X0 >= wn) return;
-    const int np = a.pupil.size;
-    const int off = a.off;
+    const int lo = a.off + a.row_lo;
+    const int rn = a.row_n;
     const int stride = a.win_stride;
-    const float2* in = a.rows + static_cast<size_t>(b) * np * stride;
+    const float2* in = a.rows + static_cast<size_t>(b) * rn * stride;
     float* outw = a.win + static_cast<size_t>(b) * stride * stride;
-    smem_fill<T, C>(smem, a.S, [&](int idx, int col) -> float2 {
-        const int g = idx - off;
+    smem_fill<T, C>(smem, a.S, [=](int idx, int col) -> float2 {
+        const int g = idx - lo;
         const int X = X0 + col;
-        if (g < 0 || g >= np || X >= wn) return make_float2(0.0f, 0.0f);
+        if (g < 0 || g >= rn || X >= wn) return make_float2(0.0f, 0.0f);
         return in[static_cast<size_t>(g) * stride + X];
     });
     fft_run<T, C, NMAX, false>(a.plan_s, smem);
@@ -179,18 +225,21 @@ __device__ __forceinline__ int tile_ring_base(int tx0, int ty0, int c, int cap) 
 
 // grid (ceil(K/32), ceil(K/32), B), block (32, 8).
 __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
-    __shared__ double ring[kRingSpan];
+    __shared__ float ring[kRingSpan];
     const int b = blockIdx.z;
     const WavelengthInfo* wi = a.wl + b;
     const int K = a.K, R = a.R;
     const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
     const int tid = threadIdx.x + threadIdx.y * 32;
     const int rbase = tile_ring_base(tx0, ty0, R, R);
-    for (int i = tid; i < kRingSpan; i += 256) ring[i] = 0.0;
+    for (int i = tid; i < kRingSpan; i += 256) ring[i] = 0.0f;
     __syncthreads();
-    Window w{a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride, a.win_stride, wi->win_x0, wi->win_n, a.S};
+    const Window w{a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride, a.win_stride, wi->win_x0,
+                   wi->win_n, a.S};
     const float kc = static_cast<float>(K - 1) * 0.5f;
     const float inv = wi->inv_scale;
+    const int taps = wi->taps;
+    const float step = wi->step;
     const float rc = a.raw_center;
     float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
     double lsum = 0.0;
@@ -198,22 +247,23 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
 #pragma unroll
     for (int i = 0; i < kTile / 8; ++i) {
         const int y = ty0 + threadIdx.y + 8 * i;
-        if (x < K && y < K) {
+        const bool in = x < K && y < K;
+        float v = 0.0f;
+        int slot = -1;
+        if (in) {
             const float dx = static_cast<float>(x) - kc;
             const float dy = static_cast<float>(y) - kc;
-            const float sx = rc + dx * inv;
-            const float sy = rc + dy * inv;
-            const float v = sample_filtered(w, sx, sy, inv, wi->taps, wi->step);
+            v = sample_filtered(w, rc + dx * inv, rc + dy * inv, inv, taps, step);
             canvas[static_cast<size_t>(y) * K + x] = v;
             lsum += v;
-            const int r = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy))));
-            atomicAdd(&ring[r - rbase], static_cast<double>(v));
+            slot = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy)))) - rbase;
         }
+        if (warp_run_reduce<false>(slot, v)) atomicAdd(&ring[slot], v);
     }
     __syncthreads();
     double* gring = a.ring_round + static_cast<size_t>(b) * (R + 1);
     for (int i = tid; i < kRingSpan; i += 256) {
-        if (ring[i] != 0.0 && rbase + i <= R) atomicAdd(&gring[rbase + i], ring[i]);
+        if (ring[i] != 0.0f && rbase + i <= R) atomicAdd(&gring[rbase + i], static_cast<double>(ring[i]));
     }
     const double tot = block_sum(lsum);
     if (tid == 0) atomicAdd(&a.scalars[b].s1, tot);
@@ -221,14 +271,13 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
 
 // Sum over rings of the unnormalised azimuthal mean, i.e. the normaliser of
 // azimuthalMeanKernel: sum_r count[r] * (ring[r] / s1) / count[r].
-__device__ double mean_kernel_sum(const PsfBankArgs& a, int b, double s1) {
-    const double* ring = a.ring_round + static_cast<size_t>(b) * (a.R + 1);
+__device__ double mean_kernel_sum(const double* ring, const int* count, int R, double s1) {
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
     const int nth = blockDim.x * blockDim.y;
     double acc = 0.0;
-    for (int r = tid; r <= a.R; r += nth) {
-        const int c = max(1, a.count_round[r]);
-        acc += static_cast<double>(a.count_round[r]) * ((ring[r] / s1) / c);
+    for (int r = tid; r <= R; r += nth) {
+        const int c = max(1, count[r]);
+        acc += static_cast<double>(count[r]) * ((ring[r] / s1) / c);
     }
     __shared__ double s2_shared;
     const double t = block_sum(acc);
@@ -237,130 +286,149 @@ __device__ double mean_kernel_sum(const PsfBankArgs& a, int b, double s1) {
     return s2_shared;
 }
 
-struct ShapeCtx {
-    const float* canvas;
-    const double* ring;
-    const int* count;
-    float inv_s1;     // 1 / s1
-    double s1, s2;
-    float gain;
-    int R, K;
-    float kc;
-};
-
-// reshapeAnisotropy value of one canvas pixel (unnormalised shaped kernel),
-// from the resampled value and its ring mean (LensDiffCpuReference.cpp:1088-1135).
-__device__ __forceinline__ float shaped_value(const ShapeCtx& c, int x, int y, float dx, float dy) {
-    const float base = c.canvas[static_cast<size_t>(y) * c.K + x] * c.inv_s1;
-    const int r = min(c.R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy))));
-    const float mean = static_cast<float>(((c.ring[r] / c.s1) / max(1, c.count[r])) / c.s2);
-    return fmaxf(0.0f, mean + (base - mean) * c.gain);
-}
-
-__device__ __forceinline__ ShapeCtx make_shape_ctx(const PsfBankArgs& a, int b, double s2) {
-    ShapeCtx c;
-    c.canvas = a.canvas + static_cast<size_t>(b) * a.K * a.K;
-    c.ring = a.ring_round + static_cast<size_t>(b) * (a.R + 1);
-    c.count = a.count_round;
-    c.s1 = a.scalars[b].s1;
-    c.inv_s1 = static_cast<float>(1.0 / c.s1);
-    c.s2 = s2;
-    c.gain = a.gain;
-    c.R = a.R;
-    c.K = a.K;
-    c.kc = static_cast<float>(a.K - 1) * 0.5f;
-    return c;
-}
-
-// grid (ceil(K/32), ceil(K/32), B): shaped kernel sums, ring energy/peak by
-// ceil(r) (estimateAdaptiveSupportRadius, LensDiffCpuReference.cpp:984-1007).
+// grid (ceil(K/32), ceil(K/32), B): shaped kernel (reshapeAnisotropy of the
+// base kernel against its azimuthal mean, LensDiffCpuReference.cpp:1088-1135)
+// written in place, its sum, and its ring energy / peak by ceil(r)
+// (estimateAdaptiveSupportRadius, :984-1007).
 __global__ void __launch_bounds__(256) shape_stats_kernel(PsfBankArgs a) {
-    __shared__ double ring_e[kRingSpan];
+    __shared__ float ring_e[kRingSpan];
     __shared__ unsigned int ring_p[kRingSpan];
+    __shared__ float mean_r[kRingSpan];
     const int b = blockIdx.z;
     const int tid = threadIdx.x + threadIdx.y * 32;
     const double s1 = a.scalars[b].s1;
-    const double s2 = mean_kernel_sum(a, b, s1);
+    const double s2 = mean_kernel_sum(a.ring_round + static_cast<size_t>(b) * (a.R + 1), a.count_round, a.R, s1);
     if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) a.scalars[b].s2 = s2;
-    const ShapeCtx c = make_shape_ctx(a, b, s2);
+    const int K = a.K, R = a.R;
     const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
-    const int rbase = tile_ring_base(tx0, ty0, a.R, a.R);
+    const int rbase = tile_ring_base(tx0, ty0, R, R);
+    // ring means (round(r) rings) the tile can touch
+    const double* rr = a.ring_round + static_cast<size_t>(b) * (R + 1);
     for (int i = tid; i < kRingSpan; i += 256) {
-        ring_e[i] = 0.0;
+        ring_e[i] = 0.0f;
         ring_p[i] = 0u;
+        const int r = rbase + i;
+        mean_r[i] = r <= R ? static_cast<float>(((rr[r] / s1) / max(1, a.count_round[r])) / s2) : 0.0f;
     }
     __syncthreads();
+    const float inv_s1 = static_cast<float>(1.0 / s1);
+    const float gain = a.gain;
+    const float kc = static_cast<float>(K - 1) * 0.5f;
+    float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
     double lsum = 0.0;
     unsigned int lpeak = 0u;
     const int x = tx0 + threadIdx.x;
 #pragma unroll
     for (int i = 0; i < kTile / 8; ++i) {
         const int y = ty0 + threadIdx.y + 8 * i;
-        if (x < a.K && y < a.K) {
-            const float dx = static_cast<float>(x) - c.kc;
-            const float dy = static_cast<float>(y) - c.kc;
-            const float v = shaped_value(c, x, y, dx, dy);
+        const bool in = x < K && y < K;
+        float v = 0.0f;
+        int slot = -1;
+        if (in) {
+            const float dx = static_cast<float>(x) - kc;
+            const float dy = static_cast<float>(y) - kc;
+            const float rad = sqrtf(dx * dx + dy * dy);
+            const size_t idx = static_cast<size_t>(y) * K + x;
+            const float base = canvas[idx] * inv_s1;
+            const float mean = mean_r[min(R, static_cast<int>(roundf(rad))) - rbase];
+            v = fmaxf(0.0f, mean + (base - mean) * gain);
+            canvas[idx] = v;
             lsum += v;
-            const unsigned int bits = __float_as_uint(v);
-            lpeak = max(lpeak, bits);
-            const int r = min(a.R, static_cast<int>(ceilf(sqrtf(dx * dx + dy * dy))));
-            atomicAdd(&ring_e[r - rbase], static_cast<double>(v));
-            atomicMax(&ring_p[r - rbase], bits);
+            lpeak = max(lpeak, __float_as_uint(v));
+            slot = min(R, static_cast<int>(ceilf(rad))) - rbase;
         }
+        float pk = v;
+        const bool tail_e = warp_run_reduce<false>(slot, v);
+        const bool tail_p = warp_run_reduce<true>(slot, pk);
+        if (tail_e) atomicAdd(&ring_e[slot], v);
+        if (tail_p) atomicMax(&ring_p[slot], __float_as_uint(pk));
     }
     __syncthreads();
-    const size_t ro = static_cast<size_t>(b) * (a.R + 1);
+    const size_t ro = static_cast<size_t>(b) * (R + 1);
     for (int i = tid; i < kRingSpan; i += 256) {
-        if (rbase + i <= a.R) {
-            if (ring_e[i] != 0.0) atomicAdd(&a.ring_ceil[ro + rbase + i], ring_e[i]);
+        if (rbase + i <= R) {
+            if (ring_e[i] != 0.0f) atomicAdd(&a.ring_ceil[ro + rbase + i], static_cast<double>(ring_e[i]));
             if (ring_p[i] != 0u) atomicMax(&a.ring_peak[ro + rbase + i], ring_p[i]);
         }
     }
-    // block max of the peak
     for (int o = 16; o > 0; o >>= 1) lpeak = max(lpeak, __shfl_xor_sync(0xffffffffu, lpeak, o));
     if ((tid & 31) == 0 && lpeak != 0u) atomicMax(&a.scalars[b].peak, lpeak);
     const double tot = block_sum(lsum);
     if (tid == 0) atomicAdd(&a.scalars[b].s3, tot);
 }
 
-// grid (B), block 32: adaptive support radius and taper constants
+// grid (B), block 256: adaptive support radius and taper constants
 // (estimateAdaptiveSupportRadius :1009-1030, paddedAdaptiveSupportRadius
 // :1033-1036, cropKernelToRadius :1039, applySupportBoundaryTaper :962-965).
-__global__ void support_kernel(PsfBankArgs a) {
+// Suffix maxima of the ring peaks and prefix sums of the ring energies are
+// block scans over per-thread chunks of rings.
+__global__ void __launch_bounds__(256) support_kernel(PsfBankArgs a) {
+    __shared__ float chunk_max[256];
+    __shared__ double chunk_sum[256];
+    __shared__ int first_hit;
     const int b = blockIdx.x;
-    if (threadIdx.x != 0) return;
+    const int tid = threadIdx.x;
     PsfScalars& sc = a.scalars[b];
     const int R = a.R;
-    const int radius_max = min(R, a.K / 2);
+    const int rm = min(R, a.K / 2);
+    const int nr = rm + 1;
+    const int per = (nr + 255) / 256;
+    const int r0 = tid * per, r1 = min(nr, r0 + per);
     const double* e = a.ring_ceil + static_cast<size_t>(b) * (R + 1);
     const unsigned int* pk = a.ring_peak + static_cast<size_t>(b) * (R + 1);
     const double total = sc.s3;
     const float peak = __uint_as_float(sc.peak);
-    int est = max(4, radius_max);
-    // thresholds apply to the normalised kernel: total 1, peak = peak / total
-    const bool degenerate = !(total > 0.0) || (static_cast<double>(peak) / total <= 1e-6);
-    if (!degenerate) {
-        // outsidePeak (suffix maxima of the ring peaks) written in place, then
-        // the first ring where captured energy and the remaining peak both pass.
-        double cum = 0.0;
-        float run = 0.0f;
-        unsigned int* pw = a.ring_peak + static_cast<size_t>(b) * (R + 1);
-        for (int r = radius_max; r >= 0; --r) {
-            run = fmaxf(run, __uint_as_float(pk[r]));
-            pw[r] = __float_as_uint(run);
+    float lmax = 0.0f;
+    double lsum = 0.0;
+    for (int r = r0; r < r1; ++r) {
+        lmax = fmaxf(lmax, __uint_as_float(pk[r]));
+        lsum += e[r];
+    }
+    chunk_max[tid] = lmax;
+    chunk_sum[tid] = lsum;
+    if (tid == 0) first_hit = 1 << 30;
+    __syncthreads();
+    if (tid == 0) {  // exclusive prefix sums / suffix maxima over the 256 chunks
+        double run = 0.0;
+        for (int t = 0; t < 256; ++t) {
+            const double s = chunk_sum[t];
+            chunk_sum[t] = run;
+            run += s;
         }
+        float m = 0.0f;
+        for (int t = 255; t >= 0; --t) {
+            const float v = chunk_max[t];
+            chunk_max[t] = m;  // maximum over the chunks after t
+            m = fmaxf(m, v);
+        }
+    }
+    __syncthreads();
+    // the normalised kernel has total 1 and peak = peak / total
+    const bool degenerate = !(total > 0.0) || (static_cast<double>(peak) / total <= 1e-6);
+    if (!degenerate && r0 < r1) {
+        // suffix maxima inside this chunk, then the first ring that passes
+        float suffix[64];
+        const int len = r1 - r0;  // <= 64 for R <= 16383
+        float m = chunk_max[tid];
+        for (int k = len - 1; k >= 0; --k) {
+            suffix[k] = m;  // maximum over rings > r0 + k
+            m = fmaxf(m, __uint_as_float(pk[r0 + k]));
+        }
+        double cum = chunk_sum[tid];
         const double thr_cap = static_cast<double>(0.9999f);
         const float thr_peak = peak * 2e-4f;
-        for (int r = 0; r <= radius_max; ++r) {
-            cum += e[r];
-            const double captured = cum / total;
-            const float remaining = (r + 1 <= radius_max) ? __uint_as_float(pw[r + 1]) : 0.0f;
-            if (captured >= thr_cap && remaining <= thr_peak) {
-                est = max(4, r + 1);
+        for (int k = 0; k < len; ++k) {
+            cum += e[r0 + k];
+            if (cum / total >= thr_cap && suffix[k] <= thr_peak) {
+                atomicMin(&first_hit, r0 + k);
                 break;
             }
         }
     }
+    __syncthreads();
+    if (tid != 0) return;
+    int est = max(4, rm);
+    if (!degenerate && first_hit < (1 << 30)) est = max(4, first_hit + 1);
     const int pad = max(6, min(24, static_cast<int>(ceilf(static_cast<float>(max(1, est)) * 0.05f))));
     int rho = min(max(est + pad, 4), max(4, R));
     rho = min(max(rho, 1), a.K / 2);
@@ -372,79 +440,82 @@ __global__ void support_kernel(PsfBankArgs a) {
     sc.start = fmaxf(0.0f, extent - fade);
 }
 
-// grid (ceil(K/32), ceil(K/32), B): s4 = sum of taper * normalised shaped kernel
-// over the crop box (the normaliser of cropKernelToRadius).
+// grid (ceil(K/32), ceil(K/32), B): crop + taper in place (0 outside the
+// crop box) and s4 = sum of taper * normalised shaped kernel, the normaliser
+// of cropKernelToRadius.
 __global__ void __launch_bounds__(256) crop_sum_kernel(PsfBankArgs a) {
     const int b = blockIdx.z;
     const PsfScalars& sc = a.scalars[b];
-    const ShapeCtx c = make_shape_ctx(a, b, sc.s2);
     const float inv_s3 = static_cast<float>(1.0 / sc.s3);
     const int rho = sc.radius;
+    const int K = a.K, R = a.R;
+    float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
     const int x = blockIdx.x * kTile + threadIdx.x;
     double lsum = 0.0;
 #pragma unroll
     for (int i = 0; i < kTile / 8; ++i) {
         const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
-        if (x < a.K && y < a.K) {
-            const int ix = x - a.R, iy = y - a.R;
+        if (x < K && y < K) {
+            const int ix = x - R, iy = y - R;
+            const size_t idx = static_cast<size_t>(y) * K + x;
+            float t = 0.0f;
             if (abs(ix) <= rho && abs(iy) <= rho) {
                 const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
-                const float v = shaped_value(c, x, y, static_cast<float>(x) - c.kc, static_cast<float>(y) - c.kc) * inv_s3;
                 const float wgt = taper_weight(sqrtf(dx * dx + dy * dy), sc.extent, sc.fade, sc.start);
-                lsum += static_cast<double>(v * wgt);
+                t = canvas[idx] * wgt;
+                lsum += static_cast<double>((canvas[idx] * inv_s3) * wgt);
             }
+            canvas[idx] = t;
         }
     }
     const double tot = block_sum(lsum);
     if (threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(&a.scalars[b].s4, tot);
 }
 
-// Final kernel value of wavelength b at canvas pixel (x, y), 0 outside its crop.
-__device__ __forceinline__ float final_value(const PsfBankArgs& a, int b, int x, int y) {
-    const PsfScalars& sc = a.scalars[b];
-    const int ix = x - a.R, iy = y - a.R;
-    if (abs(ix) > sc.radius || abs(iy) > sc.radius) return 0.0f;
-    const ShapeCtx c = make_shape_ctx(a, b, sc.s2);
-    const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
-    const float v = shaped_value(c, x, y, static_cast<float>(x) - c.kc, static_cast<float>(y) - c.kc) *
-                    static_cast<float>(1.0 / sc.s3);
-    const float wgt = taper_weight(sqrtf(dx * dx + dy * dy), sc.extent, sc.fade, sc.start);
-    return (v * wgt) * static_cast<float>(1.0 / sc.s4);
-}
-
-// grid (ceil(K/32), ceil(K/32)), block (32, 8).
+// grid (ceil(K/32), ceil(K/32)), block (32, 8): out[k] = sum_b coef[k][b] *
+// final_b with final_b = canvas_b / (s3_b * s4_b).
 __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
+    __shared__ float inv[kMaxBins];
+    const int tid = threadIdx.x + threadIdx.y * 32;
+    const int B = a.bank.B;
+    for (int b = tid; b < B; b += 256) {
+        const PsfScalars& sc = a.bank.scalars[b];
+        inv[b] = static_cast<float>(1.0 / (sc.s3 * sc.s4));
+    }
+    __syncthreads();
     const int x = blockIdx.x * kTile + threadIdx.x;
     const int K = a.bank.K;
+    const size_t plane = static_cast<size_t>(K) * K;
 #pragma unroll 1
     for (int i = 0; i < kTile / 8; ++i) {
         const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
         if (x >= K || y >= K) continue;
+        const size_t idx = static_cast<size_t>(y) * K + x;
         float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        for (int b = 0; b < a.bank.B; ++b) {
-            const float v = final_value(a.bank, b, x, y);
-            if (v != 0.0f) {
+        for (int b = 0; b < B; ++b) {
+            const float v = a.bank.canvas[b * plane + idx] * inv[b];
 #pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (k < a.n_ker) acc[k] += a.coef[k][b] * v;
-            }
+            for (int k = 0; k < 4; ++k) acc[k] += a.coef[k][b] * v;
         }
-        for (int k = 0; k < a.n_ker; ++k) a.out[(static_cast<size_t>(k) * K + y) * K + x] = acc[k];
+        for (int k = 0; k < a.n_ker; ++k) a.out[k * plane + idx] = acc[k];
     }
 }
 
 // grid (ceil(K/32), ceil(K/32), B): final kernels packed at offsets[b].
 __global__ void __launch_bounds__(256) export_kernel(PsfBankArgs a, const int64_t* offsets, float* out) {
     const int b = blockIdx.z;
-    const int rho = a.scalars[b].radius;
+    const PsfScalars& sc = a.scalars[b];
+    const int rho = sc.radius;
     const int side = 2 * rho + 1;
+    const float inv = static_cast<float>(1.0 / (sc.s3 * sc.s4));
+    const float* canvas = a.canvas + static_cast<size_t>(b) * a.K * a.K;
     const int x = blockIdx.x * kTile + threadIdx.x;
     for (int i = 0; i < kTile / 8; ++i) {
         const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
         if (x >= a.K || y >= a.K) continue;
         const int ix = x - a.R + rho, iy = y - a.R + rho;
         if (ix < 0 || iy < 0 || ix >= side || iy >= side) continue;
-        out[offsets[b] + static_cast<int64_t>(iy) * side + ix] = final_value(a, b, x, y);
+        out[offsets[b] + static_cast<int64_t>(iy) * side + ix] = canvas[static_cast<size_t>(y) * a.K + x] * inv;
     }
 }
 
@@ -562,7 +633,7 @@ __global__ void normalize_psf_kernel(float* psf, int64_t n, const PsfScalars* sc
 // ---- launch helpers ---------------------------------------------------------------
 template <int T, int NMAX>
 void rows_launch(const PsfBankArgs& a, cudaStream_t s) {
-    dim3 grid(a.pupil.size, a.B);
+    dim3 grid(a.row_n, a.B);
     psf_rows_kernel<T, NMAX><<<grid, T, a.S * sizeof(float2), s>>>(a);
 }
 
@@ -572,26 +643,36 @@ void cols_launch(const PsfBankArgs& a, cudaStream_t s) {
     psf_cols_kernel<T, C, NMAX><<<grid, T, static_cast<size_t>(a.S) * C * sizeof(float2), s>>>(a);
 }
 
+dim3 canvas_grid(const PsfBankArgs& a, int z) {
+    return dim3((a.K + kTile - 1) / kTile, (a.K + kTile - 1) / kTile, z);
+}
+
+template <class Kern>
+void opt_in(Kern k, size_t bytes) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
 }  // namespace
 
+void launch_pupil_pre(const PsfBankArgs& a, cudaStream_t s) {
+    const int n = a.pupil.size * a.pupil.size;
+    pupil_pre_kernel<<<(n + 255) / 256, 256, 0, s>>>(a);
+}
+
 void launch_psf_rows(const PsfBankArgs& a, cudaStream_t s) {
-    if (a.S <= 1024) rows_launch<64, 1024>(a, s);
-    else if (a.S <= 2048) rows_launch<128, 2048>(a, s);
-    else if (a.S <= 4096) rows_launch<256, 4096>(a, s);
-    else if (a.S <= 8192) rows_launch<512, 8192>(a, s);
+    if (a.S <= 1024) rows_launch<128, 1024>(a, s);
+    else if (a.S <= 2048) rows_launch<256, 2048>(a, s);
+    else if (a.S <= 4096) rows_launch<512, 4096>(a, s);
+    else if (a.S <= 8192) rows_launch<1024, 8192>(a, s);
     else rows_launch<1024, 16384>(a, s);
 }
 
 void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s) {
-    if (a.S <= 1024) cols_launch<256, 4, 1024>(a, s);
-    else if (a.S <= 2048) cols_launch<512, 4, 2048>(a, s);
-    else if (a.S <= 4096) cols_launch<1024, 4, 4096>(a, s);
-    else if (a.S <= 8192) cols_launch<1024, 2, 8192>(a, s);
+    if (a.S <= 1024) cols_launch<512, 4, 1024>(a, s);
+    else if (a.S <= 2048) cols_launch<1024, 4, 2048>(a, s);
+    else if (a.S <= 4096) cols_launch<1024, 2, 4096>(a, s);
+    else if (a.S <= 8192) cols_launch<1024, 1, 8192>(a, s);
     else cols_launch<1024, 1, 16384>(a, s);
-}
-
-static dim3 canvas_grid(const PsfBankArgs& a, int z) {
-    return dim3((a.K + kTile - 1) / kTile, (a.K + kTile - 1) / kTile, z);
 }
 
 void launch_resample(const PsfBankArgs& a, cudaStream_t s) {
@@ -602,7 +683,7 @@ void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s) {
     shape_stats_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
 }
 
-void launch_support(const PsfBankArgs& a, cudaStream_t s) { support_kernel<<<a.B, 32, 0, s>>>(a); }
+void launch_support(const PsfBankArgs& a, cudaStream_t s) { support_kernel<<<a.B, 256, 0, s>>>(a); }
 
 void launch_crop_sum(const PsfBankArgs& a, cudaStream_t s) {
     crop_sum_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
@@ -628,23 +709,16 @@ void launch_normalize_psf(float* psf, int n, const PsfScalars* sc, cudaStream_t 
     normalize_psf_kernel<<<592, 256, 0, s>>>(psf, static_cast<int64_t>(n), sc);
 }
 
-namespace {
-template <class Kern>
-void opt_in(Kern k, size_t bytes) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-}
-}  // namespace
-
 void configure_psf_kernels() {
-    opt_in(psf_rows_kernel<64, 1024>, 1024 * 8);
-    opt_in(psf_rows_kernel<128, 2048>, 2048 * 8);
-    opt_in(psf_rows_kernel<256, 4096>, 4096 * 8);
-    opt_in(psf_rows_kernel<512, 8192>, 8192 * 8);
+    opt_in(psf_rows_kernel<128, 1024>, 1024 * 8);
+    opt_in(psf_rows_kernel<256, 2048>, 2048 * 8);
+    opt_in(psf_rows_kernel<512, 4096>, 4096 * 8);
+    opt_in(psf_rows_kernel<1024, 8192>, 8192 * 8);
     opt_in(psf_rows_kernel<1024, 16384>, 16384 * 8);
-    opt_in(psf_cols_kernel<256, 4, 1024>, 1024 * 4 * 8);
-    opt_in(psf_cols_kernel<512, 4, 2048>, 2048 * 4 * 8);
-    opt_in(psf_cols_kernel<1024, 4, 4096>, 4096 * 4 * 8);
-    opt_in(psf_cols_kernel<1024, 2, 8192>, 8192 * 2 * 8);
+    opt_in(psf_cols_kernel<512, 4, 1024>, 1024 * 4 * 8);
+    opt_in(psf_cols_kernel<1024, 4, 2048>, 2048 * 4 * 8);
+    opt_in(psf_cols_kernel<1024, 2, 4096>, 4096 * 2 * 8);
+    opt_in(psf_cols_kernel<1024, 1, 8192>, 8192 * 8);
     opt_in(psf_cols_kernel<1024, 1, 16384>, 16384 * 8);
 }
 
