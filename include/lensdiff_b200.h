@@ -266,6 +266,19 @@ int ld_export_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream,
 int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index,
                float* psf_out_device, void* stream, ld_status* status);
 
+/* Same output as ld_raw_psf, for callers that cannot allocate device memory
+ * (an OpenFX host that owns and budgets all GPU memory, a real-time thread
+ * that must not take cudaMalloc's implicit synchronisation, a fixed memory
+ * reservation).  No context and no allocation: the scratch is a 12 MiB
+ * file-scope device array that every GPU loading the library holds until
+ * exit.  Limit: pupil <= 512 and PSF grid <= 1024 (maximum kernel radius
+ * <= 256 px); larger requests return LD_ERR_ARG.  All calls on a device share
+ * the array, so calls that overlap on the GPU race; the first call on a
+ * device resolves the array's address and should precede any stream capture.
+ * This entry point has no counterpart in the reference. */
+int ld_raw_psf_noalloc(const ld_params* params, int wavelength_index, float* psf_out_device, void* stream,
+                       ld_status* status);
+
 /* Resolved sizes of the path for `params` (N_p, S, R_max, wavelength count). */
 int ld_resolve_sizes(const ld_params* params, int32_t* pupil_size,
                      int32_t* raw_psf_size, int32_t* max_kernel_radius,

@@ -300,6 +300,7 @@ EXPORTED_SYMBOLS = [
     "ld_build_psf_bank",
     "ld_export_psf_bank",
     "ld_raw_psf",
+    "ld_raw_psf_noalloc",
     "ld_resolve_sizes",
     "ld_gaussian_rgb_matrix",
     "ld_set_profiling",
@@ -344,6 +345,8 @@ def lib() -> ctypes.CDLL:
     L.ld_raw_psf.argtypes = [vp, ctypes.POINTER(ld_params), ctypes.c_int, vp, vp,
                              ctypes.POINTER(ld_status)]
     L.ld_raw_psf.restype = ctypes.c_int
+    L.ld_raw_psf_noalloc.argtypes = [ctypes.POINTER(ld_params), ctypes.c_int, vp, vp, ctypes.POINTER(ld_status)]
+    L.ld_raw_psf_noalloc.restype = ctypes.c_int
     L.ld_resolve_sizes.argtypes = [ctypes.POINTER(ld_params), ctypes.POINTER(c_i32),
                                    ctypes.POINTER(c_i32), ctypes.POINTER(c_i32),
                                    ctypes.POINTER(c_i32)]

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "liblensdiff_b200.so")
 ROOT = os.path.dirname(HERE)
-SOURCES = ["ld_host.cu", "ld_psf.cu", "ld_frame.cu"]
+SOURCES = ["ld_host.cu", "ld_psf.cu", "ld_frame.cu", "ld_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{os.path.join(ROOT, 'include')}"]
 

@@ -1145,3 +1145,20 @@ int run_guarded(ld_ctx* ctx, ld_status* st, const std::function<void()>& fn) {
     return LD_OK;
 }
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Parameter resolution shared with ld_noalloc.cu (same expressions as above).
+// ---------------------------------------------------------------------------
+namespace ld {
+bool host_factor_plan(int n, FftPlan* plan) { return factor_plan(n, plan); }
+PupilParams host_pupil_params(const ld_params& p) { return pupil_params(p, false); }
+PhaseCoeffs host_phase_for_wavelength(const ld_params& p, float wavelength) {
+    return phase_for_wavelength(p, wavelength);
+}
+std::vector<float> host_wavelengths(const ld_params& p) { return wavelengths_of(p); }
+void host_sizes(const ld_params& p, int* np, int* S, int* R) {
+    *np = pupil_size(p);
+    *R = max_kernel_radius(p);
+    *S = raw_psf_size(*np, *R);
+}
+}  // namespace ld
