@@ -298,6 +298,9 @@ def main():
         torch.distributed.barrier()
     stage = cache.profile_collect()
     cache.set_profiling(False)
+    dev_err = cache.check_device_errors()
+    if dev_err:
+        raise RuntimeError(f"device error word {dev_err} after the timed frames")
     clk = clocks.stop()
     per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     total_ms = evs[0].elapsed_time(evs[-1])

@@ -141,7 +141,8 @@ class LensDiffPsfBankCache:
         self._lib.ld_clear_caches(self._h)
 
     def check_device_errors(self) -> int:
-        """Reads and clears the device error word (0: no kernel gave up a wait)."""
+        """Reads and clears the device error word: 0 none, 1 a bulk-copy wait ran
+        out of time, 2 a bulk copy failed its alignment / bounds check."""
         w = ctypes.c_int32()
         self._lib.ld_check_device_errors(self._h, ctypes.byref(w))
         return int(w.value)

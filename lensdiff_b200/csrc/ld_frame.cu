@@ -4,18 +4,24 @@
 //   buildSelectionMask / applyMask / applyMaskScalarDriver :1219-1279
 //       -> fused into the fill of frame_rows_kernel
 //   convolveScalar / paddedSpectrumFromKernel / convolveRgba :1153-1217
-//       -> frame_rows_kernel (forward rows, real input, two rows per CTA)
-//          frame_cols_kernel (forward columns, spectral multiply, inverse columns)
+//       -> frame_rows_kernel (forward rows, real input)
+//          frame_cols_kernel (forward column, spectral multiply, inverse columns)
 //          frame_inverse_kernel (inverse rows, real output)
 //   MapLensDiffSpectralBins (LensDiffSpectrum.cpp:462-497), composite
 //   (:2200-2218) -> frame_inverse_kernel epilogue
 //
-// HBM layout (ld_internal.h): every array the column passes touch is stored
-// tile-major, so one column tile is one contiguous block.  The column passes
-// are persistent (one CTA per SM) and double-buffer their inputs: while a tile
-// is transformed, the bulk-copy engine (cp.async.bulk, mbarrier completion)
-// already streams the next tile's row spectra and kernel spectra into shared
-// memory.
+// HBM layout (ld_internal.h): spectrum columns are stored column-major with
+// their channels interleaved, so the column pass moves one column of every
+// channel as one contiguous block with one bulk copy (cp.async.bulk, mbarrier
+// completion) and writes its result back with one bulk store, and the row
+// passes read and write C adjacent values per spectrum bin.
+//
+// The column passes run one column per CTA.  A transform loop inside a
+// persistent column loop makes the compiler keep the register demands of all
+// stage bodies live together (spilling); straight-line, each body needs its
+// own registers only.  To keep HBM busy while an SM transforms, every CTA
+// prefetches into L2 the column the CTA one generation later will load (the
+// grid launches in blockIdx order, `ahead` CTAs resident at a time).
 #include <algorithm>
 
 #include "ld_async.cuh"
@@ -25,6 +31,11 @@ namespace ld {
 namespace {
 
 constexpr int kMaxSmem = 227 * 1024;
+
+template <int E>
+struct Fam {
+    static constexpr int max_threads = E >= kE25 ? kE25MaxThreads : kE16MaxThreads;
+};
 
 __device__ __forceinline__ float saturate(float v) { return fminf(fmaxf(v, 0.0f), 1.0f); }
 
@@ -49,17 +60,6 @@ __device__ __forceinline__ float4 load_px(const unsigned char* row, int x, bool 
     return make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3));
 }
 
-// Driver value of one pixel for plane `ch`: the scalar driver
-// (signal * mask * scale) for spectral modes, the redistributed colour
-// src_c * (mask * scale) for Mono.
-__device__ __forceinline__ float driver_value(const SelectionParams& sel, int n_drv, float4 p, int ch) {
-    float sig;
-    const float m = selection_mask(sel, p.x, p.y, p.z, &sig);
-    if (n_drv == 1) return sig * m * sel.rscale;
-    const float mm = m * sel.rscale;
-    return (ch == 0 ? p.x : (ch == 1 ? p.y : p.z)) * mm;
-}
-
 // X[k] of a real length-2M sequence from Z = FFT_M(even + i*odd):
 // X[k] = E + W^k O, E = (Z[k] + conj Z[M-k]) / 2, O = (Z[k] - conj Z[M-k]) / 2i.
 __device__ __forceinline__ float2 r2c_post(float2 zk, float2 zmk, float2 wk) {
@@ -79,187 +79,200 @@ __device__ __forceinline__ float2 c2r_pre(float2 xk, float2 xmk, float2 wk) {
     return make_float2(e.x - o.y, e.y + o.x);
 }
 
-// Writes the Px/2+1 bins of two transformed rows (interleaved in smem as
-// s[n*2 + r]) to a tile-major array out[t][row0 + r][kk] with k = t*ct + kk;
-// bins past M are zero.  The two rows of one tile are 2*ct adjacent float2.
-__device__ __forceinline__ void store_row_pair(int M, int ct, int Pw, const float2* __restrict__ tw_px,
-                                               const float2* s, float2* out, int rows_total, int row0, int T) {
-    for (int i = threadIdx.x; i < Pw * 2; i += T) {
-        const int t = i / (2 * ct);
-        const int rem = i - t * 2 * ct;
-        const int r = rem / ct;
-        const int kk = rem - r * ct;
-        const int k = t * ct + kk;
-        float2 v = make_float2(0.0f, 0.0f);
-        if (k <= M) v = r2c_post(s[(k == M ? 0 : k) * 2 + r], s[(k == 0 ? 0 : M - k) * 2 + r], __ldg(&tw_px[k]));
-        out[(static_cast<size_t>(t) * rows_total + row0 + r) * ct + kk] = v;
+// Writes the M+1 bins of the C transformed sequences in smem (s[k*C + col])
+// to a column-major array: bin k of sequence col goes to
+// out[k * col_elems + base + col].  Consecutive threads write consecutive
+// columns of one bin, so each bin is one contiguous C * 8-byte run.
+__device__ __forceinline__ void store_bins(int M, int C, int64_t col_elems, int64_t base,
+                                           const float2* __restrict__ tw_px, const float2* s, float2* out) {
+    for (int i = threadIdx.x; i < (M + 1) * C; i += blockDim.x) {
+        const int k = i / C;
+        const int col = i - k * C;
+        const float2 v = r2c_post(s[(k == M ? 0 : k) * C + col], s[(k == 0 ? 0 : M - k) * C + col], __ldg(&tw_px[k]));
+        out[k * col_elems + base + col] = v;
     }
 }
 
-// ---- forward rows: two rows per CTA -------------------------------------------------
-// (The kernels copy what their fill/drain lambdas need into registers and
-// capture by value: a lambda holding a reference to the kernel's parameter
-// block would force a copy of the block into local memory.)
-template <int T, int NMAX>
-__global__ void __launch_bounds__(T, 1) frame_rows_kernel(FrameArgs a) {
+// ---- forward rows --------------------------------------------------------------------
+// Spectral (NDRV = 1): C = 4 frame rows per CTA, the scalar driver of each.
+// Mono (NDRV = 3): C = 3, one frame row per CTA, its three colour drivers.
+// Column col of the transform is row y0 + col / NDRV, driver col % NDRV; its
+// spectrum goes to A[k][y0 + col / NDRV][col % NDRV].
+template <int E, int C, int NDRV>
+__global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_rows_kernel(FrameArgs a) {
     extern __shared__ float2 smem[];
-    const int y0 = blockIdx.x * 2;
+    constexpr int RPC = C / NDRV;  // frame rows per CTA
+    const int y0 = blockIdx.x * RPC;
     const int64_t pitch = a.src_pitch;
     const bool aligned = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(pitch)) & 15) == 0;
-    const unsigned char* row0 = a.src + static_cast<int64_t>(y0) * pitch;
-    const int W = a.W, H = a.H, n_drv = a.n_drv;
+    const int W = a.W, H = a.H, M = a.g.M;
     const SelectionParams sel = a.sel;
-    const FftPlan plan = a.g.plan_m;
-    const int M = a.g.M, ct = a.g.ct, Pw = a.g.Pw, Hp = a.Hp;
-    const float2* tw_px = a.g.tw_px;
-    float2* A = a.A;
-    const size_t plane = static_cast<size_t>(a.g.tiles) * Hp * ct;
-    for (int d = 0; d < n_drv; ++d) {
-        smem_fill<T, 2>(smem, M, [=](int idx, int r) -> float2 {
-            if (y0 + r >= H) return make_float2(0.0f, 0.0f);
-            const unsigned char* row = row0 + r * pitch;
-            const int x0 = 2 * idx;
-            float v0 = 0.0f, v1 = 0.0f;
-            if (x0 < W) v0 = driver_value(sel, n_drv, load_px(row, x0, aligned), d);
-            if (x0 + 1 < W) v1 = driver_value(sel, n_drv, load_px(row, x0 + 1, aligned), d);
-            return make_float2(v0, v1);
-        });
-        fft_run<T, 2, NMAX, false>(plan, smem);
-        store_row_pair(M, ct, Pw, tw_px, smem, A + d * plane, Hp, y0, T);
-        __syncthreads();
+    // one thread per (row, pixel pair): the selection mask is evaluated once
+    // per pixel and feeds every driver plane
+    for (int i = threadIdx.x; i < RPC * M; i += blockDim.x) {
+        const int r = i / M;
+        const int idx = i - r * M;
+        const int y = y0 + r;
+        const int x0 = 2 * idx;
+        float2 v[NDRV];
+#pragma unroll
+        for (int d = 0; d < NDRV; ++d) v[d] = make_float2(0.0f, 0.0f);
+        if (y < H) {
+            const unsigned char* row = a.src + static_cast<int64_t>(y) * pitch;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (x0 + h < W) {
+                    const float4 p = load_px(row, x0 + h, aligned);
+                    float sig;
+                    const float m = selection_mask(sel, p.x, p.y, p.z, &sig) * sel.rscale;
+                    if (NDRV == 1) {
+                        const float dv = sig * m;
+                        if (h == 0) v[0].x = dv;
+                        else v[0].y = dv;
+                    } else {
+                        const float c3[3] = {p.x * m, p.y * m, p.z * m};
+#pragma unroll
+                        for (int d = 0; d < NDRV; ++d) {
+                            if (h == 0) v[d].x = c3[d];
+                            else v[d].y = c3[d];
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < NDRV; ++d) smem[idx * C + r * NDRV + d] = v[d];
     }
+    __syncthreads();
+    fft_run<E, C, false>(a.g.plan_m, smem);
+    store_bins(M, C, static_cast<int64_t>(a.Hp) * NDRV, static_cast<int64_t>(y0) * NDRV, a.g.tw_px, smem, a.A);
 }
 
-// ---- column pass: forward, multiply by kernel spectra, inverse -----------------------
-// One CTA per SM walks column tiles.  Shared memory: W (work, Py x CT),
-// D (forward spectrum kept for every output, spectral only), Abuf (next row-
-// spectrum tile, Hp x CT), Kbuf (next kernel-spectrum tile, Py x CT), two
-// mbarriers.  Thread 0 issues the bulk copies; everyone waits on the barriers.
-template <int T, int CT, int NMAX>
-__global__ void __launch_bounds__(T, 1) frame_cols_kernel(FrameArgs a) {
+// ---- column pass, spectral: forward, multiply by NOUT kernel spectra, inverse ----------
+// Column k = blockIdx.x.  Shared memory: F [Py] (the column's row spectra land
+// in F[0, Hp), rows past Hp are the zero padding; transformed in place),
+// Wk [Py][NOUT] (the column's NOUT kernel spectra land here, are multiplied by
+// F in place and inverse-transformed together as NOUT interleaved sequences),
+// two mbarriers.  The first Hp rows of Wk go to B with one bulk store.
+template <int E, int NOUT>
+__global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_cols_kernel(FrameArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
-    const int Py = a.g.Py, H = a.H, Hp = a.Hp, tiles = a.g.tiles;
-    const int n = Py * CT;
-    const int n_drv = a.n_drv, n_out = a.n_out;
-    const bool spectral = n_drv == 1;
-    const FftPlan plan = a.g.plan_py;
-    const float2* Asrc = a.A;
-    const float2* Ksrc = a.spectra;
-    float2* Bdst = a.Bout;
-    int* err = a.err;
-    float2* W = reinterpret_cast<float2*>(smraw);
-    float2* D = W + n;
-    float2* Abuf = spectral ? D + n : W + n;
-    float2* Kbuf = Abuf + Hp * CT;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(Kbuf + n);
-    const uint32_t a_bytes = static_cast<uint32_t>(Hp * CT * sizeof(float2));
-    const uint32_t k_bytes = static_cast<uint32_t>(n * sizeof(float2));
-    int tile = blockIdx.x;
-    if (tile >= tiles) return;
-    if (threadIdx.x == 0) {
+    const int Py = a.g.Py, Hp = a.Hp, cols = a.g.cols;
+    const int k = blockIdx.x;
+    float2* F = reinterpret_cast<float2*>(smraw);
+    float2* Wk = F + Py;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Wk + static_cast<size_t>(Py) * NOUT);
+    const uint32_t a_bytes = static_cast<uint32_t>(Hp * sizeof(float2));
+    const uint32_t k_bytes = static_cast<uint32_t>(static_cast<size_t>(Py) * NOUT * sizeof(float2));
+    const bool lead = threadIdx.x == 0;
+    if (lead) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         mbar_init_fence();
     }
-    __syncthreads();
-    auto a_src = [=](int t, int d) { return Asrc + (static_cast<size_t>(d) * tiles + t) * Hp * CT; };
-    auto k_src = [=](int t, int k) { return Ksrc + (static_cast<size_t>(k) * tiles + t) * Py * CT; };
-    if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(&bars[0], a_bytes);
-        bulk_copy_g2s(Abuf, a_src(tile, 0), a_bytes, &bars[0]);
-        mbar_arrive_expect_tx(&bars[1], k_bytes);
-        bulk_copy_g2s(Kbuf, k_src(tile, 0), k_bytes, &bars[1]);
-    }
-    uint32_t pa = 0, pk = 0;
-    for (; tile < tiles; tile += gridDim.x) {
-        const int next = tile + gridDim.x;
-        for (int o = 0; o < a.n_out; ++o) {
-            if (o == 0 || !spectral) {
-                const int d = spectral ? 0 : o;
-                const bool ok = mbar_wait(&bars[0], pa, a.err);
-                pa ^= 1u;
-                if (__syncthreads_or(!ok)) return;
-                float2* F = spectral ? D : W;
-                const int filled = Hp * CT;
-                for (int i = threadIdx.x; i < n; i += T) F[i] = i < filled ? Abuf[i] : make_float2(0.0f, 0.0f);
-                __syncthreads();
-                if (threadIdx.x == 0) {  // Abuf is free: stream the next plane / tile
-                    int nt = tile, nd = d + 1;
-                    if (nd >= a.n_drv) {
-                        nt = next;
-                        nd = 0;
-                    }
-                    if (nt < tiles) {
-                        fence_proxy_async_smem();
-                        mbar_arrive_expect_tx(&bars[0], a_bytes);
-                        bulk_copy_g2s(Abuf, a_src(nt, nd), a_bytes, &bars[0]);
-                    }
-                }
-                fft_run<T, CT, NMAX, false>(a.g.plan_py, F);
-            }
-            if (o == 0 || spectral) {
-                const bool ok = mbar_wait(&bars[1], pk, a.err);
-                pk ^= 1u;
-                if (__syncthreads_or(!ok)) return;
-            }
-            if (spectral) {
-                for (int i = threadIdx.x; i < n; i += T) W[i] = cmul(D[i], Kbuf[i]);
-            } else {
-                for (int i = threadIdx.x; i < n; i += T) W[i] = cmul(W[i], Kbuf[i]);
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {  // Kbuf is free: stream the next kernel spectrum
-                int nt = -1, nk = 0;
-                if (spectral) {
-                    if (o + 1 < a.n_out) {
-                        nt = tile;
-                        nk = o + 1;
-                    } else {
-                        nt = next;
-                    }
-                } else if (o + 1 == a.n_out) {
-                    nt = next;
-                }
-                if (nt >= 0 && nt < tiles) {
-                    fence_proxy_async_smem();
-                    mbar_arrive_expect_tx(&bars[1], k_bytes);
-                    bulk_copy_g2s(Kbuf, k_src(nt, nk), k_bytes, &bars[1]);
-                }
-            }
-            fft_run<T, CT, NMAX, true>(a.g.plan_py, W);
-            float2* Bo = a.Bout + (static_cast<size_t>(o) * tiles + tile) * H * CT;
-            for (int i = threadIdx.x; i < H * CT; i += T) __stcs(&Bo[i], W[i]);
-            __syncthreads();
+    __syncthreads();  // barriers initialised before anyone waits on them
+    if (lead) {
+        bulk_load_checked(F, a.A + static_cast<size_t>(k) * Hp, a_bytes, &bars[0], smraw, a.err);
+        bulk_load_checked(Wk, a.spectra + static_cast<size_t>(k) * Py * NOUT, k_bytes, &bars[1], smraw, a.err);
+        const int later = k + a.ahead;
+        if (later < cols) {
+            bulk_prefetch_l2(a.A + static_cast<size_t>(later) * Hp, a_bytes);
+            bulk_prefetch_l2(a.spectra + static_cast<size_t>(later) * Py * NOUT, k_bytes);
         }
+    }
+    for (int i = Hp + threadIdx.x; i < Py; i += blockDim.x) F[i] = make_float2(0.0f, 0.0f);
+    if (__syncthreads_or(!mbar_wait(&bars[0], 0, a.err))) return;
+    fft_run<E, 1, false>(a.g.plan_py, F);
+    if (__syncthreads_or(!mbar_wait(&bars[1], 0, a.err))) return;
+    for (int i = threadIdx.x; i < Py * NOUT; i += blockDim.x) Wk[i] = cmul(Wk[i], F[i / NOUT]);
+    __syncthreads();
+    fft_run<E, NOUT, true>(a.g.plan_py, Wk);
+    fence_proxy_async_smem();
+    __syncthreads();
+    const uint32_t b_bytes = static_cast<uint32_t>(static_cast<size_t>(Hp) * NOUT * sizeof(float2));
+    float2* bdst = a.Bout + static_cast<size_t>(k) * Hp * NOUT;
+    if (lead && bulk_args_ok(bdst, Wk, b_bytes, smraw, a.err)) {
+        bulk_copy_s2g(bdst, Wk, b_bytes);
+        bulk_commit();
+        bulk_wait_read();
+    }
+}
+
+// ---- column pass, Mono: three colour drivers, one kernel spectrum -------------------
+// Shared memory: X [Py][3] (the column's three row spectra land in X[0, Hp)),
+// Kc [Py] (the kernel spectrum), two mbarriers.  Forward (3 sequences),
+// multiply by Kc, inverse, bulk store of the first Hp rows.
+template <int E>
+__global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_cols_mono_kernel(FrameArgs a) {
+    extern __shared__ __align__(128) unsigned char smraw[];
+    const int Py = a.g.Py, Hp = a.Hp, cols = a.g.cols;
+    const int k = blockIdx.x;
+    float2* X = reinterpret_cast<float2*>(smraw);
+    float2* Kc = X + static_cast<size_t>(Py) * 3;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Kc + Py);
+    const uint32_t a_bytes = static_cast<uint32_t>(static_cast<size_t>(Hp) * 3 * sizeof(float2));
+    const uint32_t k_bytes = static_cast<uint32_t>(Py * sizeof(float2));
+    const bool lead = threadIdx.x == 0;
+    if (lead) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();  // barriers initialised before anyone waits on them
+    if (lead) {
+        bulk_load_checked(X, a.A + static_cast<size_t>(k) * Hp * 3, a_bytes, &bars[0], smraw, a.err);
+        bulk_load_checked(Kc, a.spectra + static_cast<size_t>(k) * Py, k_bytes, &bars[1], smraw, a.err);
+        const int later = k + a.ahead;
+        if (later < cols) {
+            bulk_prefetch_l2(a.A + static_cast<size_t>(later) * Hp * 3, a_bytes);
+            bulk_prefetch_l2(a.spectra + static_cast<size_t>(later) * Py, k_bytes);
+        }
+    }
+    for (int i = Hp * 3 + threadIdx.x; i < Py * 3; i += blockDim.x) X[i] = make_float2(0.0f, 0.0f);
+    if (__syncthreads_or(!mbar_wait(&bars[0], 0, a.err))) return;
+    fft_run<E, 3, false>(a.g.plan_py, X);
+    if (__syncthreads_or(!mbar_wait(&bars[1], 0, a.err))) return;
+    for (int i = threadIdx.x; i < Py * 3; i += blockDim.x) X[i] = cmul(X[i], Kc[i / 3]);
+    __syncthreads();
+    fft_run<E, 3, true>(a.g.plan_py, X);
+    fence_proxy_async_smem();
+    __syncthreads();
+    float2* bdst = a.Bout + static_cast<size_t>(k) * Hp * 3;
+    if (lead && bulk_args_ok(bdst, X, a_bytes, smraw, a.err)) {
+        bulk_copy_s2g(bdst, X, a_bytes);
+        bulk_commit();
+        bulk_wait_read();
     }
 }
 
 // ---- inverse rows + spectral map + composite ----------------------------------------
-// grid = output rows, smem M * C float2 (C = n_out interleaved channels).
-template <int T, int NMAX, int C>
-__global__ void __launch_bounds__(T, 1) frame_inverse_kernel(FrameArgs a) {
+// One output row per CTA; smem M * C float2 (C = n_out interleaved channels).
+template <int E, int C>
+__global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_inverse_kernel(FrameArgs a) {
     extern __shared__ float2 smem[];
     const int yo = a.out_y1 + blockIdx.x;
     const int sy = yo - a.src_y1;
     const bool have = sy >= 0 && sy < a.H;
-    const int M = a.g.M, ct = a.g.ct, tiles = a.g.tiles, H = a.H;
+    const int M = a.g.M;
     if (have) {
-        const float2* Bsrc = a.Bout;
         const float2* tw_px = a.g.tw_px;
-        smem_fill<T, C>(smem, M, [=](int k, int col) -> float2 {
-            const float2* p = Bsrc + (static_cast<size_t>(col) * tiles) * H * ct;
-            const int km = M - k;
-            const float2 xk = __ldcs(&p[(static_cast<size_t>(k / ct) * H + sy) * ct + k % ct]);
-            const float2 xm = __ldcs(&p[(static_cast<size_t>(km / ct) * H + sy) * ct + km % ct]);
-            return c2r_pre(xk, xm, __ldg(&tw_px[k]));
-        });
-        fft_run<T, C, NMAX, true>(a.g.plan_m, smem);
+        const int64_t col_elems = static_cast<int64_t>(a.Hp) * C;
+        const float2* rowp = a.Bout + static_cast<int64_t>(sy) * C;
+        for (int i = threadIdx.x; i < M * C; i += blockDim.x) {
+            const int k = i / C;
+            const int col = i - k * C;
+            const float2 xk = __ldcs(&rowp[k * col_elems + col]);
+            const float2 xm = __ldcs(&rowp[(M - k) * col_elems + col]);
+            smem[i] = c2r_pre(xk, xm, __ldg(&tw_px[k]));
+        }
+        __syncthreads();
+        fft_run<E, C, true>(a.g.plan_m, smem);
     }
     const bool aligned_s = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(a.src_pitch)) & 15) == 0;
     const bool aligned_d = ((reinterpret_cast<uintptr_t>(a.dst) | static_cast<uintptr_t>(a.dst_pitch)) & 15) == 0;
     const unsigned char* srow = a.src + static_cast<int64_t>(sy) * a.src_pitch;
     unsigned char* drow = a.dst + static_cast<int64_t>(yo - a.dst_y1) * a.dst_pitch;
-    for (int x = a.out_x1 + threadIdx.x; x < a.out_x2; x += T) {
+    for (int x = a.out_x1 + threadIdx.x; x < a.out_x2; x += blockDim.x) {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         const int sx = x - a.src_x1;
         if (have && sx >= 0 && sx < a.W) {
@@ -323,74 +336,68 @@ __device__ __forceinline__ int canvas_index(int g, int P, int R) {
     return -1;
 }
 
-// grid (Kp/2, n_ker): two canvas rows per CTA -> KR tile-major.
-template <int T, int NMAX>
-__global__ void __launch_bounds__(T, 1) kspec_rows_kernel(KernelSpectraArgs a) {
+// One canvas row i = blockIdx.x of all C kernels per CTA (rows >= K are zero):
+// KR[k][i][c], k < M + 1.
+template <int E, int C>
+__global__ void __launch_bounds__(Fam<E>::max_threads, 1) kspec_rows_kernel(KernelSpectraArgs a) {
     extern __shared__ float2 smem[];
-    const int i0 = blockIdx.x * 2;
-    const int k = blockIdx.y;
+    const int i = blockIdx.x;
     const int Px = a.g.Px, R = a.R, K = a.K;
-    const float* canvas = a.canvas + static_cast<size_t>(k) * K * K;
-    smem_fill<T, 2>(smem, a.g.M, [=](int idx, int r) -> float2 {
-        const int i = i0 + r;
+    const size_t kk = static_cast<size_t>(K) * K;
+    const float* crow = a.canvas + static_cast<size_t>(i < K ? i : 0) * K;
+    smem_fill<C>(smem, a.g.M, [=](int idx, int c) -> float2 {
         if (i >= K) return make_float2(0.0f, 0.0f);
-        const float* crow = canvas + static_cast<size_t>(i) * K;
+        const float* p = crow + c * kk;
         const int j0 = canvas_index(2 * idx, Px, R);
         const int j1 = canvas_index(2 * idx + 1, Px, R);
-        return make_float2(j0 >= 0 ? crow[j0] : 0.0f, j1 >= 0 ? crow[j1] : 0.0f);
+        return make_float2(j0 >= 0 ? p[j0] : 0.0f, j1 >= 0 ? p[j1] : 0.0f);
     });
-    fft_run<T, 2, NMAX, false>(a.g.plan_m, smem);
-    store_row_pair(a.g.M, a.g.ct, a.g.Pw, a.g.tw_px, smem,
-                   a.rows + static_cast<size_t>(k) * a.g.tiles * a.Kp * a.g.ct, a.Kp, i0, T);
+    fft_run<E, C, false>(a.g.plan_m, smem);
+    store_bins(a.g.M, C, static_cast<int64_t>(a.Kp) * C, static_cast<int64_t>(i) * C, a.g.tw_px, smem, a.rows);
 }
 
-// Persistent: CTA walks (kernel, tile) items; the next item's KR tile streams
-// into shared memory while the current one is transformed.
-template <int T, int CT, int NMAX>
-__global__ void __launch_bounds__(T, 1) kspec_cols_kernel(KernelSpectraArgs a) {
+// Column k = blockIdx.x: the KR column (Kp x C, contiguous) arrives by bulk
+// copy; the wrap map places canvas row ci at grid row v and folds in the
+// inverse scale; the transformed column KS[k] (Py x C, contiguous) leaves by
+// one bulk store.
+template <int E, int C>
+__global__ void __launch_bounds__(Fam<E>::max_threads, 1) kspec_cols_kernel(KernelSpectraArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
-    const int Py = a.g.Py, tiles = a.g.tiles, Kp = a.Kp, R = a.R;
-    const int n = Py * CT;
+    const int Py = a.g.Py, cols = a.g.cols, Kp = a.Kp, R = a.R;
+    const int k = blockIdx.x;
     float2* W = reinterpret_cast<float2*>(smraw);
-    float2* Rbuf = W + n;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Rbuf + Kp * CT);
-    const uint32_t r_bytes = static_cast<uint32_t>(Kp * CT * sizeof(float2));
-    const int items = a.n_ker * tiles;
-    int item = blockIdx.x;
-    if (item >= items) return;
-    if (threadIdx.x == 0) {
+    float2* Rb = W + static_cast<size_t>(Py) * C;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Rb + static_cast<size_t>(Kp) * C);
+    const uint32_t r_bytes = static_cast<uint32_t>(static_cast<size_t>(Kp) * C * sizeof(float2));
+    const bool lead = threadIdx.x == 0;
+    if (lead) {
         mbar_init(bar, 1);
         mbar_init_fence();
     }
-    __syncthreads();
-    const float2* rows = a.rows;
-    auto r_src = [=](int it) { return rows + static_cast<size_t>(it) * Kp * CT; };  // [k][t] == item order
-    if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(bar, r_bytes);
-        bulk_copy_g2s(Rbuf, r_src(item), r_bytes, bar);
+    __syncthreads();  // barrier initialised before anyone waits on it
+    if (lead) {
+        bulk_load_checked(Rb, a.rows + static_cast<size_t>(k) * Kp * C, r_bytes, bar, smraw, a.err);
+        const int later = k + a.ahead;
+        if (later < cols) bulk_prefetch_l2(a.rows + static_cast<size_t>(later) * Kp * C, r_bytes);
     }
-    uint32_t ph = 0;
-    for (; item < items; item += gridDim.x) {
-        const bool ok = mbar_wait(bar, ph, a.err);
-        ph ^= 1u;
-        if (__syncthreads_or(!ok)) return;
-        for (int i = threadIdx.x; i < n; i += T) {
-            const int v = i / CT, col = i - (i / CT) * CT;
-            const int ci = canvas_index(v, Py, R);
-            W[i] = ci >= 0 ? Rbuf[ci * CT + col] : make_float2(0.0f, 0.0f);
-        }
-        __syncthreads();
-        const int nxt = item + gridDim.x;
-        if (threadIdx.x == 0 && nxt < items) {
-            fence_proxy_async_smem();
-            mbar_arrive_expect_tx(bar, r_bytes);
-            bulk_copy_g2s(Rbuf, r_src(nxt), r_bytes, bar);
-        }
-        fft_run<T, CT, NMAX, false>(a.g.plan_py, W);
-        float2* out = a.spectra + static_cast<size_t>(item) * Py * CT;  // [k][t][v][CT]
-        const float sc = a.scale;
-        for (int i = threadIdx.x; i < n; i += T) out[i] = cscale(W[i], sc);
-        __syncthreads();
+    if (__syncthreads_or(!mbar_wait(bar, 0, a.err))) return;
+    const float sc = a.scale;
+    for (int i = threadIdx.x; i < Py * C; i += blockDim.x) {
+        const int v = i / C;
+        const int c = i - v * C;
+        const int ci = canvas_index(v, Py, R);
+        W[i] = ci >= 0 ? cscale(Rb[ci * C + c], sc) : make_float2(0.0f, 0.0f);
+    }
+    __syncthreads();
+    fft_run<E, C, false>(a.g.plan_py, W);
+    fence_proxy_async_smem();
+    __syncthreads();
+    const uint32_t s_bytes = static_cast<uint32_t>(static_cast<size_t>(Py) * C * sizeof(float2));
+    float2* sdst = a.spectra + static_cast<size_t>(k) * Py * C;
+    if (lead && bulk_args_ok(sdst, W, s_bytes, smraw, a.err)) {
+        bulk_copy_s2g(sdst, W, s_bytes);
+        bulk_commit();
+        bulk_wait_read();
     }
 }
 
@@ -399,127 +406,147 @@ void set_smem(F f) {
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
 }
 
-}  // namespace
-
-size_t frame_cols_smem(const FrameArgs& a) {
-    const size_t n = static_cast<size_t>(a.g.Py) * a.g.ct;
-    const size_t bufs = (a.n_drv == 1 ? 3 : 2) * n + static_cast<size_t>(a.Hp) * a.g.ct;
-    return bufs * sizeof(float2) + 2 * sizeof(uint64_t);
+// CTAs of `f` resident at once on the current device (the L2 prefetch distance).
+template <class F>
+int resident_ctas(F f, int threads, size_t smem) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, threads, smem) != cudaSuccess || per < 1) per = 1;
+    return sms * per;
 }
 
-size_t kspec_cols_smem(const GridGeom& g, int Kp) {
-    return (static_cast<size_t>(g.Py) + Kp) * g.ct * sizeof(float2) + sizeof(uint64_t);
-}
-
-int frame_cols_threads(int Py) { return Py <= 1024 ? 256 : (Py <= 2048 ? 512 : 1024); }
-
-// Row transforms: two rows per CTA, length M = Px/2 <= 6912.
-void launch_frame_rows(const FrameArgs& a, cudaStream_t s) {
+// ---- launch helpers -------------------------------------------------------------------
+template <int E>
+void rows_e(const FrameArgs& a, cudaStream_t s) {
     const int M = a.g.M;
-    const dim3 grid(a.Hp / 2);
-    const size_t sm = static_cast<size_t>(M) * 2 * sizeof(float2);
-    if (M <= 1024) frame_rows_kernel<256, 1024><<<grid, 256, sm, s>>>(a);
-    else if (M <= 2048) frame_rows_kernel<512, 2048><<<grid, 512, sm, s>>>(a);
-    else if (M <= 4096) frame_rows_kernel<1024, 4096><<<grid, 1024, sm, s>>>(a);
-    else frame_rows_kernel<1024, 6912><<<grid, 1024, sm, s>>>(a);
-}
-
-template <int CT>
-static void cols_launch_ct(const FrameArgs& a, cudaStream_t s) {
-    const int Py = a.g.Py;
-    const size_t sm = frame_cols_smem(a);
-    const dim3 grid(a.col_grid);
-    if (Py <= 1024) frame_cols_kernel<256, CT, 1024><<<grid, 256, sm, s>>>(a);
-    else if (Py <= 2048) frame_cols_kernel<512, CT, 2048><<<grid, 512, sm, s>>>(a);
-    else if (Py <= 4096) frame_cols_kernel<1024, CT, 4096><<<grid, 1024, sm, s>>>(a);
-    else frame_cols_kernel<1024, CT, 6912><<<grid, 1024, sm, s>>>(a);
-}
-
-void launch_frame_cols(const FrameArgs& a, cudaStream_t s) {
-    if (a.g.ct == 2) cols_launch_ct<2>(a, s);
-    else cols_launch_ct<1>(a, s);
-}
-
-void launch_frame_inverse(const FrameArgs& a, cudaStream_t s) {
-    const int M = a.g.M;
-    const int rows = a.out_y2 - a.out_y1;
-    if (rows <= 0) return;
-    const dim3 grid(rows);
-    if (a.n_out == 4) {
+    if (a.n_drv == 1) {
         const size_t sm = static_cast<size_t>(M) * 4 * sizeof(float2);
-        if (M <= 1024) frame_inverse_kernel<512, 1024, 4><<<grid, 512, sm, s>>>(a);
-        else if (M <= 2048) frame_inverse_kernel<1024, 2048, 4><<<grid, 1024, sm, s>>>(a);
-        else if (M <= 4096) frame_inverse_kernel<1024, 4096, 4><<<grid, 1024, sm, s>>>(a);
-        else frame_inverse_kernel<1024, 6912, 4><<<grid, 1024, sm, s>>>(a);
+        frame_rows_kernel<E, 4, 1><<<a.Hp / 4, fft_threads(M, 4, E), sm, s>>>(a);
     } else {
         const size_t sm = static_cast<size_t>(M) * 3 * sizeof(float2);
-        if (M <= 1024) frame_inverse_kernel<384, 1024, 3><<<grid, 384, sm, s>>>(a);
-        else if (M <= 2048) frame_inverse_kernel<768, 2048, 3><<<grid, 768, sm, s>>>(a);
-        else if (M <= 4096) frame_inverse_kernel<1024, 4096, 3><<<grid, 1024, sm, s>>>(a);
-        else frame_inverse_kernel<1024, 6912, 3><<<grid, 1024, sm, s>>>(a);
+        frame_rows_kernel<E, 3, 3><<<a.Hp, fft_threads(M, 3, E), sm, s>>>(a);
     }
 }
 
-void launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s) {
-    const int M = a.g.M;
-    const dim3 grid(a.Kp / 2, a.n_ker);
-    const size_t sm = static_cast<size_t>(M) * 2 * sizeof(float2);
-    if (M <= 1024) kspec_rows_kernel<256, 1024><<<grid, 256, sm, s>>>(a);
-    else if (M <= 2048) kspec_rows_kernel<512, 2048><<<grid, 512, sm, s>>>(a);
-    else if (M <= 4096) kspec_rows_kernel<1024, 4096><<<grid, 1024, sm, s>>>(a);
-    else kspec_rows_kernel<1024, 6912><<<grid, 1024, sm, s>>>(a);
+template <int E, class Kern>
+void cols_launch(Kern f, FrameArgs a, int C, size_t sm, cudaStream_t s) {
+    const int T = fft_threads(a.g.Py, C, E);
+    a.ahead = resident_ctas(f, T, sm);
+    f<<<a.g.cols, T, sm, s>>>(a);
 }
 
-template <int CT>
-static void kcols_launch_ct(const KernelSpectraArgs& a, cudaStream_t s) {
-    const int Py = a.g.Py;
-    const size_t sm = kspec_cols_smem(a.g, a.Kp);
-    const dim3 grid(a.grid);
-    if (Py <= 1024) kspec_cols_kernel<256, CT, 1024><<<grid, 256, sm, s>>>(a);
-    else if (Py <= 2048) kspec_cols_kernel<512, CT, 2048><<<grid, 512, sm, s>>>(a);
-    else if (Py <= 4096) kspec_cols_kernel<1024, CT, 4096><<<grid, 1024, sm, s>>>(a);
-    else kspec_cols_kernel<1024, CT, 6912><<<grid, 1024, sm, s>>>(a);
+template <int E>
+void cols_e(const FrameArgs& a, cudaStream_t s) {
+    if (a.n_drv == 3) {
+        cols_launch<E>(frame_cols_mono_kernel<E>, a, 3, frame_cols_smem(a.g.Py, 0), s);
+    } else if (a.n_out == 4) {
+        cols_launch<E>(frame_cols_kernel<E, 4>, a, 4, frame_cols_smem(a.g.Py, 4), s);
+    } else {
+        cols_launch<E>(frame_cols_kernel<E, 3>, a, 3, frame_cols_smem(a.g.Py, 3), s);
+    }
+}
+
+template <int E>
+void inverse_e(const FrameArgs& a, int rows, cudaStream_t s) {
+    const int M = a.g.M;
+    if (a.n_out == 4) {
+        frame_inverse_kernel<E, 4><<<rows, fft_threads(M, 4, E), static_cast<size_t>(M) * 4 * sizeof(float2), s>>>(a);
+    } else {
+        frame_inverse_kernel<E, 3><<<rows, fft_threads(M, 3, E), static_cast<size_t>(M) * 3 * sizeof(float2), s>>>(a);
+    }
+}
+
+template <int E, int C>
+void kspec_rows_c(const KernelSpectraArgs& a, cudaStream_t s) {
+    kspec_rows_kernel<E, C><<<a.Kp, fft_threads(a.g.M, C, E), static_cast<size_t>(a.g.M) * C * sizeof(float2), s>>>(
+        a);
+}
+
+template <int E, int C>
+void kspec_cols_c(KernelSpectraArgs a, cudaStream_t s) {
+    const int T = fft_threads(a.g.Py, C, E);
+    const size_t sm = kspec_cols_smem(a.g.Py, a.Kp, C);
+    a.ahead = resident_ctas(kspec_cols_kernel<E, C>, T, sm);
+    kspec_cols_kernel<E, C><<<a.g.cols, T, sm, s>>>(a);
+}
+
+template <int E>
+void kspec_rows_e(const KernelSpectraArgs& a, cudaStream_t s) {
+    if (a.n_ker == 4) kspec_rows_c<E, 4>(a, s);
+    else if (a.n_ker == 3) kspec_rows_c<E, 3>(a, s);
+    else kspec_rows_c<E, 1>(a, s);
+}
+
+template <int E>
+void kspec_cols_e(const KernelSpectraArgs& a, cudaStream_t s) {
+    if (a.n_ker == 4) kspec_cols_c<E, 4>(a, s);
+    else if (a.n_ker == 3) kspec_cols_c<E, 3>(a, s);
+    else kspec_cols_c<E, 1>(a, s);
+}
+
+template <int E>
+void configure_e() {
+    set_smem(frame_rows_kernel<E, 4, 1>);
+    set_smem(frame_rows_kernel<E, 3, 3>);
+    set_smem(frame_cols_kernel<E, 3>);
+    set_smem(frame_cols_kernel<E, 4>);
+    set_smem(frame_cols_mono_kernel<E>);
+    set_smem(frame_inverse_kernel<E, 3>);
+    set_smem(frame_inverse_kernel<E, 4>);
+    set_smem(kspec_rows_kernel<E, 1>);
+    set_smem(kspec_rows_kernel<E, 3>);
+    set_smem(kspec_rows_kernel<E, 4>);
+    set_smem(kspec_cols_kernel<E, 1>);
+    set_smem(kspec_cols_kernel<E, 3>);
+    set_smem(kspec_cols_kernel<E, 4>);
+}
+
+}  // namespace
+
+size_t frame_cols_smem(int Py, int n_out) {
+    const size_t n = static_cast<size_t>(Py);
+    const size_t bufs = n_out == 0 ? 4 * n : (1 + static_cast<size_t>(n_out)) * n;
+    return bufs * sizeof(float2) + 2 * sizeof(uint64_t);
+}
+
+size_t kspec_cols_smem(int Py, int Kp, int n_ker) {
+    return (static_cast<size_t>(Py) + Kp) * n_ker * sizeof(float2) + sizeof(uint64_t);
+}
+
+void launch_frame_rows(const FrameArgs& a, cudaStream_t s) {
+    if (a.g.fam_m == kE25) rows_e<kE25>(a, s);
+    else rows_e<kE16>(a, s);
+}
+
+void launch_frame_cols(const FrameArgs& a, cudaStream_t s) {
+    if (a.g.fam_py == kE25) cols_e<kE25>(a, s);
+    else cols_e<kE16>(a, s);
+}
+
+void launch_frame_inverse(const FrameArgs& a, cudaStream_t s) {
+    const int rows = a.out_y2 - a.out_y1;
+    if (rows <= 0) return;
+    if (a.g.fam_m == kE25) inverse_e<kE25>(a, rows, s);
+    else inverse_e<kE16>(a, rows, s);
+}
+
+void launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s) {
+    if (a.g.fam_m == kE25) kspec_rows_e<kE25>(a, s);
+    else kspec_rows_e<kE16>(a, s);
 }
 
 void launch_kspec_cols(const KernelSpectraArgs& a, cudaStream_t s) {
-    if (a.g.ct == 2) kcols_launch_ct<2>(a, s);
-    else kcols_launch_ct<1>(a, s);
+    if (a.g.fam_py == kE25) kspec_cols_e<kE25>(a, s);
+    else kspec_cols_e<kE16>(a, s);
 }
 
 void configure_psf_kernels();
 
-template <int CT>
-static void configure_ct() {
-    set_smem(frame_cols_kernel<256, CT, 1024>);
-    set_smem(frame_cols_kernel<512, CT, 2048>);
-    set_smem(frame_cols_kernel<1024, CT, 4096>);
-    set_smem(frame_cols_kernel<1024, CT, 6912>);
-    set_smem(kspec_cols_kernel<256, CT, 1024>);
-    set_smem(kspec_cols_kernel<512, CT, 2048>);
-    set_smem(kspec_cols_kernel<1024, CT, 4096>);
-    set_smem(kspec_cols_kernel<1024, CT, 6912>);
-}
-
 void configure_kernels() {
     configure_psf_kernels();
-    set_smem(frame_rows_kernel<256, 1024>);
-    set_smem(frame_rows_kernel<512, 2048>);
-    set_smem(frame_rows_kernel<1024, 4096>);
-    set_smem(frame_rows_kernel<1024, 6912>);
-    configure_ct<2>();
-    configure_ct<1>();
-    set_smem(frame_inverse_kernel<512, 1024, 4>);
-    set_smem(frame_inverse_kernel<1024, 2048, 4>);
-    set_smem(frame_inverse_kernel<1024, 4096, 4>);
-    set_smem(frame_inverse_kernel<1024, 6912, 4>);
-    set_smem(frame_inverse_kernel<384, 1024, 3>);
-    set_smem(frame_inverse_kernel<768, 2048, 3>);
-    set_smem(frame_inverse_kernel<1024, 4096, 3>);
-    set_smem(frame_inverse_kernel<1024, 6912, 3>);
-    set_smem(kspec_rows_kernel<256, 1024>);
-    set_smem(kspec_rows_kernel<512, 2048>);
-    set_smem(kspec_rows_kernel<1024, 4096>);
-    set_smem(kspec_rows_kernel<1024, 6912>);
+    configure_e<kE25>();
+    configure_e<kE16>();
 }
 
 }  // namespace ld

@@ -169,41 +169,52 @@ void staged(ld_ctx* c, int stage, cudaStream_t s, F launch) {
 // ---------------------------------------------------------------------------
 // FFT plans and twiddles
 // ---------------------------------------------------------------------------
-bool factor_plan(int n, FftPlan* plan) {
-    int m = n;
-    int k = 0;
+// Radices for a 5-smooth n: pairs of fives as 25 (when allowed: E = 25
+// family only), fours of twos as 16, the rest as 8 / 4 / 2 (16*2 becomes 8*4),
+// threes as 3.  The transform runs them in the order of kPlanRadices.
+bool factor_radices(int n, bool allow25, std::vector<int>* out) {
+    if (n < 2) return false;
+    int m = n, a = 0, b = 0, c5 = 0;
+    while (m % 2 == 0) { m /= 2; ++a; }
+    while (m % 3 == 0) { m /= 3; ++b; }
+    while (m % 5 == 0) { m /= 5; ++c5; }
+    if (m != 1) return false;
+    out->clear();
+    if (allow25) {
+        for (int i = 0; i < c5 / 2; ++i) out->push_back(25);
+        if (c5 % 2) out->push_back(5);
+    } else {
+        for (int i = 0; i < c5; ++i) out->push_back(5);
+    }
+    for (int i = 0; i < b; ++i) out->push_back(3);
+    int q16 = a / 4;
+    const int rem = a % 4;
+    if (rem == 1 && q16 > 0) {
+        --q16;
+        out->push_back(8);
+        out->push_back(4);
+    }
+    for (int i = 0; i < q16; ++i) out->push_back(16);
+    if (rem == 3) out->push_back(8);
+    else if (rem == 2) out->push_back(4);
+    else if (rem == 1 && a == 1) out->push_back(2);
+    if (out->size() > static_cast<size_t>(kMaxStages)) return false;
+    for (int i = 0; i < 7; ++i)
+        if (std::count(out->begin(), out->end(), kPlanRadices[i]) > 15) return false;
+    return true;
+}
+
+bool factor_plan(int n, bool allow25, FftPlan* plan) {
     std::vector<int> r;
-    while (m % 8 == 0 && m > 8) {
-        r.push_back(8);
-        m /= 8;
-    }
-    while (m % 5 == 0) {
-        r.push_back(5);
-        m /= 5;
-    }
-    while (m % 3 == 0) {
-        r.push_back(3);
-        m /= 3;
-    }
-    while (m % 8 == 0) {
-        r.push_back(8);
-        m /= 8;
-    }
-    if (m % 4 == 0) {
-        r.push_back(4);
-        m /= 4;
-    }
-    if (m % 2 == 0) {
-        r.push_back(2);
-        m /= 2;
-    }
-    if (m != 1 || r.size() > static_cast<size_t>(kMaxStages)) return false;
-    // large radices first
-    std::sort(r.begin(), r.end(), [](int a, int b) { return a > b; });
+    if (!factor_radices(n, allow25, &r)) return false;
     plan->n = n;
     plan->nstages = static_cast<int>(r.size());
     plan->codes = 0ull;
-    for (int v : r) plan->codes |= static_cast<unsigned long long>(v) << (4 * k++);
+    for (int i = 0; i < 7; ++i) {
+        const unsigned long long cnt =
+            static_cast<unsigned long long>(std::count(r.begin(), r.end(), kPlanRadices[i]));
+        plan->codes |= cnt << (4 * i);
+    }
     return true;
 }
 
@@ -235,9 +246,9 @@ const float2* twiddles(ld_ctx* c, int n) {
     return static_cast<const float2*>(b.p);
 }
 
-FftPlan make_plan(ld_ctx* c, int n) {
+FftPlan make_plan(ld_ctx* c, int n, bool allow25) {
     FftPlan p{};
-    if (!factor_plan(n, &p)) throw Fail{LD_ERR_UNSUPPORTED, "fft-length-not-5-smooth"};
+    if (!factor_plan(n, allow25, &p)) throw Fail{LD_ERR_UNSUPPORTED, "fft-length-not-5-smooth"};
     p.tw = twiddles(c, n);
     return p;
 }
@@ -448,7 +459,7 @@ float first_zero(ld_ctx* c, int np, int S, cudaStream_t s) {
     a.half = S / 2;
     a.off = std::max(0, (S - np) / 2);
     a.win_stride = S;
-    a.plan_s = make_plan(c, S);
+    a.plan_s = make_plan(c, S, fft_family(S, 1) == kE25);
     WavelengthInfo wi{};
     wi.win_x0 = 0;
     wi.win_n = S;
@@ -573,7 +584,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     a.R = R;
     a.K = K;
     a.gain = 1.0f + std::max(0.0f, static_cast<float>(p.anisotropy_emphasis)) * 4.0f;  // :1127
-    a.plan_s = make_plan(c, S);
+    a.plan_s = make_plan(c, S, fft_family(S, 1) == kE25);
     a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(B) * a.row_n * win_stride * sizeof(float2)));
     a.win = static_cast<float*>(ensure(c, c->win, static_cast<size_t>(B) * win_stride * win_stride * sizeof(float)));
     a.canvas = static_cast<float*>(ensure(c, b.canvas, static_cast<size_t>(B) * K * K * sizeof(float)));
@@ -699,35 +710,54 @@ std::string spectra_key(const BankEntry& b, const Combination& cb, const GridGeo
 
 constexpr size_t kSmemBudget = 227 * 1024;
 
-// Smallest 5-smooth grid covering the linear convolution, both sides even (the
-// rows are real transforms of length Px = 2M; the column tiles are 16-byte
-// multiples for the bulk copies).  Column tiles are two spectrum columns wide
-// unless the column pass's shared-memory working set would not fit.
+// Shared-memory passes of a transform of length n (its stage count), or a
+// large number when n has no plan.
+int fft_passes(int n, bool allow25) {
+    std::vector<int> r;
+    return factor_radices(n, allow25, &r) ? static_cast<int>(r.size()) : 1000;
+}
+
+// Cheapest 5-smooth length >= n (a multiple of `mult`) for up to C = 4
+// interleaved sequences: cost ~ m * (stages + 1.5), the stage passes plus the
+// fill and drain, so a slightly longer length with fewer stages can win.
+int choose_length(int n, int mult) {
+    int best = -1;
+    double best_cost = 0.0;
+    const int hi = n + std::max(64, n / 10);
+    for (int m = std::max(n, 2); m <= hi; ++m) {
+        if (m % mult != 0 || !smooth(m)) continue;
+        const int fam = fft_family(m, 4);
+        if (fam == 0) continue;
+        const double cost = static_cast<double>(m) * (fft_passes(m, fam == kE25) + 1.5);
+        if (best < 0 || cost < best_cost) {
+            best = m;
+            best_cost = cost;
+        }
+    }
+    return best;
+}
+
+// 5-smooth grid covering the linear convolution: Px = 2M with M the row
+// transform length, Py even (16-byte bulk-copy sizes).  The reference pads to
+// powers of two (LensDiffCpuReference.cpp:1172-1173); any grid of at least
+// W+K-1 x H+K-1 gives the same linear convolution.
 GridGeom make_geometry(ld_ctx* c, int W, int H, int K, int n_drv, int* req_w, int* req_h) {
+    (void)n_drv;
     GridGeom g{};
     *req_w = W + K - 1;
     *req_h = H + K - 1;
-    g.Px = next_smooth(*req_w, true);
-    g.Py = next_smooth(*req_h, true);
-    g.M = g.Px / 2;
-    if (g.M > 6912 || g.Py > 6912) throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-fft-grid"};
-    const int Hp = H + (H & 1);
+    g.M = choose_length((*req_w + 1) / 2, 1);
+    g.Py = choose_length(*req_h, 2);
+    if (g.M < 0 || g.Py < 0) throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-fft-grid"};
+    g.Px = 2 * g.M;
+    g.cols = g.M + 1;
+    g.fam_m = fft_family(g.M, 4);
+    g.fam_py = fft_family(g.Py, 4);
     const int Kp = K + (K & 1);
-    g.ct = 0;
-    for (int ct : {2, 1}) {
-        g.ct = ct;
-        FrameArgs probe{};
-        probe.g = g;
-        probe.Hp = Hp;
-        probe.n_drv = n_drv;
-        if (frame_cols_smem(probe) <= kSmemBudget && kspec_cols_smem(g, Kp) <= kSmemBudget) break;
-        g.ct = 0;
-    }
-    if (g.ct == 0) throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-column-pass"};
-    g.Pw = ((g.M + 1 + g.ct - 1) / g.ct) * g.ct;
-    g.tiles = g.Pw / g.ct;
-    g.plan_m = make_plan(c, g.M);
-    g.plan_py = make_plan(c, g.Py);
+    if (frame_cols_smem(g.Py, 4) > kSmemBudget || kspec_cols_smem(g.Py, Kp, 4) > kSmemBudget)
+        throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-column-pass"};
+    g.plan_m = make_plan(c, g.M, g.fam_m == kE25);
+    g.plan_py = make_plan(c, g.Py, g.fam_py == kE25);
     g.tw_px = twiddles(c, g.Px);
     return g;
 }
@@ -760,11 +790,10 @@ SpectraEntry& ensure_spectra(ld_ctx* c, BankEntry& b, const Combination& cb, con
     ka.Kp = b.K + (b.K & 1);
     ka.canvas = ca.out;
     ka.rows = static_cast<float2*>(
-        ensure(c, c->kspec_rows, static_cast<size_t>(cb.n_ker) * g.tiles * ka.Kp * g.ct * sizeof(float2)));
+        ensure(c, c->kspec_rows, static_cast<size_t>(cb.n_ker) * g.cols * ka.Kp * sizeof(float2)));
     ka.spectra = static_cast<float2*>(
-        ensure(c, e.spectra, static_cast<size_t>(cb.n_ker) * g.tiles * g.Py * g.ct * sizeof(float2)));
+        ensure(c, e.spectra, static_cast<size_t>(cb.n_ker) * g.cols * g.Py * sizeof(float2)));
     ka.scale = static_cast<float>(1.0 / (static_cast<double>(g.M) * static_cast<double>(g.Py)));
-    ka.grid = std::min(cb.n_ker * g.tiles, sm_count(c->device));
     ka.err = c->err;
     staged(c, LD_STAGE_KSPEC_ROWS, s, [&] { launch_kspec_rows(ka, s); });
     staged(c, LD_STAGE_KSPEC_COLS, s, [&] { launch_kspec_cols(ka, s); });
@@ -990,13 +1019,12 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         fa.core_comp = static_cast<float>(std::max(0.0, p.core_compensation));
         const float protect = std::max(0.2f, static_cast<float>(std::min(std::max(p.core_preserve, 0.0), 1.0)));
         fa.max_sub = fa.sel.rscale > 1e-6f ? (1.0f - protect) / fa.sel.rscale : 0.0f;
-        fa.Hp = H + (H & 1);
+        fa.Hp = (H + 3) & ~3;
         fa.A = static_cast<float2*>(
-            ensure(ctx, ctx->frameA, static_cast<size_t>(cb.n_drv) * g.tiles * fa.Hp * g.ct * sizeof(float2)));
+            ensure(ctx, ctx->frameA, static_cast<size_t>(cb.n_drv) * g.cols * fa.Hp * sizeof(float2)));
         fa.Bout = static_cast<float2*>(
-            ensure(ctx, ctx->frameB, static_cast<size_t>(cb.n_out) * g.tiles * H * g.ct * sizeof(float2)));
+            ensure(ctx, ctx->frameB, static_cast<size_t>(cb.n_out) * g.cols * fa.Hp * sizeof(float2)));
         fa.spectra = static_cast<const float2*>(sp.spectra.p);
-        fa.col_grid = std::min(g.tiles, sm_count(ctx->device));  // one persistent CTA per SM
         fa.err = ctx->err;
         staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
         staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
@@ -1102,7 +1130,7 @@ int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float
         a.half = S / 2;
         a.off = std::max(0, (S - np) / 2);
         a.win_stride = S;
-        a.plan_s = make_plan(ctx, S);
+        a.plan_s = make_plan(ctx, S, fft_family(S, 1) == kE25);
         WavelengthInfo wi{};
         wi.phase = phase_for_wavelength(p, wl[static_cast<size_t>(wavelength_index)]);
         wi.win_x0 = 0;
@@ -1150,7 +1178,7 @@ int run_guarded(ld_ctx* ctx, ld_status* st, const std::function<void()>& fn) {
 // Parameter resolution shared with ld_noalloc.cu (same expressions as above).
 // ---------------------------------------------------------------------------
 namespace ld {
-bool host_factor_plan(int n, FftPlan* plan) { return factor_plan(n, plan); }
+bool host_factor_plan(int n, bool allow25, FftPlan* plan) { return factor_plan(n, allow25, plan); }
 PupilParams host_pupil_params(const ld_params& p) { return pupil_params(p, false); }
 PhaseCoeffs host_phase_for_wavelength(const ld_params& p, float wavelength) {
     return phase_for_wavelength(p, wavelength);

@@ -11,7 +11,6 @@
 namespace ld {
 
 constexpr int kMaxBins = 64;  // LD_MAX_WAVELENGTHS
-constexpr int kColTile = 4;   // interleaved columns per column-pass CTA
 
 // ---- PSF bank -----------------------------------------------------------------
 // Per-wavelength constants, computed on the host with the reference's float
@@ -93,19 +92,19 @@ void launch_first_zero(const float* psf, int S, double* ring_sums, int* ring_cou
 void launch_normalize_psf(float* psf, int n, const PsfScalars* sc, cudaStream_t s);
 
 // ---- kernel spectra and frame chain ------------------------------------------------
-// Column tiles are `ct` (2, or 1 for very tall grids) adjacent spectrum columns.
-// Every array the column pass touches is stored tile-major so that one tile is
-// one contiguous block that a single bulk copy moves:
-//   A  [n_drv][tiles][Hp][ct]   forward row spectra (Hp = H rounded up to even)
-//   B  [n_out][tiles][H][ct]    column-pass outputs
-//   KR [n_ker][tiles][Kp][ct]   kernel row spectra (Kp = K rounded up to even)
-//   KS [n_ker][tiles][Py][ct]   kernel spectra, scaled by 1 / (M * Py)
+// Spectrum columns k = 0..M (the M + 1 bins of the real row transforms) are
+// stored column-major with their channels interleaved, so one column of every
+// channel is one contiguous block that a single bulk copy moves, and a row
+// pass reads or writes C adjacent values per bin:
+//   A  [cols][Hp][n_drv]   forward row spectra (Hp = H rounded up to 4)
+//   B  [cols][Hp][n_out]   column-pass outputs (rows >= H unused)
+//   KR [cols][Kp][n_ker]   kernel row spectra (Kp = K rounded up to even)
+//   KS [cols][Py][n_ker]   kernel spectra, scaled by 1 / (M * Py)
 struct GridGeom {
     int Px, Py;        // FFT grid
     int M;             // Px / 2
-    int ct;            // column tile width
-    int Pw;            // padded bins per row (multiple of ct, > M)
-    int tiles;         // Pw / ct
+    int cols;          // M + 1 spectrum columns
+    int fam_m, fam_py; // FFT families (elements per thread) of the row / column transforms
     FftPlan plan_m;    // length M (real rows via half-length complex)
     FftPlan plan_py;   // length Py (columns)
     const float2* tw_px;  // exp(-2 pi i k / Px), k < Px
@@ -119,12 +118,12 @@ struct KernelSpectraArgs {
     float2* rows;         // KR
     float2* spectra;      // KS
     float scale;          // 1 / (M * Py)
-    int grid;             // persistent CTAs of the column pass
+    int ahead;            // column-pass CTAs resident at once (set by the launcher)
     int* err;             // device error word
 };
 void launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s);
 void launch_kspec_cols(const KernelSpectraArgs& a, cudaStream_t s);
-size_t kspec_cols_smem(const GridGeom& g, int Kp);
+size_t kspec_cols_smem(int Py, int Kp, int n_ker);
 
 struct SelectionParams {
     int luma;              // extraction mode
@@ -152,7 +151,7 @@ struct FrameArgs {
     float2* A;
     float2* Bout;
     const float2* spectra;
-    int col_grid;              // persistent CTAs of the column pass
+    int ahead;                 // column-pass CTAs resident at once (set by the launcher)
     int* err;                  // device error word
     // epilogue
     int mono;
@@ -163,8 +162,8 @@ struct FrameArgs {
 void launch_frame_rows(const FrameArgs& a, cudaStream_t s);
 void launch_frame_cols(const FrameArgs& a, cudaStream_t s);
 void launch_frame_inverse(const FrameArgs& a, cudaStream_t s);
-size_t frame_cols_smem(const FrameArgs& a);
-int frame_cols_threads(int Py);
+// Column-pass shared memory: spectral (n_out 3 or 4) or Mono (n_out = 0).
+size_t frame_cols_smem(int Py, int n_out);
 
 // shared-memory opt-in for every kernel instantiation (once per device)
 void configure_kernels();

@@ -32,7 +32,7 @@
 #include "ld_internal.h"
 
 namespace ld {
-bool host_factor_plan(int n, FftPlan* plan);
+bool host_factor_plan(int n, bool allow25, FftPlan* plan);
 PupilParams host_pupil_params(const ld_params& p);
 PhaseCoeffs host_phase_for_wavelength(const ld_params& p, float wavelength);
 std::vector<float> host_wavelengths(const ld_params& p);
@@ -136,7 +136,7 @@ extern "C" int ld_raw_psf_noalloc(const ld_params* params, int wavelength_index,
         return LD_ERR_ARG;
     }
     FftPlan plan{};
-    if (!host_factor_plan(S, &plan)) {
+    if (!host_factor_plan(S, fft_family(S, 1) == kE25, &plan)) {
         set_stage(st, LD_ERR_UNSUPPORTED, "fft-length-not-5-smooth");
         return LD_ERR_UNSUPPORTED;
     }

@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(256) pupil_pre_kernel(PsfBankArgs a) {
 // grid (row_n, B).  Pupil row y = row_lo + blockIdx.x, embedded at (S-N_p)/2 of
 // a length-S row; the field A exp(i 2 pi phi) is generated in the fill, the
 // window columns are written by the drain.
-template <int T, int NMAX>
-__global__ void __launch_bounds__(T) psf_rows_kernel(PsfBankArgs a) {
+template <int E>
+__global__ void __launch_bounds__(E >= kE25 ? kE25MaxThreads : kE16MaxThreads, 1) psf_rows_kernel(PsfBankArgs a) {
     extern __shared__ float2 smem[];
     const int yr = blockIdx.x;
     const int y = a.row_lo + yr;
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(T) psf_rows_kernel(PsfBankArgs a) {
     const int enabled = w->phase.enabled;
     const float c4 = w->phase.c[4];
     const float4* pre = a.pupil_pre + static_cast<size_t>(y) * np;
-    smem_fill<T, 1>(smem, a.S, [=](int idx, int) -> float2 {
+    smem_fill<1>(smem, a.S, [=](int idx, int) -> float2 {
         const int x = idx - off;
         if (x < 0 || x >= np) return make_float2(0.0f, 0.0f);
         const float4 q = pre[x];
@@ -114,12 +114,12 @@ __global__ void __launch_bounds__(T) psf_rows_kernel(PsfBankArgs a) {
         sincosf(ph * 2.0f * kPiF, &sn, &cs);
         return make_float2(q.x * cs, q.x * sn);
     });
-    fft_run<T, 1, NMAX, false>(a.plan_s, smem);
+    fft_run<E, 1, false>(a.plan_s, smem);
     const int wn = w->win_n;
     const int wx0 = w->win_x0;
     const int S = a.S;
     float2* out = a.rows + (static_cast<size_t>(b) * a.row_n + yr) * a.win_stride;
-    for (int wx = threadIdx.x; wx < wn; wx += T) {
+    for (int wx = threadIdx.x; wx < wn; wx += blockDim.x) {
         int u = wx0 + wx + a.half;  // shifted column X -> unshifted (X + S/2) mod S
         if (u >= S) u -= S;
         out[wx] = smem[u];
@@ -129,8 +129,8 @@ __global__ void __launch_bounds__(T) psf_rows_kernel(PsfBankArgs a) {
 // ---- raw PSF: column pass + |.|^2 + fftshift window -----------------------------
 // grid (ceil(win/C), B).  Columns X0..X0+C of the window; only the pupil rows
 // that can be non-zero are read, |F|^2 of the window rows is written.
-template <int T, int C, int NMAX>
-__global__ void __launch_bounds__(T) psf_cols_kernel(PsfBankArgs a) {
+template <int E, int C>
+__global__ void __launch_bounds__(E >= kE25 ? kE25MaxThreads : kE16MaxThreads, 1) psf_cols_kernel(PsfBankArgs a) {
     extern __shared__ float2 smem[];
     const int b = blockIdx.y;
     const WavelengthInfo* w = a.wl + b;
@@ -142,17 +142,17 @@ __global__ void __launch_bounds__(T) psf_cols_kernel(PsfBankArgs a) {
     const int stride = a.win_stride;
     const float2* in = a.rows + static_cast<size_t>(b) * rn * stride;
     float* outw = a.win + static_cast<size_t>(b) * stride * stride;
-    smem_fill<T, C>(smem, a.S, [=](int idx, int col) -> float2 {
+    smem_fill<C>(smem, a.S, [=](int idx, int col) -> float2 {
         const int g = idx - lo;
         const int X = X0 + col;
         if (g < 0 || g >= rn || X >= wn) return make_float2(0.0f, 0.0f);
         return in[static_cast<size_t>(g) * stride + X];
     });
-    fft_run<T, C, NMAX, false>(a.plan_s, smem);
+    fft_run<E, C, false>(a.plan_s, smem);
     const int S = a.S;
     const int wy0 = w->win_x0;
     double esum = 0.0;
-    for (int i = threadIdx.x; i < wn * C; i += T) {
+    for (int i = threadIdx.x; i < wn * C; i += blockDim.x) {
         const int wy = i / C, col = i % C;
         const int X = X0 + col;
         if (X >= wn) continue;
@@ -631,16 +631,19 @@ __global__ void normalize_psf_kernel(float* psf, int64_t n, const PsfScalars* sc
 }
 
 // ---- launch helpers ---------------------------------------------------------------
-template <int T, int NMAX>
+// Row pass: one length-S transform per CTA.  Column pass: C adjacent window
+// columns per CTA, C = 4 / 2 / 1 for S <= 2048 / 4096 / larger (S * C <= 8192
+// keeps the E = 25 family up to S = 4096).
+template <int E>
 void rows_launch(const PsfBankArgs& a, cudaStream_t s) {
     dim3 grid(a.row_n, a.B);
-    psf_rows_kernel<T, NMAX><<<grid, T, a.S * sizeof(float2), s>>>(a);
+    psf_rows_kernel<E><<<grid, fft_threads(a.S, 1, E), a.S * sizeof(float2), s>>>(a);
 }
 
-template <int T, int C, int NMAX>
+template <int E, int C>
 void cols_launch(const PsfBankArgs& a, cudaStream_t s) {
     dim3 grid((a.win_stride + C - 1) / C, a.B);
-    psf_cols_kernel<T, C, NMAX><<<grid, T, static_cast<size_t>(a.S) * C * sizeof(float2), s>>>(a);
+    psf_cols_kernel<E, C><<<grid, fft_threads(a.S, C, E), static_cast<size_t>(a.S) * C * sizeof(float2), s>>>(a);
 }
 
 dim3 canvas_grid(const PsfBankArgs& a, int z) {
@@ -660,19 +663,15 @@ void launch_pupil_pre(const PsfBankArgs& a, cudaStream_t s) {
 }
 
 void launch_psf_rows(const PsfBankArgs& a, cudaStream_t s) {
-    if (a.S <= 1024) rows_launch<128, 1024>(a, s);
-    else if (a.S <= 2048) rows_launch<256, 2048>(a, s);
-    else if (a.S <= 4096) rows_launch<512, 4096>(a, s);
-    else if (a.S <= 8192) rows_launch<1024, 8192>(a, s);
-    else rows_launch<1024, 16384>(a, s);
+    if (fft_family(a.S, 1) == kE25) rows_launch<kE25>(a, s);
+    else rows_launch<kE16>(a, s);
 }
 
 void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s) {
-    if (a.S <= 1024) cols_launch<512, 4, 1024>(a, s);
-    else if (a.S <= 2048) cols_launch<1024, 4, 2048>(a, s);
-    else if (a.S <= 4096) cols_launch<1024, 2, 4096>(a, s);
-    else if (a.S <= 8192) cols_launch<1024, 1, 8192>(a, s);
-    else cols_launch<1024, 1, 16384>(a, s);
+    if (a.S <= 2048) cols_launch<kE25, 4>(a, s);
+    else if (a.S <= 4096) cols_launch<kE25, 2>(a, s);
+    else if (fft_family(a.S, 1) == kE25) cols_launch<kE25, 1>(a, s);
+    else cols_launch<kE16, 1>(a, s);
 }
 
 void launch_resample(const PsfBankArgs& a, cudaStream_t s) {
@@ -710,16 +709,12 @@ void launch_normalize_psf(float* psf, int n, const PsfScalars* sc, cudaStream_t 
 }
 
 void configure_psf_kernels() {
-    opt_in(psf_rows_kernel<128, 1024>, 1024 * 8);
-    opt_in(psf_rows_kernel<256, 2048>, 2048 * 8);
-    opt_in(psf_rows_kernel<512, 4096>, 4096 * 8);
-    opt_in(psf_rows_kernel<1024, 8192>, 8192 * 8);
-    opt_in(psf_rows_kernel<1024, 16384>, 16384 * 8);
-    opt_in(psf_cols_kernel<512, 4, 1024>, 1024 * 4 * 8);
-    opt_in(psf_cols_kernel<1024, 4, 2048>, 2048 * 4 * 8);
-    opt_in(psf_cols_kernel<1024, 2, 4096>, 4096 * 2 * 8);
-    opt_in(psf_cols_kernel<1024, 1, 8192>, 8192 * 8);
-    opt_in(psf_cols_kernel<1024, 1, 16384>, 16384 * 8);
+    opt_in(psf_rows_kernel<kE25>, 12800 * 8);
+    opt_in(psf_rows_kernel<kE16>, 16384 * 8);
+    opt_in(psf_cols_kernel<kE25, 4>, 2048 * 4 * 8);
+    opt_in(psf_cols_kernel<kE25, 2>, 4096 * 2 * 8);
+    opt_in(psf_cols_kernel<kE25, 1>, 12800 * 8);
+    opt_in(psf_cols_kernel<kE16, 1>, 16384 * 8);
 }
 
 }  // namespace ld

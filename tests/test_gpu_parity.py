@@ -63,6 +63,7 @@ def render_gpu(cache, p, src, src_origin=(0, 0), dst_shape=None, dst_origin=None
                         render_window=render_window, frame_short_side=p.frameShortSidePx)
     st = cache.render(req, p)
     torch.cuda.synchronize()
+    assert cache.check_device_errors() == 0, "a kernel recorded a device error (timeout or bad bulk copy)"
     return d.cpu().numpy(), st
 
 
