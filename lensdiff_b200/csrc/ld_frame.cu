@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_rows_kernel(Fram
     const SelectionParams sel = a.sel;
     // one thread per (row, pixel pair): the selection mask is evaluated once
     // per pixel and feeds every driver plane
+#pragma unroll 2
     for (int i = threadIdx.x; i < RPC * M; i += blockDim.x) {
         const int r = i / M;
         const int idx = i - r * M;
@@ -258,12 +259,29 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_inverse_kernel(F
         const float2* tw_px = a.g.tw_px;
         const int64_t col_elems = static_cast<int64_t>(a.Hp) * C;
         const float2* rowp = a.Bout + static_cast<int64_t>(sy) * C;
-        for (int i = threadIdx.x; i < M * C; i += blockDim.x) {
-            const int k = i / C;
-            const int col = i - k * C;
-            const float2 xk = __ldcs(&rowp[k * col_elems + col]);
-            const float2 xm = __ldcs(&rowp[(M - k) * col_elems + col]);
-            smem[i] = c2r_pre(xk, xm, __ldg(&tw_px[k]));
+        // kU entries per thread in flight: the bin reads are scattered (one
+        // C * 8-byte run per bin), so their latency is hidden by issuing a
+        // batch of them before the first is used
+        constexpr int kU = 4;
+        const int T = blockDim.x;
+        for (int i0 = threadIdx.x; i0 < M * C; i0 += kU * T) {
+            float2 xk[kU], xm[kU], w[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int i = i0 + u * T;
+                if (i < M * C) {
+                    const int k = i / C;
+                    const int col = i - k * C;
+                    xk[u] = __ldcs(&rowp[k * col_elems + col]);
+                    xm[u] = __ldcs(&rowp[(M - k) * col_elems + col]);
+                    w[u] = __ldg(&tw_px[k]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int i = i0 + u * T;
+                if (i < M * C) smem[i] = c2r_pre(xk[u], xm[u], w[u]);
+            }
         }
         __syncthreads();
         fft_run<E, C, true>(a.g.plan_m, smem);
@@ -272,6 +290,7 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_inverse_kernel(F
     const bool aligned_d = ((reinterpret_cast<uintptr_t>(a.dst) | static_cast<uintptr_t>(a.dst_pitch)) & 15) == 0;
     const unsigned char* srow = a.src + static_cast<int64_t>(sy) * a.src_pitch;
     unsigned char* drow = a.dst + static_cast<int64_t>(yo - a.dst_y1) * a.dst_pitch;
+#pragma unroll 2
     for (int x = a.out_x1 + threadIdx.x; x < a.out_x2; x += blockDim.x) {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         const int sx = x - a.src_x1;

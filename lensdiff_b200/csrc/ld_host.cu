@@ -41,7 +41,7 @@ struct BankEntry {
     int B = 0, np = 0, S = 0, R = 0, K = 0;
     int win_stride = 0;
     std::vector<float> wavelengths;
-    DevBuf canvas, ring_round, ring_ceil, ring_peak, scalars, wl;
+    DevBuf canvas, ring_round, ring_ceil, ring_peak, ring_mean, scalars, wl;
     PsfBankArgs args{};
 };
 
@@ -592,6 +592,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     a.ring_round = static_cast<double*>(ensure(c, b.ring_round, ringn * sizeof(double)));
     a.ring_ceil = static_cast<double*>(ensure(c, b.ring_ceil, ringn * sizeof(double)));
     a.ring_peak = static_cast<unsigned int*>(ensure(c, b.ring_peak, ringn * sizeof(unsigned int)));
+    a.ring_mean = static_cast<float*>(ensure(c, b.ring_mean, ringn * sizeof(float)));
     a.scalars = static_cast<PsfScalars*>(ensure(c, b.scalars, static_cast<size_t>(B) * sizeof(PsfScalars)));
     WavelengthInfo* dwl = static_cast<WavelengthInfo*>(ensure(c, b.wl, static_cast<size_t>(B) * sizeof(WavelengthInfo)));
     a.wl = dwl;
@@ -892,7 +893,7 @@ void ld_destroy(ld_ctx* c) {
                       &c->frameB, &c->calib, &c->calib_psf,  &c->err_word, &c->pupil_pre};
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
-    DevBuf* bb[] = {&c->bank.canvas, &c->bank.ring_round, &c->bank.ring_ceil, &c->bank.ring_peak,
+    DevBuf* bb[] = {&c->bank.canvas, &c->bank.ring_round, &c->bank.ring_ceil, &c->bank.ring_peak, &c->bank.ring_mean,
                     &c->bank.scalars, &c->bank.wl,        &c->spectra.spectra};
     for (DevBuf* b : bb) free_buf(c, *b);
     delete c;

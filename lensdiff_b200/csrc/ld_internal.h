@@ -57,6 +57,7 @@ struct PsfBankArgs {
     double* ring_round;          // [B][R+1] sums by round(r)
     double* ring_ceil;           // [B][R+1] sums by ceil(r)
     unsigned int* ring_peak;     // [B][R+1] max by ceil(r) (float bits)
+    float* ring_mean;            // [B][R+1] normalised azimuthal mean by round(r)
     const int* count_round;      // [R+1] pixel counts by round(r)
     PsfScalars* scalars;         // [B]
     int want_energy;

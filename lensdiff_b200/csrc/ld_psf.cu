@@ -286,6 +286,21 @@ __device__ double mean_kernel_sum(const double* ring, const int* count, int R, d
     return s2_shared;
 }
 
+// grid (B), block 256: s2 (the normaliser of azimuthalMeanKernel) and the
+// normalised azimuthal mean of every round(r) ring, once per wavelength, for
+// shape_stats_kernel to read.
+__global__ void __launch_bounds__(256) ring_mean_kernel(PsfBankArgs a) {
+    const int b = blockIdx.x;
+    const int R = a.R;
+    const double s1 = a.scalars[b].s1;
+    const double* rr = a.ring_round + static_cast<size_t>(b) * (R + 1);
+    const double s2 = mean_kernel_sum(rr, a.count_round, R, s1);
+    if (threadIdx.x == 0) a.scalars[b].s2 = s2;
+    float* out = a.ring_mean + static_cast<size_t>(b) * (R + 1);
+    for (int r = threadIdx.x; r <= R; r += blockDim.x)
+        out[r] = static_cast<float>(((rr[r] / s1) / max(1, a.count_round[r])) / s2);
+}
+
 // grid (ceil(K/32), ceil(K/32), B): shaped kernel (reshapeAnisotropy of the
 // base kernel against its azimuthal mean, LensDiffCpuReference.cpp:1088-1135)
 // written in place, its sum, and its ring energy / peak by ceil(r)
@@ -297,18 +312,16 @@ __global__ void __launch_bounds__(256) shape_stats_kernel(PsfBankArgs a) {
     const int b = blockIdx.z;
     const int tid = threadIdx.x + threadIdx.y * 32;
     const double s1 = a.scalars[b].s1;
-    const double s2 = mean_kernel_sum(a.ring_round + static_cast<size_t>(b) * (a.R + 1), a.count_round, a.R, s1);
-    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) a.scalars[b].s2 = s2;
     const int K = a.K, R = a.R;
     const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
     const int rbase = tile_ring_base(tx0, ty0, R, R);
     // ring means (round(r) rings) the tile can touch
-    const double* rr = a.ring_round + static_cast<size_t>(b) * (R + 1);
+    const float* rm = a.ring_mean + static_cast<size_t>(b) * (R + 1);
     for (int i = tid; i < kRingSpan; i += 256) {
         ring_e[i] = 0.0f;
         ring_p[i] = 0u;
         const int r = rbase + i;
-        mean_r[i] = r <= R ? static_cast<float>(((rr[r] / s1) / max(1, a.count_round[r])) / s2) : 0.0f;
+        mean_r[i] = r <= R ? rm[r] : 0.0f;
     }
     __syncthreads();
     const float inv_s1 = static_cast<float>(1.0 / s1);
@@ -679,6 +692,7 @@ void launch_resample(const PsfBankArgs& a, cudaStream_t s) {
 }
 
 void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s) {
+    ring_mean_kernel<<<a.B, 256, 0, s>>>(a);
     shape_stats_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
 }
 
