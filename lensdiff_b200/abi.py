@@ -308,7 +308,7 @@ EXPORTED_SYMBOLS = [
 ]
 
 STAGE_NAMES = ["psf_rows", "psf_cols", "resample", "shape_stats", "support", "crop_sum", "combine",
-               "kspec_rows", "kspec_cols", "frame_rows", "frame_cols", "frame_inverse", "pupil"]
+               "kspec_rows", "kspec_cols", "frame_rows", "frame_cols", "frame_inverse", "pupil", "composite"]
 
 
 def lib() -> ctypes.CDLL:

@@ -19,7 +19,9 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "liblensdiff_b200.so")
 ROOT = os.path.dirname(HERE)
-SOURCES = ["ld_host.cu", "ld_psf.cu", "ld_frame.cu", "ld_noalloc.cu"]
+SOURCES = ["ld_host.cu", "ld_psf.cu", "ld_frame.cu", "ld_noalloc.cu", "ld_cufft.cu"]
+# cuFFT backs only the comparator form (fft_form LD_FFT_CUFFT)
+LIBS = ["-L/usr/local/cuda/lib64", "-lcufft", "-Xlinker", "-rpath", "-Xlinker", "/usr/local/cuda/lib64"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{os.path.join(ROOT, 'include')}"]
 
@@ -65,7 +67,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
     tmp = OUT + ".tmp"
-    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
+    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, *LIBS]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stderr[-4000:]}")

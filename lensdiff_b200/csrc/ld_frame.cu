@@ -26,6 +26,7 @@
 
 #include "ld_async.cuh"
 #include "ld_internal.h"
+#include "ld_pixel.cuh"
 
 namespace ld {
 namespace {
@@ -36,29 +37,6 @@ template <int E>
 struct Fam {
     static constexpr int max_threads = E >= kE25 ? kE25MaxThreads : kE16MaxThreads;
 };
-
-__device__ __forceinline__ float saturate(float v) { return fminf(fmaxf(v, 0.0f), 1.0f); }
-
-// buildSelectionMask per pixel (LensDiffCpuReference.cpp:1225-1245).
-__device__ __forceinline__ float selection_mask(const SelectionParams& s, float r, float g, float b, float* signal) {
-    const float maxrgb = fmaxf(fmaxf(r, g), b);
-    const float sig = s.luma ? 0.2126f * r + 0.7152f * g + 0.0722f * b : maxrgb;
-    *signal = sig;
-    float gate = 0.0f;
-    if (sig > 0.0f) {
-        const float stops = log2f(fmaxf(sig, 1e-6f) / 0.18f);
-        const float t = saturate((stops - s.edge0) / fmaxf(s.edge1 - s.edge0, 1e-4f));
-        gate = t * t * (3.0f - 2.0f * t);
-    }
-    const float boost = 1.0f + s.point_emphasis * fmaxf(0.0f, maxrgb / fmaxf(s.thr_linear, 1e-4f) - 1.0f);
-    return saturate(gate * boost);
-}
-
-__device__ __forceinline__ float4 load_px(const unsigned char* row, int x, bool aligned) {
-    if (aligned) return __ldg(reinterpret_cast<const float4*>(row) + x);
-    const float* p = reinterpret_cast<const float*>(row) + 4 * x;
-    return make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3));
-}
 
 // X[k] of a real length-2M sequence from Z = FFT_M(even + i*odd):
 // X[k] = E + W^k O, E = (Z[k] + conj Z[M-k]) / 2, O = (Z[k] - conj Z[M-k]) / 2i.
@@ -247,11 +225,38 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_cols_mono_kernel
 }
 
 // ---- inverse rows + spectral map + composite ----------------------------------------
-// One output row per CTA; smem M * C float2 (C = n_out interleaved channels).
+// The spectral map of pixel sx of the inverse-transformed row in smem.
+template <int C>
+__device__ __forceinline__ float3 mapped_effect(const FrameArgs& a, const float2* smem, int sx) {
+    const int nn = sx >> 1;
+    const bool odd = sx & 1;
+    float e[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const float2 z = smem[nn * C + c];
+        e[c] = odd ? z.y : z.x;
+    }
+    return map_effect<C>(a, e);
+}
+
+// Tent weight of field zone z along one axis (accumulateWeightedImage,
+// LensDiffCpuReference.cpp:1458-1466; the reference's grid is n = 3).
+__device__ __forceinline__ float zone_weight(int v, int extent, int z, int n) {
+    const float denom = static_cast<float>(max(1, extent - 1));
+    const float pv = (static_cast<float>(v) / denom) * static_cast<float>(n - 1);
+    return fmaxf(0.0f, 1.0f - fabsf(pv - static_cast<float>(z)));
+}
+
+// One row per CTA; smem M * C float2 (C = n_out interleaved channels).  The
+// row is output row out_y1 + blockIdx.x (kEffectComposite), source row
+// blockIdx.x (kEffectStore) or source row row0 + blockIdx.x
+// (kEffectAccumulate); see FrameArgs::effect_mode.
 template <int E, int C>
 __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_inverse_kernel(FrameArgs a) {
     extern __shared__ float2 smem[];
-    const int yo = a.out_y1 + blockIdx.x;
+    const int bid = static_cast<int>(blockIdx.x);
+    const int yo = a.effect_mode == kEffectComposite ? a.out_y1 + bid
+                                                     : a.src_y1 + (a.effect_mode == kEffectStore ? bid : a.row0 + bid);
     const int sy = yo - a.src_y1;
     const bool have = sy >= 0 && sy < a.H;
     const int M = a.g.M;
@@ -287,61 +292,97 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_inverse_kernel(F
         fft_run<E, C, true>(a.g.plan_m, smem);
     }
     const bool aligned_s = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(a.src_pitch)) & 15) == 0;
-    const bool aligned_d = ((reinterpret_cast<uintptr_t>(a.dst) | static_cast<uintptr_t>(a.dst_pitch)) & 15) == 0;
     const unsigned char* srow = a.src + static_cast<int64_t>(sy) * a.src_pitch;
+    if (a.effect_mode == kEffectAccumulate) {
+        if (!have) return;
+        const float wy = zone_weight(sy, a.H, a.zone_y, a.zone_n);
+        if (wy <= 0.0f) return;
+        float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
+        for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
+            const float wgt = zone_weight(sx, a.W, a.zone_x, a.zone_n) * wy;
+            if (wgt <= 0.0f) continue;
+            const float3 e = mapped_effect<C>(a, smem, sx);
+            float4 acc = erow[sx];
+            acc.x += e.x * wgt;
+            acc.y += e.y * wgt;
+            acc.z += e.z * wgt;
+            erow[sx] = acc;
+        }
+        return;
+    }
+    if (a.effect_mode == kEffectStore) {
+        double l_in = 0.0, l_eff = 0.0;
+        float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
+        for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
+            const float3 e = mapped_effect<C>(a, smem, sx);
+            erow[sx] = make_float4(e.x, e.y, e.z, 0.0f);
+            const float4 p = load_px(srow, sx, aligned_s);
+            float sig;
+            const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
+            l_in += static_cast<double>(luma(p.x * m, p.y * m, p.z * m));
+            l_eff += static_cast<double>(luma(e.x, e.y, e.z));
+        }
+        block_add2(l_in, l_eff, a.sums);
+        return;
+    }
+    const bool aligned_d = ((reinterpret_cast<uintptr_t>(a.dst) | static_cast<uintptr_t>(a.dst_pitch)) & 15) == 0;
     unsigned char* drow = a.dst + static_cast<int64_t>(yo - a.dst_y1) * a.dst_pitch;
 #pragma unroll 2
     for (int x = a.out_x1 + threadIdx.x; x < a.out_x2; x += blockDim.x) {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         const int sx = x - a.src_x1;
+        if (have && sx >= 0 && sx < a.W)
+            out = composite_px(a, load_px(srow, sx, aligned_s), mapped_effect<C>(a, smem, sx));
+        store_px(drow, x - a.dst_x1, aligned_d, out);
+    }
+}
+
+// Luma sums of the redistributed source and of the stored effect over the
+// whole source frame (field zones with Preserve energy); one source row per CTA.
+__global__ void __launch_bounds__(256) effect_sums_kernel(FrameArgs a) {
+    const int sy = blockIdx.x;
+    const bool aligned_s = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(a.src_pitch)) & 15) == 0;
+    const unsigned char* srow = a.src + static_cast<int64_t>(sy) * a.src_pitch;
+    const float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
+    double l_in = 0.0, l_eff = 0.0;
+    for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
+        const float4 p = load_px(srow, sx, aligned_s);
+        float sig;
+        const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
+        l_in += static_cast<double>(luma(p.x * m, p.y * m, p.z * m));
+        const float4 e = erow[sx];
+        l_eff += static_cast<double>(luma(e.x, e.y, e.z));
+    }
+    block_add2(l_in, l_eff, a.sums);
+}
+
+// Output rows of the render window from the stored effect: scaled, with
+// Preserve energy, by (luma sum of the redistributed source) / (luma sum of
+// the effect) as LensDiffCpuReference.cpp:2172-2178 does (scaleImage with the
+// float quotient of the two sums), then composited.
+__global__ void __launch_bounds__(256) composite_kernel(FrameArgs a) {
+    const int yo = a.out_y1 + blockIdx.x;
+    const int sy = yo - a.src_y1;
+    const bool have = sy >= 0 && sy < a.H;
+    float scale = 1.0f;
+    if (a.preserve) {
+        const float in_e = static_cast<float>(a.sums[0]);
+        const float eff_e = static_cast<float>(a.sums[1]);
+        if (eff_e > 1e-6f) scale = in_e / eff_e;
+    }
+    const bool aligned_s = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(a.src_pitch)) & 15) == 0;
+    const bool aligned_d = ((reinterpret_cast<uintptr_t>(a.dst) | static_cast<uintptr_t>(a.dst_pitch)) & 15) == 0;
+    const unsigned char* srow = a.src + static_cast<int64_t>(sy) * a.src_pitch;
+    unsigned char* drow = a.dst + static_cast<int64_t>(yo - a.dst_y1) * a.dst_pitch;
+    const float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
+    for (int x = a.out_x1 + threadIdx.x; x < a.out_x2; x += blockDim.x) {
+        float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        const int sx = x - a.src_x1;
         if (have && sx >= 0 && sx < a.W) {
-            const int nn = sx >> 1;
-            const bool odd = sx & 1;
-            float e[C];
-#pragma unroll
-            for (int c = 0; c < C; ++c) {
-                const float2 z = smem[nn * C + c];
-                e[c] = odd ? z.y : z.x;
-            }
-            float r = fmaxf(0.0f, e[0]);
-            float g = fmaxf(0.0f, e[1]);
-            float b = fmaxf(0.0f, e[2]);
-            if (!a.mono) {
-                if (a.saturation != 1.0f) {
-                    const float gray = 0.2126f * r + 0.7152f * g + 0.0722f * b;
-                    r = gray + (r - gray) * a.saturation;
-                    g = gray + (g - gray) * a.saturation;
-                    b = gray + (b - gray) * a.saturation;
-                }
-                if (C == 4 && a.luma_lock) {
-                    const float cur = 0.2126f * r + 0.7152f * g + 0.0722f * b;
-                    if (cur > 1e-6f) {
-                        const float sc = e[C - 1] / cur;
-                        r *= sc;
-                        g *= sc;
-                        b *= sc;
-                    }
-                }
-            }
-            const float4 p = load_px(srow, sx, aligned_s);
-            float sig;
-            const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
-            const float rr = p.x * m, rg = p.y * m, rb = p.z * m;
-            out.x = fmaxf(fmaxf(0.0f, p.x - a.core_comp * rr + a.effect_gain * r), fmaxf(0.0f, p.x - rr * a.max_sub));
-            out.y = fmaxf(fmaxf(0.0f, p.y - a.core_comp * rg + a.effect_gain * g), fmaxf(0.0f, p.y - rg * a.max_sub));
-            out.z = fmaxf(fmaxf(0.0f, p.z - a.core_comp * rb + a.effect_gain * b), fmaxf(0.0f, p.z - rb * a.max_sub));
-            out.w = p.w;
+            const float4 e = erow[sx];
+            out = composite_px(a, load_px(srow, sx, aligned_s), make_float3(e.x * scale, e.y * scale, e.z * scale));
         }
-        const int dx = x - a.dst_x1;
-        if (aligned_d) {
-            reinterpret_cast<float4*>(drow)[dx] = out;
-        } else {
-            float* q = reinterpret_cast<float*>(drow) + 4 * dx;
-            q[0] = out.x;
-            q[1] = out.y;
-            q[2] = out.z;
-            q[3] = out.w;
-        }
+        store_px(drow, x - a.dst_x1, aligned_d, out);
     }
 }
 
@@ -420,9 +461,10 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) kspec_cols_kernel(Kern
     }
 }
 
+// Dynamic shared-memory opt-in, leaving 1 KB for a kernel's static arrays.
 template <class F>
 void set_smem(F f) {
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem - 1024);
 }
 
 // CTAs of `f` resident at once on the current device (the L2 prefetch distance).
@@ -467,7 +509,7 @@ void cols_e(const FrameArgs& a, cudaStream_t s) {
 }
 
 template <int E>
-void inverse_e(const FrameArgs& a, int rows, cudaStream_t s) {
+void inverse_e(const FrameArgs& a, int rows, cudaStream_t s) {  // rows: grid size
     const int M = a.g.M;
     if (a.n_out == 4) {
         frame_inverse_kernel<E, 4><<<rows, fft_threads(M, 4, E), static_cast<size_t>(M) * 4 * sizeof(float2), s>>>(a);
@@ -544,10 +586,24 @@ void launch_frame_cols(const FrameArgs& a, cudaStream_t s) {
 }
 
 void launch_frame_inverse(const FrameArgs& a, cudaStream_t s) {
-    const int rows = a.out_y2 - a.out_y1;
+    const int rows = a.effect_mode == kEffectStore ? a.H : a.out_y2 - a.out_y1;
     if (rows <= 0) return;
     if (a.g.fam_m == kE25) inverse_e<kE25>(a, rows, s);
     else inverse_e<kE16>(a, rows, s);
+}
+
+void launch_frame_inverse_rows(const FrameArgs& a, int rows, cudaStream_t s) {
+    if (rows <= 0) return;
+    if (a.g.fam_m == kE25) inverse_e<kE25>(a, rows, s);
+    else inverse_e<kE16>(a, rows, s);
+}
+
+void launch_effect_sums(const FrameArgs& a, cudaStream_t s) { effect_sums_kernel<<<a.H, 256, 0, s>>>(a); }
+
+void launch_composite(const FrameArgs& a, cudaStream_t s) {
+    const int rows = a.out_y2 - a.out_y1;
+    if (rows <= 0) return;
+    composite_kernel<<<rows, 256, 0, s>>>(a);
 }
 
 void launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s) {

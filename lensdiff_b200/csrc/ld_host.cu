@@ -41,6 +41,7 @@ struct BankEntry {
     int B = 0, np = 0, S = 0, R = 0, K = 0;
     int win_stride = 0;
     std::vector<float> wavelengths;
+    bool cufft = false;  // built with the comparator form (its spectra follow)
     DevBuf canvas, ring_round, ring_ceil, ring_peak, ring_mean, scalars, wl;
     PsfBankArgs args{};
 };
@@ -66,8 +67,12 @@ struct ld_ctx {
     std::map<int, DevBuf> ring_counts;  // by R
     BankEntry bank;
     SpectraEntry spectra;
+    std::vector<SpectraEntry> zone_spectra;  // field zones, zy * n + zx
     // work buffers, grown on demand
-    DevBuf rows, win, combine_out, kspec_rows, frameA, frameB, calib, calib_psf, pupil_pre;
+    DevBuf rows, win, combine_out, kspec_rows, frameA, frameB, calib, calib_psf, pupil_pre, effect;
+    // comparator form (cuFFT): plans and its own work buffers
+    CufftPlanCache cufft;
+    DevBuf cf_grid, cf_planes, cf_sd, cf_prod;
     DevBuf err_word;    // device int: nonzero after a bounded wait gave up
     int* err = nullptr;
     int launches = 0;
@@ -287,6 +292,8 @@ std::vector<float> wavelengths_of(const ld_params& p) {  // CpuReference.cpp:160
     }
 }
 
+constexpr int kMaxFieldGrid = 16;
+
 bool has_field_phase(const ld_params& p) {  // LensDiffPhase.cpp:40-57
     if (p.phase_mode != LD_PHASE_ENABLED || std::abs(p.phase_field_strength) <= 1e-6) return false;
     const double v[] = {p.phase_field_defocus, p.phase_field_astig_radial, p.phase_field_astig_tangential,
@@ -298,6 +305,44 @@ bool has_field_phase(const ld_params& p) {  // LensDiffPhase.cpp:40-57
     for (double x : v)
         if (std::abs(x) > 1e-6) return true;
     return false;
+}
+
+// ResolveLensDiffFieldZoneParams (LensDiffPhase.cpp:98-168), FP64 as the
+// reference: the zone's own Zernike coefficients at normalised field position
+// (nx, ny); the field terms are cleared so the zone bank has no zones.
+void add_orientation_pair(double radial, double tangential, double angle, int harmonic, double* x, double* y) {
+    const double base = static_cast<double>(harmonic) * angle;
+    const double cs = std::cos(base), sn = std::sin(base);
+    *x += radial * cs - tangential * sn;
+    *y += radial * sn + tangential * cs;
+}
+
+ld_params zone_params(const ld_params& p, float nx, float ny) {
+    ld_params q = p;
+    q.phase_field_strength = 0.0;
+    const double radial = std::min(1.0, std::sqrt(static_cast<double>(nx) * nx + static_cast<double>(ny) * ny) /
+                                            std::sqrt(2.0));
+    const double bias = std::min(std::max(p.phase_field_edge_bias, 0.0), 1.0);
+    const double scale = p.phase_field_strength * std::pow(radial, 1.0 + bias * 2.0);
+    if (std::abs(scale) <= 1e-9) return q;
+    const double angle = std::atan2(static_cast<double>(ny), static_cast<double>(nx));
+    q.phase_defocus += p.phase_field_defocus * scale;
+    q.phase_spherical += p.phase_field_spherical * scale;
+    add_orientation_pair(p.phase_field_astig_radial * scale, p.phase_field_astig_tangential * scale, angle, 2,
+                         &q.phase_astigmatism0, &q.phase_astigmatism45);
+    add_orientation_pair(p.phase_field_coma_radial * scale, p.phase_field_coma_tangential * scale, angle, 1,
+                         &q.phase_coma_x, &q.phase_coma_y);
+    add_orientation_pair(p.phase_field_trefoil_radial * scale, p.phase_field_trefoil_tangential * scale, angle, 3,
+                         &q.phase_trefoil_x, &q.phase_trefoil_y);
+    add_orientation_pair(p.phase_field_secondary_astig_radial * scale,
+                         p.phase_field_secondary_astig_tangential * scale, angle, 2,
+                         &q.phase_secondary_astigmatism0, &q.phase_secondary_astigmatism45);
+    add_orientation_pair(p.phase_field_quadrafoil_radial * scale, p.phase_field_quadrafoil_tangential * scale,
+                         angle, 4, &q.phase_quadrafoil0, &q.phase_quadrafoil45);
+    add_orientation_pair(p.phase_field_secondary_coma_radial * scale,
+                         p.phase_field_secondary_coma_tangential * scale, angle, 1, &q.phase_secondary_coma_x,
+                         &q.phase_secondary_coma_y);
+    return q;
 }
 
 // Noll-indexed coefficients for one wavelength: the named terms
@@ -389,13 +434,13 @@ std::string bank_key(const ld_params& p, const std::vector<float>& wl) {
     k = append_bytes(k, dbl, sizeof(dbl));
     k = append_bytes(k, p.noll, sizeof(p.noll));
     k = append_bytes(k, wl.data(), wl.size() * sizeof(float));
+    k = append_bytes(k, &p.fft_form, sizeof(p.fft_form));
     return k;
 }
 
 void validate_params(const ld_params& p) {
     if (p.debug_view != LD_DEBUG_FINAL) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-debug-view"};
     if (p.look_mode != LD_LOOK_PHYSICAL) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-look-mode-split"};
-    if (p.energy_mode != LD_ENERGY_AUGMENT) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-energy-mode-preserve"};
     if (p.input_transfer != LD_TRANSFER_LINEAR) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-input-transfer"};
     if (p.resolution_aware) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-resolution-aware"};
     if (p.aperture_mode != LD_APERTURE_CIRCLE && p.aperture_mode != LD_APERTURE_POLYGON &&
@@ -403,7 +448,8 @@ void validate_params(const ld_params& p) {
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-aperture-mode"};
     if (p.apodization_mode < 0 || p.apodization_mode > 2) throw Fail{LD_ERR_ARG, "invalid-apodization-mode"};
     if (p.spectral_mode < 0 || p.spectral_mode > 3) throw Fail{LD_ERR_ARG, "invalid-spectral-mode"};
-    if (has_field_phase(p)) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-field-phase"};
+    if (p.field_grid != 0 && (p.field_grid < 2 || p.field_grid > kMaxFieldGrid))
+        throw Fail{LD_ERR_ARG, "invalid-field-grid"};
     if (p.scatter_amount > 1e-6 && percent_to_px(p.scatter_radius, optics_short_side(p)) > 0.25)
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-scatter"};
     if (percent_to_px(p.creative_fringe, optics_short_side(p)) > 1e-6)
@@ -411,7 +457,10 @@ void validate_params(const ld_params& p) {
     if (p.wavelength_count < 0 || p.wavelength_count > LD_MAX_WAVELENGTHS)
         throw Fail{LD_ERR_ARG, "invalid-wavelength-count"};
     if (p.vane_count > kMaxVanes) throw Fail{LD_ERR_UNSUPPORTED, "too-many-vanes"};
-    if (p.fft_form != LD_FFT_OWN_FP32) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-fft-form"};
+    if (p.fft_form != LD_FFT_OWN_FP32 && p.fft_form != LD_FFT_CUFFT)
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-fft-form"};
+    if (p.fft_form == LD_FFT_CUFFT && has_field_phase(p))
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-field-zones-with-cufft-form"};
 }
 
 size_t align256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
@@ -604,8 +653,14 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     check_cuda(cudaMemsetAsync(a.ring_ceil, 0, ringn * sizeof(double), s), "bank-memset");
     check_cuda(cudaMemsetAsync(a.ring_peak, 0, ringn * sizeof(unsigned int), s), "bank-memset");
     check_cuda(cudaMemsetAsync(a.scalars, 0, static_cast<size_t>(B) * sizeof(PsfScalars), s), "bank-memset");
-    staged(c, LD_STAGE_PSF_ROWS, s, [&] { launch_psf_rows(a, s); });
-    staged(c, LD_STAGE_PSF_COLS, s, [&] { launch_psf_cols(a, s); });
+    if (p.fft_form == LD_FFT_CUFFT) {
+        float2* grid = static_cast<float2*>(
+            ensure(c, c->cf_grid, cf_psf_chunk(S, B) * static_cast<size_t>(S) * S * sizeof(float2)));
+        staged(c, LD_STAGE_PSF_ROWS, s, [&] { cf_psf_transform(a, grid, c->cufft, s); });
+    } else {
+        staged(c, LD_STAGE_PSF_ROWS, s, [&] { launch_psf_rows(a, s); });
+        staged(c, LD_STAGE_PSF_COLS, s, [&] { launch_psf_cols(a, s); });
+    }
     staged(c, LD_STAGE_RESAMPLE, s, [&] { launch_resample(a, s); });
     staged(c, LD_STAGE_SHAPE_STATS, s, [&] { launch_shape_stats(a, s); });
     staged(c, LD_STAGE_SUPPORT, s, [&] { launch_support(a, s); });
@@ -618,6 +673,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     b.K = K;
     b.win_stride = win_stride;
     b.wavelengths = wl;
+    b.cufft = p.fft_form == LD_FFT_CUFFT;
     b.key = key;
     b.valid = true;
     c->spectra.valid = false;
@@ -700,8 +756,8 @@ Combination make_combination(const ld_params& p, const std::vector<float>& wl) {
     return cb;
 }
 
-std::string spectra_key(const BankEntry& b, const Combination& cb, const GridGeom& g) {
-    std::string k = b.key;
+std::string spectra_key_for(const std::string& bank_key_s, const Combination& cb, const GridGeom& g) {
+    std::string k = bank_key_s;
     k = append_bytes(k, &cb.n_ker, sizeof(int));
     k = append_bytes(k, cb.coef, sizeof(cb.coef));
     k = append_bytes(k, &g.Px, sizeof(int));
@@ -769,11 +825,12 @@ int sm_count(int device) {
     return sms;
 }
 
-SpectraEntry& ensure_spectra(ld_ctx* c, BankEntry& b, const Combination& cb, const GridGeom& g, cudaStream_t s,
-                             bool* rebuilt) {
-    const std::string key = spectra_key(b, cb, g);
+// Kernel spectra of bank `b` into entry `e` (combination, row and column
+// transforms), unless `e` already holds them.
+SpectraEntry& ensure_spectra_in(ld_ctx* c, SpectraEntry& e, BankEntry& b, const Combination& cb, const GridGeom& g,
+                                cudaStream_t s, bool* rebuilt) {
+    const std::string key = spectra_key_for(b.key, cb, g);
     *rebuilt = false;
-    SpectraEntry& e = c->spectra;
     if (e.valid && e.key == key) return e;
     e.valid = false;
     CombineArgs ca{};
@@ -796,8 +853,15 @@ SpectraEntry& ensure_spectra(ld_ctx* c, BankEntry& b, const Combination& cb, con
         ensure(c, e.spectra, static_cast<size_t>(cb.n_ker) * g.cols * g.Py * sizeof(float2)));
     ka.scale = static_cast<float>(1.0 / (static_cast<double>(g.M) * static_cast<double>(g.Py)));
     ka.err = c->err;
-    staged(c, LD_STAGE_KSPEC_ROWS, s, [&] { launch_kspec_rows(ka, s); });
-    staged(c, LD_STAGE_KSPEC_COLS, s, [&] { launch_kspec_cols(ka, s); });
+    if (b.cufft) {
+        // cuFFT layout: KS [n_ker][Py][Px/2+1], the same size as the own layout
+        float* planes = static_cast<float*>(
+            ensure(c, c->cf_planes, static_cast<size_t>(cb.n_ker) * g.Px * g.Py * sizeof(float)));
+        staged(c, LD_STAGE_KSPEC_COLS, s, [&] { cf_kernel_spectra(ka, planes, c->cufft, s); });
+    } else {
+        staged(c, LD_STAGE_KSPEC_ROWS, s, [&] { launch_kspec_rows(ka, s); });
+        staged(c, LD_STAGE_KSPEC_COLS, s, [&] { launch_kspec_cols(ka, s); });
+    }
     check_launch("kernel-spectra");
     e.g = g;
     e.n_ker = cb.n_ker;
@@ -805,6 +869,45 @@ SpectraEntry& ensure_spectra(ld_ctx* c, BankEntry& b, const Combination& cb, con
     e.valid = true;
     *rebuilt = true;
     return e;
+}
+
+SpectraEntry& ensure_spectra(ld_ctx* c, BankEntry& b, const Combination& cb, const GridGeom& g, cudaStream_t s,
+                             bool* rebuilt) {
+    return ensure_spectra_in(c, c->spectra, b, cb, g, s, rebuilt);
+}
+
+// Field zones: the kernel spectra of every zone of an n x n grid, in the
+// reference's order (zy outer, zx inner, LensDiffCpuReference.cpp:1779-1783),
+// each zone's bank built from its resolved parameters (makeFieldZoneCache,
+// :1736-1756) only when that zone's spectra are not cached already.
+std::vector<const SpectraEntry*> ensure_zone_spectra(ld_ctx* c, const ld_params& p, int n, const Combination& cb,
+                                                     const GridGeom& g, cudaStream_t s, bool* bank_rebuilt,
+                                                     bool* spectra_rebuilt) {
+    if (static_cast<int>(c->zone_spectra.size()) != n * n) {
+        for (auto& z : c->zone_spectra) free_buf(c, z.spectra);
+        c->zone_spectra.clear();
+        c->zone_spectra.resize(static_cast<size_t>(n) * n);
+    }
+    const std::vector<float> wl = wavelengths_of(p);
+    std::vector<const SpectraEntry*> out;
+    for (int zy = 0; zy < n; ++zy) {
+        for (int zx = 0; zx < n; ++zx) {
+            const float nx = (2.0f * static_cast<float>(zx)) / static_cast<float>(n - 1) - 1.0f;
+            const float ny = (2.0f * static_cast<float>(zy)) / static_cast<float>(n - 1) - 1.0f;
+            const ld_params zp = zone_params(p, nx, ny);
+            SpectraEntry& e = c->zone_spectra[static_cast<size_t>(zy) * n + zx];
+            const std::string key = spectra_key_for(bank_key(zp, wl), cb, g);
+            if (!(e.valid && e.key == key)) {
+                bool rb = false, rs = false;
+                BankEntry& b = ensure_bank(c, zp, s, &rb);
+                ensure_spectra_in(c, e, b, cb, g, s, &rs);
+                *bank_rebuilt = *bank_rebuilt || rb;
+                *spectra_rebuilt = *spectra_rebuilt || rs;
+            }
+            out.push_back(&e);
+        }
+    }
+    return out;
 }
 
 void fill_sizes(ld_status* st, const ld_params& p) {
@@ -889,13 +992,16 @@ void ld_destroy(ld_ctx* c) {
     DeviceGuard g(c->device);
     for (auto& kv : c->twiddles) free_buf(c, kv.second);
     for (auto& kv : c->ring_counts) free_buf(c, kv.second);
-    DevBuf* bufs[] = {&c->rows,   &c->win,  &c->combine_out, &c->kspec_rows, &c->frameA,
-                      &c->frameB, &c->calib, &c->calib_psf,  &c->err_word, &c->pupil_pre};
+    DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,    &c->frameB,
+                      &c->calib,  &c->calib_psf, &c->err_word,  &c->pupil_pre,  &c->effect,    &c->cf_grid,
+                      &c->cf_planes, &c->cf_sd,  &c->cf_prod};
+    c->cufft.release();
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
     DevBuf* bb[] = {&c->bank.canvas, &c->bank.ring_round, &c->bank.ring_ceil, &c->bank.ring_peak, &c->bank.ring_mean,
                     &c->bank.scalars, &c->bank.wl,        &c->spectra.spectra};
     for (DevBuf* b : bb) free_buf(c, *b);
+    for (auto& z : c->zone_spectra) free_buf(c, z.spectra);
     delete c;
 }
 
@@ -939,6 +1045,7 @@ void ld_clear_caches(ld_ctx* c) {
     std::lock_guard<std::mutex> lock(c->mu);
     c->bank.valid = false;
     c->spectra.valid = false;
+    for (auto& z : c->zone_spectra) z.valid = false;
 }
 
 int ld_resolve_sizes(const ld_params* p, int32_t* np, int32_t* S, int32_t* R, int32_t* B) {
@@ -985,11 +1092,20 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         fill_sizes(st, p);
         ctx->launches = 0;
         bool bank_rebuilt = false, spectra_rebuilt = false;
-        BankEntry& bank = ensure_bank(ctx, p, s, &bank_rebuilt);
-        const Combination cb = make_combination(p, bank.wavelengths);
+        const bool zones = has_field_phase(p);
+        const int zn = p.field_grid > 0 ? p.field_grid : 3;
+        const std::vector<float> wl = wavelengths_of(p);
+        const Combination cb = make_combination(p, wl);
         int rw = 0, rh = 0;
-        const GridGeom g = make_geometry(ctx, W, H, bank.K, cb.n_drv, &rw, &rh);
-        SpectraEntry& sp = ensure_spectra(ctx, bank, cb, g, s, &spectra_rebuilt);
+        const GridGeom g = make_geometry(ctx, W, H, 2 * max_kernel_radius(p) + 1, cb.n_drv, &rw, &rh);
+        std::vector<const SpectraEntry*> spectra;
+        if (zones) {
+            spectra = ensure_zone_spectra(ctx, p, zn, cb, g, s, &bank_rebuilt, &spectra_rebuilt);
+        } else {
+            BankEntry& bank = ensure_bank(ctx, p, s, &bank_rebuilt);
+            spectra.push_back(&ensure_spectra(ctx, bank, cb, g, s, &spectra_rebuilt));
+        }
+        const SpectraEntry& sp = *spectra.front();
 
         FrameArgs fa{};
         fa.g = g;
@@ -1015,9 +1131,15 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         fa.mono = cb.mono;
         fa.saturation = cb.saturation;
         fa.luma_lock = cb.luma_lock;
-        // Augment: effect gain and core compensation (CpuReference.cpp:2104-2109)
-        fa.effect_gain = static_cast<float>(std::max(0.0, p.effect_gain));
-        fa.core_comp = static_cast<float>(std::max(0.0, p.core_compensation));
+        // effect gain and core compensation per energy mode (CpuReference.cpp:2104-2109)
+        fa.preserve = p.energy_mode == LD_ENERGY_PRESERVE ? 1 : 0;
+        if (fa.preserve) {
+            fa.effect_gain = static_cast<float>(std::min(std::max(p.effect_gain, 0.0), 1.0));
+            fa.core_comp = fa.effect_gain;
+        } else {
+            fa.effect_gain = static_cast<float>(std::max(0.0, p.effect_gain));
+            fa.core_comp = static_cast<float>(std::max(0.0, p.core_compensation));
+        }
         const float protect = std::max(0.2f, static_cast<float>(std::min(std::max(p.core_preserve, 0.0), 1.0)));
         fa.max_sub = fa.sel.rscale > 1e-6f ? (1.0f - protect) / fa.sel.rscale : 0.0f;
         fa.Hp = (H + 3) & ~3;
@@ -1027,9 +1149,62 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             ensure(ctx, ctx->frameB, static_cast<size_t>(cb.n_out) * g.cols * fa.Hp * sizeof(float2)));
         fa.spectra = static_cast<const float2*>(sp.spectra.p);
         fa.err = ctx->err;
+        fa.effect_mode = zones ? kEffectAccumulate : (fa.preserve ? kEffectStore : kEffectComposite);
+        if (fa.effect_mode != kEffectComposite) {
+            fa.effect = static_cast<float4*>(
+                ensure(ctx, ctx->effect, static_cast<size_t>(W) * H * sizeof(float4) + 2 * sizeof(double)));
+            fa.sums = reinterpret_cast<double*>(fa.effect + static_cast<size_t>(W) * H);
+            check_cuda(cudaMemsetAsync(fa.sums, 0, 2 * sizeof(double), s), "effect-memset");
+            if (zones)
+                check_cuda(cudaMemsetAsync(fa.effect, 0, static_cast<size_t>(W) * H * sizeof(float4), s),
+                           "effect-memset");
+        }
+        if (p.fft_form == LD_FFT_CUFFT) {
+            const size_t P = static_cast<size_t>(g.Px) * g.Py;
+            const size_t half = static_cast<size_t>(g.Py) * (g.Px / 2 + 1);
+            const int nc = std::max(cb.n_drv, cb.n_out);
+            float* planes = static_cast<float*>(ensure(ctx, ctx->cf_planes, nc * P * sizeof(float)));
+            float2* sd = static_cast<float2*>(ensure(ctx, ctx->cf_sd, cb.n_drv * half * sizeof(float2)));
+            float2* prod = static_cast<float2*>(ensure(ctx, ctx->cf_prod, cb.n_out * half * sizeof(float2)));
+            staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { cf_frame_forward(fa, planes, sd, ctx->cufft, s); });
+            staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { cf_frame_multiply(fa, sd, prod, s); });
+            staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { cf_frame_inverse(fa, prod, planes, ctx->cufft, s); });
+            if (fa.effect_mode != kEffectComposite)
+                staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fa, s); });
+            check_launch("frame-chain");
+            if (st) {
+                st->bank_rebuilt = bank_rebuilt;
+                st->spectra_rebuilt = spectra_rebuilt;
+                st->grid_requested_w = rw;
+                st->grid_requested_h = rh;
+                st->grid_used_w = g.Px;
+                st->grid_used_h = g.Py;
+                st->kernel_launches = ctx->launches;
+            }
+            return;
+        }
         staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
-        staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
-        staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse(fa, s); });
+        if (!zones) {
+            staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
+            staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse(fa, s); });
+        } else {
+            fa.zone_n = zn;
+            for (int z = 0; z < zn * zn; ++z) {
+                fa.spectra = static_cast<const float2*>(spectra[static_cast<size_t>(z)]->spectra.p);
+                fa.zone_x = z % zn;
+                fa.zone_y = z / zn;
+                // source rows whose tent weight can be non-zero (the kernel
+                // evaluates the weight itself; one row of margin each side)
+                const double step = static_cast<double>(std::max(1, H - 1)) / static_cast<double>(zn - 1);
+                const int r0 = std::max(0, static_cast<int>(std::floor((fa.zone_y - 1) * step)) - 1);
+                const int r1 = std::min(H, static_cast<int>(std::ceil((fa.zone_y + 1) * step)) + 2);
+                fa.row0 = r0;
+                staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
+                staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse_rows(fa, r1 - r0, s); });
+            }
+            if (fa.preserve) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_effect_sums(fa, s); });
+        }
+        if (fa.effect_mode != kEffectComposite) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fa, s); });
         check_launch("frame-chain");
         if (st) {
             st->bank_rebuilt = bank_rebuilt;
@@ -1166,6 +1341,9 @@ int run_guarded(ld_ctx* ctx, ld_status* st, const std::function<void()>& fn) {
     } catch (const Fail& f) {
         set_status(st, f.code, f.stage);
         return f.code;
+    } catch (const CufftError& e) {
+        set_status(st, LD_ERR_CUDA, std::string(e.what) + "-" + std::to_string(e.code));
+        return LD_ERR_CUDA;
     } catch (const std::exception& e) {
         set_status(st, LD_ERR_CUDA, e.what());
         return LD_ERR_CUDA;

@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <tuple>
+
 #include "ld_fft.cuh"
 #include "ld_optics.cuh"
 
@@ -135,6 +138,8 @@ struct SelectionParams {
     float rscale;          // 1 - corePreserve
 };
 
+enum { kEffectComposite = 0, kEffectStore = 1, kEffectAccumulate = 2 };
+
 struct FrameArgs {
     GridGeom g;
     SelectionParams sel;
@@ -154,6 +159,21 @@ struct FrameArgs {
     const float2* spectra;
     int ahead;                 // column-pass CTAs resident at once (set by the launcher)
     int* err;                  // device error word
+    // What the inverse pass does with the mapped effect of a row:
+    //   kEffectComposite: composite the render window directly (Augment);
+    //   kEffectStore: write every source pixel's effect to `effect` and add the
+    //     luma sums of the redistributed source and of the effect to sums[0],
+    //     sums[1] (Preserve energy, LensDiffCpuReference.cpp:2172-2178);
+    //   kEffectAccumulate: add the tent-weighted effect of field zone
+    //     (zone_x, zone_y) of a zone_n x zone_n grid to `effect`, source rows
+    //     row0 + blockIdx.x (accumulateWeightedImage, :1452-1475).
+    // composite_kernel then finishes the last two, scaling the effect by
+    // sums[0] / sums[1] when `preserve`.
+    int effect_mode;
+    int preserve;
+    int zone_x, zone_y, zone_n, row0;
+    float4* effect;            // [H][W]
+    double* sums;              // [2]
     // epilogue
     int mono;
     float saturation;
@@ -163,10 +183,35 @@ struct FrameArgs {
 void launch_frame_rows(const FrameArgs& a, cudaStream_t s);
 void launch_frame_cols(const FrameArgs& a, cudaStream_t s);
 void launch_frame_inverse(const FrameArgs& a, cudaStream_t s);
+void launch_composite(const FrameArgs& a, cudaStream_t s);
+// Inverse pass over `rows` CTAs (kEffectAccumulate: source rows row0 + i).
+void launch_frame_inverse_rows(const FrameArgs& a, int rows, cudaStream_t s);
+void launch_effect_sums(const FrameArgs& a, cudaStream_t s);
 // Column-pass shared memory: spectral (n_out 3 or 4) or Mono (n_out = 0).
 size_t frame_cols_smem(int Py, int n_out);
 
 // shared-memory opt-in for every kernel instantiation (once per device)
 void configure_kernels();
+
+// ---- comparator form: the same chain with cuFFT transforms (ld_cufft.cu) -----------
+struct CufftError {
+    int code;
+    const char* what;
+};
+
+// cuFFT plans by (type, ny, nx, batch), destroyed with the cache.
+struct CufftPlanCache {
+    std::map<std::tuple<int, int, int, int>, int> plans;
+    int get(int type, int ny, int nx, int batch);
+    void release();
+    ~CufftPlanCache();
+};
+
+size_t cf_psf_chunk(int S, int B);  // wavelengths per batched S x S transform
+void cf_psf_transform(const PsfBankArgs& a, float2* grid, CufftPlanCache& plans, cudaStream_t s);
+void cf_kernel_spectra(const KernelSpectraArgs& a, float* planes, CufftPlanCache& plans, cudaStream_t s);
+void cf_frame_forward(const FrameArgs& a, float* planes, float2* sd, CufftPlanCache& plans, cudaStream_t s);
+void cf_frame_multiply(const FrameArgs& a, const float2* sd, float2* prod, cudaStream_t s);
+void cf_frame_inverse(const FrameArgs& a, float2* prod, float* planes, CufftPlanCache& plans, cudaStream_t s);
 
 }  // namespace ld

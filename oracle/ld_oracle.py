@@ -696,11 +696,82 @@ def soft_shoulder(v: np.ndarray, shoulder: float) -> np.ndarray:
     return shoulder * (1.0 - np.exp(-x / shoulder))
 
 
+# ---------------------------------------------------------------- field zones
+FIELD_TERMS = [  # (radial, tangential, x target, y target, harmonic) — LensDiffPhase.cpp:131-166
+    ("phaseFieldAstigRadial", "phaseFieldAstigTangential", "phaseAstigmatism0", "phaseAstigmatism45", 2),
+    ("phaseFieldComaRadial", "phaseFieldComaTangential", "phaseComaX", "phaseComaY", 1),
+    ("phaseFieldTrefoilRadial", "phaseFieldTrefoilTangential", "phaseTrefoilX", "phaseTrefoilY", 3),
+    ("phaseFieldSecondaryAstigRadial", "phaseFieldSecondaryAstigTangential", "phaseSecondaryAstigmatism0",
+     "phaseSecondaryAstigmatism45", 2),
+    ("phaseFieldQuadrafoilRadial", "phaseFieldQuadrafoilTangential", "phaseQuadrafoil0", "phaseQuadrafoil45", 4),
+    ("phaseFieldSecondaryComaRadial", "phaseFieldSecondaryComaTangential", "phaseSecondaryComaX",
+     "phaseSecondaryComaY", 1),
+]
+
+
+def has_field_phase(p) -> bool:
+    """HasLensDiffFieldPhase, LensDiffPhase.cpp:40-57."""
+    if int(p.phaseMode) != 1 or abs(p.phaseFieldStrength) <= 1e-6:
+        return False
+    names = ["phaseFieldDefocus", "phaseFieldSpherical"] + [t[0] for t in FIELD_TERMS] + [t[1] for t in FIELD_TERMS]
+    return any(abs(getattr(p, n)) > 1e-6 for n in names)
+
+
+def resolve_field_zone(p, nx: float, ny: float):
+    """ResolveLensDiffFieldZoneParams, LensDiffPhase.cpp:112-168 (FP64 as the
+    reference): the zone's own Zernike coefficients; the field terms are
+    cleared so the zone bank is built without zones."""
+    q = p.copy()
+    if not has_field_phase(p):
+        return q
+    radial = min(1.0, math.sqrt(float(nx) * nx + float(ny) * ny) / math.sqrt(2.0))
+    bias = min(max(float(p.phaseFieldEdgeBias), 0.0), 1.0)
+    scale = float(p.phaseFieldStrength) * radial ** (1.0 + bias * 2.0)
+    q = q.copy(phaseFieldStrength=0.0)
+    if abs(scale) <= 1e-9:
+        return q
+    ang = math.atan2(float(ny), float(nx))
+    ch = {"phaseDefocus": p.phaseDefocus + p.phaseFieldDefocus * scale,
+          "phaseSpherical": p.phaseSpherical + p.phaseFieldSpherical * scale}
+    for rad, tan, xt, yt, h in FIELD_TERMS:
+        rv, tv = getattr(p, rad) * scale, getattr(p, tan) * scale
+        cs, sn = math.cos(h * ang), math.sin(h * ang)
+        ch[xt] = getattr(p, xt) + rv * cs - tv * sn
+        ch[yt] = getattr(p, yt) + rv * sn + tv * cs
+    return q.copy(**ch)
+
+
+def field_zone_weights(w: int, h: int, zx: int, zy: int, n: int = 3) -> np.ndarray:
+    """accumulateWeightedImage tent weights, LensDiffCpuReference.cpp:1452-1475
+    (float32 as the reference; n x n zones, the reference's n = 3)."""
+    dx = F(max(1, w - 1))
+    dy = F(max(1, h - 1))
+    px = (np.arange(w, dtype=np.float32) / dx) * F(n - 1)
+    py = (np.arange(h, dtype=np.float32) / dy) * F(n - 1)
+    wx = np.maximum(F(0), F(1) - np.abs(px - F(zx)))
+    wy = np.maximum(F(0), F(1) - np.abs(py - F(zy)))
+    return (wy[:, None] * wx[None, :]).astype(np.float32)
+
+
+def field_zone_banks(p, n: int = 3):
+    """makeFieldZoneCache for every zone in the reference's order (zy outer,
+    zx inner), LensDiffCpuReference.cpp:1779-1783."""
+    out = []
+    for zy in range(n):
+        for zx in range(n):
+            nx = 2.0 * zx / (n - 1) - 1.0
+            ny = 2.0 * zy / (n - 1) - 1.0
+            out.append((zx, zy, build_psf_bank(resolve_field_zone(p, F(nx), F(ny)))))
+    return out
+
+
 def render(src: np.ndarray, p, bank: PsfBank, natural: Optional[np.ndarray] = None,
            style: Optional[np.ndarray] = None, src_origin=(0, 0), dst_bounds=None,
-           render_window=None) -> np.ndarray:
-    """RunLensDiffCpuReference, LensDiffCpuReference.cpp:2073-2261 (no field zones,
-    no resolution-aware resample, no scatter / creative fringe, Final view).
+           render_window=None, field_grid: int = 3) -> np.ndarray:
+    """RunLensDiffCpuReference, LensDiffCpuReference.cpp:2073-2261 (no
+    resolution-aware resample, no scatter / creative fringe, Final view).
+    With field phase on, `bank` is ignored and the effect is the tent-weighted
+    sum of the zones' effects (:2161-2170); `field_grid` zones per side.
 
     src: (H, W, 4) float array at bounds origin `src_origin`.  Returns the dst
     image (dh, dw, 4) for `dst_bounds` = (x1, y1, x2, y2) (defaults to src)."""
@@ -719,19 +790,26 @@ def render(src: np.ndarray, p, bank: PsfBank, natural: Optional[np.ndarray] = No
     spectral = int(p.spectralMode) != 0
     split = int(p.lookMode) == 1
 
-    def effect_for(kind: str) -> np.ndarray:
+    def effect_for(bk, kind: str) -> np.ndarray:
         if not spectral:
-            ker = getattr(bank.bins[0], kind)
+            ker = getattr(bk.bins[0], kind)
             return np.stack([convolve(redist[..., c], ker) for c in range(3)], axis=-1)
-        planes = np.stack([convolve(driver, getattr(b, kind)) for b in bank.bins], axis=-1)
+        planes = np.stack([convolve(driver, getattr(b, kind)) for b in bk.bins], axis=-1)
         return map_bins(planes, natural, style if style is not None else natural, p)
 
-    if split:
-        core = soft_shoulder(effect_for("core"), float(F(p.coreShoulder)))
-        struct = soft_shoulder(effect_for("structure"), float(F(p.structureShoulder)))
-        effect = core * max(0.0, float(p.coreGain)) + struct * max(0.0, float(p.structureGain))
+    def effect_of(bk) -> np.ndarray:
+        if split:
+            core = soft_shoulder(effect_for(bk, "core"), float(F(p.coreShoulder)))
+            struct = soft_shoulder(effect_for(bk, "structure"), float(F(p.structureShoulder)))
+            return core * max(0.0, float(p.coreGain)) + struct * max(0.0, float(p.structureGain))
+        return effect_for(bk, "full")
+
+    if has_field_phase(p):
+        effect = np.zeros((h, w, 3))
+        for zx, zy, bk in field_zone_banks(p, field_grid):
+            effect += effect_of(bk) * field_zone_weights(w, h, zx, zy, field_grid)[..., None]
     else:
-        effect = effect_for("full")
+        effect = effect_of(bank)
     if preserve:
         lw = np.array([0.2126, 0.7152, 0.0722])
         e_in = float((redist @ lw).sum())

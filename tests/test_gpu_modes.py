@@ -1,0 +1,181 @@
+"""Render modes beyond the Augment composite, through the C ABI on the GPU,
+against the reference's own CPU renderer (RunLensDiffCpuReference compiled
+from the reference sources into oracle/_ref) and the FP64 oracle.
+
+Preserve energy (LensDiffCpuReference.cpp:2104-2109, :2172-2178): the effect
+is scaled so that its luma sum over the whole source frame equals the luma sum
+of the redistributed highlights, whatever the render window; effect gain is
+clamped to [0, 1] and the core compensation equals it.
+
+The reference accumulates the two luma sums in sequential float; the GPU path
+sums in FP64.  At the frame sizes here the float sums are exact to ~1e-6
+relative, far below the output tolerance (2e-4 of the frame maximum).
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from lensdiff_b200 import synthetic as S  # noqa: E402
+from lensdiff_b200.backend import LensDiffPsfBankCache, image_request  # noqa: E402
+from lensdiff_b200.types import LensDiffApertureMode, LensDiffEnergyMode, LensDiffSpectralMode  # noqa: E402
+from oracle import ld_oracle as O  # noqa: E402
+from oracle import ref_lib as R  # noqa: E402
+from tests.helpers import OUT_TOL, rel_err, spectrum_matrices, with_matrices  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cache():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    c = LensDiffPsfBankCache(0)
+    yield c
+    c.close()
+
+
+def _lens(**kw):
+    p = S.base_params(144)
+    p.apertureMode = LensDiffApertureMode.Polygon
+    p.bladeCount = 7
+    p.roundness = 0.3
+    p.pupilResolution = 128
+    p.phaseDefocus = 0.2
+    p.phaseComaX = 0.1
+    p.maxKernelRadiusPx = S.radius_percent(27, 144)
+    p.diffractionScalePx = 3.0
+    p.spectralMode = LensDiffSpectralMode.Tristimulus
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _render(cache, p, src, src_origin=(0, 0), dst_shape=None, dst_origin=None, render_window=None):
+    stream = torch.cuda.Stream()
+    s = torch.from_numpy(np.ascontiguousarray(src, np.float32)).cuda()
+    d = torch.full(dst_shape or src.shape, -7.0, device="cuda", dtype=torch.float32)
+    req = image_request(s, d, stream, src_origin=src_origin, dst_origin=dst_origin, render_window=render_window,
+                        frame_short_side=p.frameShortSidePx)
+    st = cache.render(req, p)
+    torch.cuda.synchronize()
+    assert st.ok, st
+    assert cache.check_device_errors() == 0
+    return d.cpu().numpy()
+
+
+def _oracle(p, src, **kw):
+    mats = () if p.spectralMode == LensDiffSpectralMode.Mono else spectrum_matrices(p)
+    return O.render(src, p, O.build_psf_bank(p), *mats, **kw)
+
+
+def _reference_available():
+    if not R.available():
+        pytest.skip("the compiled reference (oracle/_ref) is not present")
+
+
+@pytest.mark.parametrize("mode,gain", [(LensDiffSpectralMode.Tristimulus, 0.8),
+                                       (LensDiffSpectralMode.Mono, 1.0),
+                                       (LensDiffSpectralMode.Spectral5, 0.5)])
+def test_preserve_energy_matches_reference(cache, mode, gain):
+    _reference_available()
+    p = _lens(spectralMode=mode, energyMode=LensDiffEnergyMode.Preserve, effectGain=gain, corePreserve=0.1)
+    src = S.make_frame(224, 144, 20, 1.0, 80.0, seed=11)
+    out = _render(cache, with_matrices(p), src)
+    ref = R.render(p, src)
+    assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
+    orc = _oracle(p, src)
+    assert rel_err(out, orc, orc[..., :3].max()) < OUT_TOL
+
+
+def test_preserve_energy_sums_over_whole_frame_not_window(cache):
+    _reference_available()
+    p = _lens(energyMode=LensDiffEnergyMode.Preserve, effectGain=1.0)
+    src = S.make_frame(200, 120, 16, 1.0, 60.0, seed=12)
+    window = (30, 10, 150, 90)
+    out = _render(cache, with_matrices(p), src, render_window=window)
+    ref = R.render(p, src, render_window=window)
+    x1, y1, x2, y2 = window
+    assert np.all(out[:y1] == -7.0) and np.all(out[:, :x1] == -7.0)
+    inside = out[y1:y2, x1:x2]
+    refin = ref[y1:y2, x1:x2]
+    assert rel_err(inside, refin, refin[..., :3].max()) < OUT_TOL
+
+
+# ------------------------------------------------------------ field zones ----
+# Field-varying aberrations (ResolveLensDiffFieldZoneParams, LensDiffPhase.cpp:
+# 112-168): every zone of a 3 x 3 grid gets its own Zernike coefficients, its
+# own PSF bank and its own convolution; the zone effects are blended with tent
+# weights (accumulateWeightedImage, LensDiffCpuReference.cpp:1452-1475).
+def _field_lens(**kw):
+    from lensdiff_b200.types import LensDiffPhaseMode
+    return _lens(phaseMode=LensDiffPhaseMode.Enabled, phaseFieldStrength=1.0, phaseFieldEdgeBias=0.5,
+                 phaseFieldComaRadial=0.3, phaseFieldAstigTangential=0.2, phaseFieldDefocus=0.1, **kw)
+
+
+@pytest.mark.parametrize("energy", [LensDiffEnergyMode.Augment, LensDiffEnergyMode.Preserve])
+def test_field_zones_match_reference(cache, energy):
+    _reference_available()
+    p = _field_lens(energyMode=energy)
+    src = S.make_frame(200, 120, 16, 1.0, 60.0, seed=13)
+    out = _render(cache, with_matrices(p), src)
+    ref = R.render(p, src)
+    assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
+    # the zones matter: without them the result is measurably different
+    flat = R.render(p.copy(phaseFieldStrength=0.0), src)
+    assert rel_err(flat, ref, ref[..., :3].max()) > 20 * OUT_TOL
+
+
+def test_field_zones_cached_and_window(cache):
+    _reference_available()
+    p = _field_lens(spectralMode=LensDiffSpectralMode.Mono)
+    src = S.make_frame(180, 110, 12, 1.0, 50.0, seed=14)
+    window = (20, 15, 160, 100)
+    first = _render(cache, with_matrices(p), src, render_window=window)
+    again = _render(cache, with_matrices(p), src, render_window=window)  # all nine zones cached
+    assert np.array_equal(first, again)
+    ref = R.render(p, src, render_window=window)
+    x1, y1, x2, y2 = window
+    assert rel_err(first[y1:y2, x1:x2], ref[y1:y2, x1:x2], ref[y1:y2, x1:x2, :3].max()) < OUT_TOL
+
+
+def test_field_grid_8x8_matches_oracle(cache):
+    """The 8 x 8 zone grid of the batching workload (an extension: the
+    reference's grid is 3 x 3), against the FP64 oracle restated from the
+    same zone rules."""
+    p = _field_lens(fieldGrid=8, pupilResolution=64, maxKernelRadiusPx=S.radius_percent(12, 144))
+    src = S.make_frame(160, 96, 10, 1.0, 40.0, seed=15)
+    out = _render(cache, with_matrices(p), src)
+    orc = _oracle(p, src, field_grid=8)
+    assert rel_err(out, orc, orc[..., :3].max()) < OUT_TOL
+
+
+# ------------------------------------------------------- cuFFT comparator ----
+# fft_form LD_FFT_CUFFT runs the same bank and frame chain with cuFFT doing the
+# transforms (the library the reference CUDA backend uses); it is the timing
+# comparator and must meet the same parity bar.
+@pytest.mark.parametrize("mode,energy", [(LensDiffSpectralMode.Tristimulus, LensDiffEnergyMode.Augment),
+                                         (LensDiffSpectralMode.Mono, LensDiffEnergyMode.Augment),
+                                         (LensDiffSpectralMode.Spectral5, LensDiffEnergyMode.Preserve)])
+def test_cufft_form_matches_reference(cache, mode, energy):
+    from lensdiff_b200.types import LensDiffFftForm
+    _reference_available()
+    p = _lens(spectralMode=mode, energyMode=energy, chromaticFocus=0.3)
+    src = S.make_frame(224, 144, 20, 1.0, 80.0, seed=16)
+    own = _render(cache, with_matrices(p), src)
+    cuf = _render(cache, with_matrices(p.copy(fftForm=LensDiffFftForm.Cufft)), src)
+    ref = R.render(p, src)
+    scale = ref[..., :3].max()
+    assert rel_err(cuf, ref, scale) < OUT_TOL
+    assert rel_err(own, ref, scale) < OUT_TOL
+
+
+def test_cufft_form_rejects_field_zones(cache):
+    from lensdiff_b200.types import LensDiffFftForm
+    p = _field_lens(fftForm=LensDiffFftForm.Cufft)
+    src = S.make_frame(64, 48, 4, 1.0, 10.0, seed=17)
+    stream = torch.cuda.Stream()
+    s = torch.from_numpy(src).cuda()
+    d = torch.zeros_like(s)
+    st = cache.render(image_request(s, d, stream, frame_short_side=p.frameShortSidePx), with_matrices(p))
+    assert not st.ok and "field-zones" in st.stage
