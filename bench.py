@@ -43,6 +43,10 @@ WORKLOADS = {
 METRIC = "UHD frames/s (31-wavelength PSF bank, FFT convolution, composite)"
 
 
+FFT_FORMS = {"own": 0, "chosen": 1, "cufft": 2}
+FORM_NAMES = {"own": "own_fp32", "chosen": "own_chosen", "cufft": "cufft"}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -53,6 +57,10 @@ def parse():
     ap.add_argument("--bank", default="cold", choices=["cold", "warm"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fft-form", default="own", choices=sorted(FFT_FORMS),
+                    help="transform chain of the headline line (own: hand-written FP32)")
+    ap.add_argument("--no-comparators", action="store_true",
+                    help="skip timing the other transform chains on the same workload")
     return ap.parse_args()
 
 
@@ -249,6 +257,7 @@ def main():
     from lensdiff_b200.backend import LensDiffPsfBankCache, image_request
 
     p, frame = getattr(S, WORKLOADS[args.workload])(seed=1003 + rank)
+    p = p.copy(fftForm=FFT_FORMS[args.fft_form])
     H, W = frame.shape[:2]
     dev = torch.device("cuda", local)
     cache = LensDiffPsfBankCache(local)
@@ -368,6 +377,45 @@ def main():
                     "frac": None, "peak_source": peak_src, "traffic": None}
     stage_ms = {k: round(v[0] / max(1, args.steps), 4) for k, v in stage.items() if v[1]}
 
+    # ---- the other transform chains on the same workload (device time) ------
+    comparators = {}
+    if not args.no_comparators:
+        for name in ("own", "cufft"):
+            if name == args.fft_form:
+                continue
+            base = p.copy(fftForm=FFT_FORMS[name])
+            k = [0]
+
+            def cmp_step():
+                k[0] += 1
+                pp = base.copy(phaseDefocus=base.phaseDefocus + 1e-6 * (k[0] + 10000)) if args.bank == "cold" \
+                    else base
+                st = cache.render(req, pp)
+                if not st.ok:
+                    raise RuntimeError(f"{name} render failed: {st}")
+
+            with torch.cuda.stream(stream):
+                for _ in range(args.warmup):
+                    cmp_step()
+            torch.cuda.synchronize(dev)
+            cev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+            with torch.cuda.stream(stream):
+                cev[0].record(stream)
+                for i in range(args.steps):
+                    cmp_step()
+                    cev[i + 1].record(stream)
+            torch.cuda.synchronize(dev)
+            cps = sorted(cev[i].elapsed_time(cev[i + 1]) for i in range(args.steps))
+            ctot = torch.tensor([cev[0].elapsed_time(cev[-1])], device=dev, dtype=torch.float64)
+            if ws > 1:
+                torch.distributed.all_reduce(ctot, op=torch.distributed.ReduceOp.MAX)
+            ctot = float(ctot.item())
+            comparators[FORM_NAMES[name]] = {
+                "value": ws * args.steps / (ctot / 1000.0), "unit": "frames/s", "ms_per_step": ctot / args.steps,
+                "p50_ms": cps[len(cps) // 2], "p99_ms": cps[min(len(cps) - 1, int(math.ceil(0.99 * len(cps))) - 1)]}
+        if cache.check_device_errors():
+            raise RuntimeError("device error word set by a comparator chain")
+
     # ---- CPU baseline (rank 0, N=1) ----------------------------------------
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -390,7 +438,7 @@ def main():
                        "pupil": st0.pupil_size, "psf": st0.raw_psf_size,
                        "max_kernel_radius": st0.max_kernel_radius, "bank": args.bank,
                        "grid_requested": list(st0.grid_requested), "grid_used": list(st0.grid_used),
-                       "fft_form": "own_fp32", "parallelism": f"replicas x{ws}",
+                       "fft_form": FORM_NAMES[args.fft_form], "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2 (frame 133 MB + spectra > 1 GB)"},
             "gpu_launches": launches_per_frame[0] * args.steps,
             "stage_ms_per_frame": stage_ms,
@@ -398,6 +446,7 @@ def main():
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "comparators": comparators,
         }
         print(json.dumps(line))
     cache.close()
