@@ -86,41 +86,55 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_rows_kernel(Fram
     const int W = a.W, H = a.H, M = a.g.M;
     const SelectionParams sel = a.sel;
     // one thread per (row, pixel pair): the selection mask is evaluated once
-    // per pixel and feeds every driver plane
-#pragma unroll 2
-    for (int i = threadIdx.x; i < RPC * M; i += blockDim.x) {
-        const int r = i / M;
-        const int idx = i - r * M;
-        const int y = y0 + r;
-        const int x0 = 2 * idx;
-        float2 v[NDRV];
+    // per pixel and feeds every driver plane.  kU pairs per thread are loaded
+    // before any is used, so enough source reads are in flight to cover HBM
+    // latency at one CTA per SM.
+    constexpr int kU = 4;
+    const int T = blockDim.x;
+    for (int i0 = threadIdx.x; i0 < RPC * M; i0 += kU * T) {
+        float4 px[kU][2];
 #pragma unroll
-        for (int d = 0; d < NDRV; ++d) v[d] = make_float2(0.0f, 0.0f);
-        if (y < H) {
+        for (int u = 0; u < kU; ++u) {
+            const int i = i0 + u * T;
+            const int r = i / M;
+            const int idx = i - r * M;
+            const int y = y0 + r;
+            const int x0 = 2 * idx;
             const unsigned char* row = a.src + static_cast<int64_t>(y) * pitch;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (x0 + h < W) {
-                    const float4 p = load_px(row, x0 + h, aligned);
-                    float sig;
-                    const float m = selection_mask(sel, p.x, p.y, p.z, &sig) * sel.rscale;
-                    if (NDRV == 1) {
-                        const float dv = sig * m;
-                        if (h == 0) v[0].x = dv;
-                        else v[0].y = dv;
-                    } else {
-                        const float c3[3] = {p.x * m, p.y * m, p.z * m};
+            for (int h = 0; h < 2; ++h)
+                px[u][h] = (i < RPC * M && y < H && x0 + h < W) ? load_px(row, x0 + h, aligned)
+                                                                 : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
 #pragma unroll
-                        for (int d = 0; d < NDRV; ++d) {
-                            if (h == 0) v[d].x = c3[d];
-                            else v[d].y = c3[d];
-                        }
+        for (int u = 0; u < kU; ++u) {
+            const int i = i0 + u * T;
+            if (i >= RPC * M) break;
+            const int r = i / M;
+            const int idx = i - r * M;
+            float2 v[NDRV];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const float4 p = px[u][h];
+                float sig;
+                // zero pixels (outside the frame or black) give a zero driver
+                const float m = selection_mask(sel, p.x, p.y, p.z, &sig) * sel.rscale;
+                if (NDRV == 1) {
+                    const float dv = sig * m;
+                    if (h == 0) v[0].x = dv;
+                    else v[0].y = dv;
+                } else {
+                    const float c3[3] = {p.x * m, p.y * m, p.z * m};
+#pragma unroll
+                    for (int d = 0; d < NDRV; ++d) {
+                        if (h == 0) v[d].x = c3[d];
+                        else v[d].y = c3[d];
                     }
                 }
             }
-        }
 #pragma unroll
-        for (int d = 0; d < NDRV; ++d) smem[idx * C + r * NDRV + d] = v[d];
+            for (int d = 0; d < NDRV; ++d) smem[idx * C + r * NDRV + d] = v[d];
+        }
     }
     __syncthreads();
     fft_run<E, C, false>(a.g.plan_m, smem);
@@ -267,7 +281,7 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_inverse_kernel(F
         // kU entries per thread in flight: the bin reads are scattered (one
         // C * 8-byte run per bin), so their latency is hidden by issuing a
         // batch of them before the first is used
-        constexpr int kU = 4;
+        constexpr int kU = 8;
         const int T = blockDim.x;
         for (int i0 = threadIdx.x; i0 < M * C; i0 += kU * T) {
             float2 xk[kU], xm[kU], w[kU];
@@ -327,13 +341,25 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_inverse_kernel(F
     }
     const bool aligned_d = ((reinterpret_cast<uintptr_t>(a.dst) | static_cast<uintptr_t>(a.dst_pitch)) & 15) == 0;
     unsigned char* drow = a.dst + static_cast<int64_t>(yo - a.dst_y1) * a.dst_pitch;
-#pragma unroll 2
-    for (int x = a.out_x1 + threadIdx.x; x < a.out_x2; x += blockDim.x) {
-        float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-        const int sx = x - a.src_x1;
-        if (have && sx >= 0 && sx < a.W)
-            out = composite_px(a, load_px(srow, sx, aligned_s), mapped_effect<C>(a, smem, sx));
-        store_px(drow, x - a.dst_x1, aligned_d, out);
+    constexpr int kV = 4;  // source pixels loaded ahead of use, per thread
+    const int T = blockDim.x;
+    for (int x0 = a.out_x1 + threadIdx.x; x0 < a.out_x2; x0 += kV * T) {
+        float4 px[kV];
+#pragma unroll
+        for (int u = 0; u < kV; ++u) {
+            const int sx = x0 + u * T - a.src_x1;
+            px[u] = (have && x0 + u * T < a.out_x2 && sx >= 0 && sx < a.W) ? load_px(srow, sx, aligned_s)
+                                                                           : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        }
+#pragma unroll
+        for (int u = 0; u < kV; ++u) {
+            const int x = x0 + u * T;
+            if (x >= a.out_x2) break;
+            const int sx = x - a.src_x1;
+            float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            if (have && sx >= 0 && sx < a.W) out = composite_px(a, px[u], mapped_effect<C>(a, smem, sx));
+            store_px(drow, x - a.dst_x1, aligned_d, out);
+        }
     }
 }
 
