@@ -76,8 +76,8 @@ __device__ __forceinline__ void store_bins(int M, int C, int64_t col_elems, int6
 // Mono (NDRV = 3): C = 3, one frame row per CTA, its three colour drivers.
 // Column col of the transform is row y0 + col / NDRV, driver col % NDRV; its
 // spectrum goes to A[k][y0 + col / NDRV][col % NDRV].
-template <int E, int C, int NDRV>
-__global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_rows_kernel(FrameArgs a) {
+template <int E, int C, int NDRV, int MAXT = Fam<E>::max_threads, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
     extern __shared__ float2 smem[];
     constexpr int RPC = C / NDRV;  // frame rows per CTA
     const int y0 = blockIdx.x * RPC;
@@ -147,8 +147,8 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_rows_kernel(Fram
 // Wk [Py][NOUT] (the column's NOUT kernel spectra land here, are multiplied by
 // F in place and inverse-transformed together as NOUT interleaved sequences),
 // two mbarriers.  The first Hp rows of Wk go to B with one bulk store.
-template <int E, int NOUT>
-__global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_cols_kernel(FrameArgs a) {
+template <int E, int NOUT, int MAXT = Fam<E>::max_threads, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) frame_cols_kernel(FrameArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const int Py = a.g.Py, Hp = a.Hp, cols = a.g.cols;
     const int k = blockIdx.x;
@@ -265,8 +265,8 @@ __device__ __forceinline__ float zone_weight(int v, int extent, int z, int n) {
 // row is output row out_y1 + blockIdx.x (kEffectComposite), source row
 // blockIdx.x (kEffectStore) or source row row0 + blockIdx.x
 // (kEffectAccumulate); see FrameArgs::effect_mode.
-template <int E, int C>
-__global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_inverse_kernel(FrameArgs a) {
+template <int E, int C, int MAXT = Fam<E>::max_threads, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) {
     extern __shared__ float2 smem[];
     const int bid = static_cast<int>(blockIdx.x);
     const int yo = a.effect_mode == kEffectComposite ? a.out_y1 + bid
@@ -446,8 +446,8 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) kspec_rows_kernel(Kern
 // copy; the wrap map places canvas row ci at grid row v and folds in the
 // inverse scale; the transformed column KS[k] (Py x C, contiguous) leaves by
 // one bulk store.
-template <int E, int C>
-__global__ void __launch_bounds__(Fam<E>::max_threads, 1) kspec_cols_kernel(KernelSpectraArgs a) {
+template <int E, int C, int MAXT = Fam<E>::max_threads, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) kspec_cols_kernel(KernelSpectraArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const int Py = a.g.Py, cols = a.g.cols, Kp = a.Kp, R = a.R;
     const int k = blockIdx.x;
@@ -508,8 +508,15 @@ template <int E>
 void rows_e(const FrameArgs& a, cudaStream_t s) {
     const int M = a.g.M;
     if (a.n_drv == 1) {
-        const size_t sm = static_cast<size_t>(M) * 4 * sizeof(float2);
-        frame_rows_kernel<E, 4, 1><<<a.Hp / 4, fft_threads(M, 4, E), sm, s>>>(a);
+        // two rows per CTA and three CTAs per SM (register cap 80) when the
+        // transform fits 224 threads; else four rows per CTA
+        if (fft_threads(M, 2, E) <= 224) {
+            const size_t sm = static_cast<size_t>(M) * 2 * sizeof(float2);
+            frame_rows_kernel<E, 2, 1, 224, 3><<<a.Hp / 2, fft_threads(M, 2, E), sm, s>>>(a);
+        } else {
+            const size_t sm = static_cast<size_t>(M) * 4 * sizeof(float2);
+            frame_rows_kernel<E, 4, 1><<<a.Hp / 4, fft_threads(M, 4, E), sm, s>>>(a);
+        }
     } else {
         const size_t sm = static_cast<size_t>(M) * 3 * sizeof(float2);
         frame_rows_kernel<E, 3, 3><<<a.Hp, fft_threads(M, 3, E), sm, s>>>(a);
@@ -523,14 +530,25 @@ void cols_launch(Kern f, FrameArgs a, int C, size_t sm, cudaStream_t s) {
     f<<<a.g.cols, T, sm, s>>>(a);
 }
 
+// Spectral column pass: two CTAs per SM (register cap 85) when the transform
+// fits 384 threads and two working sets fit shared memory.
+template <int E, int NOUT>
+void cols_spectral(const FrameArgs& a, cudaStream_t s) {
+    const size_t sm = frame_cols_smem(a.g.Py, NOUT);
+    if (fft_threads(a.g.Py, NOUT, E) <= 384 && 2 * sm + 2048 <= static_cast<size_t>(kMaxSmem))
+        cols_launch<E>(frame_cols_kernel<E, NOUT, 384, 2>, a, NOUT, sm, s);
+    else
+        cols_launch<E>(frame_cols_kernel<E, NOUT>, a, NOUT, sm, s);
+}
+
 template <int E>
 void cols_e(const FrameArgs& a, cudaStream_t s) {
     if (a.n_drv == 3) {
         cols_launch<E>(frame_cols_mono_kernel<E>, a, 3, frame_cols_smem(a.g.Py, 0), s);
     } else if (a.n_out == 4) {
-        cols_launch<E>(frame_cols_kernel<E, 4>, a, 4, frame_cols_smem(a.g.Py, 4), s);
+        cols_spectral<E, 4>(a, s);
     } else {
-        cols_launch<E>(frame_cols_kernel<E, 3>, a, 3, frame_cols_smem(a.g.Py, 3), s);
+        cols_spectral<E, 3>(a, s);
     }
 }
 
@@ -538,9 +556,16 @@ template <int E>
 void inverse_e(const FrameArgs& a, int rows, cudaStream_t s) {  // rows: grid size
     const int M = a.g.M;
     if (a.n_out == 4) {
-        frame_inverse_kernel<E, 4><<<rows, fft_threads(M, 4, E), static_cast<size_t>(M) * 4 * sizeof(float2), s>>>(a);
+        const int T = fft_threads(M, 4, E);
+        const size_t sm = static_cast<size_t>(M) * 4 * sizeof(float2);
+        if (T <= 320) frame_inverse_kernel<E, 4, 320, 2><<<rows, T, sm, s>>>(a);
+        else frame_inverse_kernel<E, 4><<<rows, T, sm, s>>>(a);
     } else {
-        frame_inverse_kernel<E, 3><<<rows, fft_threads(M, 3, E), static_cast<size_t>(M) * 3 * sizeof(float2), s>>>(a);
+        const int T = fft_threads(M, 3, E);
+        const size_t sm = static_cast<size_t>(M) * 3 * sizeof(float2);
+        // two CTAs per SM when the transform fits 320 threads (register cap 102)
+        if (T <= 320) frame_inverse_kernel<E, 3, 320, 2><<<rows, T, sm, s>>>(a);
+        else frame_inverse_kernel<E, 3><<<rows, T, sm, s>>>(a);
     }
 }
 
@@ -554,8 +579,16 @@ template <int E, int C>
 void kspec_cols_c(KernelSpectraArgs a, cudaStream_t s) {
     const int T = fft_threads(a.g.Py, C, E);
     const size_t sm = kspec_cols_smem(a.g.Py, a.Kp, C);
-    a.ahead = resident_ctas(kspec_cols_kernel<E, C>, T, sm);
-    kspec_cols_kernel<E, C><<<a.g.cols, T, sm, s>>>(a);
+    if (C > 1 && T <= 384 && 2 * sm + 2048 <= static_cast<size_t>(kMaxSmem)) {  // C == 1: Mono, one kernel
+        // two CTAs per SM (register cap 80)
+        auto f = kspec_cols_kernel<E, C, 384, 2>;
+        a.ahead = resident_ctas(f, T, sm);
+        f<<<a.g.cols, T, sm, s>>>(a);
+    } else {
+        auto f = kspec_cols_kernel<E, C>;
+        a.ahead = resident_ctas(f, T, sm);
+        f<<<a.g.cols, T, sm, s>>>(a);
+    }
 }
 
 template <int E>
@@ -581,6 +614,13 @@ void configure_e() {
     set_smem(frame_cols_mono_kernel<E>);
     set_smem(frame_inverse_kernel<E, 3>);
     set_smem(frame_inverse_kernel<E, 4>);
+    set_smem(frame_inverse_kernel<E, 3, 320, 2>);
+    set_smem(frame_cols_kernel<E, 3, 384, 2>);
+    set_smem(frame_cols_kernel<E, 4, 384, 2>);
+    set_smem(frame_rows_kernel<E, 2, 1, 224, 3>);
+    set_smem(kspec_cols_kernel<E, 3, 384, 2>);
+    set_smem(kspec_cols_kernel<E, 4, 384, 2>);
+    set_smem(frame_inverse_kernel<E, 4, 320, 2>);
     set_smem(kspec_rows_kernel<E, 1>);
     set_smem(kspec_rows_kernel<E, 3>);
     set_smem(kspec_rows_kernel<E, 4>);
