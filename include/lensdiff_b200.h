@@ -266,6 +266,41 @@ int ld_export_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream,
 int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index,
                float* psf_out_device, void* stream, ld_status* status);
 
+/* ---- device memory estimate ------------------------------------------------------
+ * Upper estimate of the device bytes one context grows to for rendering a
+ * width x height frame with these parameters (PSF bank, kernel spectra, frame
+ * work buffers; field zones counted); used for HBM admission.  No counterpart
+ * in the reference (it allocates per call). */
+size_t ld_estimate_device_bytes(const ld_params* params, int32_t width, int32_t height);
+
+/* ---- frame serving with continuous batching ----------------------------------------
+ * No counterpart in the reference (it renders one frame per host call,
+ * LensDiff.cpp:3833).  A server keeps `slots` contexts, each with its own
+ * stream, device PSF-bank cache and worker thread, on one GPU.  Submitted
+ * frames (host RGBA float32, width x height, rows packed) wait in FIFO order
+ * and start the moment a slot is free and the HBM budget (0: none) allows;
+ * frames with the same lens parameters go to the slot that has them cached.
+ * Host buffers must stay valid until ld_server_wait returns for the ticket. */
+typedef struct ld_server ld_server;
+
+typedef struct ld_server_stats {
+    uint64_t completed, pending, cache_hits, max_concurrent;
+    double p50_ms, p99_ms, mean_ms;   /* submit -> result on the host */
+    double frames_per_s;              /* completed / (first submit -> last completion) */
+    size_t device_bytes, reserved_bytes;
+} ld_server_stats;
+
+int ld_server_create(ld_server** out, int device, int slots, size_t hbm_budget_bytes);
+void ld_server_destroy(ld_server* server);
+int ld_server_submit(ld_server* server, const float* src_host, float* dst_host, int32_t width, int32_t height,
+                     const ld_params* params, uint64_t* ticket);
+/* Waits up to timeout_s for the frame; LD_ERR_TIMEOUT if it is not done (the
+ * ticket stays valid), else the frame's status code (the ticket is released). */
+int ld_server_wait(ld_server* server, uint64_t ticket, double timeout_s, ld_status* status, double* latency_ms);
+int ld_server_get_stats(ld_server* server, ld_server_stats* out);
+void ld_server_reset_stats(ld_server* server);
+
+
 /* Same output as ld_raw_psf, for callers that cannot allocate device memory
  * (an OpenFX host that owns and budgets all GPU memory, a real-time thread
  * that must not take cudaMalloc's implicit synchronisation, a fixed memory

@@ -305,7 +305,23 @@ EXPORTED_SYMBOLS = [
     "ld_gaussian_rgb_matrix",
     "ld_set_profiling",
     "ld_profile_collect",
+    "ld_estimate_device_bytes",
+    "ld_server_create",
+    "ld_server_destroy",
+    "ld_server_submit",
+    "ld_server_wait",
+    "ld_server_get_stats",
+    "ld_server_reset_stats",
 ]
+
+
+class ld_server_stats(ctypes.Structure):
+    _fields_ = [
+        ("completed", ctypes.c_uint64), ("pending", ctypes.c_uint64), ("cache_hits", ctypes.c_uint64),
+        ("max_concurrent", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+        ("mean_ms", ctypes.c_double), ("frames_per_s", ctypes.c_double), ("device_bytes", ctypes.c_size_t),
+        ("reserved_bytes", ctypes.c_size_t),
+    ]
 
 STAGE_NAMES = ["psf_rows", "psf_cols", "resample", "shape_stats", "support", "crop_sum", "combine",
                "kspec_rows", "kspec_cols", "frame_rows", "frame_cols", "frame_inverse", "pupil", "composite"]
@@ -360,6 +376,22 @@ def lib() -> ctypes.CDLL:
     L.ld_set_profiling.restype = ctypes.c_int
     L.ld_profile_collect.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_i32), c_i32]
     L.ld_profile_collect.restype = ctypes.c_int
+    L.ld_estimate_device_bytes.argtypes = [ctypes.POINTER(ld_params), c_i32, c_i32]
+    L.ld_estimate_device_bytes.restype = ctypes.c_size_t
+    L.ld_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_size_t]
+    L.ld_server_create.restype = ctypes.c_int
+    L.ld_server_destroy.argtypes = [vp]
+    L.ld_server_destroy.restype = None
+    L.ld_server_submit.argtypes = [vp, vp, vp, c_i32, c_i32, ctypes.POINTER(ld_params),
+                                   ctypes.POINTER(ctypes.c_uint64)]
+    L.ld_server_submit.restype = ctypes.c_int
+    L.ld_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(ld_status),
+                                 ctypes.POINTER(ctypes.c_double)]
+    L.ld_server_wait.restype = ctypes.c_int
+    L.ld_server_get_stats.argtypes = [vp, ctypes.POINTER(ld_server_stats)]
+    L.ld_server_get_stats.restype = ctypes.c_int
+    L.ld_server_reset_stats.argtypes = [vp]
+    L.ld_server_reset_stats.restype = None
     if L.ld_abi_version() != 1:
         raise RuntimeError("liblensdiff_b200.so ABI version mismatch")
     _LIB = L
@@ -373,5 +405,5 @@ def is_spectral(p: LensDiffParams) -> bool:
 
 __all__ = [
     "ld_rect", "ld_image_view", "ld_render_request", "ld_params", "ld_status",
-    "to_abi_params", "lib", "LIB_PATH", "EXPORTED_SYMBOLS", "LensDiffRgbMode",
+    "to_abi_params", "lib", "LIB_PATH", "EXPORTED_SYMBOLS", "LensDiffRgbMode", "ld_server_stats",
 ]

@@ -774,16 +774,16 @@ int fft_passes(int n, bool allow25) {
     return factor_radices(n, allow25, &r) ? static_cast<int>(r.size()) : 1000;
 }
 
-// Cheapest 5-smooth length >= n (a multiple of `mult`) for up to C = 4
+// Cheapest 5-smooth length >= n (a multiple of `mult`) for up to C
 // interleaved sequences: cost ~ m * (stages + 1.5), the stage passes plus the
 // fill and drain, so a slightly longer length with fewer stages can win.
-int choose_length(int n, int mult) {
+int choose_length(int n, int mult, int C) {
     int best = -1;
     double best_cost = 0.0;
     const int hi = n + std::max(64, n / 10);
     for (int m = std::max(n, 2); m <= hi; ++m) {
         if (m % mult != 0 || !smooth(m)) continue;
-        const int fam = fft_family(m, 4);
+        const int fam = fft_family(m, C);
         if (fam == 0) continue;
         const double cost = static_cast<double>(m) * (fft_passes(m, fam == kE25) + 1.5);
         if (best < 0 || cost < best_cost) {
@@ -797,21 +797,22 @@ int choose_length(int n, int mult) {
 // 5-smooth grid covering the linear convolution: Px = 2M with M the row
 // transform length, Py even (16-byte bulk-copy sizes).  The reference pads to
 // powers of two (LensDiffCpuReference.cpp:1172-1173); any grid of at least
-// W+K-1 x H+K-1 gives the same linear convolution.
-GridGeom make_geometry(ld_ctx* c, int W, int H, int K, int n_drv, int* req_w, int* req_h) {
-    (void)n_drv;
+// W+K-1 x H+K-1 gives the same linear convolution.  c_rows / c_cols: the
+// most interleaved sequences any row / column kernel of the chain transforms
+// (they pick the FFT family).
+GridGeom make_geometry(ld_ctx* c, int W, int H, int K, int c_rows, int c_cols, int* req_w, int* req_h) {
     GridGeom g{};
     *req_w = W + K - 1;
     *req_h = H + K - 1;
-    g.M = choose_length((*req_w + 1) / 2, 1);
-    g.Py = choose_length(*req_h, 2);
+    g.M = choose_length((*req_w + 1) / 2, 1, c_rows);
+    g.Py = choose_length(*req_h, 2, c_cols);
     if (g.M < 0 || g.Py < 0) throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-fft-grid"};
     g.Px = 2 * g.M;
     g.cols = g.M + 1;
-    g.fam_m = fft_family(g.M, 4);
-    g.fam_py = fft_family(g.Py, 4);
+    g.fam_m = fft_family(g.M, c_rows);
+    g.fam_py = fft_family(g.Py, c_cols);
     const int Kp = K + (K & 1);
-    if (frame_cols_smem(g.Py, 4) > kSmemBudget || kspec_cols_smem(g.Py, Kp, 4) > kSmemBudget)
+    if (frame_cols_smem(g.Py, c_cols) > kSmemBudget || kspec_cols_smem(g.Py, Kp, c_cols) > kSmemBudget)
         throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-column-pass"};
     g.plan_m = make_plan(c, g.M, g.fam_m == kE25);
     g.plan_py = make_plan(c, g.Py, g.fam_py == kE25);
@@ -1064,6 +1065,45 @@ int ld_gaussian_rgb_matrix(const float* wl, int32_t count, const float* center, 
     return LD_OK;
 }
 
+size_t ld_estimate_device_bytes(const ld_params* params, int32_t width, int32_t height) {
+    if (!params || width <= 0 || height <= 0) return 0;
+    try {
+        const ld_params& p = *params;
+        const size_t np = pupil_size(p), R = max_kernel_radius(p);
+        const size_t S = raw_psf_size(static_cast<int>(np), static_cast<int>(R));
+        const size_t K = 2 * R + 1, Kp = K + (K & 1);
+        const size_t B = wavelengths_of(p).size();
+        const Combination cb = make_combination(p, wavelengths_of(p));
+        const int c_rows = std::max(std::max(cb.n_drv == 1 ? 4 : 3, cb.n_out), cb.n_ker);
+        const int c_cols = std::max(std::max(cb.n_out, cb.n_ker), cb.n_drv);
+        const int M = choose_length((width + static_cast<int>(K) - 1 + 1) / 2, 1, c_rows);
+        const int Py = choose_length(height + static_cast<int>(K) - 1, 2, c_cols);
+        if (M < 0 || Py < 0) return 0;
+        const size_t cols = static_cast<size_t>(M) + 1, Hp = (static_cast<size_t>(height) + 3) & ~size_t(3);
+        const size_t zones = has_field_phase(p) ? static_cast<size_t>(p.field_grid > 0 ? p.field_grid : 3) *
+                                                      (p.field_grid > 0 ? p.field_grid : 3)
+                                                : 1;
+        size_t t = 0;
+        t += np * np * 16;                              // pupil pre-pass
+        t += B * np * S * 8 + B * S * S * 4;            // row spectra + |F|^2 windows (window <= S)
+        t += 2 * S * S * 4;                             // calibration PSF
+        t += B * K * K * 4 + B * (R + 1) * 24;          // canvases + ring statistics
+        t += static_cast<size_t>(cb.n_ker) * K * K * 4; // combined kernels
+        t += static_cast<size_t>(cb.n_ker) * cols * Kp * 8;                 // kernel row spectra
+        t += zones * static_cast<size_t>(cb.n_ker) * cols * Py * 8;         // kernel spectra
+        t += static_cast<size_t>(cb.n_drv + cb.n_out) * cols * Hp * 8;      // frame A, B
+        if (zones > 1 || p.energy_mode == LD_ENERGY_PRESERVE) t += static_cast<size_t>(width) * height * 16;
+        if (p.fft_form == LD_FFT_CUFFT) {
+            const size_t P = static_cast<size_t>(2 * M) * Py, half = static_cast<size_t>(Py) * (M + 1);
+            t += cf_psf_chunk(static_cast<int>(S), static_cast<int>(B)) * S * S * 8;
+            t += std::max(cb.n_drv, cb.n_out) * P * 4 + (cb.n_drv + cb.n_out) * half * 8;
+        }
+        return t + (size_t(16) << 20);  // twiddles, plans, scalars
+    } catch (...) {
+        return 0;
+    }
+}
+
 int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params, ld_status* st) {
     if (st) std::memset(st, 0, sizeof(*st));
     if (!ctx || !rq || !params) {
@@ -1097,7 +1137,9 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         const std::vector<float> wl = wavelengths_of(p);
         const Combination cb = make_combination(p, wl);
         int rw = 0, rh = 0;
-        const GridGeom g = make_geometry(ctx, W, H, 2 * max_kernel_radius(p) + 1, cb.n_drv, &rw, &rh);
+        const int c_rows = std::max(std::max(cb.n_drv == 1 ? 4 : 3, cb.n_out), cb.n_ker);
+        const int c_cols = std::max(std::max(cb.n_out, cb.n_ker), cb.n_drv);
+        const GridGeom g = make_geometry(ctx, W, H, 2 * max_kernel_radius(p) + 1, c_rows, c_cols, &rw, &rh);
         std::vector<const SpectraEntry*> spectra;
         if (zones) {
             spectra = ensure_zone_spectra(ctx, p, zn, cb, g, s, &bank_rebuilt, &spectra_rebuilt);
