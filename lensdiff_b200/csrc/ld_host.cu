@@ -48,6 +48,7 @@ struct BankEntry {
 
 struct SpectraEntry {
     bool valid = false;
+    uint64_t last_use = 0;
     std::string key;
     DevBuf spectra;
     GridGeom g{};
@@ -68,6 +69,11 @@ struct ld_ctx {
     BankEntry bank;
     SpectraEntry spectra;
     std::vector<SpectraEntry> zone_spectra;  // field zones, zy * n + zx
+    // kernel spectra of recent (lens, frame size) pairs, least recently used
+    // replaced first: a context serving one lens at several frame sizes keeps
+    // them all without rebuilding the bank
+    std::vector<SpectraEntry> spectra_lru;
+    uint64_t spectra_clock = 0;
     // work buffers, grown on demand
     DevBuf rows, win, combine_out, kspec_rows, frameA, frameB, calib, calib_psf, pupil_pre, effect;
     // comparator form (cuFFT): plans and its own work buffers
@@ -872,9 +878,32 @@ SpectraEntry& ensure_spectra_in(ld_ctx* c, SpectraEntry& e, BankEntry& b, const 
     return e;
 }
 
-SpectraEntry& ensure_spectra(ld_ctx* c, BankEntry& b, const Combination& cb, const GridGeom& g, cudaStream_t s,
-                             bool* rebuilt) {
-    return ensure_spectra_in(c, c->spectra, b, cb, g, s, rebuilt);
+constexpr size_t kSpectraCache = 4;
+
+// Kernel spectra for (lens p, geometry g) from the context's LRU cache; the
+// bank is built (or reused) only on a miss.
+SpectraEntry& cached_spectra(ld_ctx* c, const ld_params& p, const Combination& cb, const GridGeom& g, cudaStream_t s,
+                             bool* bank_rebuilt, bool* spectra_rebuilt) {
+    const std::string key = spectra_key_for(bank_key(p, wavelengths_of(p)), cb, g);
+    for (auto& e : c->spectra_lru) {
+        if (e.valid && e.key == key) {
+            e.last_use = ++c->spectra_clock;
+            return e;
+        }
+    }
+    if (c->spectra_lru.size() < kSpectraCache) c->spectra_lru.emplace_back();
+    SpectraEntry* victim = &c->spectra_lru.front();
+    for (auto& e : c->spectra_lru) {
+        if (!e.valid) {
+            victim = &e;
+            break;
+        }
+        if (e.last_use < victim->last_use) victim = &e;
+    }
+    BankEntry& b = ensure_bank(c, p, s, bank_rebuilt);
+    ensure_spectra_in(c, *victim, b, cb, g, s, spectra_rebuilt);
+    victim->last_use = ++c->spectra_clock;
+    return *victim;
 }
 
 // Field zones: the kernel spectra of every zone of an n x n grid, in the
@@ -1003,6 +1032,7 @@ void ld_destroy(ld_ctx* c) {
                     &c->bank.scalars, &c->bank.wl,        &c->spectra.spectra};
     for (DevBuf* b : bb) free_buf(c, *b);
     for (auto& z : c->zone_spectra) free_buf(c, z.spectra);
+    for (auto& z : c->spectra_lru) free_buf(c, z.spectra);
     delete c;
 }
 
@@ -1047,6 +1077,7 @@ void ld_clear_caches(ld_ctx* c) {
     c->bank.valid = false;
     c->spectra.valid = false;
     for (auto& z : c->zone_spectra) z.valid = false;
+    for (auto& z : c->spectra_lru) z.valid = false;
 }
 
 int ld_resolve_sizes(const ld_params* p, int32_t* np, int32_t* S, int32_t* R, int32_t* B) {
@@ -1144,8 +1175,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         if (zones) {
             spectra = ensure_zone_spectra(ctx, p, zn, cb, g, s, &bank_rebuilt, &spectra_rebuilt);
         } else {
-            BankEntry& bank = ensure_bank(ctx, p, s, &bank_rebuilt);
-            spectra.push_back(&ensure_spectra(ctx, bank, cb, g, s, &spectra_rebuilt));
+            spectra.push_back(&cached_spectra(ctx, p, cb, g, s, &bank_rebuilt, &spectra_rebuilt));
         }
         const SpectraEntry& sp = *spectra.front();
 

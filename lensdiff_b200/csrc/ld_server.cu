@@ -224,6 +224,8 @@ void worker(ld_server* s, Slot* sl) {
             j->latency_ms = std::chrono::duration<double, std::milli>(now - j->submitted).count();
             j->done = true;
             sl->lens = j->status.code == LD_OK ? j->lens : std::string();
+            // what the slot really holds now (caches included) counts from here on
+            sl->reserved = std::max(sl->reserved, ld_device_bytes(sl->ctx) + 2 * sl->frame_bytes);
             sl->job.reset();
             sl->busy = false;
             if (j->status.code == LD_OK) {
