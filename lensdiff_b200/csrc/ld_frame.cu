@@ -57,6 +57,25 @@ __device__ __forceinline__ float2 c2r_pre(float2 xk, float2 xmk, float2 wk) {
     return make_float2(e.x - o.y, e.y + o.x);
 }
 
+// Column-pass outputs B are grouped four spectrum columns at a time,
+// B[k / 4][row][k % 4][c]: a column writes 24- or 32-byte runs four apart
+// (the four columns of a group run together and their partial sectors merge
+// in L2), and a row of the inverse pass reads one aligned run of
+// 4 * C * 8 bytes per group instead of C * 8 bytes per column.
+constexpr int kBGroup = 4;
+__device__ __forceinline__ int64_t b_index(int k, int row, int c, int Hp, int C) {
+    return ((static_cast<int64_t>(k / kBGroup) * Hp + row) * kBGroup + (k % kBGroup)) * C + c;
+}
+
+// Writes a transformed column (rows [0, Hp) of s[row * C + c]) to B.
+__device__ __forceinline__ void store_b_column(const float2* s, float2* B, int k, int Hp, int C) {
+    for (int i = threadIdx.x; i < Hp * C; i += blockDim.x) {
+        const int row = i / C;
+        const int c = i - row * C;
+        B[b_index(k, row, c, Hp, C)] = s[i];
+    }
+}
+
 // Writes the M+1 bins of the C transformed sequences in smem (s[k*C + col])
 // to a column-major array: bin k of sequence col goes to
 // out[k * col_elems + base + col].  Consecutive threads write consecutive
@@ -180,15 +199,7 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_cols_kernel(FrameArgs a) {
     for (int i = threadIdx.x; i < Py * NOUT; i += blockDim.x) Wk[i] = cmul(Wk[i], F[i / NOUT]);
     __syncthreads();
     fft_run<E, NOUT, true>(a.g.plan_py, Wk);
-    fence_proxy_async_smem();
-    __syncthreads();
-    const uint32_t b_bytes = static_cast<uint32_t>(static_cast<size_t>(Hp) * NOUT * sizeof(float2));
-    float2* bdst = a.Bout + static_cast<size_t>(k) * Hp * NOUT;
-    if (lead && bulk_args_ok(bdst, Wk, b_bytes, smraw, a.err)) {
-        bulk_copy_s2g(bdst, Wk, b_bytes);
-        bulk_commit();
-        bulk_wait_read();
-    }
+    store_b_column(Wk, a.Bout, k, Hp, NOUT);
 }
 
 // ---- column pass, Mono: three colour drivers, one kernel spectrum -------------------
@@ -228,14 +239,7 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) frame_cols_mono_kernel
     for (int i = threadIdx.x; i < Py * 3; i += blockDim.x) X[i] = cmul(X[i], Kc[i / 3]);
     __syncthreads();
     fft_run<E, 3, true>(a.g.plan_py, X);
-    fence_proxy_async_smem();
-    __syncthreads();
-    float2* bdst = a.Bout + static_cast<size_t>(k) * Hp * 3;
-    if (lead && bulk_args_ok(bdst, X, a_bytes, smraw, a.err)) {
-        bulk_copy_s2g(bdst, X, a_bytes);
-        bulk_commit();
-        bulk_wait_read();
-    }
+    store_b_column(X, a.Bout, k, Hp, 3);
 }
 
 // ---- inverse rows + spectral map + composite ----------------------------------------
@@ -276,30 +280,38 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
     const int M = a.g.M;
     if (have) {
         const float2* tw_px = a.g.tw_px;
-        const int64_t col_elems = static_cast<int64_t>(a.Hp) * C;
-        const float2* rowp = a.Bout + static_cast<int64_t>(sy) * C;
-        // kU entries per thread in flight: the bin reads are scattered (one
-        // C * 8-byte run per bin), so their latency is hidden by issuing a
-        // batch of them before the first is used
-        constexpr int kU = 8;
+        // Hermitian pairs: one load of X[p] and X[M-p] per channel gives both
+        // Z[p] and Z[M-p] (p = 0 pairs with the Nyquist bin M and gives Z[0]
+        // only; p = M/2 pairs with itself).  kU pairs per thread are loaded
+        // before any is used: the reads are scattered, one run per bin group.
+        const int Hp = a.Hp;
+        const int half = M / 2;
+        const int npair = (half + 1) * C;
+        constexpr int kU = 4;
         const int T = blockDim.x;
-        for (int i0 = threadIdx.x; i0 < M * C; i0 += kU * T) {
-            float2 xk[kU], xm[kU], w[kU];
+        for (int i0 = threadIdx.x; i0 < npair; i0 += kU * T) {
+            float2 xp[kU], xq[kU], wp[kU], wq[kU];
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 const int i = i0 + u * T;
-                if (i < M * C) {
-                    const int k = i / C;
-                    const int col = i - k * C;
-                    xk[u] = __ldcs(&rowp[k * col_elems + col]);
-                    xm[u] = __ldcs(&rowp[(M - k) * col_elems + col]);
-                    w[u] = __ldg(&tw_px[k]);
+                if (i < npair) {
+                    const int pk = i / C;
+                    const int c = i - pk * C;
+                    xp[u] = __ldcs(&a.Bout[b_index(pk, sy, c, Hp, C)]);
+                    xq[u] = __ldcs(&a.Bout[b_index(M - pk, sy, c, Hp, C)]);
+                    wp[u] = __ldg(&tw_px[pk]);
+                    wq[u] = __ldg(&tw_px[M - pk]);
                 }
             }
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 const int i = i0 + u * T;
-                if (i < M * C) smem[i] = c2r_pre(xk[u], xm[u], w[u]);
+                if (i < npair) {
+                    const int pk = i / C;
+                    const int c = i - pk * C;
+                    if (pk < M) smem[pk * C + c] = c2r_pre(xp[u], xq[u], wp[u]);
+                    if (pk > 0 && M - pk != pk && M - pk < M) smem[(M - pk) * C + c] = c2r_pre(xq[u], xp[u], wq[u]);
+                }
             }
         }
         __syncthreads();

@@ -236,12 +236,6 @@ bool smooth(int n) {
     return n == 1;
 }
 
-int next_smooth(int n, bool even) {
-    int m = std::max(n, 2);
-    while (!(smooth(m) && (!even || (m % 2 == 0)))) ++m;
-    return m;
-}
-
 const float2* twiddles(ld_ctx* c, int n) {
     auto it = c->twiddles.find(n);
     if (it != c->twiddles.end()) return static_cast<const float2*>(it->second.p);
@@ -826,12 +820,6 @@ GridGeom make_geometry(ld_ctx* c, int W, int H, int K, int c_rows, int c_cols, i
     return g;
 }
 
-int sm_count(int device) {
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    return sms;
-}
-
 // Kernel spectra of bank `b` into entry `e` (combination, row and column
 // transforms), unless `e` already holds them.
 SpectraEntry& ensure_spectra_in(ld_ctx* c, SpectraEntry& e, BankEntry& b, const Combination& cb, const GridGeom& g,
@@ -1217,8 +1205,10 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         fa.Hp = (H + 3) & ~3;
         fa.A = static_cast<float2*>(
             ensure(ctx, ctx->frameA, static_cast<size_t>(cb.n_drv) * g.cols * fa.Hp * sizeof(float2)));
+        // column outputs in groups of four columns (ld_frame.cu b_index)
+        const size_t bcols = (static_cast<size_t>(g.cols) + 3) / 4 * 4;
         fa.Bout = static_cast<float2*>(
-            ensure(ctx, ctx->frameB, static_cast<size_t>(cb.n_out) * g.cols * fa.Hp * sizeof(float2)));
+            ensure(ctx, ctx->frameB, static_cast<size_t>(cb.n_out) * bcols * fa.Hp * sizeof(float2)));
         fa.spectra = static_cast<const float2*>(sp.spectra.p);
         fa.err = ctx->err;
         fa.effect_mode = zones ? kEffectAccumulate : (fa.preserve ? kEffectStore : kEffectComposite);
