@@ -234,6 +234,13 @@ enum {
     LD_STAGE_KSPEC_COLS, LD_STAGE_FRAME_ROWS, LD_STAGE_FRAME_COLS, LD_STAGE_FRAME_INVERSE,
     LD_STAGE_PUPIL, LD_STAGE_COMPOSITE, LD_STAGE_COUNT
 };
+/* Per-frame chains are captured into CUDA graphs on first use and replayed
+ * when a later frame issues identical launches (same buffers, geometry and
+ * parameters); enable = 0 launches every kernel directly.  On by default;
+ * graphs are never used while stage profiling is on or when the caller's
+ * stream is being captured.  No counterpart in the reference. */
+int ld_set_graphs(ld_ctx* ctx, int enable);
+
 /* When enabled, every kernel launch of ld_render / ld_build_psf_bank is
  * bracketed by a pair of CUDA events on its stream. */
 int ld_set_profiling(ld_ctx* ctx, int enable);

@@ -306,6 +306,7 @@ EXPORTED_SYMBOLS = [
     "ld_set_profiling",
     "ld_profile_collect",
     "ld_estimate_device_bytes",
+    "ld_set_graphs",
     "ld_server_create",
     "ld_server_destroy",
     "ld_server_submit",
@@ -376,6 +377,8 @@ def lib() -> ctypes.CDLL:
     L.ld_set_profiling.restype = ctypes.c_int
     L.ld_profile_collect.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_i32), c_i32]
     L.ld_profile_collect.restype = ctypes.c_int
+    L.ld_set_graphs.argtypes = [vp, ctypes.c_int]
+    L.ld_set_graphs.restype = ctypes.c_int
     L.ld_estimate_device_bytes.argtypes = [ctypes.POINTER(ld_params), c_i32, c_i32]
     L.ld_estimate_device_bytes.restype = ctypes.c_size_t
     L.ld_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_size_t]

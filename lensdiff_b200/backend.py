@@ -147,6 +147,10 @@ class LensDiffPsfBankCache:
         self._lib.ld_check_device_errors(self._h, ctypes.byref(w))
         return int(w.value)
 
+    def set_graphs(self, enable: bool) -> None:
+        """Replay per-frame chains as CUDA graphs (default on)."""
+        self._lib.ld_set_graphs(self._h, 1 if enable else 0)
+
     def set_profiling(self, enable: bool) -> None:
         self._lib.ld_set_profiling(self._h, 1 if enable else 0)
 

@@ -74,6 +74,16 @@ struct ld_ctx {
     // them all without rebuilding the bank
     std::vector<SpectraEntry> spectra_lru;
     uint64_t spectra_clock = 0;
+    // per-frame chains captured as CUDA graphs, by the bytes of their arguments
+    struct GraphEntry {
+        std::string key;
+        cudaGraphExec_t exec = nullptr;
+        int launches = 0;
+        uint64_t last_use = 0;
+    };
+    std::vector<GraphEntry> graphs;
+    uint64_t graph_clock = 0;
+    bool graphs_enabled = true;
     // work buffers, grown on demand
     DevBuf rows, win, combine_out, kspec_rows, frameA, frameB, calib, calib_psf, pupil_pre, effect;
     // comparator form (cuFFT): plans and its own work buffers
@@ -1021,6 +1031,7 @@ void ld_destroy(ld_ctx* c) {
     for (DevBuf* b : bb) free_buf(c, *b);
     for (auto& z : c->zone_spectra) free_buf(c, z.spectra);
     for (auto& z : c->spectra_lru) free_buf(c, z.spectra);
+    for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
     delete c;
 }
 
@@ -1081,6 +1092,85 @@ int ld_resolve_sizes(const ld_params* p, int32_t* np, int32_t* S, int32_t* R, in
 int ld_gaussian_rgb_matrix(const float* wl, int32_t count, const float* center, float sigma, float* out) {
     if (!wl || !center || !out || count <= 0 || count > LD_MAX_WAVELENGTHS || !(sigma > 0.0f)) return LD_ERR_ARG;
     gaussian_matrix(wl, count, center, sigma, out);
+    return LD_OK;
+}
+
+namespace {
+
+constexpr size_t kGraphCache = 4;
+
+// Issues a frame chain through a cached CUDA graph: on the first call with a
+// given key the chain is captured (thread-local capture mode) and
+// instantiated, later calls with the same key launch the graph.  The key is
+// the bytes of every argument the chain's launches take, so a graph is only
+// replayed for identical launches (buffer contents may differ: the kernels
+// read them when the graph runs).  Direct launches when profiling (stage
+// events), when graphs are off, or when the caller's stream is capturing.
+void run_chain(ld_ctx* c, cudaStream_t s, const std::string& key, const std::function<void()>& chain) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (c->profiling || !c->graphs_enabled || cudaStreamIsCapturing(s, &cs) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        chain();
+        return;
+    }
+    for (auto& g : c->graphs) {
+        if (g.exec && g.key == key) {
+            g.last_use = ++c->graph_clock;
+            c->launches += g.launches;
+            check_cuda(cudaGraphLaunch(g.exec, s), "graph-launch");
+            return;
+        }
+    }
+    const int before = c->launches;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        chain();
+        return;
+    }
+    try {
+        chain();
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const bool ok = cudaStreamEndCapture(s, &graph) == cudaSuccess && graph &&
+                    cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {  // not capturable here: launch directly
+        cudaGetLastError();
+        c->launches = before;
+        chain();
+        return;
+    }
+    ld_ctx::GraphEntry* slot = nullptr;
+    if (c->graphs.size() < kGraphCache) {
+        c->graphs.emplace_back();
+        slot = &c->graphs.back();
+    } else {
+        slot = &c->graphs.front();
+        for (auto& g : c->graphs)
+            if (g.last_use < slot->last_use) slot = &g;
+        cudaGraphExecDestroy(slot->exec);
+    }
+    slot->key = key;
+    slot->exec = exec;
+    slot->launches = c->launches - before;
+    slot->last_use = ++c->graph_clock;
+    check_cuda(cudaGraphLaunch(exec, s), "graph-launch");
+}
+
+}  // namespace
+
+int ld_set_graphs(ld_ctx* c, int enable) {
+    if (!c) return LD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->graphs_enabled = enable != 0;
     return LD_OK;
 }
 
@@ -1167,7 +1257,8 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         }
         const SpectraEntry& sp = *spectra.front();
 
-        FrameArgs fa{};
+        FrameArgs fa;
+        std::memset(&fa, 0, sizeof(fa));  // padding too: the bytes key the frame graphs
         fa.g = g;
         fa.sel = selection_params(p);
         fa.W = W;
@@ -1216,11 +1307,14 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             fa.effect = static_cast<float4*>(
                 ensure(ctx, ctx->effect, static_cast<size_t>(W) * H * sizeof(float4) + 2 * sizeof(double)));
             fa.sums = reinterpret_cast<double*>(fa.effect + static_cast<size_t>(W) * H);
+        }
+        auto clear_effect = [&]() {
+            if (fa.effect_mode == kEffectComposite) return;
             check_cuda(cudaMemsetAsync(fa.sums, 0, 2 * sizeof(double), s), "effect-memset");
             if (zones)
                 check_cuda(cudaMemsetAsync(fa.effect, 0, static_cast<size_t>(W) * H * sizeof(float4), s),
                            "effect-memset");
-        }
+        };
         if (p.fft_form == LD_FFT_CUFFT) {
             const size_t P = static_cast<size_t>(g.Px) * g.Py;
             const size_t half = static_cast<size_t>(g.Py) * (g.Px / 2 + 1);
@@ -1228,6 +1322,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             float* planes = static_cast<float*>(ensure(ctx, ctx->cf_planes, nc * P * sizeof(float)));
             float2* sd = static_cast<float2*>(ensure(ctx, ctx->cf_sd, cb.n_drv * half * sizeof(float2)));
             float2* prod = static_cast<float2*>(ensure(ctx, ctx->cf_prod, cb.n_out * half * sizeof(float2)));
+            clear_effect();
             staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { cf_frame_forward(fa, planes, sd, ctx->cufft, s); });
             staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { cf_frame_multiply(fa, sd, prod, s); });
             staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { cf_frame_inverse(fa, prod, planes, ctx->cufft, s); });
@@ -1245,28 +1340,36 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             }
             return;
         }
-        staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
-        if (!zones) {
-            staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
-            staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse(fa, s); });
-        } else {
-            fa.zone_n = zn;
-            for (int z = 0; z < zn * zn; ++z) {
-                fa.spectra = static_cast<const float2*>(spectra[static_cast<size_t>(z)]->spectra.p);
-                fa.zone_x = z % zn;
-                fa.zone_y = z / zn;
-                // source rows whose tent weight can be non-zero (the kernel
-                // evaluates the weight itself; one row of margin each side)
-                const double step = static_cast<double>(std::max(1, H - 1)) / static_cast<double>(zn - 1);
-                const int r0 = std::max(0, static_cast<int>(std::floor((fa.zone_y - 1) * step)) - 1);
-                const int r1 = std::min(H, static_cast<int>(std::ceil((fa.zone_y + 1) * step)) + 2);
-                fa.row0 = r0;
+        // graph key: the launch arguments (the zone loop derives the rest)
+        std::string gkey(reinterpret_cast<const char*>(&fa), sizeof(fa));
+        for (const SpectraEntry* e : spectra) gkey = append_bytes(gkey, &e->spectra.p, sizeof(void*));
+        gkey = append_bytes(gkey, &zn, sizeof(zn));
+        auto chain = [&, fa]() mutable {  // the zone loop edits this copy
+            clear_effect();
+            staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
+            if (!zones) {
                 staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
-                staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse_rows(fa, r1 - r0, s); });
+                staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse(fa, s); });
+            } else {
+                fa.zone_n = zn;
+                for (int z = 0; z < zn * zn; ++z) {
+                    fa.spectra = static_cast<const float2*>(spectra[static_cast<size_t>(z)]->spectra.p);
+                    fa.zone_x = z % zn;
+                    fa.zone_y = z / zn;
+                    // source rows whose tent weight can be non-zero (the kernel
+                    // evaluates the weight itself; one row of margin each side)
+                    const double step = static_cast<double>(std::max(1, H - 1)) / static_cast<double>(zn - 1);
+                    const int r0 = std::max(0, static_cast<int>(std::floor((fa.zone_y - 1) * step)) - 1);
+                    const int r1 = std::min(H, static_cast<int>(std::ceil((fa.zone_y + 1) * step)) + 2);
+                    fa.row0 = r0;
+                    staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
+                    staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse_rows(fa, r1 - r0, s); });
+                }
+                if (fa.preserve) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_effect_sums(fa, s); });
             }
-            if (fa.preserve) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_effect_sums(fa, s); });
-        }
-        if (fa.effect_mode != kEffectComposite) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fa, s); });
+            if (fa.effect_mode != kEffectComposite) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fa, s); });
+        };
+        run_chain(ctx, s, gkey, chain);
         check_launch("frame-chain");
         if (st) {
             st->bank_rebuilt = bank_rebuilt;
