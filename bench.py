@@ -221,6 +221,13 @@ class Clocks:
                 "samples": len(sms)}
 
 
+# DRAM bytes per launch (read + write) of the frame kernels on the UHD
+# 31-wavelength workload, from the one-pass ncu capture summarised in
+# profiles/frame_*_hd16.md (writes still resident in L2 at kernel end are not
+# counted by DRAM counters).
+MEASURED_TRAFFIC_UHD31 = {"frame_rows": 156.4e6, "frame_cols": 322.9e6, "frame_inverse": 352.6e6}
+
+
 # ---------------------------------------------------------------------------
 # algorithmic bytes per launch of the frame-chain kernels
 # ---------------------------------------------------------------------------
@@ -506,8 +513,9 @@ def main():
     if dominant in alg and dom_n:
         per_launch_ms = dom_ms / dom_n
         achieved = alg[dominant] / (per_launch_ms / 1000.0) / 1e9
+        traffic = MEASURED_TRAFFIC_UHD31.get(dominant) if args.workload == "uhd31" else None
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "peak_source": peak_src, "traffic": None,
+                    "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                     "algorithmic_bytes_per_launch": alg[dominant], "launch_ms": per_launch_ms}
     else:
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": None, "peak": peak, "unit": "GB/s",
