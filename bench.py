@@ -525,7 +525,7 @@ def main():
     # ---- the other transform chains on the same workload (device time) ------
     comparators = {}
     if not args.no_comparators:
-        for name in ("own", "cufft"):
+        for name in ("own", "chosen", "cufft"):
             if name == args.fft_form:
                 continue
             base = p.copy(fftForm=FFT_FORMS[name])

@@ -24,6 +24,8 @@
 // grid launches in blockIdx order, `ahead` CTAs resident at a time).
 #include <algorithm>
 
+#include <cuda_fp16.h>
+
 #include "ld_async.cuh"
 #include "ld_internal.h"
 #include "ld_pixel.cuh"
@@ -73,6 +75,48 @@ __device__ __forceinline__ void store_b_column(const float2* s, float2* B, int k
         const int row = i / C;
         const int c = i - row * C;
         B[b_index(k, row, c, Hp, C)] = s[i];
+    }
+}
+
+// ---- FP16 spectra with a per-column scale (the chosen form) ------------------------
+// A spectrum column is stored as half2 values v * (kHalfTop / m), m = the
+// largest |real| or |imag| of the column, with m / kHalfTop kept as the
+// column's float scale: every value keeps FP16's 11-bit mantissa down to
+// 4e-9 m, and nothing overflows.
+constexpr float kHalfTop = 16384.0f;
+
+// Largest |real| / |imag| of s[0, n) over the CTA (all threads get it).
+__device__ float block_absmax(const float2* s, int n) {
+    __shared__ float part[32];
+    float m = 0.0f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, fmaxf(fabsf(s[i].x), fabsf(s[i].y)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) part[warp] = m;
+    __syncthreads();
+    m = lane < static_cast<int>((blockDim.x + 31) >> 5) ? part[lane] : 0.0f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __syncthreads();  // part[] may be reused
+    return m;
+}
+
+__device__ __forceinline__ __half2 to_half2(float2 v, float s) { return __floats2half2_rn(v.x * s, v.y * s); }
+__device__ __forceinline__ float2 from_half2(__half2 h, float scale) {
+    const float2 f = __half22float2(h);
+    return make_float2(f.x * scale, f.y * scale);
+}
+
+// Writes a transformed column to B in FP16 with its scale (see store_b_column).
+__device__ __forceinline__ void store_b_column_h16(const float2* s, __half2* B, float* bscale, int k, int Hp, int C) {
+    const float m = block_absmax(s, Hp * C);
+    const float sc = m > 0.0f ? kHalfTop / m : 1.0f;
+    if (threadIdx.x == 0) bscale[k] = m > 0.0f ? m / kHalfTop : 1.0f;
+    for (int i = threadIdx.x; i < Hp * C; i += blockDim.x) {
+        const int row = i / C;
+        const int c = i - row * C;
+        B[b_index(k, row, c, Hp, C)] = to_half2(s[i], sc);
     }
 }
 
@@ -166,7 +210,7 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
 // Wk [Py][NOUT] (the column's NOUT kernel spectra land here, are multiplied by
 // F in place and inverse-transformed together as NOUT interleaved sequences),
 // two mbarriers.  The first Hp rows of Wk go to B with one bulk store.
-template <int E, int NOUT, int MAXT = Fam<E>::max_threads, int MINB = 1>
+template <int E, int NOUT, int MAXT = Fam<E>::max_threads, int MINB = 1, bool H16 = false>
 __global__ void __launch_bounds__(MAXT, MINB) frame_cols_kernel(FrameArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const int Py = a.g.Py, Hp = a.Hp, cols = a.g.cols;
@@ -175,7 +219,12 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_cols_kernel(FrameArgs a) {
     float2* Wk = F + Py;
     uint64_t* bars = reinterpret_cast<uint64_t*>(Wk + static_cast<size_t>(Py) * NOUT);
     const uint32_t a_bytes = static_cast<uint32_t>(Hp * sizeof(float2));
-    const uint32_t k_bytes = static_cast<uint32_t>(static_cast<size_t>(Py) * NOUT * sizeof(float2));
+    // FP16 kernel spectra land in the upper half of Wk and are widened in the multiply
+    const size_t kn = static_cast<size_t>(Py) * NOUT;
+    const uint32_t k_bytes = static_cast<uint32_t>(kn * (H16 ? sizeof(__half2) : sizeof(float2)));
+    void* kdst = H16 ? static_cast<void*>(reinterpret_cast<__half2*>(Wk) + kn) : static_cast<void*>(Wk);
+    const void* ksrc = H16 ? static_cast<const void*>(reinterpret_cast<const __half2*>(a.spectra) + k * kn)
+                           : static_cast<const void*>(a.spectra + k * kn);
     const bool lead = threadIdx.x == 0;
     if (lead) {
         mbar_init(&bars[0], 1);
@@ -185,21 +234,43 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_cols_kernel(FrameArgs a) {
     __syncthreads();  // barriers initialised before anyone waits on them
     if (lead) {
         bulk_load_checked(F, a.A + static_cast<size_t>(k) * Hp, a_bytes, &bars[0], smraw, a.err);
-        bulk_load_checked(Wk, a.spectra + static_cast<size_t>(k) * Py * NOUT, k_bytes, &bars[1], smraw, a.err);
+        bulk_load_checked(kdst, ksrc, k_bytes, &bars[1], smraw, a.err);
         const int later = k + a.ahead;
         if (later < cols) {
             bulk_prefetch_l2(a.A + static_cast<size_t>(later) * Hp, a_bytes);
-            bulk_prefetch_l2(a.spectra + static_cast<size_t>(later) * Py * NOUT, k_bytes);
+            bulk_prefetch_l2(static_cast<const char*>(ksrc) + (later - k) * static_cast<size_t>(k_bytes), k_bytes);
         }
     }
     for (int i = Hp + threadIdx.x; i < Py; i += blockDim.x) F[i] = make_float2(0.0f, 0.0f);
     if (__syncthreads_or(!mbar_wait(&bars[0], 0, a.err))) return;
     fft_run<E, 1, false>(a.g.plan_py, F);
     if (__syncthreads_or(!mbar_wait(&bars[1], 0, a.err))) return;
-    for (int i = threadIdx.x; i < Py * NOUT; i += blockDim.x) Wk[i] = cmul(Wk[i], F[i / NOUT]);
+    if constexpr (H16) {
+        // every thread widens its (at most E) kernel values before any
+        // product overwrites the half2 area they came from
+        const float ks = a.kscale[k];
+        const __half2* kh = reinterpret_cast<const __half2*>(Wk) + kn;
+        float2 kv[E];
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+            const int i = threadIdx.x + j * static_cast<int>(blockDim.x);
+            kv[j] = i < static_cast<int>(kn) ? from_half2(kh[i], ks) : make_float2(0.0f, 0.0f);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+            const int i = threadIdx.x + j * static_cast<int>(blockDim.x);
+            if (i < static_cast<int>(kn)) Wk[i] = cmul(kv[j], F[i / NOUT]);
+        }
+    } else {
+        for (int i = threadIdx.x; i < Py * NOUT; i += blockDim.x) Wk[i] = cmul(Wk[i], F[i / NOUT]);
+    }
     __syncthreads();
     fft_run<E, NOUT, true>(a.g.plan_py, Wk);
-    store_b_column(Wk, a.Bout, k, Hp, NOUT);
+    if constexpr (H16)
+        store_b_column_h16(Wk, reinterpret_cast<__half2*>(a.Bout), a.bscale, k, Hp, NOUT);
+    else
+        store_b_column(Wk, a.Bout, k, Hp, NOUT);
 }
 
 // ---- column pass, Mono: three colour drivers, one kernel spectrum -------------------
@@ -269,7 +340,7 @@ __device__ __forceinline__ float zone_weight(int v, int extent, int z, int n) {
 // row is output row out_y1 + blockIdx.x (kEffectComposite), source row
 // blockIdx.x (kEffectStore) or source row row0 + blockIdx.x
 // (kEffectAccumulate); see FrameArgs::effect_mode.
-template <int E, int C, int MAXT = Fam<E>::max_threads, int MINB = 1>
+template <int E, int C, int MAXT = Fam<E>::max_threads, int MINB = 1, bool H16 = false>
 __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) {
     extern __shared__ float2 smem[];
     const int bid = static_cast<int>(blockIdx.x);
@@ -297,8 +368,14 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
                 if (i < npair) {
                     const int pk = i / C;
                     const int c = i - pk * C;
-                    xp[u] = __ldcs(&a.Bout[b_index(pk, sy, c, Hp, C)]);
-                    xq[u] = __ldcs(&a.Bout[b_index(M - pk, sy, c, Hp, C)]);
+                    if constexpr (H16) {
+                        const __half2* Bh = reinterpret_cast<const __half2*>(a.Bout);
+                        xp[u] = from_half2(__ldcs(&Bh[b_index(pk, sy, c, Hp, C)]), __ldg(&a.bscale[pk]));
+                        xq[u] = from_half2(__ldcs(&Bh[b_index(M - pk, sy, c, Hp, C)]), __ldg(&a.bscale[M - pk]));
+                    } else {
+                        xp[u] = __ldcs(&a.Bout[b_index(pk, sy, c, Hp, C)]);
+                        xq[u] = __ldcs(&a.Bout[b_index(M - pk, sy, c, Hp, C)]);
+                    }
                     wp[u] = __ldg(&tw_px[pk]);
                     wq[u] = __ldg(&tw_px[M - pk]);
                 }
@@ -458,7 +535,7 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) kspec_rows_kernel(Kern
 // copy; the wrap map places canvas row ci at grid row v and folds in the
 // inverse scale; the transformed column KS[k] (Py x C, contiguous) leaves by
 // one bulk store.
-template <int E, int C, int MAXT = Fam<E>::max_threads, int MINB = 1>
+template <int E, int C, int MAXT = Fam<E>::max_threads, int MINB = 1, bool H16 = false>
 __global__ void __launch_bounds__(MAXT, MINB) kspec_cols_kernel(KernelSpectraArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const int Py = a.g.Py, cols = a.g.cols, Kp = a.Kp, R = a.R;
@@ -488,6 +565,14 @@ __global__ void __launch_bounds__(MAXT, MINB) kspec_cols_kernel(KernelSpectraArg
     }
     __syncthreads();
     fft_run<E, C, false>(a.g.plan_py, W);
+    if constexpr (H16) {
+        const float m = block_absmax(W, Py * C);
+        const float sc = m > 0.0f ? kHalfTop / m : 1.0f;
+        if (lead) a.kscale[k] = m > 0.0f ? m / kHalfTop : 1.0f;
+        __half2* out = reinterpret_cast<__half2*>(a.spectra) + static_cast<size_t>(k) * Py * C;
+        for (int i = threadIdx.x; i < Py * C; i += blockDim.x) out[i] = to_half2(W[i], sc);
+        return;
+    }
     fence_proxy_async_smem();
     __syncthreads();
     const uint32_t s_bytes = static_cast<uint32_t>(static_cast<size_t>(Py) * C * sizeof(float2));
@@ -544,13 +629,19 @@ void cols_launch(Kern f, FrameArgs a, int C, size_t sm, cudaStream_t s) {
 
 // Spectral column pass: two CTAs per SM (register cap 85) when the transform
 // fits 384 threads and two working sets fit shared memory.
-template <int E, int NOUT>
-void cols_spectral(const FrameArgs& a, cudaStream_t s) {
+template <int E, int NOUT, bool H16>
+void cols_spectral_h(const FrameArgs& a, cudaStream_t s) {
     const size_t sm = frame_cols_smem(a.g.Py, NOUT);
     if (fft_threads(a.g.Py, NOUT, E) <= 384 && 2 * sm + 2048 <= static_cast<size_t>(kMaxSmem))
-        cols_launch<E>(frame_cols_kernel<E, NOUT, 384, 2>, a, NOUT, sm, s);
+        cols_launch<E>(frame_cols_kernel<E, NOUT, 384, 2, H16>, a, NOUT, sm, s);
     else
-        cols_launch<E>(frame_cols_kernel<E, NOUT>, a, NOUT, sm, s);
+        cols_launch<E>(frame_cols_kernel<E, NOUT, Fam<E>::max_threads, 1, H16>, a, NOUT, sm, s);
+}
+
+template <int E, int NOUT>
+void cols_spectral(const FrameArgs& a, cudaStream_t s) {
+    if (a.h16) cols_spectral_h<E, NOUT, true>(a, s);
+    else cols_spectral_h<E, NOUT, false>(a, s);
 }
 
 template <int E>
@@ -564,20 +655,24 @@ void cols_e(const FrameArgs& a, cudaStream_t s) {
     }
 }
 
+template <int E, int C, bool H16>
+void inverse_c(const FrameArgs& a, int rows, cudaStream_t s) {
+    const int M = a.g.M;
+    const int T = fft_threads(M, C, E);
+    const size_t sm = static_cast<size_t>(M) * C * sizeof(float2);
+    // two CTAs per SM when the transform fits 320 threads (register cap 102)
+    if (T <= 320) frame_inverse_kernel<E, C, 320, 2, H16><<<rows, T, sm, s>>>(a);
+    else frame_inverse_kernel<E, C, Fam<E>::max_threads, 1, H16><<<rows, T, sm, s>>>(a);
+}
+
 template <int E>
 void inverse_e(const FrameArgs& a, int rows, cudaStream_t s) {  // rows: grid size
-    const int M = a.g.M;
     if (a.n_out == 4) {
-        const int T = fft_threads(M, 4, E);
-        const size_t sm = static_cast<size_t>(M) * 4 * sizeof(float2);
-        if (T <= 320) frame_inverse_kernel<E, 4, 320, 2><<<rows, T, sm, s>>>(a);
-        else frame_inverse_kernel<E, 4><<<rows, T, sm, s>>>(a);
+        if (a.h16) inverse_c<E, 4, true>(a, rows, s);
+        else inverse_c<E, 4, false>(a, rows, s);
     } else {
-        const int T = fft_threads(M, 3, E);
-        const size_t sm = static_cast<size_t>(M) * 3 * sizeof(float2);
-        // two CTAs per SM when the transform fits 320 threads (register cap 102)
-        if (T <= 320) frame_inverse_kernel<E, 3, 320, 2><<<rows, T, sm, s>>>(a);
-        else frame_inverse_kernel<E, 3><<<rows, T, sm, s>>>(a);
+        if (a.h16) inverse_c<E, 3, true>(a, rows, s);
+        else inverse_c<E, 3, false>(a, rows, s);
     }
 }
 
@@ -587,20 +682,26 @@ void kspec_rows_c(const KernelSpectraArgs& a, cudaStream_t s) {
         a);
 }
 
-template <int E, int C>
-void kspec_cols_c(KernelSpectraArgs a, cudaStream_t s) {
+template <int E, int C, bool H16>
+void kspec_cols_h(KernelSpectraArgs a, cudaStream_t s) {
     const int T = fft_threads(a.g.Py, C, E);
     const size_t sm = kspec_cols_smem(a.g.Py, a.Kp, C);
     if (C > 1 && T <= 384 && 2 * sm + 2048 <= static_cast<size_t>(kMaxSmem)) {  // C == 1: Mono, one kernel
         // two CTAs per SM (register cap 80)
-        auto f = kspec_cols_kernel<E, C, 384, 2>;
+        auto f = kspec_cols_kernel<E, C, 384, 2, H16>;
         a.ahead = resident_ctas(f, T, sm);
         f<<<a.g.cols, T, sm, s>>>(a);
     } else {
-        auto f = kspec_cols_kernel<E, C>;
+        auto f = kspec_cols_kernel<E, C, Fam<E>::max_threads, 1, H16>;
         a.ahead = resident_ctas(f, T, sm);
         f<<<a.g.cols, T, sm, s>>>(a);
     }
+}
+
+template <int E, int C>
+void kspec_cols_c(const KernelSpectraArgs& a, cudaStream_t s) {
+    if (a.h16) kspec_cols_h<E, C, true>(a, s);
+    else kspec_cols_h<E, C, false>(a, s);
 }
 
 template <int E>
@@ -629,6 +730,19 @@ void configure_e() {
     set_smem(frame_inverse_kernel<E, 3, 320, 2>);
     set_smem(frame_cols_kernel<E, 3, 384, 2>);
     set_smem(frame_cols_kernel<E, 4, 384, 2>);
+    set_smem(frame_cols_kernel<E, 3, 384, 2, true>);
+    set_smem(frame_cols_kernel<E, 4, 384, 2, true>);
+    set_smem(frame_cols_kernel<E, 3, Fam<E>::max_threads, 1, true>);
+    set_smem(frame_cols_kernel<E, 4, Fam<E>::max_threads, 1, true>);
+    set_smem(frame_inverse_kernel<E, 3, 320, 2, true>);
+    set_smem(frame_inverse_kernel<E, 4, 320, 2, true>);
+    set_smem(frame_inverse_kernel<E, 3, Fam<E>::max_threads, 1, true>);
+    set_smem(frame_inverse_kernel<E, 4, Fam<E>::max_threads, 1, true>);
+    set_smem(kspec_cols_kernel<E, 3, 384, 2, true>);
+    set_smem(kspec_cols_kernel<E, 4, 384, 2, true>);
+    set_smem(kspec_cols_kernel<E, 1, Fam<E>::max_threads, 1, true>);
+    set_smem(kspec_cols_kernel<E, 3, Fam<E>::max_threads, 1, true>);
+    set_smem(kspec_cols_kernel<E, 4, Fam<E>::max_threads, 1, true>);
     set_smem(frame_rows_kernel<E, 2, 1, 224, 3>);
     set_smem(kspec_cols_kernel<E, 3, 384, 2>);
     set_smem(kspec_cols_kernel<E, 4, 384, 2>);

@@ -42,6 +42,7 @@ struct BankEntry {
     int win_stride = 0;
     std::vector<float> wavelengths;
     bool cufft = false;  // built with the comparator form (its spectra follow)
+    bool h16 = false;    // chosen form: kernel spectra in FP16 with per-column scales
     DevBuf canvas, ring_round, ring_ceil, ring_peak, ring_mean, scalars, wl;
     PsfBankArgs args{};
 };
@@ -290,6 +291,10 @@ int raw_psf_size(int np, int rmax) {  // chooseRawPsfSize, CpuReference.cpp:112-
 
 bool is_mono(const ld_params& p) { return p.spectral_mode == LD_SPECTRAL_MONO; }
 
+// Chosen form: kernel spectra and column outputs in FP16 with per-column
+// scales (spectral modes; Mono keeps FP32 spectra).
+bool chosen_h16(const ld_params& p) { return p.fft_form == LD_FFT_OWN_CHOSEN && !is_mono(p); }
+
 std::vector<float> wavelengths_of(const ld_params& p) {  // CpuReference.cpp:1602-1614
     if (!is_mono(p) && p.wavelength_count > 0) {
         return std::vector<float>(p.wavelengths_nm, p.wavelengths_nm + p.wavelength_count);
@@ -467,7 +472,7 @@ void validate_params(const ld_params& p) {
     if (p.wavelength_count < 0 || p.wavelength_count > LD_MAX_WAVELENGTHS)
         throw Fail{LD_ERR_ARG, "invalid-wavelength-count"};
     if (p.vane_count > kMaxVanes) throw Fail{LD_ERR_UNSUPPORTED, "too-many-vanes"};
-    if (p.fft_form != LD_FFT_OWN_FP32 && p.fft_form != LD_FFT_CUFFT)
+    if (p.fft_form != LD_FFT_OWN_FP32 && p.fft_form != LD_FFT_CUFFT && p.fft_form != LD_FFT_OWN_CHOSEN)
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-fft-form"};
     if (p.fft_form == LD_FFT_CUFFT && has_field_phase(p))
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-field-zones-with-cufft-form"};
@@ -684,6 +689,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     b.win_stride = win_stride;
     b.wavelengths = wl;
     b.cufft = p.fft_form == LD_FFT_CUFFT;
+    b.h16 = chosen_h16(p);
     b.key = key;
     b.valid = true;
     c->spectra.valid = false;
@@ -815,7 +821,7 @@ GridGeom make_geometry(ld_ctx* c, int W, int H, int K, int c_rows, int c_cols, i
     *req_w = W + K - 1;
     *req_h = H + K - 1;
     g.M = choose_length((*req_w + 1) / 2, 1, c_rows);
-    g.Py = choose_length(*req_h, 2, c_cols);
+    g.Py = choose_length(*req_h, 4, c_cols);  // FP16 column bulk copies want Py * 3 * 4 bytes % 16 == 0
     if (g.M < 0 || g.Py < 0) throw Fail{LD_ERR_UNSUPPORTED, "frame-too-large-for-fft-grid"};
     g.Px = 2 * g.M;
     g.cols = g.M + 1;
@@ -854,8 +860,11 @@ SpectraEntry& ensure_spectra_in(ld_ctx* c, SpectraEntry& e, BankEntry& b, const 
     ka.canvas = ca.out;
     ka.rows = static_cast<float2*>(
         ensure(c, c->kspec_rows, static_cast<size_t>(cb.n_ker) * g.cols * ka.Kp * sizeof(float2)));
-    ka.spectra = static_cast<float2*>(
-        ensure(c, e.spectra, static_cast<size_t>(cb.n_ker) * g.cols * g.Py * sizeof(float2)));
+    const size_t ks_bytes = align256(static_cast<size_t>(cb.n_ker) * g.cols * g.Py * (b.h16 ? 4 : 8));
+    char* ksbuf = static_cast<char*>(ensure(c, e.spectra, ks_bytes + static_cast<size_t>(g.cols) * sizeof(float)));
+    ka.spectra = reinterpret_cast<float2*>(ksbuf);
+    ka.h16 = b.h16 ? 1 : 0;
+    ka.kscale = reinterpret_cast<float*>(ksbuf + ks_bytes);
     ka.scale = static_cast<float>(1.0 / (static_cast<double>(g.M) * static_cast<double>(g.Py)));
     ka.err = c->err;
     if (b.cufft) {
@@ -1298,9 +1307,15 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             ensure(ctx, ctx->frameA, static_cast<size_t>(cb.n_drv) * g.cols * fa.Hp * sizeof(float2)));
         // column outputs in groups of four columns (ld_frame.cu b_index)
         const size_t bcols = (static_cast<size_t>(g.cols) + 3) / 4 * 4;
-        fa.Bout = static_cast<float2*>(
-            ensure(ctx, ctx->frameB, static_cast<size_t>(cb.n_out) * bcols * fa.Hp * sizeof(float2)));
+        fa.h16 = chosen_h16(p) ? 1 : 0;
+        const size_t b_bytes = align256(static_cast<size_t>(cb.n_out) * bcols * fa.Hp * (fa.h16 ? 4 : 8));
+        char* bbuf = static_cast<char*>(ensure(ctx, ctx->frameB, b_bytes + static_cast<size_t>(g.cols) * sizeof(float)));
+        fa.Bout = reinterpret_cast<float2*>(bbuf);
+        fa.bscale = reinterpret_cast<float*>(bbuf + b_bytes);
         fa.spectra = static_cast<const float2*>(sp.spectra.p);
+        fa.kscale = reinterpret_cast<const float*>(
+            static_cast<const char*>(sp.spectra.p) +
+            align256(static_cast<size_t>(cb.n_ker) * g.cols * g.Py * (fa.h16 ? 4 : 8)));
         fa.err = ctx->err;
         fa.effect_mode = zones ? kEffectAccumulate : (fa.preserve ? kEffectStore : kEffectComposite);
         if (fa.effect_mode != kEffectComposite) {
@@ -1354,6 +1369,9 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
                 fa.zone_n = zn;
                 for (int z = 0; z < zn * zn; ++z) {
                     fa.spectra = static_cast<const float2*>(spectra[static_cast<size_t>(z)]->spectra.p);
+                    fa.kscale = reinterpret_cast<const float*>(
+                        static_cast<const char*>(spectra[static_cast<size_t>(z)]->spectra.p) +
+                        align256(static_cast<size_t>(cb.n_ker) * g.cols * g.Py * (fa.h16 ? 4 : 8)));
                     fa.zone_x = z % zn;
                     fa.zone_y = z / zn;
                     // source rows whose tent weight can be non-zero (the kernel

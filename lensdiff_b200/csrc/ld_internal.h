@@ -122,6 +122,8 @@ struct KernelSpectraArgs {
     float2* rows;         // KR
     float2* spectra;      // KS
     float scale;          // 1 / (M * Py)
+    int h16;              // chosen form: KS in FP16 (half2) with one float scale per column
+    float* kscale;        // [cols] (h16)
     int ahead;            // column-pass CTAs resident at once (set by the launcher)
     int* err;             // device error word
 };
@@ -156,7 +158,10 @@ struct FrameArgs {
     int n_ker;                 // kernels (1 for Mono)
     float2* A;
     float2* Bout;
-    const float2* spectra;
+    const float2* spectra;     // KS; half2 when h16
+    int h16;                   // chosen form: KS and B in FP16 with per-column scales
+    const float* kscale;       // [cols] (h16)
+    float* bscale;             // [cols] (h16)
     int ahead;                 // column-pass CTAs resident at once (set by the launcher)
     int* err;                  // device error word
     // What the inverse pass does with the mapped effect of a row:

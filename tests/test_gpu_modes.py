@@ -211,3 +211,30 @@ def test_graph_replay_matches_direct_launches(cache):
     for i, out in enumerate(replayed):
         assert np.array_equal(out, direct[i % 3]), i
     assert cache.check_device_errors() == 0
+
+
+# ------------------------------------------------------------ chosen form ----
+# fft_form LD_FFT_OWN_CHOSEN stores the kernel spectra and the column-pass
+# outputs in FP16 with one float scale per spectrum column (half the bytes of
+# the largest frame arrays); it must meet the same output bar.
+@pytest.mark.parametrize("kw", [{}, {"spectralMode": LensDiffSpectralMode.Spectral9, "chromaticFocus": 0.3},
+                                {"energyMode": LensDiffEnergyMode.Preserve},
+                                {"spectralMode": LensDiffSpectralMode.Mono}])
+def test_chosen_form_matches_reference(cache, kw):
+    from lensdiff_b200.types import LensDiffFftForm
+    _reference_available()
+    p = _lens(**kw)
+    src = S.make_frame(256, 144, 24, 1.0, 1000.0, seed=18)
+    out = _render(cache, with_matrices(p.copy(fftForm=LensDiffFftForm.OwnChosen)), src)
+    ref = R.render(p, src)
+    assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
+
+
+def test_chosen_form_field_zones(cache):
+    from lensdiff_b200.types import LensDiffFftForm
+    _reference_available()
+    p = _field_lens()
+    src = S.make_frame(200, 120, 16, 1.0, 300.0, seed=19)
+    out = _render(cache, with_matrices(p.copy(fftForm=LensDiffFftForm.OwnChosen)), src)
+    ref = R.render(p, src)
+    assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
