@@ -49,30 +49,44 @@ __device__ double block_sum(double v) {
     return r;
 }
 
-// Warp-segmented reduction over runs of equal `slot` in consecutive lanes
-// (slot < 0: inactive lane).  Returns true on the last lane of each run, whose
-// `v` then holds the run's sum (MAX=false) or maximum (MAX=true).  Along a
-// canvas row the ring index of consecutive pixels changes slowly, so a warp
-// of 32 pixels collapses to a few runs and one shared-memory atomic each.
-template <bool MAX>
-__device__ __forceinline__ bool warp_run_reduce(int slot, float& v) {
+// Adds each lane's v to ring[slot] (and, with PEAK, maxes it into
+// peak[slot] as float bits) where the lanes' slots form runs of equal values
+// in consecutive lanes (slot < 0: nothing to add), v >= 0.  A warp is 32
+// pixels of a canvas row: away from the axis through the centre the ring
+// index changes slowly and a warp has a few runs, each reduced with one
+// butterfly and added with one shared-memory atomic; near that axis it changes
+// at almost every pixel, and the lanes add directly (few address conflicts).
+template <bool PEAK>
+__device__ __forceinline__ void warp_runs_accumulate(int slot, float v, float* ring, unsigned int* peak) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int prev = __shfl_up_sync(full, slot, 1);
-    const int nxt = __shfl_down_sync(full, slot, 1);
-    const bool head = lane == 0 || prev != slot;
-    const unsigned heads = __ballot_sync(full, head);
+    unsigned heads = __ballot_sync(full, lane == 0 || prev != slot);
+    if (__popc(heads) > 4) {
+        if (slot >= 0) {
+            if (v != 0.0f) atomicAdd(&ring[slot], v);
+            if (PEAK && v != 0.0f) atomicMax(&peak[slot], __float_as_uint(v));
+        }
+        return;
+    }
+    while (heads) {  // warp-uniform
+        const int h = __ffs(heads) - 1;
+        heads &= heads - 1;
+        const int e = heads ? __ffs(heads) - 1 : 32;
+        const bool in = lane >= h && lane < e;
+        float x = in ? v : 0.0f;
+        float m = x;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const float o = __shfl_up_sync(full, v, d);
-        if (lane >= d) {
-            // lane-d is in this run iff no run starts in (lane-d, lane]
-            const unsigned long long span = ((2ull << lane) - 1ull) ^ ((2ull << (lane - d)) - 1ull);
-            if ((static_cast<unsigned long long>(heads) & span) == 0ull) v = MAX ? fmaxf(v, o) : v + o;
+        for (int o = 16; o > 0; o >>= 1) {
+            x += __shfl_xor_sync(full, x, o);
+            if (PEAK) m = fmaxf(m, __shfl_xor_sync(full, m, o));
+        }
+        const int sl = __shfl_sync(full, slot, h);
+        if (lane == h && sl >= 0) {
+            if (x != 0.0f) atomicAdd(&ring[sl], x);
+            if (PEAK && m != 0.0f) atomicMax(&peak[sl], __float_as_uint(m));
         }
     }
-    const bool tail = lane == 31 || nxt != slot;
-    return tail && slot >= 0;
 }
 
 // ---- pupil, once per bank --------------------------------------------------------
@@ -258,7 +272,7 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
             lsum += v;
             slot = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy)))) - rbase;
         }
-        if (warp_run_reduce<false>(slot, v)) atomicAdd(&ring[slot], v);
+        warp_runs_accumulate<false>(slot, v, ring, nullptr);
     }
     __syncthreads();
     double* gring = a.ring_round + static_cast<size_t>(b) * (R + 1);
@@ -350,11 +364,7 @@ __global__ void __launch_bounds__(256) shape_stats_kernel(PsfBankArgs a) {
             lpeak = max(lpeak, __float_as_uint(v));
             slot = min(R, static_cast<int>(ceilf(rad))) - rbase;
         }
-        float pk = v;
-        const bool tail_e = warp_run_reduce<false>(slot, v);
-        const bool tail_p = warp_run_reduce<true>(slot, pk);
-        if (tail_e) atomicAdd(&ring_e[slot], v);
-        if (tail_p) atomicMax(&ring_p[slot], __float_as_uint(pk));
+        warp_runs_accumulate<true>(slot, v, ring_e, ring_p);
     }
     __syncthreads();
     const size_t ro = static_cast<size_t>(b) * (R + 1);
