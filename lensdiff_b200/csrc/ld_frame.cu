@@ -328,6 +328,12 @@ __device__ __forceinline__ float3 mapped_effect(const FrameArgs& a, const float2
     return map_effect<C>(a, e);
 }
 
+// softShoulder (LensDiffCpuReference.cpp:84-90): s (1 - exp(-max(0, v) / s)).
+__device__ __forceinline__ float soft_shoulder(float v, float s) {
+    const float x = fmaxf(0.0f, v);
+    return s * (1.0f - expf(-x / s));
+}
+
 // Tent weight of field zone z along one axis (accumulateWeightedImage,
 // LensDiffCpuReference.cpp:1458-1466; the reference's grid is n = 3).
 __device__ __forceinline__ float zone_weight(int v, int extent, int z, int n) {
@@ -398,17 +404,19 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
     const unsigned char* srow = a.src + static_cast<int64_t>(sy) * a.src_pitch;
     if (a.effect_mode == kEffectAccumulate) {
         if (!have) return;
-        const float wy = zone_weight(sy, a.H, a.zone_y, a.zone_n);
+        const float wy = a.zone_n > 0 ? zone_weight(sy, a.H, a.zone_y, a.zone_n) : 1.0f;
         if (wy <= 0.0f) return;
+        const float gain = a.acc_gain, sh = a.acc_shoulder;
         float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
         for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
-            const float wgt = zone_weight(sx, a.W, a.zone_x, a.zone_n) * wy;
+            const float wgt = (a.zone_n > 0 ? zone_weight(sx, a.W, a.zone_x, a.zone_n) : 1.0f) * wy;
             if (wgt <= 0.0f) continue;
-            const float3 e = mapped_effect<C>(a, smem, sx);
+            float3 e = mapped_effect<C>(a, smem, sx);
+            if (sh > 0.0f) e = make_float3(soft_shoulder(e.x, sh), soft_shoulder(e.y, sh), soft_shoulder(e.z, sh));
             float4 acc = erow[sx];
-            acc.x += e.x * wgt;
-            acc.y += e.y * wgt;
-            acc.z += e.z * wgt;
+            acc.x += e.x * gain * wgt;
+            acc.y += e.y * gain * wgt;
+            acc.z += e.z * gain * wgt;
             erow[sx] = acc;
         }
         return;

@@ -43,6 +43,7 @@ struct BankEntry {
     std::vector<float> wavelengths;
     bool cufft = false;  // built with the comparator form (its spectra follow)
     bool h16 = false;    // chosen form: kernel spectra in FP16 with per-column scales
+    bool split_sums = false;  // s_core / s_struct computed (first Split render of the bank)
     DevBuf canvas, ring_round, ring_ceil, ring_peak, ring_mean, scalars, wl;
     PsfBankArgs args{};
 };
@@ -455,7 +456,9 @@ std::string bank_key(const ld_params& p, const std::vector<float>& wl) {
 
 void validate_params(const ld_params& p) {
     if (p.debug_view != LD_DEBUG_FINAL) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-debug-view"};
-    if (p.look_mode != LD_LOOK_PHYSICAL) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-look-mode-split"};
+    if (p.look_mode != LD_LOOK_PHYSICAL && p.look_mode != LD_LOOK_SPLIT) throw Fail{LD_ERR_ARG, "invalid-look-mode"};
+    if (p.look_mode == LD_LOOK_SPLIT && p.fft_form == LD_FFT_CUFFT)
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-split-look-with-cufft-form"};
     if (p.input_transfer != LD_TRANSFER_LINEAR) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-input-transfer"};
     if (p.resolution_aware) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-resolution-aware"};
     if (p.aperture_mode != LD_APERTURE_CIRCLE && p.aperture_mode != LD_APERTURE_POLYGON &&
@@ -690,6 +693,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     b.wavelengths = wl;
     b.cufft = p.fft_form == LD_FFT_CUFFT;
     b.h16 = chosen_h16(p);
+    b.split_sums = false;
     b.key = key;
     b.valid = true;
     c->spectra.valid = false;
@@ -702,6 +706,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
 // ---------------------------------------------------------------------------
 struct Combination {
     int mono = 0;
+    int parts = 1;  // kernel sets: 1 (Physical: full) or 2 (Split: core, structure)
     int n_drv = 1, n_ker = 3, n_out = 3;
     int luma_lock = 0;
     float saturation = 1.0f;
@@ -727,6 +732,7 @@ Combination make_combination(const ld_params& p, const std::vector<float>& wl) {
     const int B = static_cast<int>(wl.size());
     if (is_mono(p)) {  // convolveRgba, CpuReference.cpp:1195-1217
         cb.mono = 1;
+        cb.parts = p.look_mode == LD_LOOK_SPLIT ? 2 : 1;
         cb.n_drv = 3;
         cb.n_ker = 1;
         cb.n_out = 3;
@@ -769,11 +775,13 @@ Combination make_combination(const ld_params& p, const std::vector<float>& wl) {
     cb.n_ker = cb.luma_lock ? 4 : 3;
     cb.n_out = cb.n_ker;
     cb.n_drv = 1;
+    cb.parts = p.look_mode == LD_LOOK_SPLIT ? 2 : 1;
     return cb;
 }
 
 std::string spectra_key_for(const std::string& bank_key_s, const Combination& cb, const GridGeom& g) {
     std::string k = bank_key_s;
+    k = append_bytes(k, &cb.parts, sizeof(int));
     k = append_bytes(k, &cb.n_ker, sizeof(int));
     k = append_bytes(k, cb.coef, sizeof(cb.coef));
     k = append_bytes(k, &g.Px, sizeof(int));
@@ -836,6 +844,20 @@ GridGeom make_geometry(ld_ctx* c, int W, int H, int K, int c_rows, int c_cols, i
     return g;
 }
 
+// Layout of a kernel-spectra buffer: the parts' spectra (float2, or half2 in
+// the chosen form) back to back, 256-byte aligned, then one float scale per
+// column for each part (chosen form).
+size_t ks_part_bytes(int n_ker, const GridGeom& g, bool h16) {
+    return align256(static_cast<size_t>(n_ker) * g.cols * g.Py * (h16 ? 4 : 8));
+}
+const float2* ks_part(const void* base, int part, int n_ker, const GridGeom& g, bool h16) {
+    return reinterpret_cast<const float2*>(static_cast<const char*>(base) + part * ks_part_bytes(n_ker, g, h16));
+}
+const float* ks_scale(const void* base, int part, int parts, int n_ker, const GridGeom& g, bool h16) {
+    return reinterpret_cast<const float*>(static_cast<const char*>(base) + parts * ks_part_bytes(n_ker, g, h16)) +
+           static_cast<size_t>(part) * g.cols;
+}
+
 // Kernel spectra of bank `b` into entry `e` (combination, row and column
 // transforms), unless `e` already holds them.
 SpectraEntry& ensure_spectra_in(ld_ctx* c, SpectraEntry& e, BankEntry& b, const Combination& cb, const GridGeom& g,
@@ -844,12 +866,17 @@ SpectraEntry& ensure_spectra_in(ld_ctx* c, SpectraEntry& e, BankEntry& b, const 
     *rebuilt = false;
     if (e.valid && e.key == key) return e;
     e.valid = false;
+    if (cb.parts == 2 && !b.split_sums) {
+        staged(c, LD_STAGE_CROP_SUM, s, [&] { launch_split_sums(b.args, s); });
+        b.split_sums = true;
+    }
     CombineArgs ca{};
     ca.bank = b.args;
     ca.n_ker = cb.n_ker;
+    ca.split = cb.parts == 2 ? 1 : 0;
     std::memcpy(ca.coef, cb.coef, sizeof(ca.coef));
     const size_t kk = static_cast<size_t>(b.K) * b.K;
-    ca.out = static_cast<float*>(ensure(c, c->combine_out, cb.n_ker * kk * sizeof(float)));
+    ca.out = static_cast<float*>(ensure(c, c->combine_out, cb.parts * cb.n_ker * kk * sizeof(float)));
     staged(c, LD_STAGE_COMBINE, s, [&] { launch_combine(ca, s); });
     KernelSpectraArgs ka{};
     ka.g = g;
@@ -857,24 +884,27 @@ SpectraEntry& ensure_spectra_in(ld_ctx* c, SpectraEntry& e, BankEntry& b, const 
     ka.R = b.R;
     ka.K = b.K;
     ka.Kp = b.K + (b.K & 1);
-    ka.canvas = ca.out;
     ka.rows = static_cast<float2*>(
         ensure(c, c->kspec_rows, static_cast<size_t>(cb.n_ker) * g.cols * ka.Kp * sizeof(float2)));
-    const size_t ks_bytes = align256(static_cast<size_t>(cb.n_ker) * g.cols * g.Py * (b.h16 ? 4 : 8));
-    char* ksbuf = static_cast<char*>(ensure(c, e.spectra, ks_bytes + static_cast<size_t>(g.cols) * sizeof(float)));
-    ka.spectra = reinterpret_cast<float2*>(ksbuf);
+    const size_t part_bytes = ks_part_bytes(cb.n_ker, g, b.h16);
+    char* ksbuf = static_cast<char*>(
+        ensure(c, e.spectra, cb.parts * (part_bytes + static_cast<size_t>(g.cols) * sizeof(float))));
     ka.h16 = b.h16 ? 1 : 0;
-    ka.kscale = reinterpret_cast<float*>(ksbuf + ks_bytes);
     ka.scale = static_cast<float>(1.0 / (static_cast<double>(g.M) * static_cast<double>(g.Py)));
     ka.err = c->err;
-    if (b.cufft) {
-        // cuFFT layout: KS [n_ker][Py][Px/2+1], the same size as the own layout
-        float* planes = static_cast<float*>(
-            ensure(c, c->cf_planes, static_cast<size_t>(cb.n_ker) * g.Px * g.Py * sizeof(float)));
-        staged(c, LD_STAGE_KSPEC_COLS, s, [&] { cf_kernel_spectra(ka, planes, c->cufft, s); });
-    } else {
-        staged(c, LD_STAGE_KSPEC_ROWS, s, [&] { launch_kspec_rows(ka, s); });
-        staged(c, LD_STAGE_KSPEC_COLS, s, [&] { launch_kspec_cols(ka, s); });
+    for (int part = 0; part < cb.parts; ++part) {
+        ka.canvas = ca.out + static_cast<size_t>(part) * cb.n_ker * kk;
+        ka.spectra = const_cast<float2*>(ks_part(ksbuf, part, cb.n_ker, g, b.h16));
+        ka.kscale = const_cast<float*>(ks_scale(ksbuf, part, cb.parts, cb.n_ker, g, b.h16));
+        if (b.cufft) {
+            // cuFFT layout: KS [n_ker][Py][Px/2+1], the same size as the own layout
+            float* planes = static_cast<float*>(
+                ensure(c, c->cf_planes, static_cast<size_t>(cb.n_ker) * g.Px * g.Py * sizeof(float)));
+            staged(c, LD_STAGE_KSPEC_COLS, s, [&] { cf_kernel_spectra(ka, planes, c->cufft, s); });
+        } else {
+            staged(c, LD_STAGE_KSPEC_ROWS, s, [&] { launch_kspec_rows(ka, s); });
+            staged(c, LD_STAGE_KSPEC_COLS, s, [&] { launch_kspec_cols(ka, s); });
+        }
     }
     check_launch("kernel-spectra");
     e.g = g;
@@ -1312,12 +1342,13 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         char* bbuf = static_cast<char*>(ensure(ctx, ctx->frameB, b_bytes + static_cast<size_t>(g.cols) * sizeof(float)));
         fa.Bout = reinterpret_cast<float2*>(bbuf);
         fa.bscale = reinterpret_cast<float*>(bbuf + b_bytes);
-        fa.spectra = static_cast<const float2*>(sp.spectra.p);
-        fa.kscale = reinterpret_cast<const float*>(
-            static_cast<const char*>(sp.spectra.p) +
-            align256(static_cast<size_t>(cb.n_ker) * g.cols * g.Py * (fa.h16 ? 4 : 8)));
+        fa.spectra = ks_part(sp.spectra.p, 0, cb.n_ker, g, fa.h16);
+        fa.kscale = ks_scale(sp.spectra.p, 0, cb.parts, cb.n_ker, g, fa.h16);
         fa.err = ctx->err;
-        fa.effect_mode = zones ? kEffectAccumulate : (fa.preserve ? kEffectStore : kEffectComposite);
+        const bool split = cb.parts == 2;
+        fa.effect_mode = (zones || split) ? kEffectAccumulate : (fa.preserve ? kEffectStore : kEffectComposite);
+        fa.acc_gain = 1.0f;
+        fa.acc_shoulder = 0.0f;
         if (fa.effect_mode != kEffectComposite) {
             fa.effect = static_cast<float4*>(
                 ensure(ctx, ctx->effect, static_cast<size_t>(W) * H * sizeof(float4) + 2 * sizeof(double)));
@@ -1326,7 +1357,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         auto clear_effect = [&]() {
             if (fa.effect_mode == kEffectComposite) return;
             check_cuda(cudaMemsetAsync(fa.sums, 0, 2 * sizeof(double), s), "effect-memset");
-            if (zones)
+            if (fa.effect_mode == kEffectAccumulate)
                 check_cuda(cudaMemsetAsync(fa.effect, 0, static_cast<size_t>(W) * H * sizeof(float4), s),
                            "effect-memset");
         };
@@ -1359,29 +1390,45 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         std::string gkey(reinterpret_cast<const char*>(&fa), sizeof(fa));
         for (const SpectraEntry* e : spectra) gkey = append_bytes(gkey, &e->spectra.p, sizeof(void*));
         gkey = append_bytes(gkey, &zn, sizeof(zn));
-        auto chain = [&, fa]() mutable {  // the zone loop edits this copy
+        // Split look: core then structure, each with its gain and shoulder
+        // (LensDiffCpuReference.cpp:2123-2146); Physical: the full kernels
+        const float gains[2] = {split ? static_cast<float>(std::max(0.0, p.core_gain)) : 1.0f,
+                                static_cast<float>(std::max(0.0, p.structure_gain))};
+        const float shoulders[2] = {split ? static_cast<float>(p.core_shoulder) : 0.0f,
+                                    static_cast<float>(p.structure_shoulder)};
+        gkey = append_bytes(gkey, gains, sizeof(gains));
+        gkey = append_bytes(gkey, shoulders, sizeof(shoulders));
+        gkey = append_bytes(gkey, &cb.parts, sizeof(cb.parts));
+        auto chain = [&, fa]() mutable {  // the loops below edit this copy
             clear_effect();
             staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
-            if (!zones) {
+            if (fa.effect_mode != kEffectAccumulate) {
                 staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
                 staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse(fa, s); });
             } else {
-                fa.zone_n = zn;
-                for (int z = 0; z < zn * zn; ++z) {
-                    fa.spectra = static_cast<const float2*>(spectra[static_cast<size_t>(z)]->spectra.p);
-                    fa.kscale = reinterpret_cast<const float*>(
-                        static_cast<const char*>(spectra[static_cast<size_t>(z)]->spectra.p) +
-                        align256(static_cast<size_t>(cb.n_ker) * g.cols * g.Py * (fa.h16 ? 4 : 8)));
-                    fa.zone_x = z % zn;
-                    fa.zone_y = z / zn;
-                    // source rows whose tent weight can be non-zero (the kernel
-                    // evaluates the weight itself; one row of margin each side)
-                    const double step = static_cast<double>(std::max(1, H - 1)) / static_cast<double>(zn - 1);
-                    const int r0 = std::max(0, static_cast<int>(std::floor((fa.zone_y - 1) * step)) - 1);
-                    const int r1 = std::min(H, static_cast<int>(std::ceil((fa.zone_y + 1) * step)) + 2);
+                const int nz = zones ? zn * zn : 1;
+                fa.zone_n = zones ? zn : 0;
+                for (int z = 0; z < nz; ++z) {
+                    const void* base = spectra[static_cast<size_t>(z)]->spectra.p;
+                    int r0 = 0, r1 = H;
+                    if (zones) {
+                        fa.zone_x = z % zn;
+                        fa.zone_y = z / zn;
+                        // source rows whose tent weight can be non-zero (the kernel
+                        // evaluates the weight itself; one row of margin each side)
+                        const double step = static_cast<double>(std::max(1, H - 1)) / static_cast<double>(zn - 1);
+                        r0 = std::max(0, static_cast<int>(std::floor((fa.zone_y - 1) * step)) - 1);
+                        r1 = std::min(H, static_cast<int>(std::ceil((fa.zone_y + 1) * step)) + 2);
+                    }
                     fa.row0 = r0;
-                    staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
-                    staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse_rows(fa, r1 - r0, s); });
+                    for (int part = 0; part < cb.parts; ++part) {
+                        fa.spectra = ks_part(base, part, cb.n_ker, g, fa.h16);
+                        fa.kscale = ks_scale(base, part, cb.parts, cb.n_ker, g, fa.h16);
+                        fa.acc_gain = gains[part];
+                        fa.acc_shoulder = shoulders[part];
+                        staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
+                        staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse_rows(fa, r1 - r0, s); });
+                    }
                 }
                 if (fa.preserve) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_effect_sums(fa, s); });
             }

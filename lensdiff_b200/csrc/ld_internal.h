@@ -33,6 +33,8 @@ struct PsfScalars {      // per wavelength, FP64 sums of the shaping chain
     double s3;           // sum of the shaped kernel (unnormalised)
     double s4;           // sum of the cropped, tapered, normalised kernel
     double energy;       // sum of |F|^2 over the computed window (raw PSF export)
+    double s_core;       // Split look: sum of mean * taper over the crop box
+    double s_struct;     // Split look: sum of max(0, shaped / s3 - mean) * taper over the crop box
     unsigned int peak;   // max shaped value (float bits)
     int radius;          // adaptive support radius
     float extent, fade, start;  // taper constants
@@ -73,14 +75,20 @@ void launch_resample(const PsfBankArgs& a, cudaStream_t s);
 void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s);
 void launch_support(const PsfBankArgs& a, cudaStream_t s);
 void launch_crop_sum(const PsfBankArgs& a, cudaStream_t s);
+void launch_split_sums(const PsfBankArgs& a, cudaStream_t s);  // s_core, s_struct (Split look)
 
 // Combination of the per-wavelength final kernels into n_ker output kernels:
 // out[k][i] = sum_b coef[k][b] * final_b[i].
+// Split look: 2 * n_ker planes, the core kernels (azimuthal mean, cropped,
+// tapered, normalised; populatePsfBankCacheFromBaseKernels,
+// LensDiffCpuReference.cpp:1631-1645) then the structure kernels (positive
+// residual of the shaped kernel over the mean, same crop).
 struct CombineArgs {
     PsfBankArgs bank;
     int n_ker;
+    int split;
     float coef[4][kMaxBins];
-    float* out;                  // [n_ker][K][K]
+    float* out;                  // [n_ker][K][K], Split: [2][n_ker][K][K]
 };
 void launch_combine(const CombineArgs& a, cudaStream_t s);
 
@@ -176,7 +184,11 @@ struct FrameArgs {
     // sums[0] / sums[1] when `preserve`.
     int effect_mode;
     int preserve;
-    int zone_x, zone_y, zone_n, row0;
+    int zone_x, zone_y, zone_n, row0;  // zone_n = 0: no field zones (weight 1)
+    // kEffectAccumulate adds weight * gain * shoulder(effect): Split look
+    // (core / structure gains and soft shoulders, LensDiffCpuReference.cpp:
+    // 2123-2146, :1340-1352); 1 and 0 otherwise
+    float acc_gain, acc_shoulder;
     float4* effect;            // [H][W]
     double* sums;              // [2]
     // epilogue

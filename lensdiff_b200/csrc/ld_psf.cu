@@ -495,32 +495,103 @@ __global__ void __launch_bounds__(256) crop_sum_kernel(PsfBankArgs a) {
     if (threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(&a.scalars[b].s4, tot);
 }
 
+// grid (ceil(K/32), ceil(K/32), B): the Split look's normalisers after the
+// crop (the canvas holds shaped * taper, 0 outside the crop box):
+// s_core = sum of mean * taper, s_struct = sum of max(0, shaped * taper / s3
+// - mean * taper) over the crop box.
+__global__ void __launch_bounds__(256) split_sums_kernel(PsfBankArgs a) {
+    const int b = blockIdx.z;
+    const PsfScalars& sc = a.scalars[b];
+    const float inv_s3 = static_cast<float>(1.0 / sc.s3);
+    const int rho = sc.radius;
+    const int K = a.K, R = a.R;
+    const float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
+    const float* rm = a.ring_mean + static_cast<size_t>(b) * (R + 1);
+    const int x = blockIdx.x * kTile + threadIdx.x;
+    double lcore = 0.0, lstruct = 0.0;
+#pragma unroll
+    for (int i = 0; i < kTile / 8; ++i) {
+        const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
+        if (x < K && y < K) {
+            const int ix = x - R, iy = y - R;
+            if (abs(ix) <= rho && abs(iy) <= rho) {
+                const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
+                const float rad = sqrtf(dx * dx + dy * dy);
+                const float wgt = taper_weight(rad, sc.extent, sc.fade, sc.start);
+                const float mt = rm[min(R, static_cast<int>(roundf(rad)))] * wgt;
+                lcore += static_cast<double>(mt);
+                lstruct += static_cast<double>(fmaxf(0.0f, canvas[static_cast<size_t>(y) * K + x] * inv_s3 - mt));
+            }
+        }
+    }
+    const double tc = block_sum(lcore);
+    if (threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(&a.scalars[b].s_core, tc);
+    __syncthreads();
+    const double ts = block_sum(lstruct);
+    if (threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(&a.scalars[b].s_struct, ts);
+}
+
 // grid (ceil(K/32), ceil(K/32)), block (32, 8): out[k] = sum_b coef[k][b] *
 // final_b with final_b = canvas_b / (s3_b * s4_b).
 __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
-    __shared__ float inv[kMaxBins];
+    __shared__ float inv[kMaxBins], inv_s3[kMaxBins], inv_core[kMaxBins], inv_struct[kMaxBins];
+    __shared__ float ext[kMaxBins], fade[kMaxBins], start[kMaxBins];
+    __shared__ int rho[kMaxBins];
     const int tid = threadIdx.x + threadIdx.y * 32;
     const int B = a.bank.B;
     for (int b = tid; b < B; b += 256) {
         const PsfScalars& sc = a.bank.scalars[b];
         inv[b] = static_cast<float>(1.0 / (sc.s3 * sc.s4));
+        inv_s3[b] = static_cast<float>(1.0 / sc.s3);
+        inv_core[b] = sc.s_core > 0.0 ? static_cast<float>(1.0 / sc.s_core) : 0.0f;
+        inv_struct[b] = sc.s_struct > 0.0 ? static_cast<float>(1.0 / sc.s_struct) : 0.0f;
+        ext[b] = sc.extent;
+        fade[b] = sc.fade;
+        start[b] = sc.start;
+        rho[b] = sc.radius;
     }
     __syncthreads();
     const int x = blockIdx.x * kTile + threadIdx.x;
-    const int K = a.bank.K;
+    const int K = a.bank.K, R = a.bank.R;
     const size_t plane = static_cast<size_t>(K) * K;
 #pragma unroll 1
     for (int i = 0; i < kTile / 8; ++i) {
         const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
         if (x >= K || y >= K) continue;
         const size_t idx = static_cast<size_t>(y) * K + x;
-        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        for (int b = 0; b < B; ++b) {
-            const float v = a.bank.canvas[b * plane + idx] * inv[b];
+        if (!a.split) {
+            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            for (int b = 0; b < B; ++b) {
+                const float v = a.bank.canvas[b * plane + idx] * inv[b];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) acc[k] += a.coef[k][b] * v;
+                for (int k = 0; k < 4; ++k) acc[k] += a.coef[k][b] * v;
+            }
+            for (int k = 0; k < a.n_ker; ++k) a.out[k * plane + idx] = acc[k];
+            continue;
         }
-        for (int k = 0; k < a.n_ker; ++k) a.out[k * plane + idx] = acc[k];
+        // Split: core = mean * taper / s_core, structure = max(0, shaped / s3
+        // - mean) * taper / s_struct; the canvas holds shaped * taper
+        const int ix = x - R, iy = y - R;
+        const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
+        const float rad = sqrtf(dx * dx + dy * dy);
+        const int ring = min(R, static_cast<int>(roundf(rad)));
+        float core[4] = {0.0f, 0.0f, 0.0f, 0.0f}, strc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (int b = 0; b < B; ++b) {
+            if (abs(ix) > rho[b] || abs(iy) > rho[b]) continue;
+            const float wgt = taper_weight(rad, ext[b], fade[b], start[b]);
+            const float mt = a.bank.ring_mean[static_cast<size_t>(b) * (R + 1) + ring] * wgt;
+            const float c = mt * inv_core[b];
+            const float st = fmaxf(0.0f, a.bank.canvas[b * plane + idx] * inv_s3[b] - mt) * inv_struct[b];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                core[k] += a.coef[k][b] * c;
+                strc[k] += a.coef[k][b] * st;
+            }
+        }
+        for (int k = 0; k < a.n_ker; ++k) {
+            a.out[k * plane + idx] = core[k];
+            a.out[(a.n_ker + k) * plane + idx] = strc[k];
+        }
     }
 }
 
@@ -710,6 +781,10 @@ void launch_support(const PsfBankArgs& a, cudaStream_t s) { support_kernel<<<a.B
 
 void launch_crop_sum(const PsfBankArgs& a, cudaStream_t s) {
     crop_sum_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
+}
+
+void launch_split_sums(const PsfBankArgs& a, cudaStream_t s) {
+    split_sums_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
 }
 
 void launch_combine(const CombineArgs& a, cudaStream_t s) {

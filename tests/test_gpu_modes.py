@@ -238,3 +238,39 @@ def test_chosen_form_field_zones(cache):
     out = _render(cache, with_matrices(p.copy(fftForm=LensDiffFftForm.OwnChosen)), src)
     ref = R.render(p, src)
     assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
+
+
+# ------------------------------------------------------------- Split look ----
+# Core (azimuthal mean) and structure (positive residual) kernels convolved
+# separately, each spectrally mapped, soft-shouldered and weighted
+# (LensDiffCpuReference.cpp:2123-2146, :1631-1645, :84-90, :1340-1368).
+@pytest.mark.parametrize("kw", [
+    {"spectralMode": LensDiffSpectralMode.Tristimulus},
+    {"spectralMode": LensDiffSpectralMode.Mono, "coreShoulder": 0.0},
+    {"spectralMode": LensDiffSpectralMode.Spectral9, "energyMode": LensDiffEnergyMode.Preserve,
+     "anisotropyEmphasis": 0.3},
+])
+def test_split_look_matches_reference(cache, kw):
+    from lensdiff_b200.types import LensDiffLookMode
+    _reference_available()
+    p = _lens(lookMode=LensDiffLookMode.Split, coreGain=0.8, structureGain=1.4, coreShoulder=2.0,
+              structureShoulder=0.5, **{k: v for k, v in kw.items() if k != "coreShoulder"})
+    if "coreShoulder" in kw:
+        p = p.copy(coreShoulder=kw["coreShoulder"])
+    src = S.make_frame(224, 144, 20, 1.0, 80.0, seed=51)
+    out = _render(cache, with_matrices(p), src)
+    ref = R.render(p, src)
+    assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
+    phys = R.render(p.copy(lookMode=LensDiffLookMode.Physical), src)
+    assert rel_err(phys, ref, ref[..., :3].max()) > 20 * OUT_TOL  # the look matters here
+
+
+def test_split_look_with_field_zones_and_chosen_form(cache):
+    from lensdiff_b200.types import LensDiffFftForm, LensDiffLookMode
+    _reference_available()
+    p = _field_lens(lookMode=LensDiffLookMode.Split, coreGain=1.0, structureGain=1.2, structureShoulder=1.0)
+    src = S.make_frame(200, 120, 16, 1.0, 60.0, seed=52)
+    ref = R.render(p, src)
+    for form in (LensDiffFftForm.OwnFp32, LensDiffFftForm.OwnChosen):
+        out = _render(cache, with_matrices(p.copy(fftForm=form)), src)
+        assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL, form
