@@ -424,6 +424,34 @@ PupilParams pupil_params(const ld_params& p, bool circle_reference) {
     pp.decy = static_cast<float>(p.pupil_decenter_y);
     pp.phase_cs = std::cos(-pp.rotation);  // LensDiffPhase.cpp:225-226
     pp.phase_sn = std::sin(-pp.rotation);
+    // per-mode constants with the reference's float expressions
+    const float outer = 0.86f;
+    const float rnd = pp.roundness;
+    auto clampf = [](float v, float lo, float hi) { return std::min(std::max(v, lo), hi); };
+    pp.star_inner = outer * clampf(0.18f + rnd * 0.62f, 0.1f, 0.95f);  // CpuReference.cpp:776, :520
+    pp.spiral_twist = 4.0f + (1.0f - clampf(rnd, 0.0f, 1.0f)) * 8.0f;  // :663-664
+    pp.spiral_opening = 0.18f + clampf(rnd, 0.0f, 1.0f) * 0.26f;
+    pp.grid_half = outer * 0.82f;  // :586-594
+    pp.grid_pitch = (2.0f * pp.grid_half) / static_cast<float>(pp.sides);
+    pp.grid_bar = pp.grid_pitch * (0.06f + (1.0f - clampf(rnd, 0.0f, 1.0f)) * 0.12f);
+    pp.snow_levels = std::min(std::max(std::max(2, std::max(3, p.blade_count) / 2), 2), 5);  // :619-623
+    pp.snow_main = outer * 0.92f;
+    pp.snow_thick = outer * (0.045f + (1.0f - clampf(rnd, 0.0f, 1.0f)) * 0.05f);
+    const float branch_angle = kPiRef / 5.5f;
+    for (int arm = 0; arm < 6; ++arm) {
+        const float angle = pp.rotation - kPiRef * 0.5f + static_cast<float>(arm) * (kPiRef / 3.0f);
+        pp.snow_arm_cs[arm] = std::cos(angle);
+        pp.snow_arm_sn[arm] = std::sin(angle);
+        for (int side = 0; side < 2; ++side) {
+            const float theta = angle + static_cast<float>(side == 0 ? -1 : 1) * branch_angle;
+            pp.snow_br_cs[arm][side] = std::cos(theta);
+            pp.snow_br_sn[arm][side] = std::sin(theta);
+        }
+    }
+    for (int level = 0; level < pp.snow_levels; ++level) {
+        pp.snow_t[level] = 0.34f + static_cast<float>(level) * (0.44f / static_cast<float>(std::max(1, pp.snow_levels - 1)));
+        pp.snow_len[level] = outer * (0.16f + 0.03f * static_cast<float>(level));
+    }
     return pp;
 }
 
@@ -461,9 +489,10 @@ void validate_params(const ld_params& p) {
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-split-look-with-cufft-form"};
     if (p.input_transfer != LD_TRANSFER_LINEAR) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-input-transfer"};
     if (p.resolution_aware) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-resolution-aware"};
-    if (p.aperture_mode != LD_APERTURE_CIRCLE && p.aperture_mode != LD_APERTURE_POLYGON &&
-        p.aperture_mode != LD_APERTURE_HEXAGON)
-        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-aperture-mode"};
+    if (p.aperture_mode == LD_APERTURE_CUSTOM)  // image loader: WIC / ImageIO only (LensDiffApertureImage.cpp)
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-custom-aperture"};
+    if (p.aperture_mode < LD_APERTURE_CIRCLE || p.aperture_mode > LD_APERTURE_SNOWFLAKE)
+        throw Fail{LD_ERR_ARG, "invalid-aperture-mode"};
     if (p.apodization_mode < 0 || p.apodization_mode > 2) throw Fail{LD_ERR_ARG, "invalid-apodization-mode"};
     if (p.spectral_mode < 0 || p.spectral_mode > 3) throw Fail{LD_ERR_ARG, "invalid-spectral-mode"};
     if (p.field_grid != 0 && (p.field_grid < 2 || p.field_grid > kMaxFieldGrid))
@@ -1521,9 +1550,9 @@ int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float
     return run_guarded(ctx, st, [&]() {
         const ld_params& p = *params;
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        if (p.aperture_mode != LD_APERTURE_CIRCLE && p.aperture_mode != LD_APERTURE_POLYGON &&
-            p.aperture_mode != LD_APERTURE_HEXAGON)
-            throw Fail{LD_ERR_UNSUPPORTED, "unsupported-aperture-mode"};
+        if (p.aperture_mode == LD_APERTURE_CUSTOM) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-custom-aperture"};
+        if (p.aperture_mode < LD_APERTURE_CIRCLE || p.aperture_mode > LD_APERTURE_SNOWFLAKE)
+            throw Fail{LD_ERR_ARG, "invalid-aperture-mode"};
         fill_sizes(st, p);
         const std::vector<float> wl = wavelengths_of(p);
         if (wavelength_index < 0 || wavelength_index >= static_cast<int>(wl.size()))

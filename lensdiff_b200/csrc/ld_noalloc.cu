@@ -114,8 +114,8 @@ extern "C" int ld_raw_psf_noalloc(const ld_params* params, int wavelength_index,
         return LD_ERR_ARG;
     }
     const ld_params& p = *params;
-    if (p.aperture_mode != LD_APERTURE_CIRCLE && p.aperture_mode != LD_APERTURE_POLYGON &&
-        p.aperture_mode != LD_APERTURE_HEXAGON) {
+    if (p.aperture_mode == LD_APERTURE_CUSTOM || p.aperture_mode < LD_APERTURE_CIRCLE ||
+        p.aperture_mode > LD_APERTURE_SNOWFLAKE) {
         set_stage(st, LD_ERR_UNSUPPORTED, "unsupported-aperture-mode");
         return LD_ERR_UNSUPPORTED;
     }

@@ -3,7 +3,7 @@
 // Each function restates a reference function with the same float32
 // expression order, so that discrete decisions (inside/outside the aperture,
 // ring index of a pixel) agree with the reference's CPU code:
-//   pupil amplitude  LensDiffCpuReference.cpp:451-488, :670-680, :758-822
+//   pupil amplitude  LensDiffCpuReference.cpp:451-488, :509-668, :670-680, :758-822
 //   Zernike phase    LensDiffPhase.cpp:170-243 (Noll 4..17) + standard Noll
 //                    j = 1..3, 18..22 (extension)
 //   kernel taper     LensDiffCpuReference.cpp:957-982
@@ -20,8 +20,8 @@ constexpr int kMaxVanes = 16;
 
 struct PupilParams {
     int size;          // N_p
-    int mode;          // aperture mode (0 circle, 1 polygon, 5 hexagon)
-    int sides;         // polygon sides
+    int mode;          // aperture mode (LD_APERTURE_*; hexagon is a 6-sided polygon)
+    int sides;         // polygon sides / star points / grid divisions / spiral arms (>= 3)
     int apod;          // apodisation mode
     int vanes;         // vane line count (0: none)
     float roundness;   // clamped to [0,1]
@@ -33,6 +33,16 @@ struct PupilParams {
     float vane_sn[kMaxVanes];
     // phase raster
     float phase_cs, phase_sn;  // cos/sin(-rotation)
+    // per-mode constants, computed on the host with the reference's float
+    // expressions (they are the same for every pixel)
+    float star_inner;          // Star: inner radius (outer * clamped inner ratio)
+    float spiral_twist, spiral_opening;
+    float grid_half, grid_pitch, grid_bar;  // SquareGrid
+    int snow_levels;                        // Snowflake
+    float snow_main, snow_thick;
+    float snow_arm_cs[6], snow_arm_sn[6];
+    float snow_br_cs[6][2], snow_br_sn[6][2];
+    float snow_t[5], snow_len[5];
 };
 
 struct PhaseCoeffs {
@@ -66,6 +76,87 @@ __device__ __forceinline__ float apodization(int mode, float radial) {
     return 1.0f;
 }
 
+// starMetric (LensDiffCpuReference.cpp:509-536)
+__device__ __forceinline__ float star_metric(float nx, float ny, int points, float inner, float rotation) {
+    const float radius = sqrtf(nx * nx + ny * ny);
+    if (radius <= 1e-6f) return 0.0f;
+    const float angle = atan2f(ny, nx) - rotation + kPiF * 0.5f;
+    const float sector = 2.0f * kPiF / static_cast<float>(points);
+    float local = fmodf(angle, sector);
+    if (local < 0.0f) local += sector;
+    const float half = sector * 0.5f;
+    const float t = local <= half ? local / fmaxf(half, 1e-6f) : (sector - local) / fmaxf(half, 1e-6f);
+    const float boundary = inner + (kOuterRadius - inner) * fminf(fmaxf(t, 0.0f), 1.0f);
+    return radius / fmaxf(boundary, 1e-5f);
+}
+
+// distancePointToSegment (LensDiffCpuReference.cpp:558-574)
+__device__ __forceinline__ float segment_distance(float px, float py, float ax, float ay, float bx, float by) {
+    const float vx = bx - ax;
+    const float vy = by - ay;
+    const float len2 = vx * vx + vy * vy;
+    if (len2 <= 1e-10f) {
+        const float dx = px - ax;
+        const float dy = py - ay;
+        return sqrtf(dx * dx + dy * dy);
+    }
+    const float t = fminf(fmaxf(((px - ax) * vx + (py - ay) * vy) / len2, 0.0f), 1.0f);
+    const float cx = ax + t * vx;
+    const float cy = ay + t * vy;
+    const float dx = px - cx;
+    const float dy = py - cy;
+    return sqrtf(dx * dx + dy * dy);
+}
+
+// squareGridMaskOpen (LensDiffCpuReference.cpp:576-606)
+__device__ __forceinline__ bool square_grid_open(const PupilParams& p, float nx, float ny) {
+    const float rx = nx * p.phase_cs - ny * p.phase_sn;
+    const float ry = nx * p.phase_sn + ny * p.phase_cs;
+    const float h = p.grid_half;
+    if (fabsf(rx) > h || fabsf(ry) > h) return false;
+    auto nearest = [&](float v) {
+        const float wrapped = fmodf(v + h, p.grid_pitch);
+        const float positive = wrapped < 0.0f ? wrapped + p.grid_pitch : wrapped;
+        return fminf(positive, p.grid_pitch - positive);
+    };
+    const float dx = nearest(rx), dy = nearest(ry);
+    const float ex = fabsf(fabsf(rx) - h), ey = fabsf(fabsf(ry) - h);
+    return dx <= p.grid_bar || dy <= p.grid_bar || ex <= p.grid_bar || ey <= p.grid_bar;
+}
+
+// snowflakeMaskOpen (LensDiffCpuReference.cpp:608-648)
+__device__ __forceinline__ bool snowflake_open(const PupilParams& p, float nx, float ny) {
+    const float radius = sqrtf(nx * nx + ny * ny);
+    if (radius > kOuterRadius) return false;
+    float best = 3.402823466e38f;
+    for (int arm = 0; arm < 6; ++arm) {
+        const float cs = p.snow_arm_cs[arm], sn = p.snow_arm_sn[arm];
+        best = fminf(best, segment_distance(nx, ny, 0.0f, 0.0f, cs * p.snow_main, sn * p.snow_main));
+        for (int level = 0; level < p.snow_levels; ++level) {
+            const float t = p.snow_t[level];
+            const float mx = cs * p.snow_main * t;
+            const float my = sn * p.snow_main * t;
+            for (int side = 0; side < 2; ++side) {
+                const float bx = mx + p.snow_br_cs[arm][side] * p.snow_len[level];
+                const float by = my + p.snow_br_sn[arm][side] * p.snow_len[level];
+                best = fminf(best, segment_distance(nx, ny, mx, my, bx, by));
+            }
+        }
+    }
+    return best <= p.snow_thick;
+}
+
+// spiralMaskOpen (LensDiffCpuReference.cpp:650-668)
+__device__ __forceinline__ bool spiral_open(const PupilParams& p, float nx, float ny) {
+    const float radius = sqrtf(nx * nx + ny * ny);
+    if (radius > kOuterRadius) return false;
+    const float radial = radius / fmaxf(kOuterRadius, 1e-6f);
+    const float angle = atan2f(ny, nx) - p.rotation;
+    const float phase = static_cast<float>(p.sides) * angle + p.spiral_twist * radial * (2.0f * kPiF);
+    const float band = 0.5f + 0.5f * cosf(phase);
+    return band >= (1.0f - p.spiral_opening);
+}
+
 // buildPupilAmplitude per pixel (LensDiffCpuReference.cpp:778-818)
 __device__ __forceinline__ float pupil_amplitude(const PupilParams& p, int x, int y) {
     const float nx = pupil_coord(x, p.size);
@@ -74,8 +165,14 @@ __device__ __forceinline__ float pupil_amplitude(const PupilParams& p, int x, in
     const float dy = ny - p.decy;
     const float radius = sqrtf(dx * dx + dy * dy);
     bool inside;
-    if (p.mode == 0) inside = radius <= kOuterRadius;
-    else inside = polygon_metric(dx, dy, p.sides, p.roundness, p.rotation) <= 1.0f;
+    switch (p.mode) {
+        case 0: inside = radius <= kOuterRadius; break;
+        case 2: inside = star_metric(dx, dy, p.sides, p.star_inner, p.rotation) <= 1.0f; break;
+        case 3: inside = spiral_open(p, dx, dy); break;
+        case 6: inside = square_grid_open(p, dx, dy); break;
+        case 7: inside = snowflake_open(p, dx, dy); break;
+        default: inside = polygon_metric(dx, dy, p.sides, p.roundness, p.rotation) <= 1.0f; break;
+    }
     if (!inside || radius < p.obstruction) return 0.0f;
     for (int i = 0; i < p.vanes; ++i) {  // blockedByVanes, :471-488
         const float cs = p.vane_cs[i], sn = p.vane_sn[i];
