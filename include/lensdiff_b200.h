@@ -232,7 +232,7 @@ enum {
     LD_STAGE_PSF_ROWS = 0, LD_STAGE_PSF_COLS, LD_STAGE_RESAMPLE, LD_STAGE_SHAPE_STATS,
     LD_STAGE_SUPPORT, LD_STAGE_CROP_SUM, LD_STAGE_COMBINE, LD_STAGE_KSPEC_ROWS,
     LD_STAGE_KSPEC_COLS, LD_STAGE_FRAME_ROWS, LD_STAGE_FRAME_COLS, LD_STAGE_FRAME_INVERSE,
-    LD_STAGE_PUPIL, LD_STAGE_COMPOSITE, LD_STAGE_COUNT
+    LD_STAGE_PUPIL, LD_STAGE_COMPOSITE, LD_STAGE_SCATTER, LD_STAGE_WORKING_SOURCE, LD_STAGE_COUNT
 };
 /* Per-frame chains are captured into CUDA graphs on first use and replayed
  * when a later frame issues identical launches (same buffers, geometry and

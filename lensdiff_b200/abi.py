@@ -325,7 +325,8 @@ class ld_server_stats(ctypes.Structure):
     ]
 
 STAGE_NAMES = ["psf_rows", "psf_cols", "resample", "shape_stats", "support", "crop_sum", "combine",
-               "kspec_rows", "kspec_cols", "frame_rows", "frame_cols", "frame_inverse", "pupil", "composite"]
+               "kspec_rows", "kspec_cols", "frame_rows", "frame_cols", "frame_inverse", "pupil", "composite",
+               "scatter", "working_source"]
 
 
 def lib() -> ctypes.CDLL:

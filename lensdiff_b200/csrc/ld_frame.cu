@@ -139,7 +139,8 @@ __device__ __forceinline__ void store_bins(int M, int C, int64_t col_elems, int6
 // Mono (NDRV = 3): C = 3, one frame row per CTA, its three colour drivers.
 // Column col of the transform is row y0 + col / NDRV, driver col % NDRV; its
 // spectrum goes to A[k][y0 + col / NDRV][col % NDRV].
-template <int E, int C, int NDRV, int MAXT = Fam<E>::max_threads, int MINB = 1>
+// FROM_EFFECT (scatter, NDRV = 3): the drivers are the stored effect's RGB.
+template <int E, int C, int NDRV, int MAXT = Fam<E>::max_threads, int MINB = 1, bool FROM_EFFECT = false>
 __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
     extern __shared__ float2 smem[];
     constexpr int RPC = C / NDRV;  // frame rows per CTA
@@ -165,9 +166,13 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
             const int x0 = 2 * idx;
             const unsigned char* row = a.src + static_cast<int64_t>(y) * pitch;
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
-                px[u][h] = (i < RPC * M && y < H && x0 + h < W) ? load_px(row, x0 + h, aligned)
-                                                                 : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            for (int h = 0; h < 2; ++h) {
+                const bool in = i < RPC * M && y < H && x0 + h < W;
+                if constexpr (FROM_EFFECT)
+                    px[u][h] = in ? a.effect[static_cast<int64_t>(y) * W + x0 + h] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                else
+                    px[u][h] = in ? load_px(row, x0 + h, aligned) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
         }
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
@@ -181,7 +186,7 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
                 const float4 p = px[u][h];
                 float sig;
                 // zero pixels (outside the frame or black) give a zero driver
-                const float m = selection_mask(sel, p.x, p.y, p.z, &sig) * sel.rscale;
+                const float m = FROM_EFFECT ? 1.0f : selection_mask(sel, p.x, p.y, p.z, &sig) * sel.rscale;
                 if (NDRV == 1) {
                     const float dv = sig * m;
                     if (h == 0) v[0].x = dv;
@@ -344,14 +349,14 @@ __device__ __forceinline__ float zone_weight(int v, int extent, int z, int n) {
 
 // One row per CTA; smem M * C float2 (C = n_out interleaved channels).  The
 // row is output row out_y1 + blockIdx.x (kEffectComposite), source row
-// blockIdx.x (kEffectStore) or source row row0 + blockIdx.x
+// blockIdx.x (kEffectStore, kEffectScatter) or source row row0 + blockIdx.x
 // (kEffectAccumulate); see FrameArgs::effect_mode.
 template <int E, int C, int MAXT = Fam<E>::max_threads, int MINB = 1, bool H16 = false>
 __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) {
     extern __shared__ float2 smem[];
     const int bid = static_cast<int>(blockIdx.x);
     const int yo = a.effect_mode == kEffectComposite ? a.out_y1 + bid
-                                                     : a.src_y1 + (a.effect_mode == kEffectStore ? bid : a.row0 + bid);
+                                                     : a.src_y1 + (a.effect_mode == kEffectAccumulate ? a.row0 + bid : bid);
     const int sy = yo - a.src_y1;
     const bool have = sy >= 0 && sy < a.H;
     const int M = a.g.M;
@@ -421,19 +426,34 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
         }
         return;
     }
+    if (a.effect_mode == kEffectScatter) {
+        if (!have) return;
+        const float amount = a.scatter;
+        float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
+        for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
+            const float3 e = mapped_effect<C>(a, smem, sx);  // Mono map: max(0, value)
+            float4 acc = erow[sx];
+            acc.x += e.x * amount;
+            acc.y += e.y * amount;
+            acc.z += e.z * amount;
+            erow[sx] = acc;
+        }
+        return;
+    }
     if (a.effect_mode == kEffectStore) {
         double l_in = 0.0, l_eff = 0.0;
         float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
         for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
             const float3 e = mapped_effect<C>(a, smem, sx);
             erow[sx] = make_float4(e.x, e.y, e.z, 0.0f);
+            if (!a.preserve) continue;
             const float4 p = load_px(srow, sx, aligned_s);
             float sig;
             const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
             l_in += static_cast<double>(luma(p.x * m, p.y * m, p.z * m));
             l_eff += static_cast<double>(luma(e.x, e.y, e.z));
         }
-        block_add2(l_in, l_eff, a.sums);
+        if (a.preserve) block_add2(l_in, l_eff, a.sums);
         return;
     }
     const bool aligned_d = ((reinterpret_cast<uintptr_t>(a.dst) | static_cast<uintptr_t>(a.dst_pitch)) & 15) == 0;
@@ -479,10 +499,57 @@ __global__ void __launch_bounds__(256) effect_sums_kernel(FrameArgs a) {
     block_add2(l_in, l_eff, a.sums);
 }
 
+// One channel of the stored effect, bilinear at (fx, fy) clamped to the
+// frame (sampleRgbaBilinear, LensDiffCpuReference.cpp:1477-1497).
+__device__ __forceinline__ float effect_clamped(const float* e, int W, int H, float fx, float fy, int c) {
+    const float x = fminf(fmaxf(fx, 0.0f), static_cast<float>(max(0, W - 1)));
+    const float y = fminf(fmaxf(fy, 0.0f), static_cast<float>(max(0, H - 1)));
+    const int x0 = static_cast<int>(floorf(x)), y0 = static_cast<int>(floorf(y));
+    const int x1 = min(x0 + 1, W - 1), y1 = min(y0 + 1, H - 1);
+    const float tx = __fsub_rn(x, static_cast<float>(x0)), ty = __fsub_rn(y, static_cast<float>(y0));
+    const float p00 = __ldg(e + 4 * (static_cast<int64_t>(y0) * W + x0) + c);
+    const float p10 = __ldg(e + 4 * (static_cast<int64_t>(y0) * W + x1) + c);
+    const float p01 = __ldg(e + 4 * (static_cast<int64_t>(y1) * W + x0) + c);
+    const float p11 = __ldg(e + 4 * (static_cast<int64_t>(y1) * W + x1) + c);
+    const float u = p00 * (1.0f - tx) + p10 * tx;
+    const float v = p01 * (1.0f - tx) + p11 * tx;
+    return u * (1.0f - ty) + v * ty;
+}
+
+// The stored effect at working pixel (x, y), after the creative fringe when
+// FRINGE: red sampled at +shift, blue at -shift along the direction from the
+// frame centre, green unshifted (applyCreativeFringe :1499-1534).
+template <bool FRINGE>
+__device__ __forceinline__ float3 effect_px(const FrameArgs& a, int x, int y) {
+    const float4 c = __ldg(a.effect + static_cast<int64_t>(y) * a.Ww + x);
+    if (!FRINGE) return make_float3(c.x, c.y, c.z);
+    const float cx = static_cast<float>(max(0, a.Ww - 1)) * 0.5f;
+    const float cy = static_cast<float>(max(0, a.Hw - 1)) * 0.5f;
+    const float dx = __fsub_rn(static_cast<float>(x), cx), dy = __fsub_rn(static_cast<float>(y), cy);
+    const float len = sqrtf(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+    const float inv = len > 1e-6f ? __fdiv_rn(1.0f, len) : 0.0f;
+    const float shx = __fmul_rn(__fmul_rn(dx, inv), a.fringe_px);
+    const float shy = __fmul_rn(__fmul_rn(dy, inv), a.fringe_px);
+    const float* e = reinterpret_cast<const float*>(a.effect);
+    const float fxr = __fadd_rn(static_cast<float>(x), shx), fyr = __fadd_rn(static_cast<float>(y), shy);
+    const float fxb = __fsub_rn(static_cast<float>(x), shx), fyb = __fsub_rn(static_cast<float>(y), shy);
+    return make_float3(effect_clamped(e, a.Ww, a.Hw, fxr, fyr, 0), c.y, effect_clamped(e, a.Ww, a.Hw, fxb, fyb, 2));
+}
+
+__device__ __forceinline__ float3 lerp3(float3 a, float3 b, float t) {
+    return make_float3(a.x + (b.x - a.x) * t, a.y + (b.y - a.y) * t, a.z + (b.z - a.z) * t);
+}
+
 // Output rows of the render window from the stored effect: scaled, with
 // Preserve energy, by (luma sum of the redistributed source) / (luma sum of
 // the effect) as LensDiffCpuReference.cpp:2172-2178 does (scaleImage with the
-// float quotient of the two sums), then composited.
+// float quotient of the two sums), then composited.  The scale is linear and
+// commutes with the scatter, fringe and resample steps that follow it in the
+// reference, so it is applied here, last.  RESAMPLE: the effect and the
+// redistributed working source are sampled at the source pixel's position in
+// the working frame (sampleRgbaBilinearImage :373-395: zero outside it), as
+// resampleRgbaImage (:414-434) does for the whole image.
+template <bool FRINGE, bool RESAMPLE>
 __global__ void __launch_bounds__(256) composite_kernel(FrameArgs a) {
     const int yo = a.out_y1 + blockIdx.x;
     const int sy = yo - a.src_y1;
@@ -497,16 +564,74 @@ __global__ void __launch_bounds__(256) composite_kernel(FrameArgs a) {
     const bool aligned_d = ((reinterpret_cast<uintptr_t>(a.dst) | static_cast<uintptr_t>(a.dst_pitch)) & 15) == 0;
     const unsigned char* srow = a.src + static_cast<int64_t>(sy) * a.src_pitch;
     unsigned char* drow = a.dst + static_cast<int64_t>(yo - a.dst_y1) * a.dst_pitch;
-    const float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
+    // resample coordinates (float, as the reference computes them)
+    const float ksx = RESAMPLE ? __fdiv_rn(static_cast<float>(a.Ww), static_cast<float>(max(1, a.W))) : 1.0f;
+    const float ksy = RESAMPLE ? __fdiv_rn(static_cast<float>(a.Hw), static_cast<float>(max(1, a.H))) : 1.0f;
+    const float fy = __fsub_rn(__fmul_rn(__fadd_rn(static_cast<float>(sy), 0.5f), ksy), 0.5f);
     for (int x = a.out_x1 + threadIdx.x; x < a.out_x2; x += blockDim.x) {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         const int sx = x - a.src_x1;
         if (have && sx >= 0 && sx < a.W) {
-            const float4 e = erow[sx];
-            out = composite_px(a, load_px(srow, sx, aligned_s), make_float3(e.x * scale, e.y * scale, e.z * scale));
+            const float4 p = load_px(srow, sx, aligned_s);
+            if constexpr (!RESAMPLE) {
+                const float3 e = effect_px<FRINGE>(a, sx, sy);
+                out = composite_px(a, p, make_float3(e.x * scale, e.y * scale, e.z * scale));
+            } else {
+                const float fx = __fsub_rn(__fmul_rn(__fadd_rn(static_cast<float>(sx), 0.5f), ksx), 0.5f);
+                float3 rd = make_float3(0.0f, 0.0f, 0.0f), e = rd;
+                if (!(fx < 0.0f || fy < 0.0f || fx > static_cast<float>(a.Ww - 1) ||
+                      fy > static_cast<float>(a.Hw - 1))) {
+                    const int x0 = static_cast<int>(floorf(fx)), y0 = static_cast<int>(floorf(fy));
+                    const int x1 = min(x0 + 1, a.Ww - 1), y1 = min(y0 + 1, a.Hw - 1);
+                    const float tx = __fsub_rn(fx, static_cast<float>(x0));
+                    const float ty = __fsub_rn(fy, static_cast<float>(y0));
+                    const float4* wk = a.work;
+                    const float3 r00 = redistributed(a, __ldg(wk + static_cast<int64_t>(y0) * a.Ww + x0));
+                    const float3 r10 = redistributed(a, __ldg(wk + static_cast<int64_t>(y0) * a.Ww + x1));
+                    const float3 r01 = redistributed(a, __ldg(wk + static_cast<int64_t>(y1) * a.Ww + x0));
+                    const float3 r11 = redistributed(a, __ldg(wk + static_cast<int64_t>(y1) * a.Ww + x1));
+                    rd = lerp3(lerp3(r00, r10, tx), lerp3(r01, r11, tx), ty);
+                    const float3 e00 = effect_px<FRINGE>(a, x0, y0), e10 = effect_px<FRINGE>(a, x1, y0);
+                    const float3 e01 = effect_px<FRINGE>(a, x0, y1), e11 = effect_px<FRINGE>(a, x1, y1);
+                    e = lerp3(lerp3(e00, e10, tx), lerp3(e01, e11, tx), ty);
+                }
+                out = composite_rd(a, p, rd, make_float3(e.x * scale, e.y * scale, e.z * scale));
+            }
         }
         store_px(drow, x - a.dst_x1, aligned_d, out);
     }
+}
+
+// Working source of the resolution-aware path: pixel (x, y) of the a.Ww x
+// a.Hw working frame samples the source at ((x + .5) * W / Ww - .5, ...)
+// bilinearly, zero outside [0, W-1] x [0, H-1] (resampleRgbaImage
+// :414-434 with sampleRgbaBilinearImage :373-395).
+__global__ void __launch_bounds__(256) resample_source_kernel(FrameArgs a) {
+    const int y = blockIdx.y;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= a.Ww) return;
+    const float ksx = __fdiv_rn(static_cast<float>(a.W), static_cast<float>(max(1, a.Ww)));
+    const float ksy = __fdiv_rn(static_cast<float>(a.H), static_cast<float>(max(1, a.Hw)));
+    const float fx = __fsub_rn(__fmul_rn(__fadd_rn(static_cast<float>(x), 0.5f), ksx), 0.5f);
+    const float fy = __fsub_rn(__fmul_rn(__fadd_rn(static_cast<float>(y), 0.5f), ksy), 0.5f);
+    float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (!(fx < 0.0f || fy < 0.0f || fx > static_cast<float>(a.W - 1) || fy > static_cast<float>(a.H - 1))) {
+        const bool aligned = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(a.src_pitch)) & 15) == 0;
+        const int x0 = static_cast<int>(floorf(fx)), y0 = static_cast<int>(floorf(fy));
+        const int x1 = min(x0 + 1, a.W - 1), y1 = min(y0 + 1, a.H - 1);
+        const float tx = __fsub_rn(fx, static_cast<float>(x0)), ty = __fsub_rn(fy, static_cast<float>(y0));
+        const unsigned char* r0 = a.src + static_cast<int64_t>(y0) * a.src_pitch;
+        const unsigned char* r1 = a.src + static_cast<int64_t>(y1) * a.src_pitch;
+        const float4 p00 = load_px(r0, x0, aligned), p10 = load_px(r0, x1, aligned);
+        const float4 p01 = load_px(r1, x0, aligned), p11 = load_px(r1, x1, aligned);
+        const float4 u = make_float4(p00.x + (p10.x - p00.x) * tx, p00.y + (p10.y - p00.y) * tx,
+                                     p00.z + (p10.z - p00.z) * tx, p00.w + (p10.w - p00.w) * tx);
+        const float4 v = make_float4(p01.x + (p11.x - p01.x) * tx, p01.y + (p11.y - p01.y) * tx,
+                                     p01.z + (p11.z - p01.z) * tx, p01.w + (p11.w - p01.w) * tx);
+        out = make_float4(u.x + (v.x - u.x) * ty, u.y + (v.y - u.y) * ty, u.z + (v.z - u.z) * ty,
+                          u.w + (v.w - u.w) * ty);
+    }
+    a.work[static_cast<int64_t>(y) * a.Ww + x] = out;
 }
 
 // ---- kernel spectra ----------------------------------------------------------------------
@@ -624,7 +749,10 @@ void rows_e(const FrameArgs& a, cudaStream_t s) {
         }
     } else {
         const size_t sm = static_cast<size_t>(M) * 3 * sizeof(float2);
-        frame_rows_kernel<E, 3, 3><<<a.Hp, fft_threads(M, 3, E), sm, s>>>(a);
+        if (a.drv_effect)
+            frame_rows_kernel<E, 3, 3, Fam<E>::max_threads, 1, true><<<a.Hp, fft_threads(M, 3, E), sm, s>>>(a);
+        else
+            frame_rows_kernel<E, 3, 3><<<a.Hp, fft_threads(M, 3, E), sm, s>>>(a);
     }
 }
 
@@ -730,6 +858,7 @@ template <int E>
 void configure_e() {
     set_smem(frame_rows_kernel<E, 4, 1>);
     set_smem(frame_rows_kernel<E, 3, 3>);
+    set_smem(frame_rows_kernel<E, 3, 3, Fam<E>::max_threads, 1, true>);
     set_smem(frame_cols_kernel<E, 3>);
     set_smem(frame_cols_kernel<E, 4>);
     set_smem(frame_cols_mono_kernel<E>);
@@ -786,7 +915,7 @@ void launch_frame_cols(const FrameArgs& a, cudaStream_t s) {
 }
 
 void launch_frame_inverse(const FrameArgs& a, cudaStream_t s) {
-    const int rows = a.effect_mode == kEffectStore ? a.H : a.out_y2 - a.out_y1;
+    const int rows = a.effect_mode == kEffectComposite ? a.out_y2 - a.out_y1 : a.H;
     if (rows <= 0) return;
     if (a.g.fam_m == kE25) inverse_e<kE25>(a, rows, s);
     else inverse_e<kE16>(a, rows, s);
@@ -803,7 +932,19 @@ void launch_effect_sums(const FrameArgs& a, cudaStream_t s) { effect_sums_kernel
 void launch_composite(const FrameArgs& a, cudaStream_t s) {
     const int rows = a.out_y2 - a.out_y1;
     if (rows <= 0) return;
-    composite_kernel<<<rows, 256, 0, s>>>(a);
+    const bool fringe = a.fringe_px > 0.0f;
+    if (a.work) {
+        if (fringe) composite_kernel<true, true><<<rows, 256, 0, s>>>(a);
+        else composite_kernel<false, true><<<rows, 256, 0, s>>>(a);
+    } else {
+        if (fringe) composite_kernel<true, false><<<rows, 256, 0, s>>>(a);
+        else composite_kernel<false, false><<<rows, 256, 0, s>>>(a);
+    }
+}
+
+void launch_resample_source(const FrameArgs& a, cudaStream_t s) {
+    if (a.Ww <= 0 || a.Hw <= 0) return;
+    resample_source_kernel<<<dim3((a.Ww + 255) / 256, a.Hw), 256, 0, s>>>(a);
 }
 
 void launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s) {

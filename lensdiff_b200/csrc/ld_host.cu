@@ -88,6 +88,9 @@ struct ld_ctx {
     bool graphs_enabled = true;
     // work buffers, grown on demand
     DevBuf rows, win, combine_out, kspec_rows, frameA, frameB, calib, calib_psf, pupil_pre, effect;
+    // resolution-aware working source; scatter kernel canvas and spectrum
+    DevBuf work, scatter_canvas, scatter_ks;
+    std::string scatter_key;
     // comparator form (cuFFT): plans and its own work buffers
     CufftPlanCache cufft;
     DevBuf cf_grid, cf_planes, cf_sd, cf_prod;
@@ -275,6 +278,7 @@ FftPlan make_plan(ld_ctx* c, int n, bool allow25) {
 // ---------------------------------------------------------------------------
 constexpr float kPiRef = 3.14159265358979323846f;  // kPi, LensDiffCpuReference.cpp:25
 
+int frame_short_side(const ld_params& p) { return std::max(1, p.frame_short_side_px); }  // LensDiffTypes.h:294-296
 int optics_short_side(const ld_params& p) {  // LensDiffTypes.h:302-305
     return p.resolution_aware ? 2160 : std::max(1, p.frame_short_side_px);
 }
@@ -482,13 +486,47 @@ std::string bank_key(const ld_params& p, const std::vector<float>& wl) {
     return k;
 }
 
+// The steps after the effect (CpuReference.cpp:2089-2094, :2180-2198): the
+// resolution-aware working frame, scatter and creative fringe.
+struct PostEffects {
+    bool resample = false;
+    double scale = 1.0;   // working / source (ResolveLensDiffEffectWorkingScale)
+    bool scatter = false;
+    float scatter_radius = 0.0f;  // px
+    float scatter_amount = 0.0f;
+    float fringe = 0.0f;          // px; > 1e-6 when on
+    bool any() const { return resample || scatter || fringe > 1e-6f; }
+};
+
+PostEffects post_effects(const ld_params& p) {
+    PostEffects e;
+    // LensDiffTypes.h:302-305; CpuReference.cpp:2091
+    e.scale = static_cast<double>(optics_short_side(p)) / static_cast<double>(frame_short_side(p));
+    e.resample = p.resolution_aware && std::abs(e.scale - 1.0) > 1e-6;
+    // CpuReference.cpp:2181-2182
+    const double radius = percent_to_px(p.scatter_radius, optics_short_side(p));
+    e.scatter = p.scatter_amount > 1e-6 && radius > 0.25;
+    e.scatter_radius = static_cast<float>(radius);
+    e.scatter_amount = static_cast<float>(std::max(0.0, p.scatter_amount));
+    // :2188-2190 with applyCreativeFringe's threshold (:1500)
+    const float f = static_cast<float>(std::max(0.0, percent_to_px(p.creative_fringe, optics_short_side(p))));
+    e.fringe = f > 1e-6f ? f : 0.0f;
+    return e;
+}
+
+// Working frame size (CpuReference.cpp:2092-2093).
+void working_size(const PostEffects& e, int W, int H, int* Ww, int* Hw) {
+    *Ww = e.resample ? std::max(1, static_cast<int>(std::lround(W * e.scale))) : W;
+    *Hw = e.resample ? std::max(1, static_cast<int>(std::lround(H * e.scale))) : H;
+}
+constexpr int kMaxWorkingSide = 32768;
+
 void validate_params(const ld_params& p) {
     if (p.debug_view != LD_DEBUG_FINAL) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-debug-view"};
     if (p.look_mode != LD_LOOK_PHYSICAL && p.look_mode != LD_LOOK_SPLIT) throw Fail{LD_ERR_ARG, "invalid-look-mode"};
     if (p.look_mode == LD_LOOK_SPLIT && p.fft_form == LD_FFT_CUFFT)
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-split-look-with-cufft-form"};
     if (p.input_transfer != LD_TRANSFER_LINEAR) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-input-transfer"};
-    if (p.resolution_aware) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-resolution-aware"};
     if (p.aperture_mode == LD_APERTURE_CUSTOM)  // image loader: WIC / ImageIO only (LensDiffApertureImage.cpp)
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-custom-aperture"};
     if (p.aperture_mode < LD_APERTURE_CIRCLE || p.aperture_mode > LD_APERTURE_SNOWFLAKE)
@@ -497,10 +535,6 @@ void validate_params(const ld_params& p) {
     if (p.spectral_mode < 0 || p.spectral_mode > 3) throw Fail{LD_ERR_ARG, "invalid-spectral-mode"};
     if (p.field_grid != 0 && (p.field_grid < 2 || p.field_grid > kMaxFieldGrid))
         throw Fail{LD_ERR_ARG, "invalid-field-grid"};
-    if (p.scatter_amount > 1e-6 && percent_to_px(p.scatter_radius, optics_short_side(p)) > 0.25)
-        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-scatter"};
-    if (percent_to_px(p.creative_fringe, optics_short_side(p)) > 1e-6)
-        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-creative-fringe"};
     if (p.wavelength_count < 0 || p.wavelength_count > LD_MAX_WAVELENGTHS)
         throw Fail{LD_ERR_ARG, "invalid-wavelength-count"};
     if (p.vane_count > kMaxVanes) throw Fail{LD_ERR_UNSUPPORTED, "too-many-vanes"};
@@ -508,6 +542,8 @@ void validate_params(const ld_params& p) {
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-fft-form"};
     if (p.fft_form == LD_FFT_CUFFT && has_field_phase(p))
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-field-zones-with-cufft-form"};
+    if (p.fft_form == LD_FFT_CUFFT && post_effects(p).any())
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-scatter-fringe-or-resolution-aware-with-cufft-form"};
 }
 
 size_t align256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
@@ -1006,6 +1042,55 @@ std::vector<const SpectraEntry*> ensure_zone_spectra(ld_ctx* c, const ld_params&
     return out;
 }
 
+// Spectrum of the scatter kernel on grid g (one kernel, FP32 layout), built
+// on the first frame with this (radius, grid).  The kernel is the reference's
+// normalised Gaussian of radius ceil(max(.5, r)) and sigma max(.5, r / 2),
+// evaluated in float (buildGaussianKernel, CpuReference.cpp:1680-1700).
+const float2* scatter_spectrum(ld_ctx* c, float radius, const GridGeom& g, cudaStream_t s) {
+    std::string key = append_bytes(std::string(), &radius, sizeof(radius));
+    key = append_bytes(key, &g, sizeof(g));
+    if (c->scatter_ks.p && c->scatter_key == key) return static_cast<const float2*>(c->scatter_ks.p);
+    c->scatter_key.clear();
+    const int R = std::max(1, static_cast<int>(std::ceil(std::max(0.5f, radius))));
+    const int K = 2 * R + 1;
+    const float sigma = std::max(0.5f, radius * 0.5f);
+    std::vector<float> v(static_cast<size_t>(K) * K);
+    float sum = 0.0f;
+    for (int y = -R; y <= R; ++y) {
+        for (int x = -R; x <= R; ++x) {
+            const float e = std::exp(-(static_cast<float>(x * x + y * y) / (2.0f * sigma * sigma)));
+            v[static_cast<size_t>(y + R) * K + (x + R)] = e;
+            sum += e;
+        }
+    }
+    if (sum > 0.0f)
+        for (float& e : v) e /= sum;
+    float* canvas = static_cast<float*>(ensure(c, c->scatter_canvas, v.size() * sizeof(float)));
+    // pageable source: staged by the driver before the call returns
+    check_cuda(cudaMemcpyAsync(canvas, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice, s),
+               "scatter-kernel-upload");
+    KernelSpectraArgs ka{};
+    ka.g = g;
+    ka.n_ker = 1;
+    ka.R = R;
+    ka.K = K;
+    ka.Kp = K + (K & 1);
+    ka.canvas = canvas;
+    ka.rows = static_cast<float2*>(ensure(c, c->kspec_rows, static_cast<size_t>(g.cols) * ka.Kp * sizeof(float2)));
+    const size_t part_bytes = ks_part_bytes(1, g, false);
+    char* ks = static_cast<char*>(ensure(c, c->scatter_ks, part_bytes + static_cast<size_t>(g.cols) * sizeof(float)));
+    ka.spectra = reinterpret_cast<float2*>(ks);
+    ka.kscale = reinterpret_cast<float*>(ks + part_bytes);
+    ka.h16 = 0;
+    ka.scale = static_cast<float>(1.0 / (static_cast<double>(g.M) * static_cast<double>(g.Py)));
+    ka.err = c->err;
+    staged(c, LD_STAGE_KSPEC_ROWS, s, [&] { launch_kspec_rows(ka, s); });
+    staged(c, LD_STAGE_KSPEC_COLS, s, [&] { launch_kspec_cols(ka, s); });
+    check_launch("scatter-spectrum");
+    c->scatter_key = key;
+    return reinterpret_cast<const float2*>(ks);
+}
+
 void fill_sizes(ld_status* st, const ld_params& p) {
     if (!st) return;
     st->pupil_size = pupil_size(p);
@@ -1090,7 +1175,8 @@ void ld_destroy(ld_ctx* c) {
     for (auto& kv : c->ring_counts) free_buf(c, kv.second);
     DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,    &c->frameB,
                       &c->calib,  &c->calib_psf, &c->err_word,  &c->pupil_pre,  &c->effect,    &c->cf_grid,
-                      &c->cf_planes, &c->cf_sd,  &c->cf_prod};
+                      &c->cf_planes, &c->cf_sd,  &c->cf_prod,   &c->work,       &c->scatter_canvas,
+                      &c->scatter_ks};
     c->cufft.release();
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
@@ -1253,6 +1339,8 @@ size_t ld_estimate_device_bytes(const ld_params* params, int32_t width, int32_t 
         const Combination cb = make_combination(p, wavelengths_of(p));
         const int c_rows = std::max(std::max(cb.n_drv == 1 ? 4 : 3, cb.n_out), cb.n_ker);
         const int c_cols = std::max(std::max(cb.n_out, cb.n_ker), cb.n_drv);
+        const PostEffects post = post_effects(p);
+        working_size(post, width, height, &width, &height);  // the effect's frame
         const int M = choose_length((width + static_cast<int>(K) - 1 + 1) / 2, 1, c_rows);
         const int Py = choose_length(height + static_cast<int>(K) - 1, 2, c_cols);
         if (M < 0 || Py < 0) return 0;
@@ -1268,8 +1356,21 @@ size_t ld_estimate_device_bytes(const ld_params* params, int32_t width, int32_t 
         t += static_cast<size_t>(cb.n_ker) * K * K * 4; // combined kernels
         t += static_cast<size_t>(cb.n_ker) * cols * Kp * 8;                 // kernel row spectra
         t += zones * static_cast<size_t>(cb.n_ker) * cols * Py * 8;         // kernel spectra
-        t += static_cast<size_t>(cb.n_drv + cb.n_out) * cols * Hp * 8;      // frame A, B
-        if (zones > 1 || p.energy_mode == LD_ENERGY_PRESERVE) t += static_cast<size_t>(width) * height * 16;
+        size_t frame_ab = static_cast<size_t>(cb.n_drv + cb.n_out) * cols * Hp * 8;  // frame A, B
+        if (post.scatter) {
+            const size_t Rs = static_cast<size_t>(std::ceil(std::max(0.5f, post.scatter_radius)));
+            const size_t Ks = 2 * Rs + 1;
+            const int Ms = choose_length((width + static_cast<int>(Ks) - 1 + 1) / 2, 1, 3);
+            const int Pys = choose_length(height + static_cast<int>(Ks) - 1, 2, 3);
+            if (Ms < 0 || Pys < 0) return 0;
+            const size_t cs = static_cast<size_t>(Ms) + 1;
+            frame_ab = std::max(frame_ab, 6 * cs * Hp * 8);
+            t += Ks * Ks * 4 + cs * (Ks + 1) * 8 + cs * Pys * 8;  // scatter canvas, rows, spectrum
+        }
+        t += frame_ab;
+        if (zones > 1 || p.energy_mode == LD_ENERGY_PRESERVE || p.look_mode == LD_LOOK_SPLIT || post.any())
+            t += static_cast<size_t>(width) * height * 16;            // stored effect
+        if (post.resample) t += static_cast<size_t>(width) * height * 16;  // working source
         if (p.fft_form == LD_FFT_CUFFT) {
             const size_t P = static_cast<size_t>(2 * M) * Py, half = static_cast<size_t>(Py) * (M + 1);
             t += cf_psf_chunk(static_cast<int>(S), static_cast<int>(B)) * S * S * 8;
@@ -1313,10 +1414,16 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         const int zn = p.field_grid > 0 ? p.field_grid : 3;
         const std::vector<float> wl = wavelengths_of(p);
         const Combination cb = make_combination(p, wl);
+        const PostEffects post = post_effects(p);
+        // the effect is computed on the working frame (the source frame unless
+        // resolution-aware rendering resamples it, CpuReference.cpp:2089-2094)
+        int Ww = W, Hw = H;
+        working_size(post, W, H, &Ww, &Hw);
+        if (Ww > kMaxWorkingSide || Hw > kMaxWorkingSide) throw Fail{LD_ERR_ARG, "invalid-working-frame-size"};
         int rw = 0, rh = 0;
         const int c_rows = std::max(std::max(cb.n_drv == 1 ? 4 : 3, cb.n_out), cb.n_ker);
         const int c_cols = std::max(std::max(cb.n_out, cb.n_ker), cb.n_drv);
-        const GridGeom g = make_geometry(ctx, W, H, 2 * max_kernel_radius(p) + 1, c_rows, c_cols, &rw, &rh);
+        const GridGeom g = make_geometry(ctx, Ww, Hw, 2 * max_kernel_radius(p) + 1, c_rows, c_cols, &rw, &rh);
         std::vector<const SpectraEntry*> spectra;
         if (zones) {
             spectra = ensure_zone_spectra(ctx, p, zn, cb, g, s, &bank_rebuilt, &spectra_rebuilt);
@@ -1361,33 +1468,92 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         }
         const float protect = std::max(0.2f, static_cast<float>(std::min(std::max(p.core_preserve, 0.0), 1.0)));
         fa.max_sub = fa.sel.rscale > 1e-6f ? (1.0f - protect) / fa.sel.rscale : 0.0f;
-        fa.Hp = (H + 3) & ~3;
-        fa.A = static_cast<float2*>(
-            ensure(ctx, ctx->frameA, static_cast<size_t>(cb.n_drv) * g.cols * fa.Hp * sizeof(float2)));
-        // column outputs in groups of four columns (ld_frame.cu b_index)
-        const size_t bcols = (static_cast<size_t>(g.cols) + 3) / 4 * 4;
         fa.h16 = chosen_h16(p) ? 1 : 0;
-        const size_t b_bytes = align256(static_cast<size_t>(cb.n_out) * bcols * fa.Hp * (fa.h16 ? 4 : 8));
-        char* bbuf = static_cast<char*>(ensure(ctx, ctx->frameB, b_bytes + static_cast<size_t>(g.cols) * sizeof(float)));
-        fa.Bout = reinterpret_cast<float2*>(bbuf);
-        fa.bscale = reinterpret_cast<float*>(bbuf + b_bytes);
-        fa.spectra = ks_part(sp.spectra.p, 0, cb.n_ker, g, fa.h16);
-        fa.kscale = ks_scale(sp.spectra.p, 0, cb.parts, cb.n_ker, g, fa.h16);
         fa.err = ctx->err;
         const bool split = cb.parts == 2;
-        fa.effect_mode = (zones || split) ? kEffectAccumulate : (fa.preserve ? kEffectStore : kEffectComposite);
+        fa.effect_mode = (zones || split) ? kEffectAccumulate
+                                          : ((fa.preserve || post.any()) ? kEffectStore : kEffectComposite);
         fa.acc_gain = 1.0f;
         fa.acc_shoulder = 0.0f;
-        if (fa.effect_mode != kEffectComposite) {
-            fa.effect = static_cast<float4*>(
-                ensure(ctx, ctx->effect, static_cast<size_t>(W) * H * sizeof(float4) + 2 * sizeof(double)));
-            fa.sums = reinterpret_cast<double*>(fa.effect + static_cast<size_t>(W) * H);
+        fa.Ww = Ww;
+        fa.Hw = Hw;
+        fa.fringe_px = post.fringe;
+        // the chain's view of the working frame: the resampled source, or
+        // the source itself
+        FrameArgs fw = fa;
+        if (post.resample) {
+            fa.work = static_cast<float4*>(
+                ensure(ctx, ctx->work, static_cast<size_t>(Ww) * Hw * sizeof(float4)));
+            fw.src = reinterpret_cast<const unsigned char*>(fa.work);
+            fw.src_pitch = static_cast<int64_t>(Ww) * sizeof(float4);
+            fw.src_x1 = 0;
+            fw.src_y1 = 0;
+            fw.W = Ww;
+            fw.H = Hw;
         }
+        // scatter: a Mono chain over the stored effect with one Gaussian kernel
+        // on its own grid (CpuReference.cpp:2180-2186)
+        FrameArgs fs;
+        std::memset(&fs, 0, sizeof(fs));
+        GridGeom gs{};
+        if (post.scatter) {
+            const int Ks = 2 * std::max(1, static_cast<int>(std::ceil(std::max(0.5f, post.scatter_radius)))) + 1;
+            int srw = 0, srh = 0;
+            gs = make_geometry(ctx, Ww, Hw, Ks, 3, 3, &srw, &srh);
+        }
+        const int Hp = (Hw + 3) & ~3;
+        const size_t a_bytes = std::max(static_cast<size_t>(cb.n_drv) * g.cols,
+                                        post.scatter ? static_cast<size_t>(3) * gs.cols : size_t(0)) *
+                               Hp * sizeof(float2);
+        float2* abuf = static_cast<float2*>(ensure(ctx, ctx->frameA, a_bytes));
+        // column outputs in groups of four columns (ld_frame.cu b_index)
+        auto b_bytes_of = [&](int n_out, const GridGeom& gg, bool h16) {
+            const size_t bcols = (static_cast<size_t>(gg.cols) + 3) / 4 * 4;
+            return align256(static_cast<size_t>(n_out) * bcols * Hp * (h16 ? 4 : 8));
+        };
+        const size_t b_main = b_bytes_of(cb.n_out, g, fa.h16) + static_cast<size_t>(g.cols) * sizeof(float);
+        const size_t b_scatter = post.scatter ? b_bytes_of(3, gs, false) + static_cast<size_t>(gs.cols) * sizeof(float) : 0;
+        char* bbuf = static_cast<char*>(ensure(ctx, ctx->frameB, std::max(b_main, b_scatter)));
+        const float2* sks = post.scatter ? scatter_spectrum(ctx, post.scatter_radius, gs, s) : nullptr;
+        float4* effect = nullptr;
+        double* sums = nullptr;
+        if (fa.effect_mode != kEffectComposite) {
+            effect = static_cast<float4*>(
+                ensure(ctx, ctx->effect, static_cast<size_t>(Ww) * Hw * sizeof(float4) + 2 * sizeof(double)));
+            sums = reinterpret_cast<double*>(effect + static_cast<size_t>(Ww) * Hw);
+        }
+        for (FrameArgs* f : {&fa, &fw}) {
+            f->Hp = Hp;
+            f->A = abuf;
+            f->Bout = reinterpret_cast<float2*>(bbuf);
+            f->bscale = reinterpret_cast<float*>(bbuf + b_bytes_of(cb.n_out, g, fa.h16));
+            f->spectra = ks_part(sp.spectra.p, 0, cb.n_ker, g, fa.h16);
+            f->kscale = ks_scale(sp.spectra.p, 0, cb.parts, cb.n_ker, g, fa.h16);
+            f->effect = effect;
+            f->sums = sums;
+            f->work = fa.work;
+        }
+        if (post.scatter) {
+            fs = fw;
+            fs.g = gs;
+            fs.n_drv = 3;
+            fs.n_out = 3;
+            fs.n_ker = 1;
+            fs.mono = 1;
+            fs.h16 = 0;
+            fs.spectra = sks;
+            fs.kscale = nullptr;
+            fs.bscale = reinterpret_cast<float*>(bbuf + b_bytes_of(3, gs, false));
+            fs.effect_mode = kEffectScatter;
+            fs.drv_effect = 1;
+            fs.scatter = post.scatter_amount;
+        }
+        const FrameArgs fin = fa;  // the composite: source frame, stored effect
         auto clear_effect = [&]() {
             if (fa.effect_mode == kEffectComposite) return;
             check_cuda(cudaMemsetAsync(fa.sums, 0, 2 * sizeof(double), s), "effect-memset");
             if (fa.effect_mode == kEffectAccumulate)
-                check_cuda(cudaMemsetAsync(fa.effect, 0, static_cast<size_t>(W) * H * sizeof(float4), s),
+                check_cuda(cudaMemsetAsync(fa.effect, 0, static_cast<size_t>(Ww) * Hw * sizeof(float4), s),
                            "effect-memset");
         };
         if (p.fft_form == LD_FFT_CUFFT) {
@@ -1428,8 +1594,11 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         gkey = append_bytes(gkey, gains, sizeof(gains));
         gkey = append_bytes(gkey, shoulders, sizeof(shoulders));
         gkey = append_bytes(gkey, &cb.parts, sizeof(cb.parts));
-        auto chain = [&, fa]() mutable {  // the loops below edit this copy
+        gkey = append_bytes(gkey, &fw, sizeof(fw));
+        gkey = append_bytes(gkey, &fs, sizeof(fs));
+        auto chain = [&, fa = fw]() mutable {  // the loops below edit this copy
             clear_effect();
+            if (post.resample) staged(ctx, LD_STAGE_WORKING_SOURCE, s, [&] { launch_resample_source(fin, s); });
             staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
             if (fa.effect_mode != kEffectAccumulate) {
                 staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
@@ -1439,15 +1608,15 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
                 fa.zone_n = zones ? zn : 0;
                 for (int z = 0; z < nz; ++z) {
                     const void* base = spectra[static_cast<size_t>(z)]->spectra.p;
-                    int r0 = 0, r1 = H;
+                    int r0 = 0, r1 = Hw;
                     if (zones) {
                         fa.zone_x = z % zn;
                         fa.zone_y = z / zn;
-                        // source rows whose tent weight can be non-zero (the kernel
+                        // working rows whose tent weight can be non-zero (the kernel
                         // evaluates the weight itself; one row of margin each side)
-                        const double step = static_cast<double>(std::max(1, H - 1)) / static_cast<double>(zn - 1);
+                        const double step = static_cast<double>(std::max(1, Hw - 1)) / static_cast<double>(zn - 1);
                         r0 = std::max(0, static_cast<int>(std::floor((fa.zone_y - 1) * step)) - 1);
-                        r1 = std::min(H, static_cast<int>(std::ceil((fa.zone_y + 1) * step)) + 2);
+                        r1 = std::min(Hw, static_cast<int>(std::ceil((fa.zone_y + 1) * step)) + 2);
                     }
                     fa.row0 = r0;
                     for (int part = 0; part < cb.parts; ++part) {
@@ -1461,7 +1630,12 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
                 }
                 if (fa.preserve) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_effect_sums(fa, s); });
             }
-            if (fa.effect_mode != kEffectComposite) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fa, s); });
+            if (post.scatter) {
+                staged(ctx, LD_STAGE_SCATTER, s, [&] { launch_frame_rows(fs, s); });
+                staged(ctx, LD_STAGE_SCATTER, s, [&] { launch_frame_cols(fs, s); });
+                staged(ctx, LD_STAGE_SCATTER, s, [&] { launch_frame_inverse(fs, s); });
+            }
+            if (fa.effect_mode != kEffectComposite) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fin, s); });
         };
         run_chain(ctx, s, gkey, chain);
         check_launch("frame-chain");

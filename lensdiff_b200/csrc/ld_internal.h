@@ -148,7 +148,7 @@ struct SelectionParams {
     float rscale;          // 1 - corePreserve
 };
 
-enum { kEffectComposite = 0, kEffectStore = 1, kEffectAccumulate = 2 };
+enum { kEffectComposite = 0, kEffectStore = 1, kEffectAccumulate = 2, kEffectScatter = 3 };
 
 struct FrameArgs {
     GridGeom g;
@@ -180,8 +180,11 @@ struct FrameArgs {
     //   kEffectAccumulate: add the tent-weighted effect of field zone
     //     (zone_x, zone_y) of a zone_n x zone_n grid to `effect`, source rows
     //     row0 + blockIdx.x (accumulateWeightedImage, :1452-1475).
-    // composite_kernel then finishes the last two, scaling the effect by
-    // sums[0] / sums[1] when `preserve`.
+    //   kEffectScatter: the scatter convolution's inverse pass (Mono chain over
+    //     the stored effect, one Gaussian kernel): add scatter * max(0, value)
+    //     to every source pixel of `effect` (CpuReference.cpp:2180-2186).
+    // composite_kernel then finishes the stored effect, scaling it by
+    // sums[0] / sums[1] when `preserve`.  Store skips the sums without it.
     int effect_mode;
     int preserve;
     int zone_x, zone_y, zone_n, row0;  // zone_n = 0: no field zones (weight 1)
@@ -196,6 +199,19 @@ struct FrameArgs {
     float saturation;
     int luma_lock;
     float effect_gain, core_comp, max_sub;
+    // scatter chain: the forward rows take their three drivers from `effect`
+    // (drv_effect = 1) and the inverse adds scatter * max(0, value)
+    int drv_effect;
+    float scatter;
+    // composite of a stored effect (composite_kernel): the creative fringe
+    // shift in working pixels (0: off, applyCreativeFringe :1499-1534), and
+    // the resolution-aware working frame (work == null: the effect has the
+    // source's size).  With `work`, `effect` is [Hw][Ww] and both it and
+    // the redistributed working source are resampled to the source frame
+    // (resampleRgbaImage :414-434) before the composite.
+    float fringe_px;
+    float4* work;
+    int Ww, Hw;
 };
 void launch_frame_rows(const FrameArgs& a, cudaStream_t s);
 void launch_frame_cols(const FrameArgs& a, cudaStream_t s);
@@ -204,6 +220,10 @@ void launch_composite(const FrameArgs& a, cudaStream_t s);
 // Inverse pass over `rows` CTAs (kEffectAccumulate: source rows row0 + i).
 void launch_frame_inverse_rows(const FrameArgs& a, int rows, cudaStream_t s);
 void launch_effect_sums(const FrameArgs& a, cudaStream_t s);
+// Resolution-aware working source: the source frame (a.src, a.W x a.H)
+// resampled to a.Ww x a.Hw into a.work (resampleRgbaImage,
+// CpuReference.cpp:414-434).
+void launch_resample_source(const FrameArgs& a, cudaStream_t s);
 // Column-pass shared memory: spectral (n_out 3 or 4) or Mono (n_out = 0).
 size_t frame_cols_smem(int Py, int n_out);
 

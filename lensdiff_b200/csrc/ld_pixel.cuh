@@ -62,16 +62,25 @@ __device__ __forceinline__ float3 map_effect(const FrameArgs& a, const float* e)
 
 // Final composite of one pixel (LensDiffCpuReference.cpp:2200-2218): the
 // effect is already multiplied by its energy scale.
-__device__ __forceinline__ float4 composite_px(const FrameArgs& a, float4 p, float3 eff) {
-    float sig;
-    const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
-    const float rr = p.x * m, rg = p.y * m, rb = p.z * m;
+// `rd`: the redistributed source at the pixel (src * mask * (1 - corePreserve)).
+__device__ __forceinline__ float4 composite_rd(const FrameArgs& a, float4 p, float3 rd, float3 eff) {
+    const float rr = rd.x, rg = rd.y, rb = rd.z;
     float4 out;
     out.x = fmaxf(fmaxf(0.0f, p.x - a.core_comp * rr + a.effect_gain * eff.x), fmaxf(0.0f, p.x - rr * a.max_sub));
     out.y = fmaxf(fmaxf(0.0f, p.y - a.core_comp * rg + a.effect_gain * eff.y), fmaxf(0.0f, p.y - rg * a.max_sub));
     out.z = fmaxf(fmaxf(0.0f, p.z - a.core_comp * rb + a.effect_gain * eff.z), fmaxf(0.0f, p.z - rb * a.max_sub));
     out.w = p.w;
     return out;
+}
+
+__device__ __forceinline__ float3 redistributed(const FrameArgs& a, float4 p) {
+    float sig;
+    const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
+    return make_float3(p.x * m, p.y * m, p.z * m);
+}
+
+__device__ __forceinline__ float4 composite_px(const FrameArgs& a, float4 p, float3 eff) {
+    return composite_rd(a, p, redistributed(a, p), eff);
 }
 
 __device__ __forceinline__ void store_px(unsigned char* drow, int dx, bool aligned, float4 out) {

@@ -765,25 +765,121 @@ def field_zone_banks(p, n: int = 3):
     return out
 
 
+# ------------------------------------------------------- after the effect
+def working_frame(p, w: int, h: int) -> Tuple[bool, int, int]:
+    """Resolution-aware working frame: ResolveLensDiffEffectWorkingScale
+    (LensDiffTypes.h:294-310) and the working size (CpuReference.cpp:2090-2093,
+    std::lround of the double product)."""
+    scale = float(optics_short_side(p)) / float(max(1, int(p.frameShortSidePx)))
+    if not (_p(p, "resolutionAware", False) and abs(scale - 1.0) > 1e-6):
+        return False, w, h
+    return True, max(1, int(math.floor(w * scale + 0.5))), max(1, int(math.floor(h * scale + 0.5)))
+
+
+def resample_rgba(img: np.ndarray, ow: int, oh: int) -> np.ndarray:
+    """resampleRgbaImage (CpuReference.cpp:414-434) with
+    sampleRgbaBilinearImage (:373-395): pixel centres mapped in float, zero
+    outside [0, w-1] x [0, h-1], lerp form of the bilinear blend."""
+    h, w = img.shape[:2]
+    if (w, h) == (ow, oh):
+        return img
+    fx = ((np.arange(ow, dtype=np.float32) + F(0.5)) * (F(w) / F(max(1, ow))) - F(0.5)).astype(np.float32)
+    fy = ((np.arange(oh, dtype=np.float32) + F(0.5)) * (F(h) / F(max(1, oh))) - F(0.5)).astype(np.float32)
+    okx = (fx >= 0) & (fx <= F(w - 1))
+    oky = (fy >= 0) & (fy <= F(h - 1))
+    x0 = np.clip(np.floor(fx).astype(np.int64), 0, w - 1)
+    y0 = np.clip(np.floor(fy).astype(np.int64), 0, h - 1)
+    x1 = np.minimum(x0 + 1, w - 1)
+    y1 = np.minimum(y0 + 1, h - 1)
+    tx = (fx - x0.astype(np.float32)).astype(np.float64)[None, :, None]
+    ty = (fy - y0.astype(np.float32)).astype(np.float64)[:, None, None]
+    src = img.astype(np.float64)
+    p00, p10 = src[np.ix_(y0, x0)], src[np.ix_(y0, x1)]
+    p01, p11 = src[np.ix_(y1, x0)], src[np.ix_(y1, x1)]
+    vx0 = p00 + (p10 - p00) * tx
+    vx1 = p01 + (p11 - p01) * tx
+    out = vx0 + (vx1 - vx0) * ty
+    return out * (oky[:, None] & okx[None, :])[..., None]
+
+
+def gaussian_kernel(radius_px: float) -> np.ndarray:
+    """buildGaussianKernel, CpuReference.cpp:1680-1700: radius
+    ceil(max(.5, r)), sigma max(.5, r / 2), values in float, normalised."""
+    r = F(radius_px)
+    rad = max(1, int(math.ceil(max(0.5, float(r)))))
+    sigma = max(F(0.5), F(r * F(0.5)))
+    yy, xx = np.mgrid[-rad:rad + 1, -rad:rad + 1]
+    d = (xx * xx + yy * yy).astype(np.float32)
+    v = np.exp(-(d / (F(2.0) * sigma * sigma))).astype(np.float32).astype(np.float64)
+    return v / v.sum()
+
+
+def _sample_clamped(plane: np.ndarray, fx: np.ndarray, fy: np.ndarray) -> np.ndarray:
+    """sampleRgbaBilinear (CpuReference.cpp:1477-1497) on one channel:
+    coordinates clamped to the frame, (1 - t) weights."""
+    h, w = plane.shape
+    x = np.clip(fx, F(0), F(max(0, w - 1))).astype(np.float32)
+    y = np.clip(fy, F(0), F(max(0, h - 1))).astype(np.float32)
+    x0 = np.floor(x).astype(np.int64)
+    y0 = np.floor(y).astype(np.int64)
+    x1 = np.minimum(x0 + 1, w - 1)
+    y1 = np.minimum(y0 + 1, h - 1)
+    tx = (x - x0.astype(np.float32)).astype(np.float64)
+    ty = (y - y0.astype(np.float32)).astype(np.float64)
+    a = plane[y0, x0] * (1.0 - tx) + plane[y0, x1] * tx
+    b = plane[y1, x0] * (1.0 - tx) + plane[y1, x1] * tx
+    return a * (1.0 - ty) + b * ty
+
+
+def creative_fringe(effect: np.ndarray, amount: float) -> np.ndarray:
+    """applyCreativeFringe, CpuReference.cpp:1499-1534: red sampled at +shift,
+    blue at -shift along the direction from the frame centre (float
+    geometry), green unshifted."""
+    amt = F(amount)
+    if amt <= F(1e-6):
+        return effect
+    h, w = effect.shape[:2]
+    cx = F(max(0, w - 1)) * F(0.5)
+    cy = F(max(0, h - 1)) * F(0.5)
+    y, x = np.mgrid[0:h, 0:w]
+    x = x.astype(np.float32)
+    y = y.astype(np.float32)
+    dx = (x - cx).astype(np.float32)
+    dy = (y - cy).astype(np.float32)
+    length = np.sqrt(dx * dx + dy * dy).astype(np.float32)
+    with np.errstate(divide="ignore"):
+        inv = np.where(length > F(1e-6), F(1.0) / length, F(0.0)).astype(np.float32)
+    shx = (dx * inv * amt).astype(np.float32)
+    shy = (dy * inv * amt).astype(np.float32)
+    out = effect.copy()
+    out[..., 0] = _sample_clamped(effect[..., 0], (x + shx).astype(np.float32), (y + shy).astype(np.float32))
+    out[..., 2] = _sample_clamped(effect[..., 2], (x - shx).astype(np.float32), (y - shy).astype(np.float32))
+    return out
+
+
 def render(src: np.ndarray, p, bank: PsfBank, natural: Optional[np.ndarray] = None,
            style: Optional[np.ndarray] = None, src_origin=(0, 0), dst_bounds=None,
            render_window=None, field_grid: int = 3) -> np.ndarray:
-    """RunLensDiffCpuReference, LensDiffCpuReference.cpp:2073-2261 (no
-    resolution-aware resample, no scatter / creative fringe, Final view).
-    With field phase on, `bank` is ignored and the effect is the tent-weighted
-    sum of the zones' effects (:2161-2170); `field_grid` zones per side.
+    """RunLensDiffCpuReference, LensDiffCpuReference.cpp:2073-2261 (Final
+    view).  With field phase on, `bank` is ignored and the effect is the
+    tent-weighted sum of the zones' effects (:2161-2170); `field_grid` zones
+    per side.  The effect is computed on the working frame (the source,
+    resampled when resolution-aware, :2089-2094), then scattered, fringed
+    and resampled back (:2180-2198) before the composite.
 
     src: (H, W, 4) float array at bounds origin `src_origin`.  Returns the dst
     image (dh, dw, 4) for `dst_bounds` = (x1, y1, x2, y2) (defaults to src)."""
-    h, w = src.shape[:2]
+    sh, sw = src.shape[:2]
     srcd = src.astype(np.float64)
-    mask = selection_mask(src, p)
+    resample, w, h = working_frame(p, sw, sh)
+    work = resample_rgba(src, w, h).astype(np.float32) if resample else src
+    mask = selection_mask(work, p)
     rscale = 1.0 - min(max(float(p.corePreserve), 0.0), 1.0)
     rscale = float(F(rscale))
     protect = max(0.2, float(F(min(max(float(p.corePreserve), 0.0), 1.0))))
     max_sub = (1.0 - protect) / rscale if rscale > 1e-6 else 0.0
-    redist = srcd[..., :3] * (mask * rscale)[..., None]
-    driver = extraction_signal(src, p) * mask * rscale
+    redist = work.astype(np.float64)[..., :3] * (mask * rscale)[..., None]
+    driver = extraction_signal(work, p) * mask * rscale
     preserve = int(p.energyMode) == 0
     gain = min(max(float(p.effectGain), 0.0), 1.0) if preserve else max(0.0, float(p.effectGain))
     cc = gain if preserve else max(0.0, float(p.coreCompensation))
@@ -816,9 +912,21 @@ def render(src: np.ndarray, p, bank: PsfBank, natural: Optional[np.ndarray] = No
         e_fx = float((effect @ lw).sum())
         if e_fx > 1e-6:
             effect = effect * (e_in / e_fx)
+    scatter_px = percent_to_px(_p(p, "scatterRadius", 0.0), optics_short_side(p))
+    scatter_amount = float(_p(p, "scatterAmount", 0.0))
+    if scatter_amount > 1e-6 and scatter_px > 0.25:
+        g = gaussian_kernel(scatter_px)
+        scat = np.stack([convolve(effect[..., c], g) for c in range(3)], axis=-1)
+        effect = effect + scat * float(F(max(0.0, scatter_amount)))
+    fringe_px = max(0.0, percent_to_px(_p(p, "creativeFringe", 0.0), optics_short_side(p)))
+    effect = creative_fringe(effect, fringe_px)
+    if resample:
+        redist = resample_rgba(redist, sw, sh)
+        effect = resample_rgba(effect, sw, sh)
     raw = np.maximum(0.0, srcd[..., :3] - cc * redist + gain * effect)
     floor = np.maximum(0.0, srcd[..., :3] - redist * max_sub)
     final = np.concatenate([np.maximum(raw, floor), srcd[..., 3:4]], axis=-1)
+    h, w = sh, sw
 
     sx1, sy1 = src_origin
     if dst_bounds is None:

@@ -63,6 +63,19 @@ def golden_params():
     cases["tristimulus_style_force"] = base.copy(spectralMode=LensDiffSpectralMode.Tristimulus,
                                                  spectrumStyle=LensDiffSpectrumStyle.CyanMagenta,
                                                  spectrumForce=0.6, spectrumSaturation=1.3)
+    # after the effect: scatter, creative fringe, the resolution-aware working
+    # frame (percentages of the 2160-pixel optics short side when
+    # resolution-aware; 4320 halves the working frame, 1080 doubles it)
+    cases["tristimulus_scatter_fringe"] = base.copy(spectralMode=LensDiffSpectralMode.Tristimulus,
+                                                    scatterAmount=0.6, scatterRadius=8.0, creativeFringe=2.5)
+    aware = base.copy(resolutionAware=True, diffractionScalePx=2.0 * 72 / 2160)
+    cases["spectral5_aware_up_scatter_preserve"] = aware.copy(
+        spectralMode=LensDiffSpectralMode.Spectral5, frameShortSidePx=1080,
+        maxKernelRadiusPx=S.radius_percent(20, 2160), energyMode=LensDiffEnergyMode.Preserve, corePreserve=0.1,
+        scatterAmount=0.4, scatterRadius=0.4, creativeFringe=0.05)
+    cases["mono_aware_down_fringe"] = aware.copy(
+        spectralMode=LensDiffSpectralMode.Mono, apertureMode=LensDiffApertureMode.Circle, frameShortSidePx=4320,
+        maxKernelRadiusPx=S.radius_percent(10, 2160), creativeFringe=0.1)
     return cases
 
 

@@ -73,7 +73,10 @@ def _lens(**kw):
 @pytest.mark.parametrize("kw", [{}, {"spectralMode": LensDiffSpectralMode.Mono},
                                 {"energyMode": LensDiffEnergyMode.Preserve, "effectGain": 0.7},
                                 {"phaseMode": LensDiffPhaseMode.Enabled, "phaseFieldStrength": 1.0,
-                                 "phaseFieldComaRadial": 0.3, "phaseFieldDefocus": 0.1}])
+                                 "phaseFieldComaRadial": 0.3, "phaseFieldDefocus": 0.1},
+                                {"scatterAmount": 0.5, "scatterRadius": 8.0, "creativeFringe": 1.5},
+                                {"resolutionAware": True, "frameShortSidePx": 1080,
+                                 "maxKernelRadiusPx": 1.25, "diffractionScalePx": 0.2}])
 def test_run_lensdiff_cuda_matches_reference_cpu(adapter, kw):
     p = _lens(**kw)
     src = S.make_frame(200, 120, 14, 1.0, 60.0, seed=41)

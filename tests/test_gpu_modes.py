@@ -302,3 +302,99 @@ def test_aperture_modes_match_reference(cache, mode, blades, rnd):
     img = _render(cache, with_matrices(p), src)
     refimg = R.render(p, src)
     assert rel_err(img, refimg, refimg[..., :3].max()) < OUT_TOL
+
+
+# ------------------------------------- scatter, creative fringe, working frame ---
+# After the effect (LensDiffCpuReference.cpp:2180-2198): scatter adds
+# amount * (effect convolved with a normalised Gaussian, :1680-1700); the
+# creative fringe samples red and blue bilinearly at +/- a radial shift
+# (:1499-1534); resolution-aware rendering computes the effect on the source
+# resampled to a 2160-pixel short side and resamples the redistributed source
+# and the effect back (:2089-2094, :2192-2196, :414-434).
+@pytest.mark.parametrize("kw", [
+    {"scatterAmount": 0.5, "scatterRadius": 10.0},
+    {"scatterAmount": 0.8, "scatterRadius": 4.0, "spectralMode": LensDiffSpectralMode.Mono},
+    {"scatterAmount": 0.3, "scatterRadius": 25.0, "energyMode": LensDiffEnergyMode.Preserve,
+     "spectralMode": LensDiffSpectralMode.Spectral5},
+    {"creativeFringe": 2.0},
+    {"creativeFringe": 1.0, "scatterAmount": 0.4, "scatterRadius": 6.0, "spectralMode": LensDiffSpectralMode.Mono},
+])
+def test_scatter_and_fringe_match_reference(cache, kw):
+    _reference_available()
+    p = _lens(**kw)
+    src = S.make_frame(224, 144, 20, 1.0, 80.0, seed=71)
+    out = _render(cache, with_matrices(p), src)
+    ref = R.render(p, src)
+    assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
+    plain = R.render(p.copy(scatterAmount=0.0, creativeFringe=0.0), src)
+    assert rel_err(plain, ref, ref[..., :3].max()) > 5 * OUT_TOL  # the step matters here
+
+
+def _aware_lens(short_side, **kw):
+    # percentages of the 2160-pixel optics short side
+    return _lens(resolutionAware=True, frameShortSidePx=short_side, maxKernelRadiusPx=S.radius_percent(30, 2160),
+                 diffractionScalePx=3.0 * 144 / 2160, **kw)
+
+
+@pytest.mark.parametrize("short_side,kw", [
+    (1080, {}),
+    (4320, {"spectralMode": LensDiffSpectralMode.Mono}),
+    (1440, {"scatterAmount": 0.4, "scatterRadius": 0.5, "creativeFringe": 0.1}),
+    (2880, {"energyMode": LensDiffEnergyMode.Preserve, "creativeFringe": 0.08,
+            "spectralMode": LensDiffSpectralMode.Spectral5}),
+])
+def test_resolution_aware_matches_reference(cache, short_side, kw):
+    _reference_available()
+    p = _aware_lens(short_side, **kw)
+    src = S.make_frame(224, 144, 20, 1.0, 80.0, seed=72)
+    out = _render(cache, with_matrices(p), src)
+    ref = R.render(p, src)
+    assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
+    orc = _oracle(p, src)
+    assert rel_err(out, orc, orc[..., :3].max()) < OUT_TOL
+
+
+def test_resolution_aware_window_and_origins(cache):
+    _reference_available()
+    p = _aware_lens(1080, scatterAmount=0.3, scatterRadius=0.6)
+    src = S.make_frame(200, 120, 16, 1.0, 60.0, seed=73)
+    window = (30, 10, 150, 90)
+    out = _render(cache, with_matrices(p), src, render_window=window)
+    ref = R.render(p, src, render_window=window)
+    x1, y1, x2, y2 = window
+    assert np.all(out[:y1] == -7.0) and np.all(out[:, :x1] == -7.0)
+    assert rel_err(out[y1:y2, x1:x2], ref[y1:y2, x1:x2], ref[y1:y2, x1:x2, :3].max()) < OUT_TOL
+
+
+def test_post_effects_with_field_zones_split_and_chosen_form(cache):
+    from lensdiff_b200.types import LensDiffFftForm, LensDiffLookMode
+    _reference_available()
+    p = _field_lens(lookMode=LensDiffLookMode.Split, coreGain=1.0, structureGain=1.2, structureShoulder=1.0,
+                    scatterAmount=0.5, scatterRadius=8.0, creativeFringe=1.5)
+    src = S.make_frame(200, 120, 16, 1.0, 60.0, seed=74)
+    ref = R.render(p, src)
+    for form in (LensDiffFftForm.OwnFp32, LensDiffFftForm.OwnChosen):
+        out = _render(cache, with_matrices(p.copy(fftForm=form)), src)
+        assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL, form
+
+
+def test_post_effects_graph_replay(cache):
+    """A second frame with the same settings replays the captured chain
+    (scatter and composite included) and still follows its own source."""
+    _reference_available()
+    p = _aware_lens(1440, scatterAmount=0.4, scatterRadius=0.5, creativeFringe=0.1)
+    for seed in (75, 76):
+        src = S.make_frame(224, 144, 20, 1.0, 80.0, seed=seed)
+        out = _render(cache, with_matrices(p), src)
+        ref = R.render(p, src)
+        assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
+
+
+def test_post_effects_refused_with_cufft_form(cache):
+    from lensdiff_b200.types import LensDiffFftForm
+    p = _lens(scatterAmount=0.5, scatterRadius=10.0, fftForm=LensDiffFftForm.Cufft)
+    stream = torch.cuda.Stream()
+    s = torch.zeros(64, 64, 4, device="cuda")
+    d = torch.zeros_like(s)
+    st = cache.render(image_request(s, d, stream), with_matrices(p))
+    assert not st.ok and st.stage == "unsupported-scatter-fringe-or-resolution-aware-with-cufft-form"

@@ -128,9 +128,7 @@ def test_bank_tier_x_matches_oracle(cache):
 
 
 # ------------------------------------------------------------- render ------
-@pytest.mark.parametrize("name", ["tristimulus_physical_augment", "mono_physical_augment",
-                                  "spectral9_chromatic", "tristimulus_style_force",
-                                  "spectral5_split_preserve"])
+@pytest.mark.parametrize("name", sorted(golden_cases().keys()))
 def test_render_matches_reference_fixture(cache, name):
     p, src, dst, _, _, _ = golden_case(name)
     p = with_matrices(p)
@@ -235,7 +233,7 @@ def test_error_behaviour_mirrors_reference(cache):
     req = image_request(src, dst, stream, frame_short_side=144)
     st = cache.render(req, p.copy(debugView=3))
     assert st.code == 6 and "debug" in st.stage
-    st = cache.render(req, p.copy(creativeFringe=0.5))  # not built: refused, never silently wrong
-    assert st.code == 6 and "fringe" in st.stage
+    st = cache.render(req, p.copy(inputTransfer=1))  # not built: refused, never silently wrong
+    assert st.code == 6 and "transfer" in st.stage
     st = cache.render(req, p)
     assert st.ok
