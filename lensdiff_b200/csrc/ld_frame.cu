@@ -961,6 +961,7 @@ void configure_psf_kernels();
 
 void configure_kernels() {
     configure_psf_kernels();
+    configure_dft_kernels();
     configure_e<kE25>();
     configure_e<kE16>();
 }

@@ -90,6 +90,8 @@ struct ld_ctx {
     DevBuf rows, win, combine_out, kspec_rows, frameA, frameB, calib, calib_psf, pupil_pre, effect;
     // resolution-aware working source; scatter kernel canvas and spectrum
     DevBuf work, scatter_canvas, scatter_ks;
+    // chosen form's DFT-as-GEMM operand images and per-wavelength tiles
+    DevBuf dft;
     std::string scatter_key;
     // comparator form (cuFFT): plans and its own work buffers
     CufftPlanCache cufft;
@@ -686,6 +688,137 @@ const int* ring_counts(ld_ctx* c, int R) {
     return static_cast<const int*>(b.p);
 }
 
+// Pupil pixels along one axis whose centres lie within the outer radius of
+// the (decentred) aperture: only they can be non-zero.
+void pupil_extent(int n, float dec, int* lo_out, int* n_out) {
+    int lo = n, hi = 0;
+    for (int i = 0; i < n; ++i) {
+        const float v = ((static_cast<float>(i) + 0.5f) / static_cast<float>(n) - 0.5f) * 2.0f;
+        if (std::abs(v - dec) <= 0.8601f) {
+            lo = std::min(lo, i);
+            hi = std::max(hi, i + 1);
+        }
+    }
+    if (hi <= lo) {
+        lo = 0;
+        hi = 1;
+    }
+    *lo_out = lo;
+    *n_out = hi - lo;
+}
+
+// Tiles of the chosen form's DFT-as-GEMM for the bank's windows: one union
+// window origin, each wavelength's first computed column rounded down to a
+// multiple of 4 (basis tiles then start on 8-row boundaries), and the operand
+// image sizes (ld_dftgemm.cu).
+DftPlan plan_dft(const PsfBankArgs& a, const std::vector<WavelengthInfo>& infos, std::vector<DftLambda>* lam) {
+    DftPlan d{};
+    pupil_extent(a.pupil.size, a.pupil.decx, &d.col_lo, &d.col_n);
+    d.mt_rows = (a.row_n + 127) / 128;
+    d.kc_rows = (d.col_n + 31) / 32;
+    d.kc_cols = (a.row_n + 31) / 32;
+    int x0 = a.S;
+    for (const WavelengthInfo& w : infos) x0 = std::min(x0, w.win_x0);
+    d.x0 = x0;
+    int width = 0;
+    lam->assign(infos.size(), DftLambda{});
+    for (size_t i = 0; i < infos.size(); ++i) {
+        DftLambda& l = (*lam)[i];
+        l.n0 = (infos[i].win_x0 - x0) / 4 * 4;
+        l.shift = infos[i].win_x0 - x0 - l.n0;
+        l.nt = (l.shift + infos[i].win_n + 127) / 128;
+        d.nt_max = std::max(d.nt_max, l.nt);
+        width = std::max(width, l.n0 + l.nt * 128);
+    }
+    d.basis_rows = 2 * width;
+    d.pf_slab = static_cast<size_t>(d.mt_rows) * 128 * 128;
+    d.pf_lambda = d.pf_slab * d.kc_rows;
+    d.dx_slab = static_cast<size_t>(d.basis_rows) * 128;
+    d.dy_slab = d.dx_slab;
+    d.yt_slab = static_cast<size_t>(d.nt_max) * 128 * 128;
+    d.yt_lambda = d.yt_slab * d.mt_rows * 4;
+    return d;
+}
+
+size_t dft_bytes(const DftPlan& d, int B) {
+    return 2 * (static_cast<size_t>(B) * (d.pf_lambda + d.yt_lambda) + d.dx_slab * d.kc_rows +
+                d.dy_slab * d.kc_cols) +
+           align256(static_cast<size_t>(B) * sizeof(DftLambda)) + 8 * 1024;
+}
+
+// Chosen form: the bank's |F|^2 windows by DFT-as-GEMM on the tensor cores
+// in place of the row and column FFTs (ld_dftgemm.cu).
+void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthInfo>& infos, cudaStream_t s) {
+    std::vector<DftLambda> lam;
+    DftPlan d = plan_dft(a, infos, &lam);
+    const int B = a.B;
+    char* p = static_cast<char*>(ensure(c, c->dft, dft_bytes(d, B)));
+    auto take = [&](size_t bytes) {
+        char* q = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~static_cast<uintptr_t>(1023));
+        p = q + bytes;
+        return reinterpret_cast<unsigned char*>(q);
+    };
+    d.pf_hi = take(B * d.pf_lambda);
+    d.pf_lo = take(B * d.pf_lambda);
+    d.yt_hi = take(B * d.yt_lambda);
+    d.yt_lo = take(B * d.yt_lambda);
+    d.dx_hi = take(d.dx_slab * d.kc_rows);
+    d.dx_lo = take(d.dx_slab * d.kc_rows);
+    d.dy_hi = take(d.dy_slab * d.kc_cols);
+    d.dy_lo = take(d.dy_slab * d.kc_cols);
+    DftLambda* dl = reinterpret_cast<DftLambda*>(take(B * sizeof(DftLambda)));
+    d.lam = dl;
+    check_cuda(cudaMemcpyAsync(dl, lam.data(), lam.size() * sizeof(DftLambda), cudaMemcpyHostToDevice, s),
+               "dft-upload");
+    DftBasisArgs bx{d.dx_hi, d.dx_lo, d.dx_slab, d.basis_rows, d.kc_rows, d.col_n, a.off + d.col_lo, d.x0, a.S / 2, a.S};
+    DftBasisArgs by{d.dy_hi, d.dy_lo, d.dy_slab, d.basis_rows, d.kc_cols, a.row_n, a.off + a.row_lo, d.x0, a.S / 2, a.S};
+    DftGemmArgs gr{};
+    gr.a_hi = d.pf_hi;
+    gr.a_lo = d.pf_lo;
+    gr.a_lambda = d.pf_lambda;
+    gr.a_slab = d.pf_slab;
+    gr.b_hi = d.dx_hi;
+    gr.b_lo = d.dx_lo;
+    gr.b_lambda = 0;
+    gr.b_slab = d.dx_slab;
+    gr.kc = d.kc_rows;
+    gr.mt_fixed = d.mt_rows;
+    gr.mt_max = d.mt_rows;
+    gr.mode = kDftRows;
+    gr.lam = d.lam;
+    gr.y_hi = d.yt_hi;
+    gr.y_lo = d.yt_lo;
+    gr.y_lambda = d.yt_lambda;
+    gr.y_slab = d.yt_slab;
+    gr.wl = a.wl;
+    gr.err = c->err;
+    DftGemmArgs gc = gr;
+    gc.a_hi = d.yt_hi;
+    gc.a_lo = d.yt_lo;
+    gc.a_lambda = d.yt_lambda;
+    gc.a_slab = d.yt_slab;
+    gc.b_hi = d.dy_hi;
+    gc.b_lo = d.dy_lo;
+    gc.b_slab = d.dy_slab;
+    gc.kc = d.kc_cols;
+    gc.mt_fixed = 0;
+    gc.mt_max = d.nt_max;
+    gc.mode = kDftCols;
+    gc.y_hi = nullptr;
+    gc.y_lo = nullptr;
+    gc.win = a.win;
+    gc.win_stride = a.win_stride;
+    staged(c, LD_STAGE_PSF_ROWS, s, [&] {
+        launch_pupil_field(a, d, s);
+        launch_dft_basis(bx, s);
+        launch_dft_gemm(gr, B, d.nt_max, s);
+    });
+    staged(c, LD_STAGE_PSF_COLS, s, [&] {
+        launch_dft_basis(by, s);
+        launch_dft_gemm(gc, B, d.nt_max, s);
+    });
+}
+
 BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebuilt) {
     const std::vector<float> wl = wavelengths_of(p);
     const std::string key = bank_key(p, wl);
@@ -740,6 +873,8 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
         float2* grid = static_cast<float2*>(
             ensure(c, c->cf_grid, cf_psf_chunk(S, B) * static_cast<size_t>(S) * S * sizeof(float2)));
         staged(c, LD_STAGE_PSF_ROWS, s, [&] { cf_psf_transform(a, grid, c->cufft, s); });
+    } else if (p.fft_form == LD_FFT_OWN_CHOSEN) {
+        dft_gemm_psf(c, a, infos, s);
     } else {
         staged(c, LD_STAGE_PSF_ROWS, s, [&] { launch_psf_rows(a, s); });
         staged(c, LD_STAGE_PSF_COLS, s, [&] { launch_psf_cols(a, s); });
@@ -1176,7 +1311,7 @@ void ld_destroy(ld_ctx* c) {
     DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,    &c->frameB,
                       &c->calib,  &c->calib_psf, &c->err_word,  &c->pupil_pre,  &c->effect,    &c->cf_grid,
                       &c->cf_planes, &c->cf_sd,  &c->cf_prod,   &c->work,       &c->scatter_canvas,
-                      &c->scatter_ks};
+                      &c->scatter_ks, &c->dft};
     c->cufft.release();
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);

@@ -230,6 +230,61 @@ size_t frame_cols_smem(int Py, int n_out);
 // shared-memory opt-in for every kernel instantiation (once per device)
 void configure_kernels();
 
+// ---- chosen form: the pupil-to-PSF transform as DFT-as-GEMM on the tensor
+// cores (ld_dftgemm.cu).  Operands are BF16 hi/lo images in the tensor core's
+// shared-memory layout, one slab of `rows` x 128 bytes per K-chunk of 32
+// complex values.
+enum { kDftRows = 0, kDftCols = 1 };
+struct DftLambda {
+    int n0;     // first window column computed (relative to the union origin; multiple of 4)
+    int shift;  // window column 0 is computed column `shift`
+    int nt;     // 128-column tiles computed
+    int pad;
+};
+struct DftPlan {
+    int col_lo, col_n;         // pupil columns that can be non-zero
+    int mt_rows;               // row pass: 128-row tiles of pupil rows
+    int kc_rows, kc_cols;      // K-chunks of the row pass (pupil columns) and the column pass (pupil rows)
+    int nt_max;                // max tiles over wavelengths
+    int x0;                    // union window origin (shifted PSF coordinates)
+    int basis_rows;            // rows of the basis images: 2 x padded union width
+    unsigned char *pf_hi, *pf_lo;  // pupil fields [B][kc_rows][mt_rows * 128 rows]
+    size_t pf_lambda, pf_slab;
+    unsigned char *dx_hi, *dx_lo;  // row-pass basis [kc_rows][basis_rows]
+    unsigned char *dy_hi, *dy_lo;  // column-pass basis [kc_cols][basis_rows]
+    size_t dx_slab, dy_slab;
+    unsigned char *yt_hi, *yt_lo;  // row-pass output [B][mt_rows * 4][nt_max * 128 rows]
+    size_t yt_lambda, yt_slab;
+    const DftLambda* lam;      // [B]
+};
+struct DftBasisArgs {
+    unsigned char *hi, *lo;
+    size_t slab;
+    int rows, kc, k_valid, koff, x0, half, S;
+};
+struct DftGemmArgs {
+    const unsigned char *a_hi, *a_lo;
+    size_t a_lambda, a_slab;
+    const unsigned char *b_hi, *b_lo;
+    size_t b_lambda, b_slab;
+    int kc;
+    int mt_fixed;              // M tiles (0: the wavelength's nt)
+    int mt_max;                // grid.x = mt_max * N tiles
+    int mode;                  // kDftRows or kDftCols
+    const DftLambda* lam;
+    unsigned char *y_hi, *y_lo;  // kDftRows output images
+    size_t y_lambda, y_slab;
+    float* win;                // kDftCols output windows
+    int win_stride;
+    const WavelengthInfo* wl;
+    int* err;
+};
+size_t dft_gemm_smem();
+void launch_dft_basis(const DftBasisArgs& a, cudaStream_t s);
+void launch_pupil_field(const PsfBankArgs& a, const DftPlan& d, cudaStream_t s);
+void launch_dft_gemm(const DftGemmArgs& g, int B, int tiles_n, cudaStream_t s);
+void configure_dft_kernels();
+
 // ---- comparator form: the same chain with cuFFT transforms (ld_cufft.cu) -----------
 struct CufftError {
     int code;

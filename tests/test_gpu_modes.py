@@ -21,7 +21,7 @@ from lensdiff_b200.backend import LensDiffPsfBankCache, image_request  # noqa: E
 from lensdiff_b200.types import LensDiffApertureMode, LensDiffEnergyMode, LensDiffSpectralMode  # noqa: E402
 from oracle import ld_oracle as O  # noqa: E402
 from oracle import ref_lib as R  # noqa: E402
-from tests.helpers import OUT_TOL, rel_err, spectrum_matrices, with_matrices  # noqa: E402
+from tests.helpers import OUT_TOL, golden_cases, rel_err, spectrum_matrices, with_matrices  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -216,7 +216,42 @@ def test_graph_replay_matches_direct_launches(cache):
 # ------------------------------------------------------------ chosen form ----
 # fft_form LD_FFT_OWN_CHOSEN stores the kernel spectra and the column-pass
 # outputs in FP16 with one float scale per spectrum column (half the bytes of
-# the largest frame arrays); it must meet the same output bar.
+# the largest frame arrays), and builds the PSF windows by DFT-as-GEMM on the
+# tensor cores (BF16 3-way split, FP32 accumulation); it must meet the same
+# bars: the bank kernels against the reference's golden fixtures within 1e-4
+# of their peak, the output within 2e-4 of the frame maximum.
+@pytest.mark.parametrize("name", sorted(golden_cases().keys()))
+def test_chosen_form_bank_matches_reference_fixture(cache, name):
+    from lensdiff_b200.types import LensDiffFftForm, LensDiffLookMode
+    from tests.helpers import PSF_TOL, golden_case
+    p, _, _, bank, wl, meta = golden_case(name)
+    p = p.copy(fftForm=LensDiffFftForm.OwnChosen)
+    if p.lookMode != LensDiffLookMode.Physical:
+        p = p.copy(lookMode=LensDiffLookMode.Physical, energyMode=1)
+    wls, kernels, st = cache.export_psf_bank(p, torch.cuda.current_stream())
+    assert st.ok, st
+    assert cache.check_device_errors() == 0
+    assert st.support_radius == meta["support_radius"]
+    for k, ref in zip(kernels, bank):
+        assert k.shape == ref.shape
+        assert rel_err(k, ref, ref.max()) < PSF_TOL
+
+
+def test_chosen_form_bank_large_pupil_matches_fp32_form(cache):
+    """Pupil 512 -> PSF 2048 with 31 wavelengths (the UHD bank's sizes, several
+    128-column tiles per window): the tensor-core bank against the FP32 FFT bank."""
+    from lensdiff_b200.types import LensDiffFftForm
+    from tests.helpers import PSF_TOL
+    p, _ = S.workload_uhd31()
+    _, k32, st = cache.export_psf_bank(p, torch.cuda.current_stream())
+    assert st.ok, st
+    _, kch, st = cache.export_psf_bank(p.copy(fftForm=LensDiffFftForm.OwnChosen), torch.cuda.current_stream())
+    assert st.ok, st
+    assert cache.check_device_errors() == 0
+    assert len(kch) == 31
+    for a, b in zip(kch, k32):
+        assert a.shape == b.shape
+        assert rel_err(a, b, b.max()) < PSF_TOL
 @pytest.mark.parametrize("kw", [{}, {"spectralMode": LensDiffSpectralMode.Spectral9, "chromaticFocus": 0.3},
                                 {"energyMode": LensDiffEnergyMode.Preserve},
                                 {"spectralMode": LensDiffSpectralMode.Mono}])
