@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--bank", default="cold", choices=["cold", "warm"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--fft-form", default="own", choices=sorted(FFT_FORMS),
+    ap.add_argument("--fft-form", default="chosen", choices=sorted(FFT_FORMS),
                     help="transform chain of the headline line (own: hand-written FP32)")
     ap.add_argument("--serving", action="store_true",
                     help="Poisson stream of mixed-size frames through the continuous-batching server")

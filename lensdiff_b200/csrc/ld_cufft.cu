@@ -123,7 +123,7 @@ __global__ void cf_extract_kernel(FrameArgs a, float* planes) {
         const int y = static_cast<int>(i / Px), x = static_cast<int>(i - static_cast<size_t>(y) * Px);
         float v[3] = {0.0f, 0.0f, 0.0f};
         if (y < a.H && x < a.W) {
-            const float4 p = load_px(a.src + static_cast<int64_t>(y) * a.src_pitch, x, aligned);
+            const float4 p = decode_px(a.transfer, load_px(a.src + static_cast<int64_t>(y) * a.src_pitch, x, aligned));
             float sig;
             const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
             if (a.n_drv == 1) {
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(kThreads) cf_effect_kernel(FrameArgs a, const 
             for (int c = 0; c < C; ++c) e[c] = planes[c * P + static_cast<size_t>(sy) * a.g.Px + sx];
             const float3 m3 = map_effect<C>(a, e);
             a.effect[static_cast<int64_t>(sy) * a.W + sx] = make_float4(m3.x, m3.y, m3.z, 0.0f);
-            const float4 p = load_px(srow, sx, aligned_s);
+            const float4 p = decode_px(a.transfer, load_px(srow, sx, aligned_s));
             float sig;
             const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
             l_in += static_cast<double>(luma(p.x * m, p.y * m, p.z * m));
@@ -192,9 +192,9 @@ __global__ void __launch_bounds__(kThreads) cf_effect_kernel(FrameArgs a, const 
             float e[C];
 #pragma unroll
             for (int c = 0; c < C; ++c) e[c] = planes[c * P + static_cast<size_t>(sy) * a.g.Px + sx];
-            out = composite_px(a, load_px(srow, sx, aligned_s), map_effect<C>(a, e));
+            out = composite_px(a, decode_px(a.transfer, load_px(srow, sx, aligned_s)), map_effect<C>(a, e));
         }
-        store_px(drow, x - a.dst_x1, aligned_d, out);
+        store_px(drow, x - a.dst_x1, aligned_d, encode_px(a.transfer, out));
     }
 }
 

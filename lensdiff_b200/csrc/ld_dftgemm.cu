@@ -307,6 +307,7 @@ __global__ void __launch_bounds__(128, 1) dft_gemm_kernel(DftGemmArgs g) {
     // ---- epilogue: all four warps ----
     const bool ready = __all_sync(0xffffffffu, mbar_wait(done, 0, g.err));  // warp-uniform for tcgen05.ld
     tc_fence_after();
+    float esum = 0.0f;  // kDftCols with g.energy: this thread's window pixels
     if (ready) {
         const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
         const int row = tm * kTileM + warp * 32 + lane;  // M index of this thread
@@ -336,11 +337,20 @@ __global__ void __launch_bounds__(128, 1) dft_gemm_kernel(DftGemmArgs g) {
                     for (int e = 0; e < 16; ++e) {
                         const int wy = n_first + e - lam.shift;
                         const float re = __uint_as_float(v[2 * e]), im = __uint_as_float(v[2 * e + 1]);
-                        if (wy >= 0 && wy < wn) out[static_cast<size_t>(wy) * g.win_stride] = re * re + im * im;
+                        if (wy >= 0 && wy < wn) {
+                            const float I = re * re + im * im;
+                            out[static_cast<size_t>(wy) * g.win_stride] = I;
+                            esum += I;
+                        }
                     }
                 }
             }
         }
+    }
+    if (g.energy) {  // uniform
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+        if (lane == 0 && esum != 0.0f) atomicAdd(&g.energy[b * g.energy_stride], static_cast<double>(esum));
     }
     tc_fence_before();
     __syncthreads();

@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
                 if constexpr (FROM_EFFECT)
                     px[u][h] = in ? a.effect[static_cast<int64_t>(y) * W + x0 + h] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 else
-                    px[u][h] = in ? load_px(row, x0 + h, aligned) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    px[u][h] = in ? decode_px(a.transfer, load_px(row, x0 + h, aligned)) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             }
         }
 #pragma unroll
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
             const float3 e = mapped_effect<C>(a, smem, sx);
             erow[sx] = make_float4(e.x, e.y, e.z, 0.0f);
             if (!a.preserve) continue;
-            const float4 p = load_px(srow, sx, aligned_s);
+            const float4 p = decode_px(a.transfer, load_px(srow, sx, aligned_s));
             float sig;
             const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
             l_in += static_cast<double>(luma(p.x * m, p.y * m, p.z * m));
@@ -465,7 +465,8 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
 #pragma unroll
         for (int u = 0; u < kV; ++u) {
             const int sx = x0 + u * T - a.src_x1;
-            px[u] = (have && x0 + u * T < a.out_x2 && sx >= 0 && sx < a.W) ? load_px(srow, sx, aligned_s)
+            px[u] = (have && x0 + u * T < a.out_x2 && sx >= 0 && sx < a.W)
+                        ? decode_px(a.transfer, load_px(srow, sx, aligned_s))
                                                                            : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         }
 #pragma unroll
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
             const int sx = x - a.src_x1;
             float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
             if (have && sx >= 0 && sx < a.W) out = composite_px(a, px[u], mapped_effect<C>(a, smem, sx));
-            store_px(drow, x - a.dst_x1, aligned_d, out);
+            store_px(drow, x - a.dst_x1, aligned_d, encode_px(a.transfer, out));
         }
     }
 }
@@ -489,7 +490,7 @@ __global__ void __launch_bounds__(256) effect_sums_kernel(FrameArgs a) {
     const float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
     double l_in = 0.0, l_eff = 0.0;
     for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
-        const float4 p = load_px(srow, sx, aligned_s);
+        const float4 p = decode_px(a.transfer, load_px(srow, sx, aligned_s));
         float sig;
         const float m = selection_mask(a.sel, p.x, p.y, p.z, &sig) * a.sel.rscale;
         l_in += static_cast<double>(luma(p.x * m, p.y * m, p.z * m));
@@ -572,7 +573,7 @@ __global__ void __launch_bounds__(256) composite_kernel(FrameArgs a) {
         float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         const int sx = x - a.src_x1;
         if (have && sx >= 0 && sx < a.W) {
-            const float4 p = load_px(srow, sx, aligned_s);
+            const float4 p = decode_px(a.transfer, load_px(srow, sx, aligned_s));
             if constexpr (!RESAMPLE) {
                 const float3 e = effect_px<FRINGE>(a, sx, sy);
                 out = composite_px(a, p, make_float3(e.x * scale, e.y * scale, e.z * scale));
@@ -598,7 +599,7 @@ __global__ void __launch_bounds__(256) composite_kernel(FrameArgs a) {
                 out = composite_rd(a, p, rd, make_float3(e.x * scale, e.y * scale, e.z * scale));
             }
         }
-        store_px(drow, x - a.dst_x1, aligned_d, out);
+        store_px(drow, x - a.dst_x1, aligned_d, encode_px(a.transfer, out));
     }
 }
 
@@ -622,8 +623,9 @@ __global__ void __launch_bounds__(256) resample_source_kernel(FrameArgs a) {
         const float tx = __fsub_rn(fx, static_cast<float>(x0)), ty = __fsub_rn(fy, static_cast<float>(y0));
         const unsigned char* r0 = a.src + static_cast<int64_t>(y0) * a.src_pitch;
         const unsigned char* r1 = a.src + static_cast<int64_t>(y1) * a.src_pitch;
-        const float4 p00 = load_px(r0, x0, aligned), p10 = load_px(r0, x1, aligned);
-        const float4 p01 = load_px(r1, x0, aligned), p11 = load_px(r1, x1, aligned);
+        const int tf = a.transfer;
+        const float4 p00 = decode_px(tf, load_px(r0, x0, aligned)), p10 = decode_px(tf, load_px(r0, x1, aligned));
+        const float4 p01 = decode_px(tf, load_px(r1, x0, aligned)), p11 = decode_px(tf, load_px(r1, x1, aligned));
         const float4 u = make_float4(p00.x + (p10.x - p00.x) * tx, p00.y + (p10.y - p00.y) * tx,
                                      p00.z + (p10.z - p00.z) * tx, p00.w + (p10.w - p00.w) * tx);
         const float4 v = make_float4(p01.x + (p11.x - p01.x) * tx, p01.y + (p11.y - p01.y) * tx,

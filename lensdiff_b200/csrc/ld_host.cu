@@ -488,6 +488,9 @@ std::string bank_key(const ld_params& p, const std::vector<float>& wl) {
     return k;
 }
 
+static_assert(LD_TRANSFER_LINEAR == kTransferLinear && LD_TRANSFER_DAVINCI_INTERMEDIATE == kTransferDavinci,
+              "FrameArgs::transfer takes the public LD_TRANSFER_* values");
+
 // The steps after the effect (CpuReference.cpp:2089-2094, :2180-2198): the
 // resolution-aware working frame, scatter and creative fringe.
 struct PostEffects {
@@ -528,7 +531,8 @@ void validate_params(const ld_params& p) {
     if (p.look_mode != LD_LOOK_PHYSICAL && p.look_mode != LD_LOOK_SPLIT) throw Fail{LD_ERR_ARG, "invalid-look-mode"};
     if (p.look_mode == LD_LOOK_SPLIT && p.fft_form == LD_FFT_CUFFT)
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-split-look-with-cufft-form"};
-    if (p.input_transfer != LD_TRANSFER_LINEAR) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-input-transfer"};
+    if (p.input_transfer != LD_TRANSFER_LINEAR && p.input_transfer != LD_TRANSFER_DAVINCI_INTERMEDIATE)
+        throw Fail{LD_ERR_ARG, "invalid-input-transfer"};
     if (p.aperture_mode == LD_APERTURE_CUSTOM)  // image loader: WIC / ImageIO only (LensDiffApertureImage.cpp)
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-custom-aperture"};
     if (p.aperture_mode < LD_APERTURE_CIRCLE || p.aperture_mode > LD_APERTURE_SNOWFLAKE)
@@ -577,6 +581,8 @@ void setup_pupil(ld_ctx* c, PsfBankArgs& a, const ld_params& p, bool circle, cud
     staged(c, LD_STAGE_PUPIL, s, [&] { launch_pupil_pre(a, s); });
 }
 
+void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthInfo>& infos, cudaStream_t s);
+
 // ---------------------------------------------------------------------------
 // first-zero calibration of the clear circle (one host sync per (N_p, S))
 // ---------------------------------------------------------------------------
@@ -593,7 +599,6 @@ float first_zero(ld_ctx* c, int np, int S, cudaStream_t s) {
     a.half = S / 2;
     a.off = std::max(0, (S - np) / 2);
     a.win_stride = S;
-    a.plan_s = make_plan(c, S, fft_family(S, 1) == kE25);
     WavelengthInfo wi{};
     wi.win_x0 = 0;
     wi.win_n = S;
@@ -614,18 +619,51 @@ float first_zero(ld_ctx* c, int np, int S, cudaStream_t s) {
     float* r0d = reinterpret_cast<float*>(cal + o_r0);
     a.wl = dwl;
     a.scalars = dsc;
-    a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(a.row_n) * S * sizeof(float2)));
-    a.win = static_cast<float*>(ensure(c, c->calib_psf, static_cast<size_t>(S) * S * sizeof(float)));
-    check_cuda(cudaMemcpyAsync(dwl, &wi, sizeof(wi), cudaMemcpyHostToDevice, s), "calib-upload");
-    check_cuda(cudaMemsetAsync(dsc, 0, sizeof(PsfScalars), s), "calib-memset");
-    check_cuda(cudaMemsetAsync(cal + o_sums, 0, o_r0 + 256 - o_sums, s), "calib-memset");
-    launch_psf_rows(a, s);
-    launch_psf_cols(a, s);
-    launch_first_zero(a.win, S, sums, counts, total, r0d, s);
-    check_launch("first-zero-calibration");
     float r0 = 0.0f;
-    check_cuda(cudaMemcpyAsync(&r0, r0d, sizeof(float), cudaMemcpyDeviceToHost, s), "calib-readback");
-    check_cuda(cudaStreamSynchronize(s), "calib-sync");
+    if (smooth(S)) {
+        a.plan_s = make_plan(c, S, fft_family(S, 1) == kE25);
+        a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(a.row_n) * S * sizeof(float2)));
+        a.win = static_cast<float*>(ensure(c, c->calib_psf, static_cast<size_t>(S) * S * sizeof(float)));
+        check_cuda(cudaMemcpyAsync(dwl, &wi, sizeof(wi), cudaMemcpyHostToDevice, s), "calib-upload");
+        check_cuda(cudaMemsetAsync(dsc, 0, sizeof(PsfScalars), s), "calib-memset");
+        check_cuda(cudaMemsetAsync(cal + o_sums, 0, o_r0 + 256 - o_sums, s), "calib-memset");
+        launch_psf_rows(a, s);
+        launch_psf_cols(a, s);
+        launch_first_zero(a.win, S, sums, counts, total, r0d, s);
+        check_launch("first-zero-calibration");
+        check_cuda(cudaMemcpyAsync(&r0, r0d, sizeof(float), cudaMemcpyDeviceToHost, s), "calib-readback");
+        check_cuda(cudaStreamSynchronize(s), "calib-sync");
+    } else {
+        // S with a prime factor above 5 (the reference takes Bluestein's
+        // transform, LensDiffCpuReference.cpp:234-275): the PSF window around
+        // the centre by DFT-as-GEMM.  The rings that lie wholly inside the
+        // window have the whole PSF's profile; the PSF's sum comes from the
+        // pupil by Parseval.  The window spans about four first-zero radii; a
+        // scan that finds no minimum in it is repeated over the whole PSF.
+        const int ci = S / 2;
+        const double airy = 1.22 * static_cast<double>(S) / (0.86 * static_cast<double>(np));
+        int W = std::min(S / 2, std::max(64, static_cast<int>(std::ceil(4.0 * airy)) + 8));
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            if (attempt == 1) W = S / 2;
+            wi.win_x0 = std::max(0, ci - W);
+            wi.win_n = std::min(S, ci + W + 1) - wi.win_x0;
+            a.win_stride = wi.win_n;
+            a.win = static_cast<float*>(
+                ensure(c, c->calib_psf, static_cast<size_t>(wi.win_n) * wi.win_n * sizeof(float)));
+            check_cuda(cudaMemcpyAsync(dwl, &wi, sizeof(wi), cudaMemcpyHostToDevice, s), "calib-upload");
+            check_cuda(cudaMemsetAsync(dsc, 0, sizeof(PsfScalars), s), "calib-memset");
+            check_cuda(cudaMemsetAsync(cal + o_sums, 0, o_r0 + 256 - o_sums, s), "calib-memset");
+            dft_gemm_psf(c, a, std::vector<WavelengthInfo>{wi}, s);
+            launch_pupil_energy(a, static_cast<double>(S) * static_cast<double>(S), total, s);
+            const int rings = W >= S / 2 ? S / 2 + 1 : W;
+            launch_first_zero_window(a.win, a.win_stride, wi.win_n, wi.win_x0, S, rings, sums, counts, total, false,
+                                     r0d, s);
+            check_launch("first-zero-calibration");
+            check_cuda(cudaMemcpyAsync(&r0, r0d, sizeof(float), cudaMemcpyDeviceToHost, s), "calib-readback");
+            check_cuda(cudaStreamSynchronize(s), "calib-sync");
+            if (r0 >= 0.0f) break;
+        }
+    }
     c->launches += 5;
     c->r0_cache[key] = r0;
     return r0;
@@ -808,6 +846,8 @@ void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthI
     gc.y_lo = nullptr;
     gc.win = a.win;
     gc.win_stride = a.win_stride;
+    gc.energy = a.want_energy ? &a.scalars[0].energy : nullptr;
+    gc.energy_stride = static_cast<int>(sizeof(PsfScalars) / sizeof(double));
     staged(c, LD_STAGE_PSF_ROWS, s, [&] {
         launch_pupil_field(a, d, s);
         launch_dft_basis(bx, s);
@@ -849,8 +889,13 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     a.R = R;
     a.K = K;
     a.gain = 1.0f + std::max(0.0f, static_cast<float>(p.anisotropy_emphasis)) * 4.0f;  // :1127
-    a.plan_s = make_plan(c, S, fft_family(S, 1) == kE25);
-    a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(B) * a.row_n * win_stride * sizeof(float2)));
+    // tensor-core DFT for the chosen form, and for S with a prime factor above
+    // 5 (the reference's Bluestein sizes) in every own form
+    const bool dft = p.fft_form == LD_FFT_OWN_CHOSEN || (p.fft_form == LD_FFT_OWN_FP32 && !smooth(S));
+    if (!dft && p.fft_form != LD_FFT_CUFFT) {
+        a.plan_s = make_plan(c, S, fft_family(S, 1) == kE25);
+        a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(B) * a.row_n * win_stride * sizeof(float2)));
+    }
     a.win = static_cast<float*>(ensure(c, c->win, static_cast<size_t>(B) * win_stride * win_stride * sizeof(float)));
     a.canvas = static_cast<float*>(ensure(c, b.canvas, static_cast<size_t>(B) * K * K * sizeof(float)));
     const size_t ringn = static_cast<size_t>(B) * (R + 1);
@@ -873,7 +918,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
         float2* grid = static_cast<float2*>(
             ensure(c, c->cf_grid, cf_psf_chunk(S, B) * static_cast<size_t>(S) * S * sizeof(float2)));
         staged(c, LD_STAGE_PSF_ROWS, s, [&] { cf_psf_transform(a, grid, c->cufft, s); });
-    } else if (p.fft_form == LD_FFT_OWN_CHOSEN) {
+    } else if (dft) {
         dft_gemm_psf(c, a, infos, s);
     } else {
         staged(c, LD_STAGE_PSF_ROWS, s, [&] { launch_psf_rows(a, s); });
@@ -1506,6 +1551,11 @@ size_t ld_estimate_device_bytes(const ld_params* params, int32_t width, int32_t 
         if (zones > 1 || p.energy_mode == LD_ENERGY_PRESERVE || p.look_mode == LD_LOOK_SPLIT || post.any())
             t += static_cast<size_t>(width) * height * 16;            // stored effect
         if (post.resample) t += static_cast<size_t>(width) * height * 16;  // working source
+        if (p.fft_form == LD_FFT_OWN_CHOSEN || (p.fft_form == LD_FFT_OWN_FP32 && !smooth(static_cast<int>(S)))) {
+            // tensor-core DFT images, windows bounded by S
+            const size_t mt = (np + 127) / 128, kc = (np + 31) / 32, nt = (S + 3 + 127) / 128 + 1;
+            t += 2 * (B * (mt * 128 * 128 * kc + nt * 128 * 128 * mt * 4) + 2 * (2 * nt * 128) * 128 * kc);
+        }
         if (p.fft_form == LD_FFT_CUFFT) {
             const size_t P = static_cast<size_t>(2 * M) * Py, half = static_cast<size_t>(Py) * (M + 1);
             t += cf_psf_chunk(static_cast<int>(S), static_cast<int>(B)) * S * S * 8;
@@ -1613,6 +1663,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         fa.Ww = Ww;
         fa.Hw = Hw;
         fa.fringe_px = post.fringe;
+        fa.transfer = p.input_transfer;
         // the chain's view of the working frame: the resampled source, or
         // the source itself
         FrameArgs fw = fa;
@@ -1625,6 +1676,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             fw.src_y1 = 0;
             fw.W = Ww;
             fw.H = Hw;
+            fw.transfer = LD_TRANSFER_LINEAR;  // the working source is decoded already
         }
         // scatter: a Mono chain over the stored effect with one Gaussian kernel
         // on its own grid (CpuReference.cpp:2180-2186)
@@ -1874,7 +1926,6 @@ int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float
         a.half = S / 2;
         a.off = std::max(0, (S - np) / 2);
         a.win_stride = S;
-        a.plan_s = make_plan(ctx, S, fft_family(S, 1) == kE25);
         WavelengthInfo wi{};
         wi.phase = phase_for_wavelength(p, wl[static_cast<size_t>(wavelength_index)]);
         wi.win_x0 = 0;
@@ -1885,12 +1936,17 @@ int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float
         a.wl = dwl;
         a.scalars = dsc;
         a.want_energy = 1;
-        a.rows = static_cast<float2*>(ensure(ctx, ctx->rows, static_cast<size_t>(a.row_n) * S * sizeof(float2)));
         a.win = psf_out;
         check_cuda(cudaMemcpyAsync(dwl, &wi, sizeof(wi), cudaMemcpyHostToDevice, s), "rawpsf-upload");
         check_cuda(cudaMemsetAsync(dsc, 0, sizeof(PsfScalars), s), "rawpsf-memset");
-        launch_psf_rows(a, s);
-        launch_psf_cols(a, s);
+        if (smooth(S)) {
+            a.plan_s = make_plan(ctx, S, fft_family(S, 1) == kE25);
+            a.rows = static_cast<float2*>(ensure(ctx, ctx->rows, static_cast<size_t>(a.row_n) * S * sizeof(float2)));
+            launch_psf_rows(a, s);
+            launch_psf_cols(a, s);
+        } else {  // the reference's Bluestein sizes: the whole S x S window by DFT-as-GEMM
+            dft_gemm_psf(ctx, a, std::vector<WavelengthInfo>{wi}, s);
+        }
         launch_normalize_psf(psf_out, S * S, dsc, s);
         check_launch("raw-psf");
         // the upload above reads `wi` from the stack: finish before returning

@@ -99,6 +99,14 @@ void launch_export(const PsfBankArgs& a, const int64_t* offsets_dev, float* out,
 // (LensDiffCpuReference.cpp:865-955).
 void launch_first_zero(const float* psf, int S, double* ring_sums, int* ring_counts, double* total,
                        float* r0_out, cudaStream_t s);
+// The same scan over a window of the shifted PSF: psf[y * stride + x] for
+// x, y < n is the PSF at (x0 + x, x0 + y); the first `rings` rings are
+// complete in it.  own_total = false: *total already holds the whole PSF's
+// sum.  r0 = -1 when the window holds no minimum.
+void launch_first_zero_window(const float* psf, int stride, int n, int x0, int S, int rings, double* ring_sums,
+                              int* ring_counts, double* total, bool own_total, float* r0_out, cudaStream_t s);
+// scale * sum of the squared pupil amplitude added to *out.
+void launch_pupil_energy(const PsfBankArgs& a, double scale, double* out, cudaStream_t s);
 
 // Shifted full raw PSF export: window covers all of S x S; writes psf / energy.
 void launch_normalize_psf(float* psf, int n, const PsfScalars* sc, cudaStream_t s);
@@ -147,6 +155,10 @@ struct SelectionParams {
     float point_emphasis;
     float rscale;          // 1 - corePreserve
 };
+
+// FrameArgs::transfer values (the public LD_TRANSFER_* enum)
+constexpr int kTransferLinear = 0;
+constexpr int kTransferDavinci = 1;
 
 enum { kEffectComposite = 0, kEffectStore = 1, kEffectAccumulate = 2, kEffectScatter = 3 };
 
@@ -212,6 +224,9 @@ struct FrameArgs {
     float fringe_px;
     float4* work;
     int Ww, Hw;
+    // source / output encoding (LD_TRANSFER_*): source pixels are decoded to
+    // linear as they are read, output pixels encoded as they are written
+    int transfer;
 };
 void launch_frame_rows(const FrameArgs& a, cudaStream_t s);
 void launch_frame_cols(const FrameArgs& a, cudaStream_t s);
@@ -277,6 +292,8 @@ struct DftGemmArgs {
     float* win;                // kDftCols output windows
     int win_stride;
     const WavelengthInfo* wl;
+    double* energy;            // kDftCols: sum of the window added to energy[b * energy_stride] (null: none)
+    int energy_stride;         // in doubles
     int* err;
 };
 size_t dft_gemm_smem();

@@ -275,6 +275,7 @@ __device__ __forceinline__ float2 pupil_field(const PupilParams& p, const PhaseC
 // extent/fade/start precomputed per kernel.
 __device__ __forceinline__ float taper_weight(float radius, float extent, float fade, float start) {
     if (radius >= extent) return 0.0f;
+    if (radius <= start) return 1.0f;  // t = 0 below: cos(0) = 1 exactly
     const float t = fminf(fmaxf((radius - start) / fmaxf(fade, 1e-6f), 0.0f), 1.0f);
     const float s = t * t * (3.0f - 2.0f * t);
     return fmaxf(0.0f, cosf(s * static_cast<float>(3.14159265358979323846 * 0.5)));

@@ -33,6 +33,35 @@ __device__ __forceinline__ float4 load_px(const unsigned char* row, int x, bool 
     return make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3));
 }
 
+// DaVinci Intermediate, Blackmagic's published log encoding: the decode the
+// reference applies as it loads the source (ColorManagement.cpp:168-169 via
+// loadSourceRgba, LensDiffCpuReference.cpp:174-192) and the encode of its
+// final pixels (LensDiffTransfer.cpp:8-20, LensDiffCpuReference.cpp:2248-2250).
+__device__ __forceinline__ float davinci_decode(float x) {
+    return x <= 0.02740668f ? x / 10.44426855f : exp2f(x / 0.07329248f - 7.0f) - 0.0075f;
+}
+__device__ __forceinline__ float davinci_encode(float x) {
+    return x <= 0.00262409f ? x * 10.44426855f : (log2f(fmaxf(x, 0.0f) + 0.0075f) + 7.0f) * 0.07329248f;
+}
+// Source pixel in linear light (alpha untouched).
+__device__ __forceinline__ float4 decode_px(int transfer, float4 p) {
+    if (transfer == kTransferDavinci) {
+        p.x = davinci_decode(p.x);
+        p.y = davinci_decode(p.y);
+        p.z = davinci_decode(p.z);
+    }
+    return p;
+}
+// Output pixel in the source's encoding (alpha untouched).
+__device__ __forceinline__ float4 encode_px(int transfer, float4 p) {
+    if (transfer == kTransferDavinci) {
+        p.x = davinci_encode(p.x);
+        p.y = davinci_encode(p.y);
+        p.z = davinci_encode(p.z);
+    }
+    return p;
+}
+
 // MapLensDiffSpectralBins (LensDiffSpectrum.cpp:462-497) on one pixel whose
 // C channel values are e[0..C): clamp, saturation, luma lock.
 template <int C>

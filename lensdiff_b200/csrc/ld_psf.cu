@@ -24,6 +24,10 @@ namespace {
 
 constexpr int kTile = 32;       // canvas tile side for the per-pixel kernels
 constexpr int kRingSpan = 64;   // ring indices one 32x32 tile can touch
+// The ring-statistics passes (resample, shape_stats) take 32 x 128 tiles:
+// sixteen rows per thread amortise each CTA's ring setup, flush and sums.
+constexpr int kTallH = 128;
+constexpr int kRingSpanTall = 160;  // >= sqrt(31^2 + 127^2) + 3
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -52,40 +56,32 @@ __device__ double block_sum(double v) {
 // Adds each lane's v to ring[slot] (and, with PEAK, maxes it into
 // peak[slot] as float bits) where the lanes' slots form runs of equal values
 // in consecutive lanes (slot < 0: nothing to add), v >= 0.  A warp is 32
-// pixels of a canvas row: away from the axis through the centre the ring
-// index changes slowly and a warp has a few runs, each reduced with one
-// butterfly and added with one shared-memory atomic; near that axis it changes
-// at almost every pixel, and the lanes add directly (few address conflicts).
+// pixels of a canvas row, along which the ring index is monotonic on each
+// side of the centre, so equal slots are contiguous.  One inclusive
+// segmented scan over the warp (five shuffles) gives each run's sum (and
+// maximum) in its last lane, which adds it with one shared-memory atomic:
+// a fixed cost per warp whatever the number of runs.
 template <bool PEAK>
 __device__ __forceinline__ void warp_runs_accumulate(int slot, float v, float* ring, unsigned int* peak) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int prev = __shfl_up_sync(full, slot, 1);
-    unsigned heads = __ballot_sync(full, lane == 0 || prev != slot);
-    if (__popc(heads) > 4) {
-        if (slot >= 0) {
-            if (v != 0.0f) atomicAdd(&ring[slot], v);
-            if (PEAK && v != 0.0f) atomicMax(&peak[slot], __float_as_uint(v));
-        }
-        return;
-    }
-    while (heads) {  // warp-uniform
-        const int h = __ffs(heads) - 1;
-        heads &= heads - 1;
-        const int e = heads ? __ffs(heads) - 1 : 32;
-        const bool in = lane >= h && lane < e;
-        float x = in ? v : 0.0f;
-        float m = x;
+    const unsigned heads = __ballot_sync(full, lane == 0 || prev != slot);
+    const int head = 31 - __clz(heads & (full >> (31 - lane)));  // first lane of this lane's run
+    float sum = v, m = v;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            x += __shfl_xor_sync(full, x, o);
-            if (PEAK) m = fmaxf(m, __shfl_xor_sync(full, m, o));
+    for (int o = 1; o < 32; o <<= 1) {
+        const float t = __shfl_up_sync(full, sum, o);
+        const float u = PEAK ? __shfl_up_sync(full, m, o) : 0.0f;
+        if (lane - o >= head) {
+            sum += t;
+            if (PEAK) m = fmaxf(m, u);
         }
-        const int sl = __shfl_sync(full, slot, h);
-        if (lane == h && sl >= 0) {
-            if (x != 0.0f) atomicAdd(&ring[sl], x);
-            if (PEAK && m != 0.0f) atomicMax(&peak[sl], __float_as_uint(m));
-        }
+    }
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u) != 0u;
+    if (tail && slot >= 0) {
+        if (sum != 0.0f) atomicAdd(&ring[slot], sum);
+        if (PEAK && m != 0.0f) atomicMax(&peak[slot], __float_as_uint(m));
     }
 }
 
@@ -227,26 +223,63 @@ __device__ __forceinline__ float sample_filtered(const Window& w, float x, float
     return sum / static_cast<float>(taps * taps);
 }
 
-// First ring index a 32x32 tile can touch, for a centre at (c, c) and ring
+// First ring index a 32 x TH tile can touch, for a centre at (c, c) and ring
 // indices clamped to `cap`: every pixel of the tile has a ring index in
-// [base, base + kRingSpan).
+// [base, base + span) with span <= the tile's diagonal + 3 (kRingSpan for
+// 32 x 32 tiles, kRingSpanTall for the 32 x 128 tiles of the ring-statistics
+// passes).
+template <int TH = kTile>
 __device__ __forceinline__ int tile_ring_base(int tx0, int ty0, int c, int cap) {
     const int dx = tx0 > c ? tx0 - c : (tx0 + kTile - 1 < c ? c - (tx0 + kTile - 1) : 0);
-    const int dy = ty0 > c ? ty0 - c : (ty0 + kTile - 1 < c ? c - (ty0 + kTile - 1) : 0);
+    const int dy = ty0 > c ? ty0 - c : (ty0 + TH - 1 < c ? c - (ty0 + TH - 1) : 0);
     const float r = sqrtf(static_cast<float>(dx * dx + dy * dy));
     return min(cap, max(0, static_cast<int>(r) - 1));
 }
 
-// grid (ceil(K/32), ceil(K/32), B), block (32, 8).
+// The column half of a bilinear sample of the |F|^2 window at x
+// (sampleSquareBilinear's x terms): the same for every row a thread samples.
+struct ColTap {
+    bool in;       // x inside [0, S - 1]
+    int ax0, ax1;  // window columns of x0 and x1
+    float tx;
+};
+__device__ __forceinline__ ColTap col_tap(const Window& w, float x) {
+    ColTap c;
+    c.in = !(x < 0.0f || x > static_cast<float>(w.S - 1));
+    const int x0 = static_cast<int>(floorf(x));
+    const int x1 = min(x0 + 1, w.S - 1);
+    c.tx = x - static_cast<float>(x0);
+    const int hi = w.n - 1;
+    c.ax0 = min(max(x0 - w.x0, 0), hi);
+    c.ax1 = min(max(x1 - w.x0, 0), hi);
+    return c;
+}
+// sample_bilinear with the column half precomputed (identical arithmetic).
+__device__ __forceinline__ float sample_row(const Window& w, const ColTap& c, float y) {
+    if (!c.in || y < 0.0f || y > static_cast<float>(w.S - 1)) return 0.0f;
+    const int y0 = static_cast<int>(floorf(y));
+    const int y1 = min(y0 + 1, w.S - 1);
+    const float ty = y - static_cast<float>(y0);
+    const int hi = w.n - 1;
+    const float* r0 = w.p + min(max(y0 - w.x0, 0), hi) * w.stride;
+    const float* r1 = w.p + min(max(y1 - w.x0, 0), hi) * w.stride;
+    const float v00 = __ldg(r0 + c.ax0), v10 = __ldg(r0 + c.ax1);
+    const float v01 = __ldg(r1 + c.ax0), v11 = __ldg(r1 + c.ax1);
+    const float vx0 = v00 + (v10 - v00) * c.tx;
+    const float vx1 = v01 + (v11 - v01) * c.tx;
+    return vx0 + (vx1 - vx0) * ty;
+}
+
+// grid (ceil(K/32), ceil(K/128), B), block (32, 8).
 __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
-    __shared__ float ring[kRingSpan];
+    __shared__ float ring[kRingSpanTall];
     const int b = blockIdx.z;
     const WavelengthInfo* wi = a.wl + b;
     const int K = a.K, R = a.R;
-    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
+    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTallH;
     const int tid = threadIdx.x + threadIdx.y * 32;
-    const int rbase = tile_ring_base(tx0, ty0, R, R);
-    for (int i = tid; i < kRingSpan; i += 256) ring[i] = 0.0f;
+    const int rbase = tile_ring_base<kTallH>(tx0, ty0, R, R);
+    for (int i = tid; i < kRingSpanTall; i += 256) ring[i] = 0.0f;
     __syncthreads();
     const Window w{a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride, a.win_stride, wi->win_x0,
                    wi->win_n, a.S};
@@ -256,18 +289,20 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
     const float step = wi->step;
     const float rc = a.raw_center;
     float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
-    double lsum = 0.0;
+    float lsum = 0.0f;  // this thread's pixels; one double add per thread below
     const int x = tx0 + threadIdx.x;
-#pragma unroll
-    for (int i = 0; i < kTile / 8; ++i) {
+    const float dx = static_cast<float>(x) - kc;
+    const ColTap ct = col_tap(w, rc + dx * inv);
+#pragma unroll 4
+    for (int i = 0; i < kTallH / 8; ++i) {
         const int y = ty0 + threadIdx.y + 8 * i;
         const bool in = x < K && y < K;
         float v = 0.0f;
         int slot = -1;
         if (in) {
-            const float dx = static_cast<float>(x) - kc;
             const float dy = static_cast<float>(y) - kc;
-            v = sample_filtered(w, rc + dx * inv, rc + dy * inv, inv, taps, step);
+            v = taps == 0 ? sample_row(w, ct, rc + dy * inv)
+                          : sample_filtered(w, rc + dx * inv, rc + dy * inv, inv, taps, step);
             canvas[static_cast<size_t>(y) * K + x] = v;
             lsum += v;
             slot = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy)))) - rbase;
@@ -276,10 +311,10 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
     }
     __syncthreads();
     double* gring = a.ring_round + static_cast<size_t>(b) * (R + 1);
-    for (int i = tid; i < kRingSpan; i += 256) {
+    for (int i = tid; i < kRingSpanTall; i += 256) {
         if (ring[i] != 0.0f && rbase + i <= R) atomicAdd(&gring[rbase + i], static_cast<double>(ring[i]));
     }
-    const double tot = block_sum(lsum);
+    const double tot = block_sum(static_cast<double>(lsum));
     if (tid == 0) atomicAdd(&a.scalars[b].s1, tot);
 }
 
@@ -315,23 +350,23 @@ __global__ void __launch_bounds__(256) ring_mean_kernel(PsfBankArgs a) {
         out[r] = static_cast<float>(((rr[r] / s1) / max(1, a.count_round[r])) / s2);
 }
 
-// grid (ceil(K/32), ceil(K/32), B): shaped kernel (reshapeAnisotropy of the
+// grid (ceil(K/32), ceil(K/128), B): shaped kernel (reshapeAnisotropy of the
 // base kernel against its azimuthal mean, LensDiffCpuReference.cpp:1088-1135)
 // written in place, its sum, and its ring energy / peak by ceil(r)
 // (estimateAdaptiveSupportRadius, :984-1007).
 __global__ void __launch_bounds__(256) shape_stats_kernel(PsfBankArgs a) {
-    __shared__ float ring_e[kRingSpan];
-    __shared__ unsigned int ring_p[kRingSpan];
-    __shared__ float mean_r[kRingSpan];
+    __shared__ float ring_e[kRingSpanTall];
+    __shared__ unsigned int ring_p[kRingSpanTall];
+    __shared__ float mean_r[kRingSpanTall];
     const int b = blockIdx.z;
     const int tid = threadIdx.x + threadIdx.y * 32;
     const double s1 = a.scalars[b].s1;
     const int K = a.K, R = a.R;
-    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
-    const int rbase = tile_ring_base(tx0, ty0, R, R);
+    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTallH;
+    const int rbase = tile_ring_base<kTallH>(tx0, ty0, R, R);
     // ring means (round(r) rings) the tile can touch
     const float* rm = a.ring_mean + static_cast<size_t>(b) * (R + 1);
-    for (int i = tid; i < kRingSpan; i += 256) {
+    for (int i = tid; i < kRingSpanTall; i += 256) {
         ring_e[i] = 0.0f;
         ring_p[i] = 0u;
         const int r = rbase + i;
@@ -342,11 +377,19 @@ __global__ void __launch_bounds__(256) shape_stats_kernel(PsfBankArgs a) {
     const float gain = a.gain;
     const float kc = static_cast<float>(K - 1) * 0.5f;
     float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
-    double lsum = 0.0;
+    float lsum = 0.0f;  // this thread's pixels; one double add per thread below
     unsigned int lpeak = 0u;
     const int x = tx0 + threadIdx.x;
+    // the thread's four canvas reads are issued before any is used (each
+    // element is read, then written, by this thread only)
+    float raw[kTallH / 8];
 #pragma unroll
-    for (int i = 0; i < kTile / 8; ++i) {
+    for (int i = 0; i < kTallH / 8; ++i) {
+        const int y = ty0 + threadIdx.y + 8 * i;
+        raw[i] = (x < K && y < K) ? __ldg(canvas + static_cast<size_t>(y) * K + x) : 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < kTallH / 8; ++i) {
         const int y = ty0 + threadIdx.y + 8 * i;
         const bool in = x < K && y < K;
         float v = 0.0f;
@@ -356,7 +399,7 @@ __global__ void __launch_bounds__(256) shape_stats_kernel(PsfBankArgs a) {
             const float dy = static_cast<float>(y) - kc;
             const float rad = sqrtf(dx * dx + dy * dy);
             const size_t idx = static_cast<size_t>(y) * K + x;
-            const float base = canvas[idx] * inv_s1;
+            const float base = raw[i] * inv_s1;
             const float mean = mean_r[min(R, static_cast<int>(roundf(rad))) - rbase];
             v = fmaxf(0.0f, mean + (base - mean) * gain);
             canvas[idx] = v;
@@ -368,7 +411,7 @@ __global__ void __launch_bounds__(256) shape_stats_kernel(PsfBankArgs a) {
     }
     __syncthreads();
     const size_t ro = static_cast<size_t>(b) * (R + 1);
-    for (int i = tid; i < kRingSpan; i += 256) {
+    for (int i = tid; i < kRingSpanTall; i += 256) {
         if (rbase + i <= R) {
             if (ring_e[i] != 0.0f) atomicAdd(&a.ring_ceil[ro + rbase + i], static_cast<double>(ring_e[i]));
             if (ring_p[i] != 0u) atomicMax(&a.ring_peak[ro + rbase + i], ring_p[i]);
@@ -376,7 +419,7 @@ __global__ void __launch_bounds__(256) shape_stats_kernel(PsfBankArgs a) {
     }
     for (int o = 16; o > 0; o >>= 1) lpeak = max(lpeak, __shfl_xor_sync(0xffffffffu, lpeak, o));
     if ((tid & 31) == 0 && lpeak != 0u) atomicMax(&a.scalars[b].peak, lpeak);
-    const double tot = block_sum(lsum);
+    const double tot = block_sum(static_cast<double>(lsum));
     if (tid == 0) atomicAdd(&a.scalars[b].s3, tot);
 }
 
@@ -463,40 +506,53 @@ __global__ void __launch_bounds__(256) support_kernel(PsfBankArgs a) {
     sc.start = fmaxf(0.0f, extent - fade);
 }
 
-// grid (ceil(K/32), ceil(K/32), B): crop + taper in place (0 outside the
-// crop box) and s4 = sum of taper * normalised shaped kernel, the normaliser
-// of cropKernelToRadius.
+// grid (ceil(K/8), B), block 256: s4 = sum over the crop box of taper *
+// normalised shaped kernel, the normaliser of cropKernelToRadius and
+// applySupportBoundaryTaper (LensDiffCpuReference.cpp:1038-1058, :957-982).
+// The canvas keeps the shaped kernel; the crop and the taper are applied
+// where the kernel is read (combine_kernel, split_sums_kernel, export_kernel).
+// One CTA sums 8 rows of the crop box, eight reads in flight per thread.
+constexpr int kCropRows = 8;
 __global__ void __launch_bounds__(256) crop_sum_kernel(PsfBankArgs a) {
-    const int b = blockIdx.z;
+    const int b = blockIdx.y;
     const PsfScalars& sc = a.scalars[b];
-    const float inv_s3 = static_cast<float>(1.0 / sc.s3);
     const int rho = sc.radius;
     const int K = a.K, R = a.R;
-    float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
-    const int x = blockIdx.x * kTile + threadIdx.x;
-    double lsum = 0.0;
+    const int y0 = R - rho + static_cast<int>(blockIdx.x) * kCropRows;
+    if (y0 > R + rho) return;  // uniform
+    const float inv_s3 = static_cast<float>(1.0 / sc.s3);
+    const float extent = sc.extent, fade = sc.fade, start = sc.start;
+    const float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
+    const int side = 2 * rho + 1;
+    const int rows = min(kCropRows, R + rho + 1 - y0);
+    const int items = rows * side;
+    constexpr int kU = 8;
+    float lsum = 0.0f;
+    for (int i0 = threadIdx.x; i0 < items; i0 += kU * 256) {
+        float v[kU];
 #pragma unroll
-    for (int i = 0; i < kTile / 8; ++i) {
-        const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
-        if (x < K && y < K) {
-            const int ix = x - R, iy = y - R;
-            const size_t idx = static_cast<size_t>(y) * K + x;
-            float t = 0.0f;
-            if (abs(ix) <= rho && abs(iy) <= rho) {
-                const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
-                const float wgt = taper_weight(sqrtf(dx * dx + dy * dy), sc.extent, sc.fade, sc.start);
-                t = canvas[idx] * wgt;
-                lsum += static_cast<double>((canvas[idx] * inv_s3) * wgt);
-            }
-            canvas[idx] = t;
+        for (int u = 0; u < kU; ++u) {
+            const int i = i0 + u * 256;
+            const int r = i / side;
+            const int c = i - r * side;
+            v[u] = i < items ? __ldg(canvas + static_cast<size_t>(y0 + r) * K + (R - rho + c)) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int i = i0 + u * 256;
+            if (i >= items) break;
+            const int r = i / side;
+            const float dy = static_cast<float>(y0 + r - R);
+            const float dx = static_cast<float>(i - r * side - rho);
+            lsum += (v[u] * inv_s3) * taper_weight(sqrtf(dx * dx + dy * dy), extent, fade, start);
         }
     }
-    const double tot = block_sum(lsum);
-    if (threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(&a.scalars[b].s4, tot);
+    const double tot = block_sum(static_cast<double>(lsum));
+    if (threadIdx.x == 0) atomicAdd(&a.scalars[b].s4, tot);
 }
 
 // grid (ceil(K/32), ceil(K/32), B): the Split look's normalisers after the
-// crop (the canvas holds shaped * taper, 0 outside the crop box):
+// crop (the canvas holds the shaped kernel; taper applied here):
 // s_core = sum of mean * taper, s_struct = sum of max(0, shaped * taper / s3
 // - mean * taper) over the crop box.
 __global__ void __launch_bounds__(256) split_sums_kernel(PsfBankArgs a) {
@@ -520,7 +576,7 @@ __global__ void __launch_bounds__(256) split_sums_kernel(PsfBankArgs a) {
                 const float wgt = taper_weight(rad, sc.extent, sc.fade, sc.start);
                 const float mt = rm[min(R, static_cast<int>(roundf(rad)))] * wgt;
                 lcore += static_cast<double>(mt);
-                lstruct += static_cast<double>(fmaxf(0.0f, canvas[static_cast<size_t>(y) * K + x] * inv_s3 - mt));
+                lstruct += static_cast<double>(fmaxf(0.0f, (canvas[static_cast<size_t>(y) * K + x] * wgt) * inv_s3 - mt));
             }
         }
     }
@@ -532,16 +588,35 @@ __global__ void __launch_bounds__(256) split_sums_kernel(PsfBankArgs a) {
 }
 
 // grid (ceil(K/32), ceil(K/32)), block (32, 8): out[k] = sum_b coef[k][b] *
-// final_b with final_b = canvas_b / (s3_b * s4_b).
+// final_b with final_b = crop_b(canvas_b * taper_b) / (s3_b * s4_b): the crop
+// box and boundary taper of each wavelength (cropKernelToRadius,
+// applySupportBoundaryTaper, LensDiffCpuReference.cpp:1038-1058, :957-982)
+// are applied here as the shaped kernels are read.  Eight wavelengths'
+// reads are issued before any is used.  SPLIT: the core and structure
+// kernels of the Split look instead.
+struct CombineBin {
+    float w[4];                // coef[k][b] / (s3 s4)
+    float ext, fade, start;    // taper
+    int rho;                   // crop radius
+};
+
+template <bool SPLIT>
 __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
     __shared__ float inv[kMaxBins], inv_s3[kMaxBins], inv_core[kMaxBins], inv_struct[kMaxBins];
     __shared__ float ext[kMaxBins], fade[kMaxBins], start[kMaxBins];
     __shared__ int rho[kMaxBins];
+    __shared__ CombineBin bin[kMaxBins];
     const int tid = threadIdx.x + threadIdx.y * 32;
     const int B = a.bank.B;
     for (int b = tid; b < B; b += 256) {
         const PsfScalars& sc = a.bank.scalars[b];
-        inv[b] = static_cast<float>(1.0 / (sc.s3 * sc.s4));
+        const float ib = static_cast<float>(1.0 / (sc.s3 * sc.s4));
+        for (int k = 0; k < 4; ++k) bin[b].w[k] = a.coef[k][b] * ib;
+        bin[b].ext = sc.extent;
+        bin[b].fade = sc.fade;
+        bin[b].start = sc.start;
+        bin[b].rho = sc.radius;
+        inv[b] = ib;
         inv_s3[b] = static_cast<float>(1.0 / sc.s3);
         inv_core[b] = sc.s_core > 0.0 ? static_cast<float>(1.0 / sc.s_core) : 0.0f;
         inv_struct[b] = sc.s_struct > 0.0 ? static_cast<float>(1.0 / sc.s_struct) : 0.0f;
@@ -554,43 +629,61 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
     const int x = blockIdx.x * kTile + threadIdx.x;
     const int K = a.bank.K, R = a.bank.R;
     const size_t plane = static_cast<size_t>(K) * K;
+    constexpr int kU = 8;
 #pragma unroll 1
     for (int i = 0; i < kTile / 8; ++i) {
         const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
         if (x >= K || y >= K) continue;
         const size_t idx = static_cast<size_t>(y) * K + x;
-        if (!a.split) {
-            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            for (int b = 0; b < B; ++b) {
-                const float v = a.bank.canvas[b * plane + idx] * inv[b];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) acc[k] += a.coef[k][b] * v;
-            }
-            for (int k = 0; k < a.n_ker; ++k) a.out[k * plane + idx] = acc[k];
-            continue;
-        }
-        // Split: core = mean * taper / s_core, structure = max(0, shaped / s3
-        // - mean) * taper / s_struct; the canvas holds shaped * taper
         const int ix = x - R, iy = y - R;
+        const int aix = max(abs(ix), abs(iy));  // inside the crop box of b iff aix <= rho[b]
         const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
         const float rad = sqrtf(dx * dx + dy * dy);
+        if constexpr (!SPLIT) {
+            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            for (int b0 = 0; b0 < B; b0 += kU) {
+                float v[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int b = b0 + u;
+                    v[u] = (b < B && aix <= bin[b].rho) ? __ldg(a.bank.canvas + b * plane + idx) : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    if (v[u] != 0.0f) {  // else outside the crop box, or a zero kernel value
+                        const CombineBin& cb = bin[b0 + u];
+                        const float f = v[u] * taper_weight(rad, cb.ext, cb.fade, cb.start);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) acc[k] += cb.w[k] * f;
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < a.n_ker) a.out[k * plane + idx] = acc[k];
+        } else {
+        // Split: core = mean * taper / s_core, structure = max(0, shaped *
+        // taper / s3 - mean * taper) / s_struct
         const int ring = min(R, static_cast<int>(roundf(rad)));
         float core[4] = {0.0f, 0.0f, 0.0f, 0.0f}, strc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
         for (int b = 0; b < B; ++b) {
-            if (abs(ix) > rho[b] || abs(iy) > rho[b]) continue;
+            if (aix > rho[b]) continue;
             const float wgt = taper_weight(rad, ext[b], fade[b], start[b]);
             const float mt = a.bank.ring_mean[static_cast<size_t>(b) * (R + 1) + ring] * wgt;
             const float c = mt * inv_core[b];
-            const float st = fmaxf(0.0f, a.bank.canvas[b * plane + idx] * inv_s3[b] - mt) * inv_struct[b];
+            const float st = fmaxf(0.0f, (a.bank.canvas[b * plane + idx] * wgt) * inv_s3[b] - mt) * inv_struct[b];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 core[k] += a.coef[k][b] * c;
                 strc[k] += a.coef[k][b] * st;
             }
         }
-        for (int k = 0; k < a.n_ker; ++k) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k >= a.n_ker) break;
             a.out[k * plane + idx] = core[k];
             a.out[(a.n_ker + k) * plane + idx] = strc[k];
+        }
         }
     }
 }
@@ -609,15 +702,19 @@ __global__ void __launch_bounds__(256) export_kernel(PsfBankArgs a, const int64_
         if (x >= a.K || y >= a.K) continue;
         const int ix = x - a.R + rho, iy = y - a.R + rho;
         if (ix < 0 || iy < 0 || ix >= side || iy >= side) continue;
-        out[offsets[b] + static_cast<int64_t>(iy) * side + ix] = canvas[static_cast<size_t>(y) * a.K + x] * inv;
+        const float dx = static_cast<float>(x - a.R), dy = static_cast<float>(y - a.R);
+        const float wgt = taper_weight(sqrtf(dx * dx + dy * dy), sc.extent, sc.fade, sc.start);
+        out[offsets[b] + static_cast<int64_t>(iy) * side + ix] = (canvas[static_cast<size_t>(y) * a.K + x] * wgt) * inv;
     }
 }
 
 // ---- first-minimum calibration ------------------------------------------------------
 // grid (ceil(S/32), ceil(S/32)), block (32, 8): sums and counts of the shifted
 // intensity by round(r) around shiftedSpectrumCenterCoordinate.
-__global__ void __launch_bounds__(256) profile_kernel(const float* psf, int S, double* sums, int* counts,
-                                                      double* total) {
+// The window psf[y * stride + x], x, y < n, is the square of the shifted PSF
+// starting at (x0, x0); total == null: the caller supplies the full PSF's sum.
+__global__ void __launch_bounds__(256) profile_kernel(const float* psf, int stride, int n, int x0, int S,
+                                                      double* sums, int* counts, double* total) {
     __shared__ double rs[kRingSpan];
     __shared__ int rc[kRingSpan];
     const int tid = threadIdx.x + threadIdx.y * 32;
@@ -625,7 +722,7 @@ __global__ void __launch_bounds__(256) profile_kernel(const float* psf, int S, d
     const int ci = static_cast<int>(c);
     const int rmax = S / 2;
     const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
-    const int rbase = tile_ring_base(tx0, ty0, ci, rmax);
+    const int rbase = tile_ring_base(x0 + tx0, x0 + ty0, ci, rmax);
     for (int i = tid; i < kRingSpan; i += 256) {
         rs[i] = 0.0;
         rc[i] = 0;
@@ -635,11 +732,11 @@ __global__ void __launch_bounds__(256) profile_kernel(const float* psf, int S, d
     const int x = tx0 + threadIdx.x;
     for (int i = 0; i < kTile / 8; ++i) {
         const int y = ty0 + threadIdx.y + 8 * i;
-        if (x < S && y < S) {
-            const float dx = static_cast<float>(x) - c;
-            const float dy = static_cast<float>(y) - c;
+        if (x < n && y < n) {
+            const float dx = static_cast<float>(x0 + x) - c;
+            const float dy = static_cast<float>(x0 + y) - c;
             const int r = min(rmax, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy))));
-            const float v = psf[static_cast<size_t>(y) * S + x];
+            const float v = psf[static_cast<size_t>(y) * stride + x];
             lsum += v;
             atomicAdd(&rs[r - rbase], static_cast<double>(v));
             atomicAdd(&rc[r - rbase], 1);
@@ -652,8 +749,10 @@ __global__ void __launch_bounds__(256) profile_kernel(const float* psf, int S, d
             atomicAdd(&counts[rbase + i], rc[i]);
         }
     }
-    const double tot = block_sum(lsum);
-    if (tid == 0) atomicAdd(total, tot);
+    if (total) {
+        const double tot = block_sum(lsum);
+        if (tid == 0) atomicAdd(total, tot);
+    }
 }
 
 __device__ float refine_parabolic(double l, double c, double r) {
@@ -665,10 +764,12 @@ __device__ float refine_parabolic(double l, double c, double r) {
 // One thread: radialMeanProfile normalised by the total, [1,2,1]/4 smoothing,
 // first local minimum after >= 2 descents with parabolic refinement, fallback
 // argmin over [1, max(4, S/8)] (LensDiffCpuReference.cpp:897-955).
-__global__ void first_zero_scan_kernel(const double* sums, const int* counts, const double* total, int S,
-                                       double* prof, float* r0) {
+// n: rings profiled (S / 2 + 1 for the whole PSF); truncated: the rings past
+// n exist but were not profiled, so a scan that finds no minimum inside them
+// reports r0 = -1 instead of taking the fallback over all rings.
+__global__ void first_zero_scan_kernel(const double* sums, const int* counts, const double* total, int S, int n,
+                                       int truncated, double* prof, float* r0) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const int n = S / 2 + 1;
     const double t = *total > 0.0 ? *total : 1.0;
     for (int r = 0; r < n; ++r) prof[r] = (sums[r] / t) / max(1, counts[r]);
     if (n < 4) {
@@ -701,6 +802,10 @@ __global__ void first_zero_scan_kernel(const double* sums, const int* counts, co
         bestv = sm[i];
         desc = 0;
     }
+    if (truncated) {
+        *r0 = -1.0f;
+        return;
+    }
     const int limit = max(2, min(n - 1, max(4, S / 8)));
     best = 1;
     bestv = sm[1];
@@ -714,6 +819,19 @@ __global__ void first_zero_scan_kernel(const double* sums, const int* counts, co
         *r0 = fmaxf(1.0f, static_cast<float>(best) + refine_parabolic(sm[best - 1], sm[best], sm[best + 1]));
     else
         *r0 = static_cast<float>(best);
+}
+
+// scale * sum of the squared pupil amplitude: by Parseval, the sum of the
+// unnormalised S x S PSF when scale = S^2.
+__global__ void __launch_bounds__(256) pupil_energy_kernel(PsfBankArgs a, double scale, double* out) {
+    const int n = a.pupil.size * a.pupil.size;
+    double acc = 0.0;
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+        const float amp = a.pupil_pre[i].x;
+        acc += static_cast<double>(amp) * amp;
+    }
+    const double t = block_sum(acc);
+    if (threadIdx.x == 0) atomicAdd(out, t * scale);
 }
 
 __global__ void normalize_psf_kernel(float* psf, int64_t n, const PsfScalars* sc) {
@@ -738,6 +856,10 @@ template <int E, int C>
 void cols_launch(const PsfBankArgs& a, cudaStream_t s) {
     dim3 grid((a.win_stride + C - 1) / C, a.B);
     psf_cols_kernel<E, C><<<grid, fft_threads(a.S, C, E), static_cast<size_t>(a.S) * C * sizeof(float2), s>>>(a);
+}
+
+dim3 tall_grid(const PsfBankArgs& a) {
+    return dim3((a.K + kTile - 1) / kTile, (a.K + kTallH - 1) / kTallH, a.B);
 }
 
 dim3 canvas_grid(const PsfBankArgs& a, int z) {
@@ -769,18 +891,18 @@ void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s) {
 }
 
 void launch_resample(const PsfBankArgs& a, cudaStream_t s) {
-    resample_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
+    resample_kernel<<<tall_grid(a), dim3(32, 8), 0, s>>>(a);
 }
 
 void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s) {
     ring_mean_kernel<<<a.B, 256, 0, s>>>(a);
-    shape_stats_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
+    shape_stats_kernel<<<tall_grid(a), dim3(32, 8), 0, s>>>(a);
 }
 
 void launch_support(const PsfBankArgs& a, cudaStream_t s) { support_kernel<<<a.B, 256, 0, s>>>(a); }
 
 void launch_crop_sum(const PsfBankArgs& a, cudaStream_t s) {
-    crop_sum_kernel<<<canvas_grid(a, a.B), dim3(32, 8), 0, s>>>(a);
+    crop_sum_kernel<<<dim3((a.K + kCropRows - 1) / kCropRows, a.B), 256, 0, s>>>(a);
 }
 
 void launch_split_sums(const PsfBankArgs& a, cudaStream_t s) {
@@ -788,7 +910,8 @@ void launch_split_sums(const PsfBankArgs& a, cudaStream_t s) {
 }
 
 void launch_combine(const CombineArgs& a, cudaStream_t s) {
-    combine_kernel<<<canvas_grid(a.bank, 1), dim3(32, 8), 0, s>>>(a);
+    if (a.split) combine_kernel<true><<<canvas_grid(a.bank, 1), dim3(32, 8), 0, s>>>(a);
+    else combine_kernel<false><<<canvas_grid(a.bank, 1), dim3(32, 8), 0, s>>>(a);
 }
 
 void launch_export(const PsfBankArgs& a, const int64_t* offsets_dev, float* out, cudaStream_t s) {
@@ -797,10 +920,21 @@ void launch_export(const PsfBankArgs& a, const int64_t* offsets_dev, float* out,
 
 void launch_first_zero(const float* psf, int S, double* ring_sums, int* ring_counts, double* total, float* r0_out,
                        cudaStream_t s) {
-    dim3 grid((S + kTile - 1) / kTile, (S + kTile - 1) / kTile);
-    profile_kernel<<<grid, dim3(32, 8), 0, s>>>(psf, S, ring_sums, ring_counts, total);
+    launch_first_zero_window(psf, S, S, 0, S, S / 2 + 1, ring_sums, ring_counts, total, true, r0_out, s);
+}
+
+void launch_first_zero_window(const float* psf, int stride, int n, int x0, int S, int rings, double* ring_sums,
+                              int* ring_counts, double* total, bool own_total, float* r0_out, cudaStream_t s) {
+    dim3 grid((n + kTile - 1) / kTile, (n + kTile - 1) / kTile);
+    profile_kernel<<<grid, dim3(32, 8), 0, s>>>(psf, stride, n, x0, S, ring_sums, ring_counts,
+                                                own_total ? total : nullptr);
     // profile scratch follows the ring sums: 2 * (S/2 + 1) doubles
-    first_zero_scan_kernel<<<1, 32, 0, s>>>(ring_sums, ring_counts, total, S, ring_sums + (S / 2 + 1), r0_out);
+    first_zero_scan_kernel<<<1, 32, 0, s>>>(ring_sums, ring_counts, total, S, rings, rings < S / 2 + 1 ? 1 : 0,
+                                            ring_sums + (S / 2 + 1), r0_out);
+}
+
+void launch_pupil_energy(const PsfBankArgs& a, double scale, double* out, cudaStream_t s) {
+    pupil_energy_kernel<<<64, 256, 0, s>>>(a, scale, out);
 }
 
 void launch_normalize_psf(float* psf, int n, const PsfScalars* sc, cudaStream_t s) {

@@ -765,6 +765,25 @@ def field_zone_banks(p, n: int = 3):
     return out
 
 
+# ------------------------------------------------------------ transfer
+def davinci_decode(x: np.ndarray) -> np.ndarray:
+    """DaVinci Intermediate to linear (Blackmagic's published curve; the
+    reference's decodeToLinear, ColorManagement.cpp:168-169), float."""
+    x = np.asarray(x, np.float32)
+    with np.errstate(over="ignore"):
+        lin = (np.exp2(x / F(0.07329248) - F(7.0)) - F(0.0075)).astype(np.float32)
+    return np.where(x <= F(0.02740668), (x / F(10.44426855)).astype(np.float32), lin)
+
+
+def davinci_encode(x: np.ndarray) -> np.ndarray:
+    """Linear to DaVinci Intermediate (encodeChannelFromLinear,
+    LensDiffTransfer.cpp:8-20)."""
+    x = np.asarray(x, np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        log = (np.log2(np.maximum(x, 0.0) + 0.0075) + 7.0) * 0.07329248
+    return np.where(x <= 0.00262409, x * 10.44426855, log)
+
+
 # ------------------------------------------------------- after the effect
 def working_frame(p, w: int, h: int) -> Tuple[bool, int, int]:
     """Resolution-aware working frame: ResolveLensDiffEffectWorkingScale
@@ -870,6 +889,9 @@ def render(src: np.ndarray, p, bank: PsfBank, natural: Optional[np.ndarray] = No
     src: (H, W, 4) float array at bounds origin `src_origin`.  Returns the dst
     image (dh, dw, 4) for `dst_bounds` = (x1, y1, x2, y2) (defaults to src)."""
     sh, sw = src.shape[:2]
+    davinci = int(_p(p, "inputTransfer", 0)) == 1
+    if davinci:  # loadSourceRgba decodes the source first (CpuReference.cpp:174-192)
+        src = np.concatenate([davinci_decode(src[..., :3]), np.asarray(src[..., 3:4], np.float32)], axis=-1)
     srcd = src.astype(np.float64)
     resample, w, h = working_frame(p, sw, sh)
     work = resample_rgba(src, w, h).astype(np.float32) if resample else src
@@ -925,7 +947,10 @@ def render(src: np.ndarray, p, bank: PsfBank, natural: Optional[np.ndarray] = No
         effect = resample_rgba(effect, sw, sh)
     raw = np.maximum(0.0, srcd[..., :3] - cc * redist + gain * effect)
     floor = np.maximum(0.0, srcd[..., :3] - redist * max_sub)
-    final = np.concatenate([np.maximum(raw, floor), srcd[..., 3:4]], axis=-1)
+    rgb = np.maximum(raw, floor)
+    if davinci:  # the final pixels are encoded back (:2248-2250)
+        rgb = davinci_encode(rgb)
+    final = np.concatenate([rgb, srcd[..., 3:4]], axis=-1)
     h, w = sh, sw
 
     sx1, sy1 = src_origin

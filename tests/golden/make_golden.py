@@ -76,6 +76,8 @@ def golden_params():
     cases["mono_aware_down_fringe"] = aware.copy(
         spectralMode=LensDiffSpectralMode.Mono, apertureMode=LensDiffApertureMode.Circle, frameShortSidePx=4320,
         maxKernelRadiusPx=S.radius_percent(10, 2160), creativeFringe=0.1)
+    # DaVinci Intermediate source and output encoding (frames of encoded values)
+    cases["spectral5_davinci_transfer"] = base.copy(spectralMode=LensDiffSpectralMode.Spectral5, inputTransfer=1)
     return cases
 
 
@@ -115,7 +117,8 @@ def main() -> None:
     meta = {}
     for name, p in cases.items():
         w, h = (128, 72) if "spectral9" not in name else (97, 61)
-        frame = S.make_frame(w, h, 12, 1.0, 80.0, seed=zlib.crc32(name.encode()) % 1000 + 11)
+        lo, hi = (0.55, 0.8) if "davinci" in name else (1.0, 80.0)  # encoded values decode to about 1-40
+        frame = S.make_frame(w, h, 12, lo, hi, seed=zlib.crc32(name.encode()) % 1000 + 11)
         out = R.render(p, frame)
         wl, fulls, _, _, sup = R.bank(p)
         np.savez_compressed(os.path.join(OUT, f"render_{name}.npz"), src=frame, dst=out)

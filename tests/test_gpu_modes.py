@@ -433,3 +433,76 @@ def test_post_effects_refused_with_cufft_form(cache):
     d = torch.zeros_like(s)
     st = cache.render(image_request(s, d, stream), with_matrices(p))
     assert not st.ok and st.stage == "unsupported-scatter-fringe-or-resolution-aware-with-cufft-form"
+
+
+# ------------------------------------------- PSF sizes with a prime factor > 5 ---
+# S = 4 R_max = 1204 = 4 * 7 * 43: the reference transforms it with Bluestein's
+# algorithm (LensDiffCpuReference.cpp:234-275); here the raw PSF's window (and
+# the whole S x S PSF for the raw-PSF export) comes from the tensor-core DFT,
+# and the first-zero calibration profiles a window around the centre.
+def _bluestein_lens(**kw):
+    p = _lens(pupilResolution=64, maxKernelRadiusPx=S.radius_percent(301, 144), diffractionScalePx=2.0, **kw)
+    from lensdiff_b200.backend import resolve_sizes
+    assert resolve_sizes(p)[1] == 1204
+    return p
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_non_smooth_psf_size_bank_matches_reference(cache, form):
+    from lensdiff_b200.types import LensDiffFftForm
+    from tests.helpers import PSF_TOL
+    _reference_available()
+    p = _bluestein_lens(fftForm=LensDiffFftForm(form))
+    wls, kernels, st = cache.export_psf_bank(p, torch.cuda.current_stream())
+    assert st.ok, st
+    assert cache.check_device_errors() == 0
+    rwl, rfull, _, _, rsup = R.bank(p)
+    assert st.support_radius == rsup
+    for k, ref in zip(kernels, rfull):
+        assert k.shape == ref.shape
+        assert rel_err(k, ref, ref.max()) < PSF_TOL
+
+
+def test_non_smooth_psf_size_raw_psf_and_render(cache):
+    from tests.helpers import PSF_TOL
+    _reference_available()
+    p = _bluestein_lens()
+    out = torch.zeros(1204, 1204, device="cuda")
+    st = cache.raw_psf(p, 1, out, torch.cuda.Stream())
+    assert st.ok, st
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().astype(np.float64)
+    ref = R.raw_psf(p, 550.0).astype(np.float64)
+    got /= got.sum()
+    ref /= ref.sum()
+    assert rel_err(got, ref, ref.max()) < PSF_TOL
+    src = S.make_frame(200, 120, 14, 1.0, 60.0, seed=81)
+    img = _render(cache, with_matrices(p), src)
+    refimg = R.render(p, src)
+    assert rel_err(img, refimg, refimg[..., :3].max()) < OUT_TOL
+
+
+# ------------------------------------------------ DaVinci Intermediate transfer ---
+# The source is decoded to linear as it is read and the output encoded back
+# (loadSourceRgba, LensDiffCpuReference.cpp:174-192; :2248-2250), in every
+# transform form and with the resolution-aware working frame.
+@pytest.mark.parametrize("kw", [{"fftForm": 0}, {"fftForm": 1}, {"fftForm": 2},
+                                {"fftForm": 0, "energyMode": LensDiffEnergyMode.Preserve, "creativeFringe": 1.0},
+                                {"fftForm": 1, "resolutionAware": True, "frameShortSidePx": 1080,
+                                 "maxKernelRadiusPx": 1.25, "diffractionScalePx": 0.2}])
+def test_davinci_transfer_matches_reference(cache, kw):
+    from lensdiff_b200.types import LensDiffFftForm
+    _reference_available()
+    kw = dict(kw)
+    form = LensDiffFftForm(kw.pop("fftForm"))
+    p = _lens(inputTransfer=1, **kw)
+    src = S.make_frame(224, 144, 20, 0.55, 0.8, seed=91)
+    out = _render(cache, with_matrices(p.copy(fftForm=form)), src)
+    ref = R.render(p, src)
+    # the output bar is on linear RGB: compare the decoded frames (the log
+    # curve's slope is 10.4 near black, so encoded differences of the FP16
+    # chosen form exceed the bar there while the linear ones stay within it)
+    lin, rlin = O.davinci_decode(out[..., :3]), O.davinci_decode(ref[..., :3])
+    assert rel_err(lin, rlin, rlin.max()) < OUT_TOL
+    if form != LensDiffFftForm.OwnChosen:
+        assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL

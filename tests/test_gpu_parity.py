@@ -233,7 +233,7 @@ def test_error_behaviour_mirrors_reference(cache):
     req = image_request(src, dst, stream, frame_short_side=144)
     st = cache.render(req, p.copy(debugView=3))
     assert st.code == 6 and "debug" in st.stage
-    st = cache.render(req, p.copy(inputTransfer=1))  # not built: refused, never silently wrong
-    assert st.code == 6 and "transfer" in st.stage
+    st = cache.render(req, p.copy(apertureMode=4))  # not built: refused, never silently wrong
+    assert st.code == 6 and "custom-aperture" in st.stage
     st = cache.render(req, p)
     assert st.ok
