@@ -59,7 +59,12 @@ enum { LD_SPECTRAL_MONO = 0, LD_SPECTRAL_TRISTIMULUS = 1, LD_SPECTRAL_5 = 2, LD_
 enum { LD_STYLE_NATURAL = 0, LD_STYLE_CYANMAGENTA = 1, LD_STYLE_WARMCOOL = 2 };
 enum { LD_LOOK_PHYSICAL = 0, LD_LOOK_SPLIT = 1 };
 enum { LD_ENERGY_PRESERVE = 0, LD_ENERGY_AUGMENT = 1 };
-enum { LD_DEBUG_FINAL = 0 };  /* other LensDiffDebugView values: UNSUPPORTED */
+/* LensDiffDebugView (LensDiffTypes.h:66-81), same order */
+enum {
+    LD_DEBUG_FINAL = 0, LD_DEBUG_SELECTION, LD_DEBUG_PUPIL, LD_DEBUG_PSF, LD_DEBUG_OTF, LD_DEBUG_CORE,
+    LD_DEBUG_STRUCTURE, LD_DEBUG_EFFECT, LD_DEBUG_PHASE, LD_DEBUG_PHASE_EDGE, LD_DEBUG_FIELD_PSF,
+    LD_DEBUG_CHROMATIC_SPLIT, LD_DEBUG_CREATIVE_FRINGE, LD_DEBUG_SCATTER
+};
 enum { LD_TRANSFER_LINEAR = 0, LD_TRANSFER_DAVINCI_INTERMEDIATE = 1 };
 enum { LD_PHASE_OFF = 0, LD_PHASE_ENABLED = 1 };
 

@@ -433,9 +433,13 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
         for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
             const float3 e = mapped_effect<C>(a, smem, sx);  // Mono map: max(0, value)
             float4 acc = erow[sx];
-            acc.x += e.x * amount;
-            acc.y += e.y * amount;
-            acc.z += e.z * amount;
+            if (a.scatter_replace) {
+                acc = make_float4(e.x, e.y, e.z, 0.0f);
+            } else {
+                acc.x += e.x * amount;
+                acc.y += e.y * amount;
+                acc.z += e.z * amount;
+            }
             erow[sx] = acc;
         }
         return;
@@ -541,6 +545,29 @@ __device__ __forceinline__ float3 lerp3(float3 a, float3 b, float t) {
     return make_float3(a.x + (b.x - a.x) * t, a.y + (b.y - a.y) * t, a.z + (b.z - a.z) * t);
 }
 
+// Selection mask of working pixel (x, y) (buildSelectionMask's value).
+__device__ __forceinline__ float work_mask(const FrameArgs& a, int x, int y) {
+    const float4 p = __ldg(a.work + static_cast<int64_t>(y) * a.Ww + x);
+    float sig;
+    return selection_mask(a.sel, p.x, p.y, p.z, &sig);
+}
+
+// What a working pixel contributes to an output pixel: the effect (after
+// the fringe when FRINGE), the fringe preview |fringed - plain|
+// (applyCreativeFringe's preview, LensDiffCpuReference.cpp:1527-1530), or the
+// selection mask in .x.
+template <int MODE, bool FRINGE>
+__device__ __forceinline__ float3 tap_value(const FrameArgs& a, int x, int y) {
+    if constexpr (MODE == kOutFringePreview) {
+        const float3 f = effect_px<true>(a, x, y), e = effect_px<false>(a, x, y);
+        return make_float3(fabsf(f.x - e.x), fabsf(f.y - e.y), fabsf(f.z - e.z));
+    } else if constexpr (MODE == kOutSelection) {
+        return make_float3(work_mask(a, x, y), 0.0f, 0.0f);
+    } else {
+        return effect_px<FRINGE>(a, x, y);
+    }
+}
+
 // Output rows of the render window from the stored effect: scaled, with
 // Preserve energy, by (luma sum of the redistributed source) / (luma sum of
 // the effect) as LensDiffCpuReference.cpp:2172-2178 does (scaleImage with the
@@ -550,7 +577,12 @@ __device__ __forceinline__ float3 lerp3(float3 a, float3 b, float t) {
 // redistributed working source are sampled at the source pixel's position in
 // the working frame (sampleRgbaBilinearImage :373-395: zero outside it), as
 // resampleRgbaImage (:414-434) does for the whole image.
-template <bool FRINGE, bool RESAMPLE>
+// MODE kOutComposite writes the composite (encoded to the source's
+// transfer); the debug views (renderDebugView, :1789-1824) write, unencoded
+// with alpha 1: kOutEffect the (scaled) effect, kOutFringePreview the fringe
+// preview, kOutSelection the selection mask over its maximum
+// (makeDebugFromScalar, :1370-1389; *a.mask_max from selection_max_kernel).
+template <int MODE, bool FRINGE, bool RESAMPLE>
 __global__ void __launch_bounds__(256) composite_kernel(FrameArgs a) {
     const int yo = a.out_y1 + blockIdx.x;
     const int sy = yo - a.src_y1;
@@ -560,6 +592,11 @@ __global__ void __launch_bounds__(256) composite_kernel(FrameArgs a) {
         const float in_e = static_cast<float>(a.sums[0]);
         const float eff_e = static_cast<float>(a.sums[1]);
         if (eff_e > 1e-6f) scale = in_e / eff_e;
+    }
+    float inv_max = 0.0f;
+    if constexpr (MODE == kOutSelection) {
+        const float mx = __uint_as_float(*a.mask_max);
+        inv_max = mx > 0.0f ? 1.0f / mx : 0.0f;
     }
     const bool aligned_s = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(a.src_pitch)) & 15) == 0;
     const bool aligned_d = ((reinterpret_cast<uintptr_t>(a.dst) | static_cast<uintptr_t>(a.dst_pitch)) & 15) == 0;
@@ -574,33 +611,85 @@ __global__ void __launch_bounds__(256) composite_kernel(FrameArgs a) {
         const int sx = x - a.src_x1;
         if (have && sx >= 0 && sx < a.W) {
             const float4 p = decode_px(a.transfer, load_px(srow, sx, aligned_s));
+            float3 rd = make_float3(0.0f, 0.0f, 0.0f), e = rd;
             if constexpr (!RESAMPLE) {
-                const float3 e = effect_px<FRINGE>(a, sx, sy);
-                out = composite_px(a, p, make_float3(e.x * scale, e.y * scale, e.z * scale));
+                if constexpr (MODE == kOutSelection) {
+                    float sig;
+                    e.x = selection_mask(a.sel, p.x, p.y, p.z, &sig);
+                } else {
+                    e = tap_value<MODE, FRINGE>(a, sx, sy);
+                }
+                if constexpr (MODE == kOutComposite) rd = redistributed(a, p);
             } else {
                 const float fx = __fsub_rn(__fmul_rn(__fadd_rn(static_cast<float>(sx), 0.5f), ksx), 0.5f);
-                float3 rd = make_float3(0.0f, 0.0f, 0.0f), e = rd;
                 if (!(fx < 0.0f || fy < 0.0f || fx > static_cast<float>(a.Ww - 1) ||
                       fy > static_cast<float>(a.Hw - 1))) {
                     const int x0 = static_cast<int>(floorf(fx)), y0 = static_cast<int>(floorf(fy));
                     const int x1 = min(x0 + 1, a.Ww - 1), y1 = min(y0 + 1, a.Hw - 1);
                     const float tx = __fsub_rn(fx, static_cast<float>(x0));
                     const float ty = __fsub_rn(fy, static_cast<float>(y0));
-                    const float4* wk = a.work;
-                    const float3 r00 = redistributed(a, __ldg(wk + static_cast<int64_t>(y0) * a.Ww + x0));
-                    const float3 r10 = redistributed(a, __ldg(wk + static_cast<int64_t>(y0) * a.Ww + x1));
-                    const float3 r01 = redistributed(a, __ldg(wk + static_cast<int64_t>(y1) * a.Ww + x0));
-                    const float3 r11 = redistributed(a, __ldg(wk + static_cast<int64_t>(y1) * a.Ww + x1));
-                    rd = lerp3(lerp3(r00, r10, tx), lerp3(r01, r11, tx), ty);
-                    const float3 e00 = effect_px<FRINGE>(a, x0, y0), e10 = effect_px<FRINGE>(a, x1, y0);
-                    const float3 e01 = effect_px<FRINGE>(a, x0, y1), e11 = effect_px<FRINGE>(a, x1, y1);
+                    if constexpr (MODE == kOutComposite) {
+                        const float4* wk = a.work;
+                        const float3 r00 = redistributed(a, __ldg(wk + static_cast<int64_t>(y0) * a.Ww + x0));
+                        const float3 r10 = redistributed(a, __ldg(wk + static_cast<int64_t>(y0) * a.Ww + x1));
+                        const float3 r01 = redistributed(a, __ldg(wk + static_cast<int64_t>(y1) * a.Ww + x0));
+                        const float3 r11 = redistributed(a, __ldg(wk + static_cast<int64_t>(y1) * a.Ww + x1));
+                        rd = lerp3(lerp3(r00, r10, tx), lerp3(r01, r11, tx), ty);
+                    }
+                    const float3 e00 = tap_value<MODE, FRINGE>(a, x0, y0), e10 = tap_value<MODE, FRINGE>(a, x1, y0);
+                    const float3 e01 = tap_value<MODE, FRINGE>(a, x0, y1), e11 = tap_value<MODE, FRINGE>(a, x1, y1);
                     e = lerp3(lerp3(e00, e10, tx), lerp3(e01, e11, tx), ty);
                 }
+            }
+            if constexpr (MODE == kOutComposite) {
                 out = composite_rd(a, p, rd, make_float3(e.x * scale, e.y * scale, e.z * scale));
+            } else if constexpr (MODE == kOutSelection) {
+                const float d = saturate(e.x * inv_max);
+                out = make_float4(d, d, d, 1.0f);
+            } else {
+                out = make_float4(e.x * scale, e.y * scale, e.z * scale, 1.0f);
             }
         }
-        store_px(drow, x - a.dst_x1, aligned_d, encode_px(a.transfer, out));
+        store_px(drow, x - a.dst_x1, aligned_d, MODE == kOutComposite ? encode_px(a.transfer, out) : out);
     }
+}
+
+// Maximum of the selection mask over the whole source frame (resampled from
+// the working frame when RESAMPLE, resampleScalarImage :397-412) into
+// *a.mask_max as float bits; one source row per CTA.
+template <bool RESAMPLE>
+__global__ void __launch_bounds__(256) selection_max_kernel(FrameArgs a) {
+    const int sy = blockIdx.x;
+    const bool aligned_s = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(a.src_pitch)) & 15) == 0;
+    const unsigned char* srow = a.src + static_cast<int64_t>(sy) * a.src_pitch;
+    const float ksx = RESAMPLE ? __fdiv_rn(static_cast<float>(a.Ww), static_cast<float>(max(1, a.W))) : 1.0f;
+    const float ksy = RESAMPLE ? __fdiv_rn(static_cast<float>(a.Hw), static_cast<float>(max(1, a.H))) : 1.0f;
+    const float fy = __fsub_rn(__fmul_rn(__fadd_rn(static_cast<float>(sy), 0.5f), ksy), 0.5f);
+    float m = 0.0f;
+    for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
+        float v = 0.0f;
+        if constexpr (!RESAMPLE) {
+            const float4 p = decode_px(a.transfer, load_px(srow, sx, aligned_s));
+            float sig;
+            v = selection_mask(a.sel, p.x, p.y, p.z, &sig);
+        } else {
+            const float fx = __fsub_rn(__fmul_rn(__fadd_rn(static_cast<float>(sx), 0.5f), ksx), 0.5f);
+            if (!(fx < 0.0f || fy < 0.0f || fx > static_cast<float>(a.Ww - 1) || fy > static_cast<float>(a.Hw - 1))) {
+                const int x0 = static_cast<int>(floorf(fx)), y0 = static_cast<int>(floorf(fy));
+                const int x1 = min(x0 + 1, a.Ww - 1), y1 = min(y0 + 1, a.Hw - 1);
+                const float tx = __fsub_rn(fx, static_cast<float>(x0));
+                const float ty = __fsub_rn(fy, static_cast<float>(y0));
+                const float v00 = work_mask(a, x0, y0), v10 = work_mask(a, x1, y0);
+                const float v01 = work_mask(a, x0, y1), v11 = work_mask(a, x1, y1);
+                const float vx0 = v00 + (v10 - v00) * tx, vx1 = v01 + (v11 - v01) * tx;
+                v = vx0 + (vx1 - vx0) * ty;
+            }
+        }
+        m = fmaxf(m, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(a.mask_max, __float_as_uint(m));
 }
 
 // Working source of the resolution-aware path: pixel (x, y) of the a.Ww x
@@ -931,16 +1020,40 @@ void launch_frame_inverse_rows(const FrameArgs& a, int rows, cudaStream_t s) {
 
 void launch_effect_sums(const FrameArgs& a, cudaStream_t s) { effect_sums_kernel<<<a.H, 256, 0, s>>>(a); }
 
+template <int MODE>
+void composite_launch(const FrameArgs& a, bool fringe, bool rs, int rows, cudaStream_t s) {
+    if (rs) {
+        if (fringe) composite_kernel<MODE, true, true><<<rows, 256, 0, s>>>(a);
+        else composite_kernel<MODE, false, true><<<rows, 256, 0, s>>>(a);
+    } else {
+        if (fringe) composite_kernel<MODE, true, false><<<rows, 256, 0, s>>>(a);
+        else composite_kernel<MODE, false, false><<<rows, 256, 0, s>>>(a);
+    }
+}
+
 void launch_composite(const FrameArgs& a, cudaStream_t s) {
     const int rows = a.out_y2 - a.out_y1;
     if (rows <= 0) return;
-    const bool fringe = a.fringe_px > 0.0f;
-    if (a.work) {
-        if (fringe) composite_kernel<true, true><<<rows, 256, 0, s>>>(a);
-        else composite_kernel<false, true><<<rows, 256, 0, s>>>(a);
-    } else {
-        if (fringe) composite_kernel<true, false><<<rows, 256, 0, s>>>(a);
-        else composite_kernel<false, false><<<rows, 256, 0, s>>>(a);
+    const bool fringe = a.fringe_px > 0.0f, rs = a.work != nullptr;
+    switch (a.debug) {
+        case kOutEffect:
+            composite_launch<kOutEffect>(a, fringe, rs, rows, s);
+            break;
+        case kOutFringePreview:
+            if (rs) composite_kernel<kOutFringePreview, true, true><<<rows, 256, 0, s>>>(a);
+            else composite_kernel<kOutFringePreview, true, false><<<rows, 256, 0, s>>>(a);
+            break;
+        case kOutSelection:
+            if (rs) {
+                selection_max_kernel<true><<<a.H, 256, 0, s>>>(a);
+                composite_kernel<kOutSelection, false, true><<<rows, 256, 0, s>>>(a);
+            } else {
+                selection_max_kernel<false><<<a.H, 256, 0, s>>>(a);
+                composite_kernel<kOutSelection, false, false><<<rows, 256, 0, s>>>(a);
+            }
+            break;
+        default:
+            composite_launch<kOutComposite>(a, fringe, rs, rows, s);
     }
 }
 

@@ -526,8 +526,18 @@ void working_size(const PostEffects& e, int W, int H, int* Ww, int* Hw) {
 }
 constexpr int kMaxWorkingSide = 32768;
 
+// Debug views rendered from the frame's own images (renderDebugView,
+// LensDiffCpuReference.cpp:1789-1824), as opposed to the lens's static views.
+bool frame_debug_view(int v) {
+    return v == LD_DEBUG_FINAL || v == LD_DEBUG_SELECTION || v == LD_DEBUG_CORE || v == LD_DEBUG_STRUCTURE ||
+           v == LD_DEBUG_EFFECT || v == LD_DEBUG_CREATIVE_FRINGE || v == LD_DEBUG_SCATTER;
+}
+
 void validate_params(const ld_params& p) {
-    if (p.debug_view != LD_DEBUG_FINAL) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-debug-view"};
+    if (p.debug_view < LD_DEBUG_FINAL || p.debug_view > LD_DEBUG_SCATTER) throw Fail{LD_ERR_ARG, "invalid-debug-view"};
+    if (!frame_debug_view(p.debug_view)) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-debug-view"};
+    if (p.debug_view != LD_DEBUG_FINAL && p.fft_form == LD_FFT_CUFFT)
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-debug-view-with-cufft-form"};
     if (p.look_mode != LD_LOOK_PHYSICAL && p.look_mode != LD_LOOK_SPLIT) throw Fail{LD_ERR_ARG, "invalid-look-mode"};
     if (p.look_mode == LD_LOOK_SPLIT && p.fft_form == LD_FFT_CUFFT)
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-split-look-with-cufft-form"};
@@ -972,12 +982,18 @@ void gaussian_matrix(const float* wl, int n, const float* center, float sigma, f
     }
 }
 
+// Core and structure kernel sets are needed by the Split look and by the Core
+// and Structure debug views (LensDiffCpuReference.cpp:2123-2157).
+bool split_kernels(const ld_params& p) {
+    return p.look_mode == LD_LOOK_SPLIT || p.debug_view == LD_DEBUG_CORE || p.debug_view == LD_DEBUG_STRUCTURE;
+}
+
 Combination make_combination(const ld_params& p, const std::vector<float>& wl) {
     Combination cb;
     const int B = static_cast<int>(wl.size());
     if (is_mono(p)) {  // convolveRgba, CpuReference.cpp:1195-1217
         cb.mono = 1;
-        cb.parts = p.look_mode == LD_LOOK_SPLIT ? 2 : 1;
+        cb.parts = split_kernels(p) ? 2 : 1;
         cb.n_drv = 3;
         cb.n_ker = 1;
         cb.n_out = 3;
@@ -1020,7 +1036,7 @@ Combination make_combination(const ld_params& p, const std::vector<float>& wl) {
     cb.n_ker = cb.luma_lock ? 4 : 3;
     cb.n_out = cb.n_ker;
     cb.n_drv = 1;
-    cb.parts = p.look_mode == LD_LOOK_SPLIT ? 2 : 1;
+    cb.parts = split_kernels(p) ? 2 : 1;
     return cb;
 }
 
@@ -1656,8 +1672,11 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         fa.h16 = chosen_h16(p) ? 1 : 0;
         fa.err = ctx->err;
         const bool split = cb.parts == 2;
+        const int dv = p.debug_view;
+        const bool dv_parts = dv == LD_DEBUG_CORE || dv == LD_DEBUG_STRUCTURE;
         fa.effect_mode = (zones || split) ? kEffectAccumulate
-                                          : ((fa.preserve || post.any()) ? kEffectStore : kEffectComposite);
+                                          : ((fa.preserve || post.any() || dv != LD_DEBUG_FINAL) ? kEffectStore
+                                                                                                  : kEffectComposite);
         fa.acc_gain = 1.0f;
         fa.acc_shoulder = 0.0f;
         fa.Ww = Ww;
@@ -1706,7 +1725,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         double* sums = nullptr;
         if (fa.effect_mode != kEffectComposite) {
             effect = static_cast<float4*>(
-                ensure(ctx, ctx->effect, static_cast<size_t>(Ww) * Hw * sizeof(float4) + 2 * sizeof(double)));
+                ensure(ctx, ctx->effect, static_cast<size_t>(Ww) * Hw * sizeof(float4) + 4 * sizeof(double)));
             sums = reinterpret_cast<double*>(effect + static_cast<size_t>(Ww) * Hw);
         }
         for (FrameArgs* f : {&fa, &fw}) {
@@ -1734,8 +1753,38 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             fs.effect_mode = kEffectScatter;
             fs.drv_effect = 1;
             fs.scatter = post.scatter_amount;
+            fs.scatter_replace = dv == LD_DEBUG_SCATTER ? 1 : 0;  // the view shows the convolution alone
         }
-        const FrameArgs fin = fa;  // the composite: source frame, stored effect
+        // the scatter pass runs for the final frame and the views of the final effect
+        const bool run_scatter = post.scatter && (dv == LD_DEBUG_FINAL || dv == LD_DEBUG_EFFECT ||
+                                                  dv == LD_DEBUG_CREATIVE_FRINGE || dv == LD_DEBUG_SCATTER);
+        if (!run_scatter) std::memset(&fs, 0, sizeof(fs));
+        // the composite: source frame, stored effect (or a debug view of it)
+        FrameArgs fin = fa;
+        switch (dv) {
+            case LD_DEBUG_SELECTION:
+                fin.debug = kOutSelection;
+                fin.mask_max = reinterpret_cast<unsigned int*>(sums + 2);
+                break;
+            case LD_DEBUG_EFFECT:
+                fin.debug = kOutEffect;
+                break;
+            case LD_DEBUG_CORE:
+            case LD_DEBUG_STRUCTURE:  // unscaled, unfringed (coreEffect, structureEffect)
+                fin.debug = kOutEffect;
+                fin.preserve = 0;
+                fin.fringe_px = 0.0f;
+                break;
+            case LD_DEBUG_SCATTER:  // scatterPreview: zero when scatter is off
+                fin.debug = run_scatter ? kOutEffect : kOutFringePreview;
+                fin.fringe_px = 0.0f;
+                break;
+            case LD_DEBUG_CREATIVE_FRINGE:  // creativeFringePreview: zero when the fringe is off
+                fin.debug = kOutFringePreview;
+                break;
+            default:
+                break;
+        }
         auto clear_effect = [&]() {
             if (fa.effect_mode == kEffectComposite) return;
             check_cuda(cudaMemsetAsync(fa.sums, 0, 2 * sizeof(double), s), "effect-memset");
@@ -1774,16 +1823,30 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         gkey = append_bytes(gkey, &zn, sizeof(zn));
         // Split look: core then structure, each with its gain and shoulder
         // (LensDiffCpuReference.cpp:2123-2146); Physical: the full kernels
-        const float gains[2] = {split ? static_cast<float>(std::max(0.0, p.core_gain)) : 1.0f,
-                                static_cast<float>(std::max(0.0, p.structure_gain))};
-        const float shoulders[2] = {split ? static_cast<float>(p.core_shoulder) : 0.0f,
-                                    static_cast<float>(p.structure_shoulder)};
+        // Core / Structure views: that set alone, shouldered in the Split look,
+        // without its gain (:2123-2157)
+        const bool look_split = p.look_mode == LD_LOOK_SPLIT;
+        const float gains[2] = {look_split && !dv_parts ? static_cast<float>(std::max(0.0, p.core_gain)) : 1.0f,
+                                look_split && !dv_parts ? static_cast<float>(std::max(0.0, p.structure_gain)) : 1.0f};
+        const float shoulders[2] = {look_split ? static_cast<float>(p.core_shoulder) : 0.0f,
+                                    look_split ? static_cast<float>(p.structure_shoulder) : 0.0f};
+        const int part_lo = dv == LD_DEBUG_STRUCTURE ? 1 : 0;
+        const int part_hi = dv == LD_DEBUG_CORE ? 1 : cb.parts;
         gkey = append_bytes(gkey, gains, sizeof(gains));
         gkey = append_bytes(gkey, shoulders, sizeof(shoulders));
         gkey = append_bytes(gkey, &cb.parts, sizeof(cb.parts));
         gkey = append_bytes(gkey, &fw, sizeof(fw));
         gkey = append_bytes(gkey, &fs, sizeof(fs));
+        gkey = append_bytes(gkey, &fin, sizeof(fin));
+        gkey = append_bytes(gkey, &part_lo, sizeof(part_lo));
+        gkey = append_bytes(gkey, &part_hi, sizeof(part_hi));
         auto chain = [&, fa = fw]() mutable {  // the loops below edit this copy
+            if (dv == LD_DEBUG_SELECTION) {  // the mask alone: no convolution
+                check_cuda(cudaMemsetAsync(fin.mask_max, 0, sizeof(unsigned int), s), "mask-memset");
+                if (post.resample) staged(ctx, LD_STAGE_WORKING_SOURCE, s, [&] { launch_resample_source(fin, s); });
+                staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fin, s); });
+                return;
+            }
             clear_effect();
             if (post.resample) staged(ctx, LD_STAGE_WORKING_SOURCE, s, [&] { launch_resample_source(fin, s); });
             staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
@@ -1806,7 +1869,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
                         r1 = std::min(Hw, static_cast<int>(std::ceil((fa.zone_y + 1) * step)) + 2);
                     }
                     fa.row0 = r0;
-                    for (int part = 0; part < cb.parts; ++part) {
+                    for (int part = part_lo; part < part_hi; ++part) {
                         fa.spectra = ks_part(base, part, cb.n_ker, g, fa.h16);
                         fa.kscale = ks_scale(base, part, cb.parts, cb.n_ker, g, fa.h16);
                         fa.acc_gain = gains[part];
@@ -1817,7 +1880,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
                 }
                 if (fa.preserve) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_effect_sums(fa, s); });
             }
-            if (post.scatter) {
+            if (run_scatter) {
                 staged(ctx, LD_STAGE_SCATTER, s, [&] { launch_frame_rows(fs, s); });
                 staged(ctx, LD_STAGE_SCATTER, s, [&] { launch_frame_cols(fs, s); });
                 staged(ctx, LD_STAGE_SCATTER, s, [&] { launch_frame_inverse(fs, s); });

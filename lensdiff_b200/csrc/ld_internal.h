@@ -161,6 +161,8 @@ constexpr int kTransferLinear = 0;
 constexpr int kTransferDavinci = 1;
 
 enum { kEffectComposite = 0, kEffectStore = 1, kEffectAccumulate = 2, kEffectScatter = 3 };
+// FrameArgs::debug: what composite_kernel writes (the composite, or a debug view)
+enum { kOutComposite = 0, kOutEffect = 1, kOutFringePreview = 2, kOutSelection = 3 };
 
 struct FrameArgs {
     GridGeom g;
@@ -227,6 +229,13 @@ struct FrameArgs {
     // source / output encoding (LD_TRANSFER_*): source pixels are decoded to
     // linear as they are read, output pixels encoded as they are written
     int transfer;
+    // composite_kernel output (kOut*); kOutSelection reads the mask maximum
+    // (float bits, zeroed by the host) from mask_max
+    int debug;
+    unsigned int* mask_max;
+    // kEffectScatter: store max(0, value) in place of the effect (the scatter
+    // debug view) instead of adding scatter * max(0, value)
+    int scatter_replace;
 };
 void launch_frame_rows(const FrameArgs& a, cudaStream_t s);
 void launch_frame_cols(const FrameArgs& a, cudaStream_t s);

@@ -506,3 +506,52 @@ def test_davinci_transfer_matches_reference(cache, kw):
     assert rel_err(lin, rlin, rlin.max()) < OUT_TOL
     if form != LensDiffFftForm.OwnChosen:
         assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
+
+
+# ------------------------------------------------------ frame debug views ---
+# renderDebugView (LensDiffCpuReference.cpp:1789-1824): the selection mask over
+# its maximum, the core / structure / final effects, the scatter and creative
+# fringe previews, resampled to the source frame when resolution-aware;
+# unencoded, alpha 1.
+_DV = {"selection": 1, "core": 5, "structure": 6, "effect": 7, "fringe": 12, "scatter": 13}
+
+
+@pytest.mark.parametrize("view,kw", [
+    ("selection", {}),
+    ("selection", {"resolutionAware": True, "frameShortSidePx": 1080, "maxKernelRadiusPx": 1.25,
+                   "diffractionScalePx": 0.2}),
+    ("effect", {"energyMode": LensDiffEnergyMode.Preserve, "scatterAmount": 0.5, "scatterRadius": 8.0,
+                "creativeFringe": 1.5}),
+    ("core", {}),
+    ("structure", {}),
+    ("core", {"lookMode": 1, "coreShoulder": 2.0, "coreGain": 0.7, "spectralMode": LensDiffSpectralMode.Spectral5}),
+    ("structure", {"lookMode": 1, "structureShoulder": 0.5, "structureGain": 1.3,
+                   "spectralMode": LensDiffSpectralMode.Mono}),
+    ("scatter", {"scatterAmount": 0.5, "scatterRadius": 8.0, "energyMode": LensDiffEnergyMode.Preserve}),
+    ("scatter", {}),
+    ("fringe", {"creativeFringe": 2.0, "scatterAmount": 0.3, "scatterRadius": 6.0}),
+    ("fringe", {}),
+    ("fringe", {"creativeFringe": 0.1, "resolutionAware": True, "frameShortSidePx": 1440,
+                "maxKernelRadiusPx": 1.25, "diffractionScalePx": 0.2}),
+])
+def test_frame_debug_views_match_reference(cache, view, kw):
+    _reference_available()
+    p = _lens(debugView=_DV[view], **kw)
+    src = S.make_frame(224, 144, 20, 1.0, 80.0, seed=95)
+    out = _render(cache, with_matrices(p), src)
+    ref = R.render(p, src)
+    scale = max(float(ref[..., :3].max()), 1e-30)
+    assert rel_err(out, ref, scale) < OUT_TOL
+    assert np.all(out[..., 3] == 1.0)
+
+
+def test_frame_debug_view_with_field_zones_and_window(cache):
+    _reference_available()
+    p = _field_lens(debugView=_DV["core"])
+    src = S.make_frame(200, 120, 16, 1.0, 60.0, seed=96)
+    window = (30, 10, 150, 90)
+    out = _render(cache, with_matrices(p), src, render_window=window)
+    ref = R.render(p, src, render_window=window)
+    x1, y1, x2, y2 = window
+    assert np.all(out[:y1] == -7.0)
+    assert rel_err(out[y1:y2, x1:x2], ref[y1:y2, x1:x2], ref[y1:y2, x1:x2, :3].max()) < OUT_TOL
