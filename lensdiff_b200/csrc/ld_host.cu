@@ -92,6 +92,7 @@ struct ld_ctx {
     DevBuf work, scatter_canvas, scatter_ks;
     // chosen form's DFT-as-GEMM operand images and per-wavelength tiles
     DevBuf dft;
+    DevBuf debug;  // static debug views: maxima, square images, OTF scratch
     std::string scatter_key;
     // comparator form (cuFFT): plans and its own work buffers
     CufftPlanCache cufft;
@@ -535,9 +536,8 @@ bool frame_debug_view(int v) {
 
 void validate_params(const ld_params& p) {
     if (p.debug_view < LD_DEBUG_FINAL || p.debug_view > LD_DEBUG_SCATTER) throw Fail{LD_ERR_ARG, "invalid-debug-view"};
-    if (!frame_debug_view(p.debug_view)) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-debug-view"};
-    if (p.debug_view != LD_DEBUG_FINAL && p.fft_form == LD_FFT_CUFFT)
-        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-debug-view-with-cufft-form"};
+    if (p.debug_view != LD_DEBUG_FINAL && frame_debug_view(p.debug_view) && p.fft_form == LD_FFT_CUFFT)
+        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-frame-debug-view-with-cufft-form"};
     if (p.look_mode != LD_LOOK_PHYSICAL && p.look_mode != LD_LOOK_SPLIT) throw Fail{LD_ERR_ARG, "invalid-look-mode"};
     if (p.look_mode == LD_LOOK_SPLIT && p.fft_form == LD_FFT_CUFFT)
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-split-look-with-cufft-form"};
@@ -1372,7 +1372,7 @@ void ld_destroy(ld_ctx* c) {
     DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,    &c->frameB,
                       &c->calib,  &c->calib_psf, &c->err_word,  &c->pupil_pre,  &c->effect,    &c->cf_grid,
                       &c->cf_planes, &c->cf_sd,  &c->cf_prod,   &c->work,       &c->scatter_canvas,
-                      &c->scatter_ks, &c->dft};
+                      &c->scatter_ks, &c->dft,  &c->debug};
     c->cufft.release();
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
@@ -1583,6 +1583,60 @@ size_t ld_estimate_device_bytes(const ld_params* params, int32_t width, int32_t 
     }
 }
 
+namespace {
+// The lens's static debug views (BuildLensDiffStaticDebugRgba,
+// LensDiffCpuReference.cpp:1909-1970) into the render window of `o` (its
+// source bounds give the frame the square is centred in).  The field-edge
+// views take the last field zone, (1, 1), when field phase is on
+// (cache.fieldZones.back()), else the lens itself.
+void render_static_view(ld_ctx* c, const ld_params& p, const FrameArgs& o, cudaStream_t s, bool* bank_rebuilt) {
+    const int dv = p.debug_view;
+    const bool zones = has_field_phase(p);
+    const bool edge = (dv == LD_DEBUG_PHASE_EDGE || dv == LD_DEBUG_FIELD_PSF) && zones;
+    const ld_params q = edge ? zone_params(p, 1.0f, 1.0f) : p;
+    if (dv == LD_DEBUG_PUPIL || dv == LD_DEBUG_PHASE || dv == LD_DEBUG_PHASE_EDGE) {
+        const int n = pupil_size(q);
+        const size_t nn = static_cast<size_t>(n) * n;
+        char* buf = static_cast<char*>(ensure(c, c->debug, 256 + 2 * align256(nn * sizeof(float))));
+        unsigned int* mx = reinterpret_cast<unsigned int*>(buf);
+        float* amp = reinterpret_cast<float*>(buf + 256);
+        float* phase = reinterpret_cast<float*>(buf + 256 + align256(nn * sizeof(float)));
+        check_cuda(cudaMemsetAsync(mx, 0, 256, s), "debug-memset");
+        launch_pupil_image(pupil_params(q, false), phase_for_wavelength(q, 550.0f), amp, phase, mx, mx + 1, s);
+        if (dv == LD_DEBUG_PUPIL) launch_square_view(o, amp, nullptr, n, mx, false, 7, true, s);
+        else launch_phase_view(o, amp, phase, n, mx + 1, s);
+        check_launch("debug-view");
+        return;
+    }
+    BankEntry& b = ensure_bank(c, q, s, bank_rebuilt);
+    const size_t kk = static_cast<size_t>(b.K) * b.K;
+    char* buf = static_cast<char*>(
+        ensure(c, c->debug, 256 + 3 * align256(kk * sizeof(float)) + align256(kk * sizeof(double2))));
+    unsigned int* mx = reinterpret_cast<unsigned int*>(buf);
+    float* img[3];
+    for (int i = 0; i < 3; ++i) img[i] = reinterpret_cast<float*>(buf + 256 + i * align256(kk * sizeof(float)));
+    double2* tmp = reinterpret_cast<double2*>(buf + 256 + 3 * align256(kk * sizeof(float)));
+    check_cuda(cudaMemsetAsync(mx, 0, 256, s), "debug-memset");
+    const PsfScalars* sc = b.args.scalars;
+    if (dv == LD_DEBUG_CHROMATIC_SPLIT) {  // red: last bin, green: middle, blue: first
+        const int bins[3] = {b.B - 1, b.B / 2, 0};
+        for (int ch = 0; ch < 3; ++ch) {
+            launch_kernel_image(b.args, bins[ch], img[ch], mx + ch, s);
+            launch_square_view(o, img[ch], sc + bins[ch], 0, mx + ch, true, 1 << ch, ch == 0, s);
+        }
+    } else {  // Psf, FieldPsf: bin 0; Otf: its transfer function
+        launch_kernel_image(b.args, 0, img[0], mx, s);
+        if (dv == LD_DEBUG_OTF) {
+            launch_otf_image(img[0], sc, b.K, tmp, img[1], mx + 1, s);
+            launch_square_view(o, img[1], sc, 0, mx + 1, true, 7, true, s);
+        } else {
+            launch_square_view(o, img[0], sc, 0, mx, true, 7, true, s);
+        }
+    }
+    check_launch("debug-view");
+}
+}  // namespace
+
 int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params, ld_status* st) {
     if (st) std::memset(st, 0, sizeof(*st));
     if (!ctx || !rq || !params) {
@@ -1611,6 +1665,28 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         fill_sizes(st, p);
         ctx->launches = 0;
         bool bank_rebuilt = false, spectra_rebuilt = false;
+        if (!frame_debug_view(p.debug_view)) {
+            FrameArgs o;
+            std::memset(&o, 0, sizeof(o));
+            o.W = W;
+            o.H = H;
+            o.dst = static_cast<unsigned char*>(rq->dst.data);
+            o.dst_pitch = rq->dst.row_bytes;
+            o.src_x1 = rq->src.bounds.x1;
+            o.src_y1 = rq->src.bounds.y1;
+            o.dst_x1 = rq->dst.bounds.x1;
+            o.dst_y1 = rq->dst.bounds.y1;
+            o.out_x1 = std::max(rq->render_window.x1, rq->dst.bounds.x1);
+            o.out_y1 = std::max(rq->render_window.y1, rq->dst.bounds.y1);
+            o.out_x2 = std::max(o.out_x1, std::min(rq->render_window.x2, rq->dst.bounds.x2));
+            o.out_y2 = std::max(o.out_y1, std::min(rq->render_window.y2, rq->dst.bounds.y2));
+            render_static_view(ctx, p, o, static_cast<cudaStream_t>(rq->cuda_stream), &bank_rebuilt);
+            if (st) {
+                st->bank_rebuilt = bank_rebuilt;
+                st->kernel_launches = ctx->launches;
+            }
+            return;
+        }
         const bool zones = has_field_phase(p);
         const int zn = p.field_grid > 0 ? p.field_grid : 3;
         const std::vector<float> wl = wavelengths_of(p);

@@ -311,6 +311,24 @@ void launch_pupil_field(const PsfBankArgs& a, const DftPlan& d, cudaStream_t s);
 void launch_dft_gemm(const DftGemmArgs& g, int B, int tiles_n, cudaStream_t s);
 void configure_dft_kernels();
 
+// ---- static debug views (ld_debug.cu) ----------------------------------------------
+// Kernel b of the bank after its crop, taper and normalisation (side
+// 2 radius + 1, row-major at out); its maximum (float bits) into *maxv.
+void launch_kernel_image(const PsfBankArgs& a, int b, float* out, unsigned int* maxv, cudaStream_t s);
+// Pupil amplitude and phase in waves (N_p^2 each) and their maxima.
+void launch_pupil_image(const PupilParams& pp, const PhaseCoeffs& c, float* amp, float* phase,
+                        unsigned int* amp_max, unsigned int* phase_max, cudaStream_t s);
+// OTF magnitude (fftshifted) of a kernel image whose side is 2 sc->radius + 1
+// (<= max_side); tmp holds max_side^2 complex doubles.
+void launch_otf_image(const float* img, const PsfScalars* sc, int max_side, double2* tmp, float* out,
+                      unsigned int* maxv, cudaStream_t s);
+// A square image (side 2 sc->radius + 1, or `fixed` when sc is null) drawn
+// into the centred square of the output frame: see ld_debug.cu.
+void launch_square_view(const FrameArgs& a, const float* img, const PsfScalars* sc, int fixed,
+                        const unsigned int* maxv, bool log_view, int channels, bool first, cudaStream_t s);
+void launch_phase_view(const FrameArgs& a, const float* amp, const float* phase, int n,
+                       const unsigned int* phase_max, cudaStream_t s);
+
 // ---- comparator form: the same chain with cuFFT transforms (ld_cufft.cu) -----------
 struct CufftError {
     int code;

@@ -555,3 +555,40 @@ def test_frame_debug_view_with_field_zones_and_window(cache):
     x1, y1, x2, y2 = window
     assert np.all(out[:y1] == -7.0)
     assert rel_err(out[y1:y2, x1:x2], ref[y1:y2, x1:x2], ref[y1:y2, x1:x2, :3].max()) < OUT_TOL
+
+
+# ----------------------------------------------------- static debug views ---
+# BuildLensDiffStaticDebugRgba (LensDiffCpuReference.cpp:1909-1970): the
+# pupil, PSF, OTF, phase, field-edge phase and PSF, and chromatic split drawn
+# into the centred square of the frame (values in [0, 1]).
+@pytest.mark.parametrize("view,kw", [
+    ("pupil", {}), ("psf", {}), ("otf", {}), ("phase", {}), ("split", {}),
+    ("phase_edge", {}), ("field_psf", {}),
+    ("phase_edge", {"field": True}), ("field_psf", {"field": True}),
+    ("psf", {"spectralMode": LensDiffSpectralMode.Mono, "apertureMode": LensDiffApertureMode(3), "bladeCount": 6}),
+    ("split", {"spectralMode": LensDiffSpectralMode.Spectral9, "chromaticSpread": 0.3}),
+    ("phase", {"pupilDecenterX": 0.1, "centralObstruction": 0.25, "vaneCount": 3, "vaneThickness": 0.05}),
+])
+def test_static_debug_views_match_reference(cache, view, kw):
+    _reference_available()
+    ids = {"pupil": 2, "psf": 3, "otf": 4, "phase": 8, "phase_edge": 9, "field_psf": 10, "split": 11}
+    kw = dict(kw)
+    field = kw.pop("field", False)
+    p = (_field_lens if field else _lens)(debugView=ids[view], **kw)
+    src = S.make_frame(224, 144, 20, 1.0, 80.0, seed=97)
+    out = _render(cache, with_matrices(p), src)
+    ref = R.render(p, src)
+    assert rel_err(out, ref, 1.0) < OUT_TOL
+    assert float(ref[..., :3].max()) > 0.5  # the view draws something
+
+
+def test_static_debug_view_window_and_origins(cache):
+    _reference_available()
+    p = _lens(debugView=4)
+    src = S.make_frame(200, 120, 16, 1.0, 60.0, seed=98)
+    window = (30, 10, 150, 90)
+    out = _render(cache, with_matrices(p), src, render_window=window)
+    ref = R.render(p, src, render_window=window)
+    x1, y1, x2, y2 = window
+    assert np.all(out[:y1] == -7.0) and np.all(out[:, :x1] == -7.0)
+    assert rel_err(out[y1:y2, x1:x2], ref[y1:y2, x1:x2], 1.0) < OUT_TOL

@@ -231,8 +231,8 @@ def test_error_behaviour_mirrors_reference(cache):
     assert not run_lensdiff_cuda(req, p, cache, err)
     assert err == ["missing-source-or-destination-cuda-buffer"]
     req = image_request(src, dst, stream, frame_short_side=144)
-    st = cache.render(req, p.copy(debugView=3))
-    assert st.code == 6 and "debug" in st.stage
+    st = cache.render(req, p.copy(debugView=99))
+    assert not st.ok and st.stage == "invalid-debug-view"
     st = cache.render(req, p.copy(apertureMode=4))  # not built: refused, never silently wrong
     assert st.code == 6 and "custom-aperture" in st.stage
     st = cache.render(req, p)
