@@ -225,7 +225,7 @@ class Clocks:
 # 31-wavelength workload, from the one-pass ncu capture summarised in
 # profiles/frame_*_hd16.md (writes still resident in L2 at kernel end are not
 # counted by DRAM counters).
-MEASURED_TRAFFIC_UHD31 = {"frame_rows": 156.4e6, "frame_cols": 322.9e6, "frame_inverse": 352.6e6}
+MEASURED_TRAFFIC_UHD31 = {"frame_rows": 156.4e6, "frame_cols": 322.9e6, "frame_inverse": 352.6e6, "shape_stats": 209.3e6}
 
 
 # ---------------------------------------------------------------------------
@@ -244,7 +244,7 @@ def algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, out_pixels, B=0, K=0):
     Kp = K + (K & 1)
     return {
         # bank passes over the B canvases of K x K floats (read + write)
-        "resample": canvas, "shape_stats": 2 * canvas, "crop_sum": 2 * canvas,
+        "resample": canvas, "shape_stats": 2 * canvas, "crop_sum": canvas,
         "combine": canvas + 4 * n_ker * K * K,
         "kspec_rows": 4 * n_ker * K * K + 8 * n_ker * Kp * bins,
         "kspec_cols": 8 * n_ker * Kp * bins + 8 * n_ker * Py * bins,

@@ -93,6 +93,11 @@ struct ld_ctx {
     // chosen form's DFT-as-GEMM operand images and per-wavelength tiles
     DevBuf dft;
     DevBuf debug;  // static debug views: maxima, square images, OTF scratch
+    // pinned staging ring for the small per-bank uploads (upload_async)
+    void* stage_host = nullptr;
+    std::vector<cudaEvent_t> stage_ev;
+    std::vector<bool> stage_pending;
+    int stage_next = 0;
     std::string scatter_key;
     // comparator form (cuFFT): plans and its own work buffers
     CufftPlanCache cufft;
@@ -170,6 +175,47 @@ void* ensure(ld_ctx* c, DevBuf& b, size_t bytes) {
 // ---------------------------------------------------------------------------
 // stage timing
 // ---------------------------------------------------------------------------
+constexpr size_t kStageSlot = 16384;
+constexpr int kStageSlots = 8;
+
+// One CTA copies `words` 4-byte words from mapped pinned host memory.
+__global__ void __launch_bounds__(256) host_words_kernel(uint32_t* dst, const uint32_t* src, int words) {
+    for (int i = threadIdx.x; i < words; i += 256) dst[i] = src[i];
+}
+
+// Host -> device copy of a small host array that leaves the host free: the
+// bytes go through a slot of a mapped pinned staging ring and a one-CTA
+// kernel on the stream reads them, so a frame that rebuilds its bank neither
+// waits for the frames before it (as a copy from pageable memory does) nor
+// queues behind a caller's large frame copies on the copy engine.  A slot is
+// refilled only after the kernel that last read it has finished.  Arrays
+// above one slot take a plain copy.
+void upload_async(ld_ctx* c, void* dst, const void* src, size_t bytes, cudaStream_t s, const char* what) {
+    if (bytes > kStageSlot || (bytes & 3) != 0 || (reinterpret_cast<uintptr_t>(dst) & 3) != 0) {
+        check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), what);
+        return;
+    }
+    if (!c->stage_host) {
+        check_cuda(cudaHostAlloc(&c->stage_host, kStageSlot * kStageSlots, cudaHostAllocMapped), what);
+        c->stage_ev.assign(kStageSlots, nullptr);
+        for (auto& e : c->stage_ev) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), what);
+        c->stage_pending.assign(kStageSlots, false);
+    }
+    const int i = c->stage_next;
+    c->stage_next = (i + 1) % kStageSlots;
+    if (c->stage_pending[static_cast<size_t>(i)])
+        check_cuda(cudaEventSynchronize(c->stage_ev[static_cast<size_t>(i)]), what);
+    char* h = static_cast<char*>(c->stage_host) + static_cast<size_t>(i) * kStageSlot;
+    std::memcpy(h, src, bytes);
+    void* hd = nullptr;
+    check_cuda(cudaHostGetDevicePointer(&hd, h, 0), what);
+    host_words_kernel<<<1, 256, 0, s>>>(static_cast<uint32_t*>(dst), static_cast<const uint32_t*>(hd),
+                                         static_cast<int>(bytes / 4));
+    check_launch(what);
+    check_cuda(cudaEventRecord(c->stage_ev[static_cast<size_t>(i)], s), what);
+    c->stage_pending[static_cast<size_t>(i)] = true;
+}
+
 cudaEvent_t next_event(ld_ctx* c) {
     if (c->events_used == c->event_pool.size()) {
         cudaEvent_t e;
@@ -816,8 +862,7 @@ void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthI
     d.dy_lo = take(d.dy_slab * d.kc_cols);
     DftLambda* dl = reinterpret_cast<DftLambda*>(take(B * sizeof(DftLambda)));
     d.lam = dl;
-    check_cuda(cudaMemcpyAsync(dl, lam.data(), lam.size() * sizeof(DftLambda), cudaMemcpyHostToDevice, s),
-               "dft-upload");
+    upload_async(c, dl, lam.data(), lam.size() * sizeof(DftLambda), s, "dft-upload");
     DftBasisArgs bx{d.dx_hi, d.dx_lo, d.dx_slab, d.basis_rows, d.kc_rows, d.col_n, a.off + d.col_lo, d.x0, a.S / 2, a.S};
     DftBasisArgs by{d.dy_hi, d.dy_lo, d.dy_slab, d.basis_rows, d.kc_cols, a.row_n, a.off + a.row_lo, d.x0, a.S / 2, a.S};
     DftGemmArgs gr{};
@@ -918,8 +963,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     a.wl = dwl;
     a.count_round = ring_counts(c, R);
     a.want_energy = 0;
-    check_cuda(cudaMemcpyAsync(dwl, infos.data(), infos.size() * sizeof(WavelengthInfo), cudaMemcpyHostToDevice, s),
-               "bank-upload");
+    upload_async(c, dwl, infos.data(), infos.size() * sizeof(WavelengthInfo), s, "bank-upload");
     check_cuda(cudaMemsetAsync(a.ring_round, 0, ringn * sizeof(double), s), "bank-memset");
     check_cuda(cudaMemsetAsync(a.ring_ceil, 0, ringn * sizeof(double), s), "bank-memset");
     check_cuda(cudaMemsetAsync(a.ring_peak, 0, ringn * sizeof(unsigned int), s), "bank-memset");
@@ -1376,6 +1420,8 @@ void ld_destroy(ld_ctx* c) {
     c->cufft.release();
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->stage_ev) cudaEventDestroy(e);
+    if (c->stage_host) cudaFreeHost(c->stage_host);
     DevBuf* bb[] = {&c->bank.canvas, &c->bank.ring_round, &c->bank.ring_ceil, &c->bank.ring_peak, &c->bank.ring_mean,
                     &c->bank.scalars, &c->bank.wl,        &c->spectra.spectra};
     for (DevBuf* b : bb) free_buf(c, *b);
