@@ -225,14 +225,20 @@ class Clocks:
 # 31-wavelength workload, from the one-pass ncu capture summarised in
 # profiles/frame_*_hd16.md (writes still resident in L2 at kernel end are not
 # counted by DRAM counters).
-MEASURED_TRAFFIC_UHD31 = {"frame_rows": 156.4e6, "frame_cols": 322.9e6, "frame_inverse": 352.6e6, "shape_stats": 209.3e6}
+# DRAM read + write per launch, one-pass ncu captures of the UHD 31-wavelength
+# cold workload (profiles/), by transform form
+MEASURED_TRAFFIC_UHD31 = {
+    "own": {"frame_rows": 156.4e6, "frame_cols": 322.9e6, "frame_inverse": 352.6e6},
+    "chosen": {"shape_stats": 209.3e6},
+}
 
 
 # ---------------------------------------------------------------------------
 # algorithmic bytes per launch of the frame-chain kernels
 # ---------------------------------------------------------------------------
-def algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, out_pixels, B=0, K=0):
-    """Bytes each frame kernel must move with this algorithm (complex = 8 B):
+def algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, out_pixels, B=0, K=0, h16=False):
+    """Bytes each frame kernel must move with this algorithm (complex = 8 B,
+    4 B for the kernel spectra and column outputs of the chosen form, h16):
     frame_rows reads the RGBA source and writes the H x (Px/2+1) row spectra;
     frame_cols reads them and the kernel spectra (Py x (Px/2+1) each) and writes
     H x (Px/2+1) per output; frame_inverse reads those, re-reads the source for
@@ -240,6 +246,8 @@ def algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, out_pixels, B=0, K=0):
     Px, Py = grid
     bins = Px // 2 + 1
     row_spec = 8 * H * bins
+    cplx = 4 if h16 else 8
+    out_spec = cplx * H * bins
     canvas = 4 * B * K * K
     Kp = K + (K & 1)
     return {
@@ -247,10 +255,10 @@ def algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, out_pixels, B=0, K=0):
         "resample": canvas, "shape_stats": 2 * canvas, "crop_sum": canvas,
         "combine": canvas + 4 * n_ker * K * K,
         "kspec_rows": 4 * n_ker * K * K + 8 * n_ker * Kp * bins,
-        "kspec_cols": 8 * n_ker * Kp * bins + 8 * n_ker * Py * bins,
+        "kspec_cols": 8 * n_ker * Kp * bins + cplx * n_ker * Py * bins,
         "frame_rows": 16 * W * H + n_drv * row_spec,
-        "frame_cols": n_drv * row_spec + n_ker * 8 * Py * bins + n_out * row_spec,
-        "frame_inverse": n_out * row_spec + 16 * W * H + 16 * out_pixels,
+        "frame_cols": n_drv * row_spec + n_ker * cplx * Py * bins + n_out * out_spec,
+        "frame_inverse": n_out * out_spec + 16 * W * H + 16 * out_pixels,
     }
 
 
@@ -505,7 +513,8 @@ def main():
     n_drv = 1 if spectral else 3
     n_ker = 3 if spectral else 1
     n_out = 3
-    alg = algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, W * H, B=st0.wavelength_count,
+    alg = algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, W * H, h16=(args.fft_form == "chosen" and spectral),
+                            B=st0.wavelength_count,
                             K=2 * st0.max_kernel_radius + 1)
     dominant = max(stage, key=lambda k: stage[k][0])
     dom_ms, dom_n = stage[dominant]
@@ -513,7 +522,7 @@ def main():
     if dominant in alg and dom_n:
         per_launch_ms = dom_ms / dom_n
         achieved = alg[dominant] / (per_launch_ms / 1000.0) / 1e9
-        traffic = MEASURED_TRAFFIC_UHD31.get(dominant) if args.workload == "uhd31" else None
+        traffic = MEASURED_TRAFFIC_UHD31.get(args.fft_form, {}).get(dominant) if args.workload == "uhd31" else None
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                     "algorithmic_bytes_per_launch": alg[dominant], "launch_ms": per_launch_ms}

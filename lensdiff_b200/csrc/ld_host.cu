@@ -93,6 +93,9 @@ struct ld_ctx {
     // chosen form's DFT-as-GEMM operand images and per-wavelength tiles
     DevBuf dft;
     DevBuf debug;  // static debug views: maxima, square images, OTF scratch
+    // side stream for the source's row transforms while a bank is built
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     // pinned staging ring for the small per-bank uploads (upload_async)
     void* stage_host = nullptr;
     std::vector<cudaEvent_t> stage_ev;
@@ -214,6 +217,16 @@ void upload_async(ld_ctx* c, void* dst, const void* src, size_t bytes, cudaStrea
     check_launch(what);
     check_cuda(cudaEventRecord(c->stage_ev[static_cast<size_t>(i)], s), what);
     c->stage_pending[static_cast<size_t>(i)] = true;
+}
+
+// The context's side stream and its fork / join events, created on first use.
+cudaStream_t side_stream(ld_ctx* c) {
+    if (!c->side) {
+        check_cuda(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking), "side-stream");
+        check_cuda(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming), "side-stream");
+        check_cuda(cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming), "side-stream");
+    }
+    return c->side;
 }
 
 cudaEvent_t next_event(ld_ctx* c) {
@@ -1224,6 +1237,27 @@ constexpr size_t kSpectraCache = 4;
 
 // Kernel spectra for (lens p, geometry g) from the context's LRU cache; the
 // bank is built (or reused) only on a miss.
+// Whether every kernel-spectra set a frame needs is cached already.
+bool spectra_cached(ld_ctx* c, const ld_params& p, bool zones, int zn, const Combination& cb, const GridGeom& g) {
+    const std::vector<float> wl = wavelengths_of(p);
+    if (!zones) {
+        const std::string key = spectra_key_for(bank_key(p, wl), cb, g);
+        for (const auto& e : c->spectra_lru)
+            if (e.valid && e.key == key) return true;
+        return false;
+    }
+    if (static_cast<int>(c->zone_spectra.size()) != zn * zn) return false;
+    for (int zy = 0; zy < zn; ++zy) {
+        for (int zx = 0; zx < zn; ++zx) {
+            const float nx = (2.0f * static_cast<float>(zx)) / static_cast<float>(zn - 1) - 1.0f;
+            const float ny = (2.0f * static_cast<float>(zy)) / static_cast<float>(zn - 1) - 1.0f;
+            const SpectraEntry& e = c->zone_spectra[static_cast<size_t>(zy) * zn + zx];
+            if (!(e.valid && e.key == spectra_key_for(bank_key(zone_params(p, nx, ny), wl), cb, g))) return false;
+        }
+    }
+    return true;
+}
+
 SpectraEntry& cached_spectra(ld_ctx* c, const ld_params& p, const Combination& cb, const GridGeom& g, cudaStream_t s,
                              bool* bank_rebuilt, bool* spectra_rebuilt) {
     const std::string key = spectra_key_for(bank_key(p, wavelengths_of(p)), cb, g);
@@ -1421,6 +1455,9 @@ void ld_destroy(ld_ctx* c) {
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : c->stage_ev) cudaEventDestroy(e);
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+    if (c->join_ev) cudaEventDestroy(c->join_ev);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stage_host) cudaFreeHost(c->stage_host);
     DevBuf* bb[] = {&c->bank.canvas, &c->bank.ring_round, &c->bank.ring_ceil, &c->bank.ring_peak, &c->bank.ring_mean,
                     &c->bank.scalars, &c->bank.wl,        &c->spectra.spectra};
@@ -1747,13 +1784,11 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         const int c_rows = std::max(std::max(cb.n_drv == 1 ? 4 : 3, cb.n_out), cb.n_ker);
         const int c_cols = std::max(std::max(cb.n_out, cb.n_ker), cb.n_drv);
         const GridGeom g = make_geometry(ctx, Ww, Hw, 2 * max_kernel_radius(p) + 1, c_rows, c_cols, &rw, &rh);
-        std::vector<const SpectraEntry*> spectra;
-        if (zones) {
-            spectra = ensure_zone_spectra(ctx, p, zn, cb, g, s, &bank_rebuilt, &spectra_rebuilt);
-        } else {
-            spectra.push_back(&cached_spectra(ctx, p, cb, g, s, &bank_rebuilt, &spectra_rebuilt));
-        }
-        const SpectraEntry& sp = *spectra.front();
+        // Spectra already cached (a warm frame)?  If not, the bank and kernel
+        // spectra are built on s while the source's row transforms run on a
+        // side stream: they do not depend on the lens.
+        const bool overlap_rows = p.fft_form != LD_FFT_CUFFT && p.debug_view != LD_DEBUG_SELECTION &&
+                                  !spectra_cached(ctx, p, zones, zn, cb, g);
 
         FrameArgs fa;
         std::memset(&fa, 0, sizeof(fa));  // padding too: the bytes key the frame graphs
@@ -1855,12 +1890,30 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             f->A = abuf;
             f->Bout = reinterpret_cast<float2*>(bbuf);
             f->bscale = reinterpret_cast<float*>(bbuf + b_bytes_of(cb.n_out, g, fa.h16));
-            f->spectra = ks_part(sp.spectra.p, 0, cb.n_ker, g, fa.h16);
-            f->kscale = ks_scale(sp.spectra.p, 0, cb.parts, cb.n_ker, g, fa.h16);
             f->effect = effect;
             f->sums = sums;
             f->work = fa.work;
         }
+        if (overlap_rows) {  // fork: working source and row transforms on the side stream
+            cudaStream_t ws = side_stream(ctx);
+            check_cuda(cudaEventRecord(ctx->fork_ev, s), "fork");
+            check_cuda(cudaStreamWaitEvent(ws, ctx->fork_ev, 0), "fork");
+            if (post.resample) staged(ctx, LD_STAGE_WORKING_SOURCE, ws, [&] { launch_resample_source(fa, ws); });
+            staged(ctx, LD_STAGE_FRAME_ROWS, ws, [&] { launch_frame_rows(fw, ws); });
+            check_cuda(cudaEventRecord(ctx->join_ev, ws), "fork");
+        }
+        std::vector<const SpectraEntry*> spectra;
+        if (zones) {
+            spectra = ensure_zone_spectra(ctx, p, zn, cb, g, s, &bank_rebuilt, &spectra_rebuilt);
+        } else {
+            spectra.push_back(&cached_spectra(ctx, p, cb, g, s, &bank_rebuilt, &spectra_rebuilt));
+        }
+        const SpectraEntry& sp = *spectra.front();
+        for (FrameArgs* f : {&fa, &fw}) {
+            f->spectra = ks_part(sp.spectra.p, 0, cb.n_ker, g, fa.h16);
+            f->kscale = ks_scale(sp.spectra.p, 0, cb.parts, cb.n_ker, g, fa.h16);
+        }
+        if (overlap_rows) check_cuda(cudaStreamWaitEvent(s, ctx->join_ev, 0), "join");
         if (post.scatter) {
             fs = fw;
             fs.g = gs;
@@ -1962,6 +2015,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         gkey = append_bytes(gkey, &fin, sizeof(fin));
         gkey = append_bytes(gkey, &part_lo, sizeof(part_lo));
         gkey = append_bytes(gkey, &part_hi, sizeof(part_hi));
+        gkey = append_bytes(gkey, &overlap_rows, sizeof(overlap_rows));
         auto chain = [&, fa = fw]() mutable {  // the loops below edit this copy
             if (dv == LD_DEBUG_SELECTION) {  // the mask alone: no convolution
                 check_cuda(cudaMemsetAsync(fin.mask_max, 0, sizeof(unsigned int), s), "mask-memset");
@@ -1970,8 +2024,10 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
                 return;
             }
             clear_effect();
-            if (post.resample) staged(ctx, LD_STAGE_WORKING_SOURCE, s, [&] { launch_resample_source(fin, s); });
-            staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
+            if (!overlap_rows) {  // else already on the side stream
+                if (post.resample) staged(ctx, LD_STAGE_WORKING_SOURCE, s, [&] { launch_resample_source(fin, s); });
+                staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
+            }
             if (fa.effect_mode != kEffectAccumulate) {
                 staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
                 staged(ctx, LD_STAGE_FRAME_INVERSE, s, [&] { launch_frame_inverse(fa, s); });
