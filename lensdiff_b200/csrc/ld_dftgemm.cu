@@ -32,6 +32,8 @@
 // 16-byte units XOR-ed with r % 8), so any 8-aligned run of rows is one
 // contiguous block that a single bulk copy (cp.async.bulk) brings into shared
 // memory.  No tensor map is needed.
+#include <algorithm>
+
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -210,27 +212,25 @@ __global__ void __launch_bounds__(256) pupil_field_kernel(PsfBankArgs a, DftPlan
 }
 
 // ---- the GEMM --------------------------------------------------------------------------
-// One CTA per 128 x 128-complex output tile of wavelength blockIdx.y, four
-// warps.  Thread 0 streams the K-chunks' hi and lo tiles of A and B into a
+// Persistent work queue over a table of transform problems (each one pass of
+// one wavelength of one lens, with its own operands, sizes and window): one
+// CTA per SM, four warps, tensor memory allocated once.  A CTA takes the next
+// 128 x 128-complex output tile from a global counter until none are left.
+// Per tile, thread 0 streams the K-chunks' hi and lo tiles of A and B into a
 // two-stage ring with bulk copies; thread 32 issues the tensor-core MMAs
 // (three per 16-wide K step: hi*hi, hi*lo, lo*hi) and commits each stage
 // back to the producer; then all four warps read the accumulators out of
 // TMEM (warp w owns lanes 32w..32w+31) for the epilogue:
 //   kDftRows: Y as the column pass's A images (row n, K pair m);
-//   kDftCols: |Z|^2 into the PSF window.
-// Every wait is bounded; a wait that gives up records the error and the CTA
-// releases its tensor memory and returns.
-__global__ void __launch_bounds__(128, 1) dft_gemm_kernel(DftGemmArgs g) {
+//   kDftCols: |Z|^2 into the PSF window (and its sum when asked).
+// The ring position and the barrier phases carry over from tile to tile.
+// Every wait is bounded; a wait that gives up records the error, and the CTA
+// stops taking tiles, releases its tensor memory and returns.
+__global__ void __launch_bounds__(128, 1) dft_gemm_kernel(DftBatchArgs g) {
     extern __shared__ __align__(1024) unsigned char smraw[];
     __shared__ uint64_t bars[2 * kStages + 1];
     __shared__ uint32_t tmem_slot;
-    const int b = blockIdx.y;
-    const DftLambda lam = g.lam[b];
-    const int mt = g.mt_fixed > 0 ? g.mt_fixed : lam.nt;
-    const int nt = lam.nt;
-    const int tm = static_cast<int>(blockIdx.x) % g.mt_max;
-    const int tn = static_cast<int>(blockIdx.x) / g.mt_max;
-    if (tm >= mt || tn >= nt) return;  // uniform: before any allocation
+    __shared__ int tile_sh, fail_sh;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* base =
         smraw + ((1024u - (smem_addr(smraw) & 1023u)) & 1023u);  // 1024-byte aligned stages
@@ -249,111 +249,140 @@ __global__ void __launch_bounds__(128, 1) dft_gemm_kernel(DftGemmArgs g) {
         mbar_init(done, 1);
         mbar_init_fence();
     }
+    if (threadIdx.x == 0) fail_sh = 0;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-
-    const unsigned char* a_hi = g.a_hi + static_cast<size_t>(b) * g.a_lambda + static_cast<size_t>(tm) * kImgA;
-    const unsigned char* a_lo = g.a_lo + static_cast<size_t>(b) * g.a_lambda + static_cast<size_t>(tm) * kImgA;
-    const size_t b_row0 = static_cast<size_t>(2) * (lam.n0 + tn * (kTileN / 2));  // multiple of 8
-    const unsigned char* b_hi = g.b_hi + static_cast<size_t>(b) * g.b_lambda + (b_row0 >> 3) * 1024;
-    const unsigned char* b_lo = g.b_lo + static_cast<size_t>(b) * g.b_lambda + (b_row0 >> 3) * 1024;
-    const int kc = g.kc;
-
-    if (warp == 0) {
-        if (lane == 0) {  // producer
-            for (int c = 0; c < kc; ++c) {
-                const int s = c % kStages, use = c / kStages;
-                if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, g.err)) break;
-                unsigned char* st = base + s * kStageBytes;
-                bulk_load_checked(st, a_hi + static_cast<size_t>(c) * g.a_slab, kImgA, &full[s], smraw, g.err);
-                bulk_load_checked(st + kImgA, a_lo + static_cast<size_t>(c) * g.a_slab, kImgA, &full[s], smraw,
-                                  g.err);
-                bulk_load_checked(st + 2 * kImgA, b_hi + static_cast<size_t>(c) * g.b_slab, kImgB, &full[s], smraw,
-                                  g.err);
-                bulk_load_checked(st + 2 * kImgA + kImgB, b_lo + static_cast<size_t>(c) * g.b_slab, kImgB, &full[s],
-                                  smraw, g.err);
-            }
+    uint32_t gc = 0;     // K-chunks this CTA has streamed: ring stage and barrier phases
+    uint32_t ntile = 0;  // tiles this CTA has finished: phase of `done`
+    for (;;) {
+        if (threadIdx.x == 0) tile_sh = atomicAdd(g.counter, 1);
+        __syncthreads();
+        const int t = tile_sh;
+        if (t >= g.tiles || fail_sh) break;  // uniform
+        // the problem of tile t: the last p with tile_start[p] <= t
+        int lo = 0, hi = g.problems - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&g.tile_start[mid]) <= t) lo = mid;
+            else hi = mid - 1;
         }
-        __syncwarp();
-    } else if (warp == 1) {
-        if (lane == 0) {  // MMA issuer
-            bool ok = true;
-            for (int c = 0; c < kc && ok; ++c) {
-                const int s = c % kStages, use = c / kStages;
-                if (!mbar_wait(&full[s], use & 1, g.err)) {
-                    ok = false;
-                    break;
+        const DftProblem pr = g.probs[lo];
+        const int local = t - __ldg(&g.tile_start[lo]);
+        const int tm = local % pr.mt, tn = local / pr.mt;
+        const int kc = pr.kc;
+        const unsigned char* a_hi = pr.a_hi + static_cast<size_t>(tm) * kImgA;
+        const unsigned char* a_lo = pr.a_lo + static_cast<size_t>(tm) * kImgA;
+        const size_t b_row0 = static_cast<size_t>(2) * (pr.n0 + tn * (kTileN / 2));  // multiple of 8
+        const unsigned char* b_hi = pr.b_hi + (b_row0 >> 3) * 1024;
+        const unsigned char* b_lo = pr.b_lo + (b_row0 >> 3) * 1024;
+        if (warp == 0) {
+            if (lane == 0) {  // producer
+                for (int c = 0; c < kc; ++c) {
+                    const uint32_t k = gc + static_cast<uint32_t>(c);
+                    const int s = static_cast<int>(k % kStages);
+                    const uint32_t use = k / kStages;
+                    if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, g.err)) {
+                        fail_sh = 1;
+                        break;
+                    }
+                    unsigned char* st = base + s * kStageBytes;
+                    bulk_load_checked(st, a_hi + static_cast<size_t>(c) * pr.a_slab, kImgA, &full[s], smraw, g.err);
+                    bulk_load_checked(st + kImgA, a_lo + static_cast<size_t>(c) * pr.a_slab, kImgA, &full[s], smraw,
+                                      g.err);
+                    bulk_load_checked(st + 2 * kImgA, b_hi + static_cast<size_t>(c) * pr.b_slab, kImgB, &full[s],
+                                      smraw, g.err);
+                    bulk_load_checked(st + 2 * kImgA + kImgB, b_lo + static_cast<size_t>(c) * pr.b_slab, kImgB,
+                                      &full[s], smraw, g.err);
                 }
-                tc_fence_after();
-                const uint32_t st = smem_addr(base + s * kStageBytes);
-                const uint64_t ah = smem_desc(st), al = smem_desc(st + kImgA);
-                const uint64_t bh = smem_desc(st + 2 * kImgA), bl = smem_desc(st + 2 * kImgA + kImgB);
-#pragma unroll
-                for (int kk = 0; kk < kChunkK / 16; ++kk) {
-                    const uint64_t dk = static_cast<uint64_t>(kk * 2);  // 32 bytes, in 16-byte units
-                    mma_bf16(tmem, ah + dk, bh + dk, kIdesc, (c | kk) != 0 ? 1u : 0u);
-                    mma_bf16(tmem, ah + dk, bl + dk, kIdesc, 1u);
-                    mma_bf16(tmem, al + dk, bh + dk, kIdesc, 1u);
-                }
-                mma_commit(&empty[s]);
             }
-            if (ok) mma_commit(done);
-        }
-        __syncwarp();
-    }
-
-    // ---- epilogue: all four warps ----
-    const bool ready = __all_sync(0xffffffffu, mbar_wait(done, 0, g.err));  // warp-uniform for tcgen05.ld
-    tc_fence_after();
-    float esum = 0.0f;  // kDftCols with g.energy: this thread's window pixels
-    if (ready) {
-        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
-        const int row = tm * kTileM + warp * 32 + lane;  // M index of this thread
-        for (int q = 0; q < static_cast<int>(kTmemCols) / 32; ++q) {
-            uint32_t v[32];
-            tmem_ld32(lane_addr + static_cast<uint32_t>(q * 32), v);
-            const int n_first = tn * (kTileN / 2) + q * 16;  // complex column of v[0], v[1]
-            if (g.mode == kDftRows) {
-                // Y[m = row][n]: the column pass's A image row n, K pair m
-                const size_t lam_off = static_cast<size_t>(b) * g.y_lambda + static_cast<size_t>(row >> 5) * g.y_slab;
+            __syncwarp();
+        } else if (warp == 1) {
+            if (lane == 0) {  // MMA issuer
+                bool ok = true;
+                for (int c = 0; c < kc; ++c) {
+                    const uint32_t k = gc + static_cast<uint32_t>(c);
+                    const int s = static_cast<int>(k % kStages);
+                    if (!mbar_wait(&full[s], (k / kStages) & 1, g.err)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = smem_addr(base + s * kStageBytes);
+                    const uint64_t ah = smem_desc(st), al = smem_desc(st + kImgA);
+                    const uint64_t bh = smem_desc(st + 2 * kImgA), bl = smem_desc(st + 2 * kImgA + kImgB);
 #pragma unroll
-                for (int e = 0; e < 16; ++e) {
-                    const float re = __uint_as_float(v[2 * e]), im = __uint_as_float(v[2 * e + 1]);
-                    uint32_t hi, lo;
-                    split_pair(re, im, &hi, &lo);
-                    const size_t off = lam_off + img_byte(n_first + e, 2 * (row & 31));
-                    *reinterpret_cast<uint32_t*>(g.y_hi + off) = hi;
-                    *reinterpret_cast<uint32_t*>(g.y_lo + off) = lo;
+                    for (int kk = 0; kk < kChunkK / 16; ++kk) {
+                        const uint64_t dk = static_cast<uint64_t>(kk * 2);  // 32 bytes, in 16-byte units
+                        mma_bf16(tmem, ah + dk, bh + dk, kIdesc, (c | kk) != 0 ? 1u : 0u);
+                        mma_bf16(tmem, ah + dk, bl + dk, kIdesc, 1u);
+                        mma_bf16(tmem, al + dk, bh + dk, kIdesc, 1u);
+                    }
+                    mma_commit(&empty[s]);
                 }
-            } else {
-                // Z[n = row][r]: window pixel (wy, wx) = (r, n) - shift
-                const int wx = row - lam.shift;
-                const int wn = g.wl[b].win_n;
-                if (wx >= 0 && wx < wn) {
-                    float* out = g.win + static_cast<size_t>(b) * g.win_stride * g.win_stride + wx;
+                if (ok) mma_commit(done);
+                else fail_sh = 1;
+            }
+            __syncwarp();
+        }
+
+        // ---- epilogue: all four warps ----
+        const bool ready = __all_sync(0xffffffffu, mbar_wait(done, ntile & 1, g.err));  // warp-uniform
+        tc_fence_after();
+        float esum = 0.0f;  // kDftCols: this thread's window pixels
+        if (ready) {
+            const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+            const int row = tm * kTileM + warp * 32 + lane;  // M index of this thread
+            for (int q = 0; q < static_cast<int>(kTmemCols) / 32; ++q) {
+                uint32_t v[32];
+                tmem_ld32(lane_addr + static_cast<uint32_t>(q * 32), v);
+                const int n_first = tn * (kTileN / 2) + q * 16;  // complex column of v[0], v[1]
+                if (g.mode == kDftRows) {
+                    // Y[m = row][n]: the column pass's A image row n, K pair m
+                    const size_t chunk_off = static_cast<size_t>(row >> 5) * pr.y_slab;
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
-                        const int wy = n_first + e - lam.shift;
                         const float re = __uint_as_float(v[2 * e]), im = __uint_as_float(v[2 * e + 1]);
-                        if (wy >= 0 && wy < wn) {
-                            const float I = re * re + im * im;
-                            out[static_cast<size_t>(wy) * g.win_stride] = I;
-                            esum += I;
+                        uint32_t hi2, lo2;
+                        split_pair(re, im, &hi2, &lo2);
+                        const size_t off = chunk_off + img_byte(n_first + e, 2 * (row & 31));
+                        *reinterpret_cast<uint32_t*>(pr.y_hi + off) = hi2;
+                        *reinterpret_cast<uint32_t*>(pr.y_lo + off) = lo2;
+                    }
+                } else {
+                    // Z[n = row][r]: window pixel (wy, wx) = (r, n) - shift
+                    const int wx = row - pr.shift;
+                    if (wx >= 0 && wx < pr.win_n) {
+                        float* out = pr.win + wx;
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const int wy = n_first + e - pr.shift;
+                            const float re = __uint_as_float(v[2 * e]), im = __uint_as_float(v[2 * e + 1]);
+                            if (wy >= 0 && wy < pr.win_n) {
+                                const float I = re * re + im * im;
+                                out[static_cast<size_t>(wy) * pr.win_stride] = I;
+                                esum += I;
+                            }
                         }
                     }
                 }
             }
+        } else if (threadIdx.x == 0) {
+            fail_sh = 1;
         }
-    }
-    if (g.energy) {  // uniform
+        if (pr.energy) {  // uniform
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
-        if (lane == 0 && esum != 0.0f) atomicAdd(&g.energy[b * g.energy_stride], static_cast<double>(esum));
+            for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+            if (lane == 0 && esum != 0.0f) atomicAdd(pr.energy, static_cast<double>(esum));
+        }
+        gc += static_cast<uint32_t>(kc);
+        ++ntile;
+        // every thread's TMEM reads are complete before the next tile's MMAs
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
     }
-    tc_fence_before();
-    __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, kTmemCols);
 }
 
@@ -373,9 +402,12 @@ void launch_pupil_field(const PsfBankArgs& a, const DftPlan& d, cudaStream_t s) 
     pupil_field_kernel<<<dim3(static_cast<unsigned>((total + 255) / 256), a.B), 256, 0, s>>>(a, d);
 }
 
-void launch_dft_gemm(const DftGemmArgs& g, int B, int tiles_n, cudaStream_t s) {
-    if (g.kc <= 0 || g.mt_max <= 0 || tiles_n <= 0 || B <= 0) return;
-    dft_gemm_kernel<<<dim3(static_cast<unsigned>(g.mt_max * tiles_n), B), 128, dft_gemm_smem(), s>>>(g);
+void launch_dft_gemm(const DftBatchArgs& g, cudaStream_t s) {
+    if (g.tiles <= 0 || g.problems <= 0) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    dft_gemm_kernel<<<static_cast<unsigned>(std::min(g.tiles, sms)), 128, dft_gemm_smem(), s>>>(g);
 }
 
 void configure_dft_kernels() {

@@ -179,7 +179,7 @@ void* ensure(ld_ctx* c, DevBuf& b, size_t bytes) {
 // stage timing
 // ---------------------------------------------------------------------------
 constexpr size_t kStageSlot = 16384;
-constexpr int kStageSlots = 8;
+constexpr int kStageSlots = 64;  // 16 cold frames of uploads in flight
 
 // One CTA copies `words` 4-byte words from mapped pinned host memory.
 __global__ void __launch_bounds__(256) host_words_kernel(uint32_t* dst, const uint32_t* src, int words) {
@@ -850,7 +850,8 @@ DftPlan plan_dft(const PsfBankArgs& a, const std::vector<WavelengthInfo>& infos,
 size_t dft_bytes(const DftPlan& d, int B) {
     return 2 * (static_cast<size_t>(B) * (d.pf_lambda + d.yt_lambda) + d.dx_slab * d.kc_rows +
                 d.dy_slab * d.kc_cols) +
-           align256(static_cast<size_t>(B) * sizeof(DftLambda)) + 8 * 1024;
+           2 * static_cast<size_t>(B) * sizeof(DftProblem) + (2 * static_cast<size_t>(B) + 4) * sizeof(int) +
+           16 * 1024;
 }
 
 // Chosen form: the bank's |F|^2 windows by DFT-as-GEMM on the tensor cores
@@ -873,57 +874,68 @@ void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthI
     d.dx_lo = take(d.dx_slab * d.kc_rows);
     d.dy_hi = take(d.dy_slab * d.kc_cols);
     d.dy_lo = take(d.dy_slab * d.kc_cols);
-    DftLambda* dl = reinterpret_cast<DftLambda*>(take(B * sizeof(DftLambda)));
-    d.lam = dl;
-    upload_async(c, dl, lam.data(), lam.size() * sizeof(DftLambda), s, "dft-upload");
+    // problem tables of the two passes (one problem per wavelength), their
+    // tile prefixes and the two work-queue counters
+    std::vector<DftProblem> rows(static_cast<size_t>(B)), cols(static_cast<size_t>(B));
+    std::vector<int> rstart(static_cast<size_t>(B) + 1, 0), cstart(static_cast<size_t>(B) + 1, 0);
+    for (int b = 0; b < B; ++b) {
+        const DftLambda& l = lam[static_cast<size_t>(b)];
+        DftProblem& r = rows[static_cast<size_t>(b)];
+        r.a_hi = d.pf_hi + b * d.pf_lambda;
+        r.a_lo = d.pf_lo + b * d.pf_lambda;
+        r.b_hi = d.dx_hi;
+        r.b_lo = d.dx_lo;
+        r.y_hi = d.yt_hi + b * d.yt_lambda;
+        r.y_lo = d.yt_lo + b * d.yt_lambda;
+        r.a_slab = static_cast<uint32_t>(d.pf_slab);
+        r.b_slab = static_cast<uint32_t>(d.dx_slab);
+        r.y_slab = static_cast<uint32_t>(d.yt_slab);
+        r.kc = d.kc_rows;
+        r.mt = d.mt_rows;
+        r.nt = l.nt;
+        r.n0 = l.n0;
+        r.shift = l.shift;
+        DftProblem& q = cols[static_cast<size_t>(b)];
+        q.a_hi = d.yt_hi + b * d.yt_lambda;
+        q.a_lo = d.yt_lo + b * d.yt_lambda;
+        q.b_hi = d.dy_hi;
+        q.b_lo = d.dy_lo;
+        q.win = a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride;
+        q.energy = a.want_energy ? &a.scalars[b].energy : nullptr;
+        q.a_slab = static_cast<uint32_t>(d.yt_slab);
+        q.b_slab = static_cast<uint32_t>(d.dy_slab);
+        q.kc = d.kc_cols;
+        q.mt = l.nt;
+        q.nt = l.nt;
+        q.n0 = l.n0;
+        q.shift = l.shift;
+        q.win_n = infos[static_cast<size_t>(b)].win_n;
+        q.win_stride = a.win_stride;
+        rstart[static_cast<size_t>(b) + 1] = rstart[static_cast<size_t>(b)] + r.mt * r.nt;
+        cstart[static_cast<size_t>(b) + 1] = cstart[static_cast<size_t>(b)] + q.mt * q.nt;
+    }
+    DftProblem* drows = reinterpret_cast<DftProblem*>(take(rows.size() * sizeof(DftProblem)));
+    DftProblem* dcols = reinterpret_cast<DftProblem*>(take(cols.size() * sizeof(DftProblem)));
+    int* dstart = reinterpret_cast<int*>(take(2 * (static_cast<size_t>(B) + 1) * sizeof(int) + 2 * sizeof(int)));
+    std::vector<int> starts(rstart);
+    starts.insert(starts.end(), cstart.begin(), cstart.end());
+    starts.push_back(0);  // the two counters
+    starts.push_back(0);
+    upload_async(c, drows, rows.data(), rows.size() * sizeof(DftProblem), s, "dft-upload");
+    upload_async(c, dcols, cols.data(), cols.size() * sizeof(DftProblem), s, "dft-upload");
+    upload_async(c, dstart, starts.data(), starts.size() * sizeof(int), s, "dft-upload");
     DftBasisArgs bx{d.dx_hi, d.dx_lo, d.dx_slab, d.basis_rows, d.kc_rows, d.col_n, a.off + d.col_lo, d.x0, a.S / 2, a.S};
     DftBasisArgs by{d.dy_hi, d.dy_lo, d.dy_slab, d.basis_rows, d.kc_cols, a.row_n, a.off + a.row_lo, d.x0, a.S / 2, a.S};
-    DftGemmArgs gr{};
-    gr.a_hi = d.pf_hi;
-    gr.a_lo = d.pf_lo;
-    gr.a_lambda = d.pf_lambda;
-    gr.a_slab = d.pf_slab;
-    gr.b_hi = d.dx_hi;
-    gr.b_lo = d.dx_lo;
-    gr.b_lambda = 0;
-    gr.b_slab = d.dx_slab;
-    gr.kc = d.kc_rows;
-    gr.mt_fixed = d.mt_rows;
-    gr.mt_max = d.mt_rows;
-    gr.mode = kDftRows;
-    gr.lam = d.lam;
-    gr.y_hi = d.yt_hi;
-    gr.y_lo = d.yt_lo;
-    gr.y_lambda = d.yt_lambda;
-    gr.y_slab = d.yt_slab;
-    gr.wl = a.wl;
-    gr.err = c->err;
-    DftGemmArgs gc = gr;
-    gc.a_hi = d.yt_hi;
-    gc.a_lo = d.yt_lo;
-    gc.a_lambda = d.yt_lambda;
-    gc.a_slab = d.yt_slab;
-    gc.b_hi = d.dy_hi;
-    gc.b_lo = d.dy_lo;
-    gc.b_slab = d.dy_slab;
-    gc.kc = d.kc_cols;
-    gc.mt_fixed = 0;
-    gc.mt_max = d.nt_max;
-    gc.mode = kDftCols;
-    gc.y_hi = nullptr;
-    gc.y_lo = nullptr;
-    gc.win = a.win;
-    gc.win_stride = a.win_stride;
-    gc.energy = a.want_energy ? &a.scalars[0].energy : nullptr;
-    gc.energy_stride = static_cast<int>(sizeof(PsfScalars) / sizeof(double));
+    DftBatchArgs gr{drows, dstart, B, rstart.back(), kDftRows, dstart + 2 * (B + 1), c->err};
+    DftBatchArgs gc{dcols, dstart + (B + 1), B, cstart.back(), kDftCols, dstart + 2 * (B + 1) + 1, c->err};
     staged(c, LD_STAGE_PSF_ROWS, s, [&] {
         launch_pupil_field(a, d, s);
         launch_dft_basis(bx, s);
-        launch_dft_gemm(gr, B, d.nt_max, s);
+        launch_dft_gemm(gr, s);
     });
     staged(c, LD_STAGE_PSF_COLS, s, [&] {
         launch_dft_basis(by, s);
-        launch_dft_gemm(gc, B, d.nt_max, s);
+        launch_dft_gemm(gc, s);
     });
 }
 

@@ -279,36 +279,38 @@ struct DftPlan {
     size_t dx_slab, dy_slab;
     unsigned char *yt_hi, *yt_lo;  // row-pass output [B][mt_rows * 4][nt_max * 128 rows]
     size_t yt_lambda, yt_slab;
-    const DftLambda* lam;      // [B]
 };
 struct DftBasisArgs {
     unsigned char *hi, *lo;
     size_t slab;
     int rows, kc, k_valid, koff, x0, half, S;
 };
-struct DftGemmArgs {
+// One pass of one wavelength of one lens for dft_gemm_kernel: its operands
+// (A: 128-row tiles along M; B: the basis, 2 rows per complex output), the
+// K-chunks and tile counts, and where the output goes.
+struct DftProblem {
     const unsigned char *a_hi, *a_lo;
-    size_t a_lambda, a_slab;
     const unsigned char *b_hi, *b_lo;
-    size_t b_lambda, b_slab;
-    int kc;
-    int mt_fixed;              // M tiles (0: the wavelength's nt)
-    int mt_max;                // grid.x = mt_max * N tiles
-    int mode;                  // kDftRows or kDftCols
-    const DftLambda* lam;
-    unsigned char *y_hi, *y_lo;  // kDftRows output images
-    size_t y_lambda, y_slab;
-    float* win;                // kDftCols output windows
-    int win_stride;
-    const WavelengthInfo* wl;
-    double* energy;            // kDftCols: sum of the window added to energy[b * energy_stride] (null: none)
-    int energy_stride;         // in doubles
+    unsigned char *y_hi, *y_lo;  // kDftRows: the column pass's A images of this problem
+    float* win;                  // kDftCols: the window (row-major, win_stride)
+    double* energy;              // kDftCols: sum of the window added here (null: none)
+    uint32_t a_slab, b_slab, y_slab;  // bytes per K-chunk
+    int kc, mt, nt;              // K-chunks; 128-row M tiles; 128-complex N tiles
+    int n0, shift;               // first basis column (multiple of 4); window column 0 = computed `shift`
+    int win_n, win_stride;
+};
+struct DftBatchArgs {
+    const DftProblem* probs;     // [problems]
+    const int* tile_start;       // [problems + 1]: first tile of each problem (mt * nt tiles each)
+    int problems, tiles;
+    int mode;                    // kDftRows or kDftCols
+    int* counter;                // work-queue counter, zero before the launch
     int* err;
 };
 size_t dft_gemm_smem();
 void launch_dft_basis(const DftBasisArgs& a, cudaStream_t s);
 void launch_pupil_field(const PsfBankArgs& a, const DftPlan& d, cudaStream_t s);
-void launch_dft_gemm(const DftGemmArgs& g, int B, int tiles_n, cudaStream_t s);
+void launch_dft_gemm(const DftBatchArgs& g, cudaStream_t s);
 void configure_dft_kernels();
 
 // ---- static debug views (ld_debug.cu) ----------------------------------------------
