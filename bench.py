@@ -1,7 +1,7 @@
 """Benchmark of the LensDiff diffraction path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl own|reference]
-                    [--workload uhd31|hd16|small3] [--bank cold|warm]
+                    [--workload uhd31|hd16|small3|zones8] [--bank cold|warm]
 
 A step renders one frame of the workload through the path: with --bank cold
 (the default, the headline) every frame changes the defocus coefficient by
@@ -39,6 +39,7 @@ WORKLOADS = {
     "uhd31": "workload_uhd31",
     "hd16": "workload_hd",
     "small3": "workload_small",
+    "zones8": "workload_zones8",
 }
 METRIC = "UHD frames/s (31-wavelength PSF bank, FFT convolution, composite)"
 

@@ -71,6 +71,8 @@ struct ld_ctx {
     BankEntry bank;
     SpectraEntry spectra;
     std::vector<SpectraEntry> zone_spectra;  // field zones, zy * n + zx
+    // field zones' pupils, wavelength tables and windows of one batched transform
+    std::vector<DevBuf> zone_pupil, zone_wl, zone_win;
     // kernel spectra of recent (lens, frame size) pairs, least recently used
     // replaced first: a context serving one lens at several frame sizes keeps
     // them all without rebuilding the bank
@@ -627,7 +629,8 @@ size_t align256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
 // pupil pre-pass (amplitude, the λ-independent phase, the defocus term).
 // Only pupil rows whose pixel centres lie within the outer radius of the
 // (decentred) aperture can be non-zero; the row passes skip the others.
-void setup_pupil(ld_ctx* c, PsfBankArgs& a, const ld_params& p, bool circle, cudaStream_t s) {
+void setup_pupil(ld_ctx* c, PsfBankArgs& a, const ld_params& p, bool circle, cudaStream_t s,
+                 DevBuf* target = nullptr) {
     a.pupil = pupil_params(p, circle);
     a.base_phase = circle ? PhaseCoeffs{} : phase_for_wavelength(p, 550.0f);
     a.base_phase.c[4] = 0.0f;  // defocus is carried per wavelength
@@ -646,7 +649,8 @@ void setup_pupil(ld_ctx* c, PsfBankArgs& a, const ld_params& p, bool circle, cud
     }
     a.row_lo = lo;
     a.row_n = hi - lo;
-    a.pupil_pre = static_cast<float4*>(ensure(c, c->pupil_pre, static_cast<size_t>(n) * n * sizeof(float4)));
+    a.pupil_pre = static_cast<float4*>(
+        ensure(c, target ? *target : c->pupil_pre, static_cast<size_t>(n) * n * sizeof(float4)));
     staged(c, LD_STAGE_PUPIL, s, [&] { launch_pupil_pre(a, s); });
 }
 
@@ -856,67 +860,94 @@ size_t dft_bytes(const DftPlan& d, int B) {
 
 // Chosen form: the bank's |F|^2 windows by DFT-as-GEMM on the tensor cores
 // in place of the row and column FFTs (ld_dftgemm.cu).
-void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthInfo>& infos, cudaStream_t s) {
+// The bank windows of several lenses (one PsfBankArgs and wavelength table
+// each) in one launch per pass of the persistent tensor-core GEMM: every
+// (lens, wavelength) pass is one problem of the work queue.  The lenses must
+// share the transform geometry (PSF size, pupil extent, windows), as field
+// zones of one lens do; they keep their own pupil fields and phases.
+void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
+                        const std::vector<const std::vector<WavelengthInfo>*>& infos, cudaStream_t s) {
+    const int Z = static_cast<int>(banks.size());
+    const PsfBankArgs& a0 = *banks.front();
     std::vector<DftLambda> lam;
-    DftPlan d = plan_dft(a, infos, &lam);
-    const int B = a.B;
-    char* p = static_cast<char*>(ensure(c, c->dft, dft_bytes(d, B)));
+    DftPlan d = plan_dft(a0, *infos.front(), &lam);
+    for (int z = 1; z < Z; ++z) {  // one shared plan: same geometry
+        std::vector<DftLambda> lz;
+        const DftPlan dz = plan_dft(*banks[static_cast<size_t>(z)], *infos[static_cast<size_t>(z)], &lz);
+        bool same = dz.col_lo == d.col_lo && dz.col_n == d.col_n && dz.mt_rows == d.mt_rows &&
+                    dz.kc_rows == d.kc_rows && dz.kc_cols == d.kc_cols && dz.x0 == d.x0 &&
+                    dz.basis_rows == d.basis_rows && banks[static_cast<size_t>(z)]->S == a0.S &&
+                    banks[static_cast<size_t>(z)]->B == a0.B && lz.size() == lam.size();
+        for (size_t b = 0; same && b < lam.size(); ++b)
+            same = lz[b].n0 == lam[b].n0 && lz[b].shift == lam[b].shift && lz[b].nt == lam[b].nt;
+        if (!same) {  // separate launches
+            for (int k = 0; k < Z; ++k)
+                dft_gemm_psf_batch(c, {banks[static_cast<size_t>(k)]}, {infos[static_cast<size_t>(k)]}, s);
+            return;
+        }
+    }
+    const int B = a0.B, P = Z * B;
+    char* p = static_cast<char*>(ensure(c, c->dft, dft_bytes(d, P)));
     auto take = [&](size_t bytes) {
         char* q = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~static_cast<uintptr_t>(1023));
         p = q + bytes;
         return reinterpret_cast<unsigned char*>(q);
     };
-    d.pf_hi = take(B * d.pf_lambda);
-    d.pf_lo = take(B * d.pf_lambda);
-    d.yt_hi = take(B * d.yt_lambda);
-    d.yt_lo = take(B * d.yt_lambda);
+    d.pf_hi = take(P * d.pf_lambda);
+    d.pf_lo = take(P * d.pf_lambda);
+    d.yt_hi = take(P * d.yt_lambda);
+    d.yt_lo = take(P * d.yt_lambda);
     d.dx_hi = take(d.dx_slab * d.kc_rows);
     d.dx_lo = take(d.dx_slab * d.kc_rows);
     d.dy_hi = take(d.dy_slab * d.kc_cols);
     d.dy_lo = take(d.dy_slab * d.kc_cols);
-    // problem tables of the two passes (one problem per wavelength), their
-    // tile prefixes and the two work-queue counters
-    std::vector<DftProblem> rows(static_cast<size_t>(B)), cols(static_cast<size_t>(B));
-    std::vector<int> rstart(static_cast<size_t>(B) + 1, 0), cstart(static_cast<size_t>(B) + 1, 0);
-    for (int b = 0; b < B; ++b) {
-        const DftLambda& l = lam[static_cast<size_t>(b)];
-        DftProblem& r = rows[static_cast<size_t>(b)];
-        r.a_hi = d.pf_hi + b * d.pf_lambda;
-        r.a_lo = d.pf_lo + b * d.pf_lambda;
-        r.b_hi = d.dx_hi;
-        r.b_lo = d.dx_lo;
-        r.y_hi = d.yt_hi + b * d.yt_lambda;
-        r.y_lo = d.yt_lo + b * d.yt_lambda;
-        r.a_slab = static_cast<uint32_t>(d.pf_slab);
-        r.b_slab = static_cast<uint32_t>(d.dx_slab);
-        r.y_slab = static_cast<uint32_t>(d.yt_slab);
-        r.kc = d.kc_rows;
-        r.mt = d.mt_rows;
-        r.nt = l.nt;
-        r.n0 = l.n0;
-        r.shift = l.shift;
-        DftProblem& q = cols[static_cast<size_t>(b)];
-        q.a_hi = d.yt_hi + b * d.yt_lambda;
-        q.a_lo = d.yt_lo + b * d.yt_lambda;
-        q.b_hi = d.dy_hi;
-        q.b_lo = d.dy_lo;
-        q.win = a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride;
-        q.energy = a.want_energy ? &a.scalars[b].energy : nullptr;
-        q.a_slab = static_cast<uint32_t>(d.yt_slab);
-        q.b_slab = static_cast<uint32_t>(d.dy_slab);
-        q.kc = d.kc_cols;
-        q.mt = l.nt;
-        q.nt = l.nt;
-        q.n0 = l.n0;
-        q.shift = l.shift;
-        q.win_n = infos[static_cast<size_t>(b)].win_n;
-        q.win_stride = a.win_stride;
-        rstart[static_cast<size_t>(b) + 1] = rstart[static_cast<size_t>(b)] + r.mt * r.nt;
-        cstart[static_cast<size_t>(b) + 1] = cstart[static_cast<size_t>(b)] + q.mt * q.nt;
+    // problem tables of the two passes (one problem per lens and wavelength),
+    // their tile prefixes and the two work-queue counters
+    std::vector<DftProblem> rows(static_cast<size_t>(P)), cols(static_cast<size_t>(P));
+    std::vector<int> rstart(static_cast<size_t>(P) + 1, 0), cstart(static_cast<size_t>(P) + 1, 0);
+    for (int z = 0; z < Z; ++z) {
+        const PsfBankArgs& a = *banks[static_cast<size_t>(z)];
+        for (int b = 0; b < B; ++b) {
+            const size_t i = static_cast<size_t>(z) * B + b;
+            const DftLambda& l = lam[static_cast<size_t>(b)];
+            DftProblem& r = rows[i];
+            r.a_hi = d.pf_hi + i * d.pf_lambda;
+            r.a_lo = d.pf_lo + i * d.pf_lambda;
+            r.b_hi = d.dx_hi;
+            r.b_lo = d.dx_lo;
+            r.y_hi = d.yt_hi + i * d.yt_lambda;
+            r.y_lo = d.yt_lo + i * d.yt_lambda;
+            r.a_slab = static_cast<uint32_t>(d.pf_slab);
+            r.b_slab = static_cast<uint32_t>(d.dx_slab);
+            r.y_slab = static_cast<uint32_t>(d.yt_slab);
+            r.kc = d.kc_rows;
+            r.mt = d.mt_rows;
+            r.nt = l.nt;
+            r.n0 = l.n0;
+            r.shift = l.shift;
+            DftProblem& q = cols[i];
+            q.a_hi = d.yt_hi + i * d.yt_lambda;
+            q.a_lo = d.yt_lo + i * d.yt_lambda;
+            q.b_hi = d.dy_hi;
+            q.b_lo = d.dy_lo;
+            q.win = a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride;
+            q.energy = a.want_energy ? &a.scalars[b].energy : nullptr;
+            q.a_slab = static_cast<uint32_t>(d.yt_slab);
+            q.b_slab = static_cast<uint32_t>(d.dy_slab);
+            q.kc = d.kc_cols;
+            q.mt = l.nt;
+            q.nt = l.nt;
+            q.n0 = l.n0;
+            q.shift = l.shift;
+            q.win_n = (*infos[static_cast<size_t>(z)])[static_cast<size_t>(b)].win_n;
+            q.win_stride = a.win_stride;
+            rstart[i + 1] = rstart[i] + r.mt * r.nt;
+            cstart[i + 1] = cstart[i] + q.mt * q.nt;
+        }
     }
     DftProblem* drows = reinterpret_cast<DftProblem*>(take(rows.size() * sizeof(DftProblem)));
     DftProblem* dcols = reinterpret_cast<DftProblem*>(take(cols.size() * sizeof(DftProblem)));
-    int* dstart = reinterpret_cast<int*>(take(2 * (static_cast<size_t>(B) + 1) * sizeof(int) + 2 * sizeof(int)));
+    int* dstart = reinterpret_cast<int*>(take(2 * (static_cast<size_t>(P) + 1) * sizeof(int) + 2 * sizeof(int)));
     std::vector<int> starts(rstart);
     starts.insert(starts.end(), cstart.begin(), cstart.end());
     starts.push_back(0);  // the two counters
@@ -924,12 +955,19 @@ void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthI
     upload_async(c, drows, rows.data(), rows.size() * sizeof(DftProblem), s, "dft-upload");
     upload_async(c, dcols, cols.data(), cols.size() * sizeof(DftProblem), s, "dft-upload");
     upload_async(c, dstart, starts.data(), starts.size() * sizeof(int), s, "dft-upload");
-    DftBasisArgs bx{d.dx_hi, d.dx_lo, d.dx_slab, d.basis_rows, d.kc_rows, d.col_n, a.off + d.col_lo, d.x0, a.S / 2, a.S};
-    DftBasisArgs by{d.dy_hi, d.dy_lo, d.dy_slab, d.basis_rows, d.kc_cols, a.row_n, a.off + a.row_lo, d.x0, a.S / 2, a.S};
-    DftBatchArgs gr{drows, dstart, B, rstart.back(), kDftRows, dstart + 2 * (B + 1), c->err};
-    DftBatchArgs gc{dcols, dstart + (B + 1), B, cstart.back(), kDftCols, dstart + 2 * (B + 1) + 1, c->err};
+    DftBasisArgs bx{d.dx_hi, d.dx_lo, d.dx_slab, d.basis_rows, d.kc_rows, d.col_n, a0.off + d.col_lo, d.x0, a0.S / 2,
+                    a0.S};
+    DftBasisArgs by{d.dy_hi, d.dy_lo, d.dy_slab, d.basis_rows, d.kc_cols, a0.row_n, a0.off + a0.row_lo, d.x0,
+                    a0.S / 2, a0.S};
+    DftBatchArgs gr{drows, dstart, P, rstart.back(), kDftRows, dstart + 2 * (P + 1), c->err};
+    DftBatchArgs gc{dcols, dstart + (P + 1), P, cstart.back(), kDftCols, dstart + 2 * (P + 1) + 1, c->err};
     staged(c, LD_STAGE_PSF_ROWS, s, [&] {
-        launch_pupil_field(a, d, s);
+        for (int z = 0; z < Z; ++z) {
+            DftPlan dz = d;  // this lens's pupil-field images
+            dz.pf_hi = d.pf_hi + static_cast<size_t>(z) * B * d.pf_lambda;
+            dz.pf_lo = d.pf_lo + static_cast<size_t>(z) * B * d.pf_lambda;
+            launch_pupil_field(*banks[static_cast<size_t>(z)], dz, s);
+        }
         launch_dft_basis(bx, s);
         launch_dft_gemm(gr, s);
     });
@@ -939,7 +977,19 @@ void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthI
     });
 }
 
-BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebuilt) {
+void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthInfo>& infos, cudaStream_t s) {
+    dft_gemm_psf_batch(c, {&a}, {&infos}, s);
+}
+
+// Bank windows computed ahead of the bank (several field zones' windows in
+// one batched transform): the bank build takes them instead of synthesising.
+struct PreWindows {
+    float* win;
+    WavelengthInfo* wl;  // device, the matching wavelength table
+};
+
+BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebuilt,
+                       const PreWindows* pre = nullptr) {
     const std::vector<float> wl = wavelengths_of(p);
     const std::string key = bank_key(p, wl);
     *rebuilt = false;
@@ -959,7 +1009,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
 
     PsfBankArgs& a = b.args;
     a = PsfBankArgs{};
-    setup_pupil(c, a, p, false, s);
+    if (!pre) setup_pupil(c, a, p, false, s);
     a.B = B;
     a.S = S;
     a.half = S / 2;
@@ -972,11 +1022,12 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     // tensor-core DFT for the chosen form, and for S with a prime factor above
     // 5 (the reference's Bluestein sizes) in every own form
     const bool dft = p.fft_form == LD_FFT_OWN_CHOSEN || (p.fft_form == LD_FFT_OWN_FP32 && !smooth(S));
-    if (!dft && p.fft_form != LD_FFT_CUFFT) {
+    if (!pre && !dft && p.fft_form != LD_FFT_CUFFT) {
         a.plan_s = make_plan(c, S, fft_family(S, 1) == kE25);
         a.rows = static_cast<float2*>(ensure(c, c->rows, static_cast<size_t>(B) * a.row_n * win_stride * sizeof(float2)));
     }
-    a.win = static_cast<float*>(ensure(c, c->win, static_cast<size_t>(B) * win_stride * win_stride * sizeof(float)));
+    a.win = pre ? pre->win
+                : static_cast<float*>(ensure(c, c->win, static_cast<size_t>(B) * win_stride * win_stride * sizeof(float)));
     a.canvas = static_cast<float*>(ensure(c, b.canvas, static_cast<size_t>(B) * K * K * sizeof(float)));
     const size_t ringn = static_cast<size_t>(B) * (R + 1);
     a.ring_round = static_cast<double*>(ensure(c, b.ring_round, ringn * sizeof(double)));
@@ -984,16 +1035,19 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     a.ring_peak = static_cast<unsigned int*>(ensure(c, b.ring_peak, ringn * sizeof(unsigned int)));
     a.ring_mean = static_cast<float*>(ensure(c, b.ring_mean, ringn * sizeof(float)));
     a.scalars = static_cast<PsfScalars*>(ensure(c, b.scalars, static_cast<size_t>(B) * sizeof(PsfScalars)));
-    WavelengthInfo* dwl = static_cast<WavelengthInfo*>(ensure(c, b.wl, static_cast<size_t>(B) * sizeof(WavelengthInfo)));
+    WavelengthInfo* dwl =
+        pre ? pre->wl : static_cast<WavelengthInfo*>(ensure(c, b.wl, static_cast<size_t>(B) * sizeof(WavelengthInfo)));
     a.wl = dwl;
     a.count_round = ring_counts(c, R);
     a.want_energy = 0;
-    upload_async(c, dwl, infos.data(), infos.size() * sizeof(WavelengthInfo), s, "bank-upload");
+    if (!pre) upload_async(c, dwl, infos.data(), infos.size() * sizeof(WavelengthInfo), s, "bank-upload");
     check_cuda(cudaMemsetAsync(a.ring_round, 0, ringn * sizeof(double), s), "bank-memset");
     check_cuda(cudaMemsetAsync(a.ring_ceil, 0, ringn * sizeof(double), s), "bank-memset");
     check_cuda(cudaMemsetAsync(a.ring_peak, 0, ringn * sizeof(unsigned int), s), "bank-memset");
     check_cuda(cudaMemsetAsync(a.scalars, 0, static_cast<size_t>(B) * sizeof(PsfScalars), s), "bank-memset");
-    if (p.fft_form == LD_FFT_CUFFT) {
+    if (pre) {
+        // windows already synthesised
+    } else if (p.fft_form == LD_FFT_CUFFT) {
         float2* grid = static_cast<float2*>(
             ensure(c, c->cf_grid, cf_psf_chunk(S, B) * static_cast<size_t>(S) * S * sizeof(float2)));
         staged(c, LD_STAGE_PSF_ROWS, s, [&] { cf_psf_transform(a, grid, c->cufft, s); });
@@ -1307,17 +1361,67 @@ std::vector<const SpectraEntry*> ensure_zone_spectra(ld_ctx* c, const ld_params&
         c->zone_spectra.resize(static_cast<size_t>(n) * n);
     }
     const std::vector<float> wl = wavelengths_of(p);
+    const int nz = n * n;
+    std::vector<ld_params> zps(static_cast<size_t>(nz));
+    std::vector<std::string> keys(static_cast<size_t>(nz));
+    std::vector<int> need;
+    for (int z = 0; z < nz; ++z) {
+        const float nx = (2.0f * static_cast<float>(z % n)) / static_cast<float>(n - 1) - 1.0f;
+        const float ny = (2.0f * static_cast<float>(z / n)) / static_cast<float>(n - 1) - 1.0f;
+        zps[static_cast<size_t>(z)] = zone_params(p, nx, ny);
+        keys[static_cast<size_t>(z)] = spectra_key_for(bank_key(zps[static_cast<size_t>(z)], wl), cb, g);
+        const SpectraEntry& e = c->zone_spectra[static_cast<size_t>(z)];
+        if (!(e.valid && e.key == keys[static_cast<size_t>(z)])) need.push_back(z);
+    }
+    // The zones share the transform geometry: with the tensor-core DFT, every
+    // zone's windows come from one batched launch per pass.
+    const int np = pupil_size(p), R = max_kernel_radius(p), S = raw_psf_size(np, R);
+    const bool dft = p.fft_form == LD_FFT_OWN_CHOSEN || (p.fft_form == LD_FFT_OWN_FP32 && !smooth(S));
+    std::vector<PreWindows> pre(static_cast<size_t>(nz), PreWindows{nullptr, nullptr});
+    if (dft && need.size() >= 2) {
+        c->zone_pupil.resize(static_cast<size_t>(nz));
+        c->zone_wl.resize(static_cast<size_t>(nz));
+        c->zone_win.resize(static_cast<size_t>(nz));
+        const float r0 = first_zero(c, np, S, s);
+        std::vector<PsfBankArgs> args(need.size());
+        std::vector<std::vector<WavelengthInfo>> infos(need.size());
+        std::vector<const PsfBankArgs*> bp;
+        std::vector<const std::vector<WavelengthInfo>*> ip;
+        for (size_t k = 0; k < need.size(); ++k) {
+            const int z = need[k];
+            const ld_params& zp = zps[static_cast<size_t>(z)];
+            int ws = 0;
+            fill_wavelength_infos(zp, wl, r0, S, R, &infos[k], &ws);
+            PsfBankArgs& a = args[k];
+            setup_pupil(c, a, zp, false, s, &c->zone_pupil[static_cast<size_t>(z)]);
+            a.B = static_cast<int>(wl.size());
+            a.S = S;
+            a.half = S / 2;
+            a.off = std::max(0, (S - np) / 2);
+            a.win_stride = ws;
+            a.wl = static_cast<WavelengthInfo*>(
+                ensure(c, c->zone_wl[static_cast<size_t>(z)], infos[k].size() * sizeof(WavelengthInfo)));
+            a.win = static_cast<float*>(
+                ensure(c, c->zone_win[static_cast<size_t>(z)], static_cast<size_t>(a.B) * ws * ws * sizeof(float)));
+            upload_async(c, const_cast<WavelengthInfo*>(a.wl), infos[k].data(),
+                         infos[k].size() * sizeof(WavelengthInfo), s, "zone-upload");
+            pre[static_cast<size_t>(z)] = PreWindows{a.win, const_cast<WavelengthInfo*>(a.wl)};
+            bp.push_back(&a);
+            ip.push_back(&infos[k]);
+        }
+        dft_gemm_psf_batch(c, bp, ip, s);
+    }
     std::vector<const SpectraEntry*> out;
     for (int zy = 0; zy < n; ++zy) {
         for (int zx = 0; zx < n; ++zx) {
-            const float nx = (2.0f * static_cast<float>(zx)) / static_cast<float>(n - 1) - 1.0f;
-            const float ny = (2.0f * static_cast<float>(zy)) / static_cast<float>(n - 1) - 1.0f;
-            const ld_params zp = zone_params(p, nx, ny);
-            SpectraEntry& e = c->zone_spectra[static_cast<size_t>(zy) * n + zx];
-            const std::string key = spectra_key_for(bank_key(zp, wl), cb, g);
+            const int z = zy * n + zx;
+            const ld_params& zp = zps[static_cast<size_t>(z)];
+            SpectraEntry& e = c->zone_spectra[static_cast<size_t>(z)];
+            const std::string& key = keys[static_cast<size_t>(z)];
             if (!(e.valid && e.key == key)) {
                 bool rb = false, rs = false;
-                BankEntry& b = ensure_bank(c, zp, s, &rb);
+                const PreWindows& pw = pre[static_cast<size_t>(z)];
+                BankEntry& b = ensure_bank(c, zp, s, &rb, pw.win ? &pw : nullptr);
                 ensure_spectra_in(c, e, b, cb, g, s, &rs);
                 *bank_rebuilt = *bank_rebuilt || rb;
                 *spectra_rebuilt = *spectra_rebuilt || rs;
@@ -1476,6 +1580,8 @@ void ld_destroy(ld_ctx* c) {
     for (DevBuf* b : bb) free_buf(c, *b);
     for (auto& z : c->zone_spectra) free_buf(c, z.spectra);
     for (auto& z : c->spectra_lru) free_buf(c, z.spectra);
+    for (auto* v : {&c->zone_pupil, &c->zone_wl, &c->zone_win})
+        for (auto& z : *v) free_buf(c, z);
     for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
     delete c;
 }

@@ -153,6 +153,24 @@ def workload_uhd31(seed: int = 1003, chromatic_focus: float = 0.2):
     return p, frame
 
 
+def workload_zones8(seed: int = 1004):
+    """The UHD 31-wavelength frame with field-varying aberrations on an 8 x 8
+    zone grid, each zone its own PSF bank: coma and astigmatism grow with the
+    normalised field radius (the reference's field model, a linear ramp with
+    edge bias 0), their coefficients drawn ~N(0, 0.15) waves."""
+    p, frame = workload_uhd31(seed)
+    rng = np.random.default_rng(seed)
+    coma_r, coma_t, astig_r, astig_t = (float(v) for v in rng.normal(0.0, 0.15, 4))
+    p.phaseFieldStrength = 1.0
+    p.phaseFieldEdgeBias = 0.0
+    p.phaseFieldComaRadial = coma_r
+    p.phaseFieldComaTangential = coma_t
+    p.phaseFieldAstigRadial = astig_r
+    p.phaseFieldAstigTangential = astig_t
+    p.fieldGrid = 8
+    return p, frame
+
+
 def scaled_down(p: LensDiffParams, short_side: int, pupil: Optional[int] = None,
                 max_radius_px: Optional[float] = None) -> LensDiffParams:
     """A smaller copy of a workload's lens for parity runs."""

@@ -150,6 +150,21 @@ def test_field_grid_8x8_matches_oracle(cache):
     assert rel_err(out, orc, orc[..., :3].max()) < OUT_TOL
 
 
+def test_field_grid_8x8_chosen_form_batched_windows(cache):
+    """With the chosen form, the 64 zones' PSF windows come from one batched
+    launch per pass of the persistent tensor-core GEMM; the frame still meets
+    the oracle, and a second frame that changes one zone coefficient rebuilds
+    every zone through the batch again."""
+    from lensdiff_b200.types import LensDiffFftForm
+    p = _field_lens(fieldGrid=8, pupilResolution=64, maxKernelRadiusPx=S.radius_percent(12, 144),
+                    fftForm=LensDiffFftForm.OwnChosen)
+    src = S.make_frame(160, 96, 10, 1.0, 40.0, seed=16)
+    for q in (p, p.copy(phaseFieldComaRadial=0.35)):
+        out = _render(cache, with_matrices(q), src)
+        orc = _oracle(q.copy(fftForm=LensDiffFftForm.OwnFp32), src, field_grid=8)
+        assert rel_err(out, orc, orc[..., :3].max()) < OUT_TOL
+
+
 # ------------------------------------------------------- cuFFT comparator ----
 # fft_form LD_FFT_CUFFT runs the same bank and frame chain with cuFFT doing the
 # transforms (the library the reference CUDA backend uses); it is the timing
