@@ -55,6 +55,10 @@ struct SpectraEntry {
     DevBuf spectra;
     GridGeom g{};
     int n_ker = 0;
+    // recorded on the render stream after the last frame chain that read
+    // these spectra: a rebuild on the bank stream waits for it
+    cudaEvent_t free_ev = nullptr;
+    bool free_pending = false;
 };
 
 }  // namespace
@@ -98,6 +102,14 @@ struct ld_ctx {
     // side stream for the source's row transforms while a bank is built
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // bank stream: cold frames build their bank and kernel spectra here while
+    // the render stream still runs earlier frames' chains (bank_done joins
+    // them); other users of the bank's buffers join it first and leave a
+    // fence that the next build waits for
+    cudaStream_t bank_s = nullptr;
+    cudaEvent_t bank_done = nullptr, bank_fence = nullptr;
+    bool fence_pending = false;
+    DevBuf scatter_rows;  // the scatter spectrum's row transforms (not shared with the bank stream)
     // pinned staging ring for the small per-bank uploads (upload_async)
     void* stage_host = nullptr;
     std::vector<cudaEvent_t> stage_ev;
@@ -219,6 +231,44 @@ void upload_async(ld_ctx* c, void* dst, const void* src, size_t bytes, cudaStrea
     check_launch(what);
     check_cuda(cudaEventRecord(c->stage_ev[static_cast<size_t>(i)], s), what);
     c->stage_pending[static_cast<size_t>(i)] = true;
+}
+
+// The context's bank stream and its events, created on first use.
+cudaStream_t bank_stream(ld_ctx* c) {
+    if (!c->bank_s) {
+        check_cuda(cudaStreamCreateWithFlags(&c->bank_s, cudaStreamNonBlocking), "bank-stream");
+        check_cuda(cudaEventCreateWithFlags(&c->bank_done, cudaEventDisableTiming), "bank-stream");
+        check_cuda(cudaEventCreateWithFlags(&c->bank_fence, cudaEventDisableTiming), "bank-stream");
+    }
+    return c->bank_s;
+}
+
+// Stream s is about to use the bank's buffers outside the bank stream: wait
+// for the bank stream's work so far.
+void join_bank(ld_ctx* c, cudaStream_t s) {
+    if (!c->bank_s || s == c->bank_s) return;
+    check_cuda(cudaEventRecord(c->bank_done, c->bank_s), "bank-join");
+    check_cuda(cudaStreamWaitEvent(s, c->bank_done, 0), "bank-join");
+}
+
+// Stream s has enqueued uses of the bank's buffers: the next build on the
+// bank stream waits for them.
+void fence_bank(ld_ctx* c, cudaStream_t s) {
+    if (!c->bank_s || s == c->bank_s) return;
+    check_cuda(cudaEventRecord(c->bank_fence, s), "bank-fence");
+    c->fence_pending = true;
+}
+
+// An entry about to be rebuilt on stream s: wait until no frame chain reads it.
+void wait_free(SpectraEntry& e, cudaStream_t s) {
+    if (e.free_pending) check_cuda(cudaStreamWaitEvent(s, e.free_ev, 0), "spectra-reuse");
+}
+
+// Record, on the render stream, that a chain has finished with entry e.
+void mark_used(SpectraEntry& e, cudaStream_t s) {
+    if (!e.free_ev) check_cuda(cudaEventCreateWithFlags(&e.free_ev, cudaEventDisableTiming), "spectra-event");
+    check_cuda(cudaEventRecord(e.free_ev, s), "spectra-event");
+    e.free_pending = true;
 }
 
 // The context's side stream and its fork / join events, created on first use.
@@ -1342,6 +1392,7 @@ SpectraEntry& cached_spectra(ld_ctx* c, const ld_params& p, const Combination& c
         }
         if (e.last_use < victim->last_use) victim = &e;
     }
+    wait_free(*victim, s);
     BankEntry& b = ensure_bank(c, p, s, bank_rebuilt);
     ensure_spectra_in(c, *victim, b, cb, g, s, spectra_rebuilt);
     victim->last_use = ++c->spectra_clock;
@@ -1373,6 +1424,7 @@ std::vector<const SpectraEntry*> ensure_zone_spectra(ld_ctx* c, const ld_params&
         const SpectraEntry& e = c->zone_spectra[static_cast<size_t>(z)];
         if (!(e.valid && e.key == keys[static_cast<size_t>(z)])) need.push_back(z);
     }
+    for (int z : need) wait_free(c->zone_spectra[static_cast<size_t>(z)], s);
     // The zones share the transform geometry: with the tensor-core DFT, every
     // zone's windows come from one batched launch per pass.
     const int np = pupil_size(p), R = max_kernel_radius(p), S = raw_psf_size(np, R);
@@ -1466,7 +1518,7 @@ const float2* scatter_spectrum(ld_ctx* c, float radius, const GridGeom& g, cudaS
     ka.K = K;
     ka.Kp = K + (K & 1);
     ka.canvas = canvas;
-    ka.rows = static_cast<float2*>(ensure(c, c->kspec_rows, static_cast<size_t>(g.cols) * ka.Kp * sizeof(float2)));
+    ka.rows = static_cast<float2*>(ensure(c, c->scatter_rows, static_cast<size_t>(g.cols) * ka.Kp * sizeof(float2)));
     const size_t part_bytes = ks_part_bytes(1, g, false);
     char* ks = static_cast<char*>(ensure(c, c->scatter_ks, part_bytes + static_cast<size_t>(g.cols) * sizeof(float)));
     ka.spectra = reinterpret_cast<float2*>(ks);
@@ -1574,6 +1626,13 @@ void ld_destroy(ld_ctx* c) {
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->join_ev) cudaEventDestroy(c->join_ev);
     if (c->side) cudaStreamDestroy(c->side);
+    if (c->bank_done) cudaEventDestroy(c->bank_done);
+    if (c->bank_fence) cudaEventDestroy(c->bank_fence);
+    if (c->bank_s) cudaStreamDestroy(c->bank_s);
+    free_buf(c, c->scatter_rows);
+    for (auto* v : {&c->zone_spectra, &c->spectra_lru})
+        for (auto& e : *v)
+            if (e.free_ev) cudaEventDestroy(e.free_ev);
     if (c->stage_host) cudaFreeHost(c->stage_host);
     DevBuf* bb[] = {&c->bank.canvas, &c->bank.ring_round, &c->bank.ring_ceil, &c->bank.ring_peak, &c->bank.ring_mean,
                     &c->bank.scalars, &c->bank.wl,        &c->spectra.spectra};
@@ -1881,7 +1940,10 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             o.out_y1 = std::max(rq->render_window.y1, rq->dst.bounds.y1);
             o.out_x2 = std::max(o.out_x1, std::min(rq->render_window.x2, rq->dst.bounds.x2));
             o.out_y2 = std::max(o.out_y1, std::min(rq->render_window.y2, rq->dst.bounds.y2));
-            render_static_view(ctx, p, o, static_cast<cudaStream_t>(rq->cuda_stream), &bank_rebuilt);
+            const cudaStream_t vs = static_cast<cudaStream_t>(rq->cuda_stream);
+            join_bank(ctx, vs);
+            render_static_view(ctx, p, o, vs, &bank_rebuilt);
+            fence_bank(ctx, vs);
             if (st) {
                 st->bank_rebuilt = bank_rebuilt;
                 st->kernel_launches = ctx->launches;
@@ -2020,12 +2082,27 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             staged(ctx, LD_STAGE_FRAME_ROWS, ws, [&] { launch_frame_rows(fw, ws); });
             check_cuda(cudaEventRecord(ctx->join_ev, ws), "fork");
         }
+        // Bank and kernel spectra on the bank stream, so a cold frame's bank
+        // overlaps the earlier frames' chains still running on s; s joins it
+        // before this frame's chain.  Not while s is being captured (the bank
+        // stream's work would sit outside the capture).
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        check_cuda(cudaStreamIsCapturing(s, &cap), "capture-status");
+        const bool use_bs = cap == cudaStreamCaptureStatusNone && p.fft_form != LD_FFT_CUFFT;
+        cudaStream_t bs = use_bs ? bank_stream(ctx) : s;
+        if (!use_bs) join_bank(ctx, s);
+        if (use_bs && ctx->fence_pending) {
+            check_cuda(cudaStreamWaitEvent(bs, ctx->bank_fence, 0), "bank-fence");
+            ctx->fence_pending = false;
+        }
         std::vector<const SpectraEntry*> spectra;
         if (zones) {
-            spectra = ensure_zone_spectra(ctx, p, zn, cb, g, s, &bank_rebuilt, &spectra_rebuilt);
+            spectra = ensure_zone_spectra(ctx, p, zn, cb, g, bs, &bank_rebuilt, &spectra_rebuilt);
         } else {
-            spectra.push_back(&cached_spectra(ctx, p, cb, g, s, &bank_rebuilt, &spectra_rebuilt));
+            spectra.push_back(&cached_spectra(ctx, p, cb, g, bs, &bank_rebuilt, &spectra_rebuilt));
         }
+        if (use_bs && (bank_rebuilt || spectra_rebuilt)) join_bank(ctx, s);
+        if (!use_bs) fence_bank(ctx, s);
         const SpectraEntry& sp = *spectra.front();
         for (FrameArgs* f : {&fa, &fw}) {
             f->spectra = ks_part(sp.spectra.p, 0, cb.n_ker, g, fa.h16);
@@ -2099,6 +2176,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             if (fa.effect_mode != kEffectComposite)
                 staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fa, s); });
             check_launch("frame-chain");
+            for (const SpectraEntry* e : spectra) mark_used(const_cast<SpectraEntry&>(*e), s);
             if (st) {
                 st->bank_rebuilt = bank_rebuilt;
                 st->spectra_rebuilt = spectra_rebuilt;
@@ -2184,6 +2262,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             if (fa.effect_mode != kEffectComposite) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fin, s); });
         };
         run_chain(ctx, s, gkey, chain);
+        for (const SpectraEntry* e : spectra) mark_used(const_cast<SpectraEntry&>(*e), s);
         check_launch("frame-chain");
         if (st) {
             st->bank_rebuilt = bank_rebuilt;
@@ -2207,7 +2286,10 @@ int ld_build_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream, ld_sta
         validate_params(*params);
         fill_sizes(st, *params);
         bool rebuilt = false;
-        ensure_bank(ctx, *params, static_cast<cudaStream_t>(stream), &rebuilt);
+        const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        join_bank(ctx, s);
+        ensure_bank(ctx, *params, s, &rebuilt);
+        fence_bank(ctx, s);
         if (st) st->bank_rebuilt = rebuilt;
     });
 }
@@ -2224,7 +2306,9 @@ int ld_export_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream, float
         validate_params(*params);
         fill_sizes(st, *params);
         bool rebuilt = false;
+        join_bank(ctx, s);
         BankEntry& b = ensure_bank(ctx, *params, s, &rebuilt);
+        fence_bank(ctx, s);
         std::vector<PsfScalars> sc(static_cast<size_t>(b.B));
         check_cuda(cudaMemcpyAsync(sc.data(), b.args.scalars, sc.size() * sizeof(PsfScalars), cudaMemcpyDeviceToHost, s),
                    "export-readback");
@@ -2279,6 +2363,7 @@ int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float
             throw Fail{LD_ERR_ARG, "invalid-wavelength-index"};
         const int np = pupil_size(p), R = max_kernel_radius(p), S = raw_psf_size(np, R);
         PsfBankArgs a{};
+        join_bank(ctx, s);  // the pupil, calibration and transform buffers are the bank's
         setup_pupil(ctx, a, p, false, s);
         a.B = 1;
         a.S = S;
@@ -2308,6 +2393,7 @@ int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float
         }
         launch_normalize_psf(psf_out, S * S, dsc, s);
         check_launch("raw-psf");
+        fence_bank(ctx, s);
         // the upload above reads `wi` from the stack: finish before returning
         check_cuda(cudaStreamSynchronize(s), "rawpsf-sync");
     });
