@@ -264,6 +264,20 @@ int ld_render(ld_ctx* ctx, const ld_render_request* request,
 int ld_build_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream,
                       ld_status* status);
 
+/* Builds the banks of `count` unrelated lenses on `stream` (pupil size, PSF
+ * size, wavelength count and phase terms may all differ), each as
+ * EnsureLensDiffPsfBank builds one (LensDiffCpuReference.cpp:2068-2071).
+ * With the tensor-core form the windows of every (lens, wavelength) pair
+ * come from one persistent GEMM launch per transform pass, in chunks of at
+ * most 32 GiB of scratch (a quarter of the HBM budget when that is less).
+ * The banks stay in the context until the next call or ld_clear_caches;
+ * ld_export_psf_bank and ld_render find them by their parameters.  Banks
+ * already held for the same lens at the same position are kept;
+ * status->bank_rebuilt counts the banks built and the size fields describe
+ * params[0]. */
+int ld_build_psf_banks(ld_ctx* ctx, const ld_params* params, int32_t count,
+                       void* stream, ld_status* status);
+
 /* Copies the bank's `full` kernels to HOST memory: for wavelength i,
  * sizes[i] = 2*radius_i+1 and a sizes[i]^2 row-major kernel is written at
  * kernels_out + offsets[i].  `capacity` is the float count of kernels_out.

@@ -298,6 +298,7 @@ EXPORTED_SYMBOLS = [
     "ld_check_device_errors",
     "ld_render",
     "ld_build_psf_bank",
+    "ld_build_psf_banks",
     "ld_export_psf_bank",
     "ld_raw_psf",
     "ld_raw_psf_noalloc",
@@ -355,6 +356,8 @@ def lib() -> ctypes.CDLL:
     L.ld_render.restype = ctypes.c_int
     L.ld_build_psf_bank.argtypes = [vp, ctypes.POINTER(ld_params), vp, ctypes.POINTER(ld_status)]
     L.ld_build_psf_bank.restype = ctypes.c_int
+    L.ld_build_psf_banks.argtypes = [vp, ctypes.POINTER(ld_params), ctypes.c_int32, vp, ctypes.POINTER(ld_status)]
+    L.ld_build_psf_banks.restype = ctypes.c_int
     L.ld_export_psf_bank.argtypes = [vp, ctypes.POINTER(ld_params), vp,
                                      ctypes.POINTER(c_f32), ctypes.POINTER(c_i32),
                                      ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(c_f32),

@@ -20,7 +20,7 @@ data_ptr() used).
 from __future__ import annotations
 
 import ctypes
-from typing import List, Optional, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -88,6 +88,7 @@ class LensDiffStatus:
         self.code = int(st.code)
         self.stage = st.stage.decode(errors="replace")
         self.bank_rebuilt = bool(st.bank_rebuilt)
+        self.banks_rebuilt = int(st.bank_rebuilt)  # lens sets: the banks built
         self.spectra_rebuilt = bool(st.spectra_rebuilt)
         self.pupil_size = int(st.pupil_size)
         self.raw_psf_size = int(st.raw_psf_size)
@@ -174,6 +175,17 @@ class LensDiffPsfBankCache:
         pp = abi.to_abi_params(params)
         st = abi.ld_status()
         self._lib.ld_build_psf_bank(self._h, ctypes.byref(pp), _stream(stream), ctypes.byref(st))
+        return LensDiffStatus(st)
+
+    def build_psf_banks(self, params_list: Sequence[LensDiffParams], stream=None) -> LensDiffStatus:
+        """Builds the banks of several unrelated lenses together (their
+        tensor-core windows in one launch per transform pass); they stay
+        cached until the next call, for export_psf_bank and render."""
+        arr = (abi.ld_params * len(params_list))()
+        for i, p in enumerate(params_list):
+            arr[i] = abi.to_abi_params(p)
+        st = abi.ld_status()
+        self._lib.ld_build_psf_banks(self._h, arr, len(params_list), _stream(stream), ctypes.byref(st))
         return LensDiffStatus(st)
 
     def export_psf_bank(self, params: LensDiffParams, stream=None) -> Tuple[List[float], List[np.ndarray], LensDiffStatus]:

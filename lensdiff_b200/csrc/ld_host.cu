@@ -77,6 +77,11 @@ struct ld_ctx {
     std::vector<SpectraEntry> zone_spectra;  // field zones, zy * n + zx
     // field zones' pupils, wavelength tables and windows of one batched transform
     std::vector<DevBuf> zone_pupil, zone_wl, zone_win;
+    // banks of unrelated lenses built together (ld_build_psf_banks), kept
+    // until the next such build; the pupils, wavelength tables and windows of
+    // one chunk of their batched transform
+    std::vector<BankEntry> set_banks;
+    std::vector<DevBuf> set_pupil, set_wl, set_win;
     // kernel spectra of recent (lens, frame size) pairs, least recently used
     // replaced first: a context serving one lens at several frame sizes keeps
     // them all without rebuilding the bank
@@ -674,13 +679,14 @@ void validate_params(const ld_params& p) {
 }
 
 size_t align256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
+size_t align1k(size_t n) { return (n + 1023) & ~static_cast<size_t>(1023); }
 
 // Fills the pupil part of a bank argument block and launches the per-bank
 // pupil pre-pass (amplitude, the λ-independent phase, the defocus term).
 // Only pupil rows whose pixel centres lie within the outer radius of the
 // (decentred) aperture can be non-zero; the row passes skip the others.
-void setup_pupil(ld_ctx* c, PsfBankArgs& a, const ld_params& p, bool circle, cudaStream_t s,
-                 DevBuf* target = nullptr) {
+// The pupil's parameters, base phase and the rows that can be non-zero.
+void pupil_geometry(PsfBankArgs& a, const ld_params& p, bool circle) {
     a.pupil = pupil_params(p, circle);
     a.base_phase = circle ? PhaseCoeffs{} : phase_for_wavelength(p, 550.0f);
     a.base_phase.c[4] = 0.0f;  // defocus is carried per wavelength
@@ -699,6 +705,12 @@ void setup_pupil(ld_ctx* c, PsfBankArgs& a, const ld_params& p, bool circle, cud
     }
     a.row_lo = lo;
     a.row_n = hi - lo;
+}
+
+void setup_pupil(ld_ctx* c, PsfBankArgs& a, const ld_params& p, bool circle, cudaStream_t s,
+                 DevBuf* target = nullptr) {
+    pupil_geometry(a, p, circle);
+    const int n = a.pupil.size;
     a.pupil_pre = static_cast<float4*>(
         ensure(c, target ? *target : c->pupil_pre, static_cast<size_t>(n) * n * sizeof(float4)));
     staged(c, LD_STAGE_PUPIL, s, [&] { launch_pupil_pre(a, s); });
@@ -901,72 +913,93 @@ DftPlan plan_dft(const PsfBankArgs& a, const std::vector<WavelengthInfo>& infos,
     return d;
 }
 
-size_t dft_bytes(const DftPlan& d, int B) {
-    return 2 * (static_cast<size_t>(B) * (d.pf_lambda + d.yt_lambda) + d.dx_slab * d.kc_rows +
-                d.dy_slab * d.kc_cols) +
-           2 * static_cast<size_t>(B) * sizeof(DftProblem) + (2 * static_cast<size_t>(B) + 4) * sizeof(int) +
-           16 * 1024;
-}
 
 // Chosen form: the bank's |F|^2 windows by DFT-as-GEMM on the tensor cores
 // in place of the row and column FFTs (ld_dftgemm.cu).
+// Scratch bytes of one lens's DFT-as-GEMM operands (pupil fields and row-pass
+// outputs of its B wavelengths), each image 1 KiB aligned.
+size_t dft_lens_bytes(const DftPlan& d, int B) {
+    return 2 * (align1k(static_cast<size_t>(B) * d.pf_lambda) + align1k(static_cast<size_t>(B) * d.yt_lambda));
+}
+size_t dft_basis_bytes(const DftPlan& d) {
+    return 2 * (align1k(d.dx_slab * d.kc_rows) + align1k(d.dy_slab * d.kc_cols));
+}
+
 // The bank windows of several lenses (one PsfBankArgs and wavelength table
 // each) in one launch per pass of the persistent tensor-core GEMM: every
-// (lens, wavelength) pass is one problem of the work queue.  The lenses must
-// share the transform geometry (PSF size, pupil extent, windows), as field
-// zones of one lens do; they keep their own pupil fields and phases.
+// (lens, wavelength) pass is one problem of the work queue, whatever its
+// pupil size, PSF size, window or wavelength count.  Lenses whose basis
+// geometry matches (PSF size, pupil extent, union window: the field zones of
+// one lens) share one pair of basis images; each keeps its own pupil fields.
 void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
                         const std::vector<const std::vector<WavelengthInfo>*>& infos, cudaStream_t s) {
-    const int Z = static_cast<int>(banks.size());
-    const PsfBankArgs& a0 = *banks.front();
-    std::vector<DftLambda> lam;
-    DftPlan d = plan_dft(a0, *infos.front(), &lam);
-    for (int z = 1; z < Z; ++z) {  // one shared plan: same geometry
-        std::vector<DftLambda> lz;
-        const DftPlan dz = plan_dft(*banks[static_cast<size_t>(z)], *infos[static_cast<size_t>(z)], &lz);
-        bool same = dz.col_lo == d.col_lo && dz.col_n == d.col_n && dz.mt_rows == d.mt_rows &&
-                    dz.kc_rows == d.kc_rows && dz.kc_cols == d.kc_cols && dz.x0 == d.x0 &&
-                    dz.basis_rows == d.basis_rows && banks[static_cast<size_t>(z)]->S == a0.S &&
-                    banks[static_cast<size_t>(z)]->B == a0.B && lz.size() == lam.size();
-        for (size_t b = 0; same && b < lam.size(); ++b)
-            same = lz[b].n0 == lam[b].n0 && lz[b].shift == lam[b].shift && lz[b].nt == lam[b].nt;
-        if (!same) {  // separate launches
-            for (int k = 0; k < Z; ++k)
-                dft_gemm_psf_batch(c, {banks[static_cast<size_t>(k)]}, {infos[static_cast<size_t>(k)]}, s);
-            return;
+    const size_t Z = banks.size();
+    std::vector<DftPlan> plan(Z);
+    std::vector<std::vector<DftLambda>> lam(Z);
+    std::vector<size_t> group(Z);  // index of the lens whose basis images this lens reads
+    size_t P = 0, bytes = 1024;
+    for (size_t z = 0; z < Z; ++z) {
+        const PsfBankArgs& a = *banks[z];
+        plan[z] = plan_dft(a, *infos[z], &lam[z]);
+        const DftPlan& d = plan[z];
+        group[z] = z;
+        for (size_t k = 0; k < z; ++k) {
+            const DftPlan& e = plan[k];
+            const PsfBankArgs& b = *banks[k];
+            if (group[k] == k && b.S == a.S && e.basis_rows == d.basis_rows && e.x0 == d.x0 &&
+                e.kc_rows == d.kc_rows && e.col_n == d.col_n && b.off + e.col_lo == a.off + d.col_lo &&
+                e.kc_cols == d.kc_cols && b.row_n == a.row_n && b.off + b.row_lo == a.off + a.row_lo) {
+                group[z] = k;
+                break;
+            }
         }
+        P += static_cast<size_t>(a.B);
+        bytes += dft_lens_bytes(d, a.B) + (group[z] == z ? dft_basis_bytes(d) : 0);
     }
-    const int B = a0.B, P = Z * B;
-    char* p = static_cast<char*>(ensure(c, c->dft, dft_bytes(d, P)));
-    auto take = [&](size_t bytes) {
+    bytes += align1k(2 * P * sizeof(DftProblem)) + align1k((2 * P + 4) * sizeof(int));
+    char* p = static_cast<char*>(ensure(c, c->dft, bytes));
+    auto take = [&](size_t n) {
         char* q = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~static_cast<uintptr_t>(1023));
-        p = q + bytes;
+        p = q + n;
         return reinterpret_cast<unsigned char*>(q);
     };
-    d.pf_hi = take(P * d.pf_lambda);
-    d.pf_lo = take(P * d.pf_lambda);
-    d.yt_hi = take(P * d.yt_lambda);
-    d.yt_lo = take(P * d.yt_lambda);
-    d.dx_hi = take(d.dx_slab * d.kc_rows);
-    d.dx_lo = take(d.dx_slab * d.kc_rows);
-    d.dy_hi = take(d.dy_slab * d.kc_cols);
-    d.dy_lo = take(d.dy_slab * d.kc_cols);
+    for (size_t z = 0; z < Z; ++z) {
+        DftPlan& d = plan[z];
+        const int B = banks[z]->B;
+        d.pf_hi = take(B * d.pf_lambda);
+        d.pf_lo = take(B * d.pf_lambda);
+        d.yt_hi = take(B * d.yt_lambda);
+        d.yt_lo = take(B * d.yt_lambda);
+        if (group[z] == z) {
+            d.dx_hi = take(d.dx_slab * d.kc_rows);
+            d.dx_lo = take(d.dx_slab * d.kc_rows);
+            d.dy_hi = take(d.dy_slab * d.kc_cols);
+            d.dy_lo = take(d.dy_slab * d.kc_cols);
+        } else {
+            const DftPlan& g = plan[group[z]];
+            d.dx_hi = g.dx_hi;
+            d.dx_lo = g.dx_lo;
+            d.dy_hi = g.dy_hi;
+            d.dy_lo = g.dy_lo;
+        }
+    }
     // problem tables of the two passes (one problem per lens and wavelength),
     // their tile prefixes and the two work-queue counters
-    std::vector<DftProblem> rows(static_cast<size_t>(P)), cols(static_cast<size_t>(P));
-    std::vector<int> rstart(static_cast<size_t>(P) + 1, 0), cstart(static_cast<size_t>(P) + 1, 0);
-    for (int z = 0; z < Z; ++z) {
-        const PsfBankArgs& a = *banks[static_cast<size_t>(z)];
-        for (int b = 0; b < B; ++b) {
-            const size_t i = static_cast<size_t>(z) * B + b;
-            const DftLambda& l = lam[static_cast<size_t>(b)];
+    std::vector<DftProblem> rows(P), cols(P);
+    std::vector<int> rstart(P + 1, 0), cstart(P + 1, 0);
+    size_t i = 0;
+    for (size_t z = 0; z < Z; ++z) {
+        const PsfBankArgs& a = *banks[z];
+        const DftPlan& d = plan[z];
+        for (int b = 0; b < a.B; ++b, ++i) {
+            const DftLambda& l = lam[z][static_cast<size_t>(b)];
             DftProblem& r = rows[i];
-            r.a_hi = d.pf_hi + i * d.pf_lambda;
-            r.a_lo = d.pf_lo + i * d.pf_lambda;
+            r.a_hi = d.pf_hi + b * d.pf_lambda;
+            r.a_lo = d.pf_lo + b * d.pf_lambda;
             r.b_hi = d.dx_hi;
             r.b_lo = d.dx_lo;
-            r.y_hi = d.yt_hi + i * d.yt_lambda;
-            r.y_lo = d.yt_lo + i * d.yt_lambda;
+            r.y_hi = d.yt_hi + b * d.yt_lambda;
+            r.y_lo = d.yt_lo + b * d.yt_lambda;
             r.a_slab = static_cast<uint32_t>(d.pf_slab);
             r.b_slab = static_cast<uint32_t>(d.dx_slab);
             r.y_slab = static_cast<uint32_t>(d.yt_slab);
@@ -976,8 +1009,8 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
             r.n0 = l.n0;
             r.shift = l.shift;
             DftProblem& q = cols[i];
-            q.a_hi = d.yt_hi + i * d.yt_lambda;
-            q.a_lo = d.yt_lo + i * d.yt_lambda;
+            q.a_hi = d.yt_hi + b * d.yt_lambda;
+            q.a_lo = d.yt_lo + b * d.yt_lambda;
             q.b_hi = d.dy_hi;
             q.b_lo = d.dy_lo;
             q.win = a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride;
@@ -989,15 +1022,16 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
             q.nt = l.nt;
             q.n0 = l.n0;
             q.shift = l.shift;
-            q.win_n = (*infos[static_cast<size_t>(z)])[static_cast<size_t>(b)].win_n;
+            q.win_n = (*infos[z])[static_cast<size_t>(b)].win_n;
             q.win_stride = a.win_stride;
             rstart[i + 1] = rstart[i] + r.mt * r.nt;
             cstart[i + 1] = cstart[i] + q.mt * q.nt;
         }
     }
-    DftProblem* drows = reinterpret_cast<DftProblem*>(take(rows.size() * sizeof(DftProblem)));
-    DftProblem* dcols = reinterpret_cast<DftProblem*>(take(cols.size() * sizeof(DftProblem)));
-    int* dstart = reinterpret_cast<int*>(take(2 * (static_cast<size_t>(P) + 1) * sizeof(int) + 2 * sizeof(int)));
+    const int np = static_cast<int>(P);
+    DftProblem* drows = reinterpret_cast<DftProblem*>(take(2 * P * sizeof(DftProblem)));
+    DftProblem* dcols = drows + P;
+    int* dstart = reinterpret_cast<int*>(take((2 * P + 4) * sizeof(int)));
     std::vector<int> starts(rstart);
     starts.insert(starts.end(), cstart.begin(), cstart.end());
     starts.push_back(0);  // the two counters
@@ -1005,24 +1039,24 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
     upload_async(c, drows, rows.data(), rows.size() * sizeof(DftProblem), s, "dft-upload");
     upload_async(c, dcols, cols.data(), cols.size() * sizeof(DftProblem), s, "dft-upload");
     upload_async(c, dstart, starts.data(), starts.size() * sizeof(int), s, "dft-upload");
-    DftBasisArgs bx{d.dx_hi, d.dx_lo, d.dx_slab, d.basis_rows, d.kc_rows, d.col_n, a0.off + d.col_lo, d.x0, a0.S / 2,
-                    a0.S};
-    DftBasisArgs by{d.dy_hi, d.dy_lo, d.dy_slab, d.basis_rows, d.kc_cols, a0.row_n, a0.off + a0.row_lo, d.x0,
-                    a0.S / 2, a0.S};
-    DftBatchArgs gr{drows, dstart, P, rstart.back(), kDftRows, dstart + 2 * (P + 1), c->err};
-    DftBatchArgs gc{dcols, dstart + (P + 1), P, cstart.back(), kDftCols, dstart + 2 * (P + 1) + 1, c->err};
+    DftBatchArgs gr{drows, dstart, np, rstart.back(), kDftRows, dstart + 2 * (np + 1), c->err};
+    DftBatchArgs gc{dcols, dstart + (np + 1), np, cstart.back(), kDftCols, dstart + 2 * (np + 1) + 1, c->err};
+    auto basis = [&](const PsfBankArgs& a, const DftPlan& d, bool rows_pass) {
+        return rows_pass ? DftBasisArgs{d.dx_hi, d.dx_lo, d.dx_slab, d.basis_rows, d.kc_rows, d.col_n,
+                                        a.off + d.col_lo, d.x0, a.S / 2, a.S}
+                         : DftBasisArgs{d.dy_hi, d.dy_lo, d.dy_slab, d.basis_rows, d.kc_cols, a.row_n,
+                                        a.off + a.row_lo, d.x0, a.S / 2, a.S};
+    };
     staged(c, LD_STAGE_PSF_ROWS, s, [&] {
-        for (int z = 0; z < Z; ++z) {
-            DftPlan dz = d;  // this lens's pupil-field images
-            dz.pf_hi = d.pf_hi + static_cast<size_t>(z) * B * d.pf_lambda;
-            dz.pf_lo = d.pf_lo + static_cast<size_t>(z) * B * d.pf_lambda;
-            launch_pupil_field(*banks[static_cast<size_t>(z)], dz, s);
+        for (size_t z = 0; z < Z; ++z) {
+            launch_pupil_field(*banks[z], plan[z], s);
+            if (group[z] == z) launch_dft_basis(basis(*banks[z], plan[z], true), s);
         }
-        launch_dft_basis(bx, s);
         launch_dft_gemm(gr, s);
     });
     staged(c, LD_STAGE_PSF_COLS, s, [&] {
-        launch_dft_basis(by, s);
+        for (size_t z = 0; z < Z; ++z)
+            if (group[z] == z) launch_dft_basis(basis(*banks[z], plan[z], false), s);
         launch_dft_gemm(gc, s);
     });
 }
@@ -1038,13 +1072,20 @@ struct PreWindows {
     WavelengthInfo* wl;  // device, the matching wavelength table
 };
 
+// The bank of `p`: the context's bank or a bank of the last lens set when
+// one matches, else built into the context's bank.  With `into`, built into
+// that entry unconditionally (lens sets).
 BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebuilt,
-                       const PreWindows* pre = nullptr) {
+                       const PreWindows* pre = nullptr, BankEntry* into = nullptr) {
     const std::vector<float> wl = wavelengths_of(p);
     const std::string key = bank_key(p, wl);
     *rebuilt = false;
-    if (c->bank.valid && c->bank.key == key) return c->bank;
-    BankEntry& b = c->bank;
+    if (!into) {
+        if (c->bank.valid && c->bank.key == key) return c->bank;
+        for (BankEntry& e : c->set_banks)
+            if (e.valid && e.key == key) return e;
+    }
+    BankEntry& b = into ? *into : c->bank;
     b.valid = false;
     const int np = pupil_size(p);
     const int R = max_kernel_radius(p);
@@ -1124,7 +1165,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     b.split_sums = false;
     b.key = key;
     b.valid = true;
-    c->spectra.valid = false;
+    if (!into) c->spectra.valid = false;
     *rebuilt = true;
     return b;
 }
@@ -1484,6 +1525,109 @@ std::vector<const SpectraEntry*> ensure_zone_spectra(ld_ctx* c, const ld_params&
     return out;
 }
 
+// Scratch of one chunk of a lens set's batched transform (pupils, windows,
+// DFT operand images): lenses join a chunk while its scratch stays within
+// this, or a quarter of the context's HBM budget when that is smaller.
+constexpr size_t kSetChunkBytes = size_t(32) << 30;
+
+// The banks of `n` unrelated lenses (pupil size, PSF size, wavelengths and
+// phase all free), each as EnsureLensDiffPsfBank builds one
+// (LensDiffCpuReference.cpp:2068-2071).  Banks already built for the same
+// lens at the same position are kept.  The lenses whose windows come from
+// the tensor-core DFT have them computed together: one launch per transform
+// pass of the persistent GEMM per chunk, every (lens, wavelength) pair a
+// problem of its work queue.  The other lenses are built one by one.
+void build_lens_set(ld_ctx* c, const ld_params* ps, size_t n, cudaStream_t s, int* rebuilt_count) {
+    for (size_t i = n; i < c->set_banks.size(); ++i) {
+        BankEntry& e = c->set_banks[i];
+        for (DevBuf* b : {&e.canvas, &e.ring_round, &e.ring_ceil, &e.ring_peak, &e.ring_mean, &e.scalars, &e.wl})
+            free_buf(c, *b);
+    }
+    c->set_banks.resize(n);
+    struct Lens {
+        size_t i;
+        PsfBankArgs a;
+        std::vector<WavelengthInfo> infos;
+        size_t bytes;
+    };
+    std::vector<Lens> dft;
+    std::vector<size_t> other;
+    for (size_t i = 0; i < n; ++i) {
+        const ld_params& p = ps[i];
+        const std::vector<float> wl = wavelengths_of(p);
+        BankEntry& e = c->set_banks[i];
+        if (e.valid && e.key == bank_key(p, wl)) continue;
+        e.valid = false;
+        const int np = pupil_size(p), R = max_kernel_radius(p), S = raw_psf_size(np, R);
+        if (static_cast<int>(wl.size()) > kMaxBins) throw Fail{LD_ERR_ARG, "too-many-wavelengths"};
+        if (!(p.fft_form == LD_FFT_OWN_CHOSEN || (p.fft_form == LD_FFT_OWN_FP32 && !smooth(S)))) {
+            other.push_back(i);
+            continue;
+        }
+        // every calibration runs before the first chunk uses the DFT scratch
+        const float r0 = first_zero(c, np, S, s);
+        Lens l;
+        l.i = i;
+        l.a = PsfBankArgs{};
+        int ws = 0;
+        fill_wavelength_infos(p, wl, r0, S, R, &l.infos, &ws);
+        pupil_geometry(l.a, p, false);
+        l.a.B = static_cast<int>(wl.size());
+        l.a.S = S;
+        l.a.half = S / 2;
+        l.a.off = std::max(0, (S - np) / 2);
+        l.a.win_stride = ws;
+        std::vector<DftLambda> lam;
+        const DftPlan d = plan_dft(l.a, l.infos, &lam);
+        l.bytes = static_cast<size_t>(np) * np * sizeof(float4) +
+                  static_cast<size_t>(l.a.B) * ws * ws * sizeof(float) + dft_lens_bytes(d, l.a.B) +
+                  dft_basis_bytes(d);
+        dft.push_back(std::move(l));
+    }
+    const size_t budget = c->budget ? std::min(kSetChunkBytes, c->budget / 4) : kSetChunkBytes;
+    for (size_t k = 0; k < dft.size();) {
+        size_t m = k, used = 0;
+        while (m < dft.size() && (m == k || used + dft[m].bytes <= budget)) used += dft[m++].bytes;
+        if (c->set_pupil.size() < m - k) {
+            c->set_pupil.resize(m - k);
+            c->set_win.resize(m - k);
+        }
+        std::vector<const PsfBankArgs*> bp;
+        std::vector<const std::vector<WavelengthInfo>*> ip;
+        for (size_t j = k; j < m; ++j) {
+            Lens& l = dft[j];
+            BankEntry& e = c->set_banks[l.i];
+            setup_pupil(c, l.a, ps[l.i], false, s, &c->set_pupil[j - k]);
+            l.a.wl = static_cast<WavelengthInfo*>(ensure(c, e.wl, l.infos.size() * sizeof(WavelengthInfo)));
+            l.a.win = static_cast<float*>(ensure(c, c->set_win[j - k], static_cast<size_t>(l.a.B) * l.a.win_stride *
+                                                                           l.a.win_stride * sizeof(float)));
+            upload_async(c, const_cast<WavelengthInfo*>(l.a.wl), l.infos.data(),
+                         l.infos.size() * sizeof(WavelengthInfo), s, "set-upload");
+            bp.push_back(&l.a);
+            ip.push_back(&l.infos);
+        }
+        dft_gemm_psf_batch(c, bp, ip, s);
+        for (size_t j = k; j < m; ++j) {
+            const Lens& l = dft[j];
+            BankEntry& e = c->set_banks[l.i];
+            const PreWindows pre{l.a.win, const_cast<WavelengthInfo*>(l.a.wl)};
+            bool rb = false;
+            ensure_bank(c, ps[l.i], s, &rb, &pre, &e);
+            e.args.win = nullptr;  // chunk scratch, reused by the next chunk
+            ++*rebuilt_count;
+        }
+        k = m;
+    }
+    for (size_t i : other) {
+        BankEntry& e = c->set_banks[i];
+        bool rb = false;
+        ensure_bank(c, ps[i], s, &rb, nullptr, &e);
+        e.args.win = nullptr;  // the context's shared scratch
+        e.args.rows = nullptr;
+        ++*rebuilt_count;
+    }
+}
+
 // Spectrum of the scatter kernel on grid g (one kernel, FP32 layout), built
 // on the first frame with this (radius, grid).  The kernel is the reference's
 // normalised Gaussian of radius ceil(max(.5, r)) and sigma max(.5, r / 2),
@@ -1639,8 +1783,11 @@ void ld_destroy(ld_ctx* c) {
     for (DevBuf* b : bb) free_buf(c, *b);
     for (auto& z : c->zone_spectra) free_buf(c, z.spectra);
     for (auto& z : c->spectra_lru) free_buf(c, z.spectra);
-    for (auto* v : {&c->zone_pupil, &c->zone_wl, &c->zone_win})
+    for (auto* v : {&c->zone_pupil, &c->zone_wl, &c->zone_win, &c->set_pupil, &c->set_win})
         for (auto& z : *v) free_buf(c, z);
+    for (BankEntry& e : c->set_banks)
+        for (DevBuf* b : {&e.canvas, &e.ring_round, &e.ring_ceil, &e.ring_peak, &e.ring_mean, &e.scalars, &e.wl})
+            free_buf(c, *b);
     for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
     delete c;
 }
@@ -1685,6 +1832,7 @@ void ld_clear_caches(ld_ctx* c) {
     std::lock_guard<std::mutex> lock(c->mu);
     c->bank.valid = false;
     c->spectra.valid = false;
+    for (auto& e : c->set_banks) e.valid = false;
     for (auto& z : c->zone_spectra) z.valid = false;
     for (auto& z : c->spectra_lru) z.valid = false;
 }
@@ -2289,6 +2437,28 @@ int ld_build_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream, ld_sta
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
         join_bank(ctx, s);
         ensure_bank(ctx, *params, s, &rebuilt);
+        fence_bank(ctx, s);
+        if (st) st->bank_rebuilt = rebuilt;
+    });
+}
+
+int ld_build_psf_banks(ld_ctx* ctx, const ld_params* params, int32_t count, void* stream, ld_status* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (!ctx || !params) {
+        set_status(st, LD_ERR_ARG, "null-argument");
+        return LD_ERR_ARG;
+    }
+    if (count <= 0) {
+        set_status(st, LD_ERR_ARG, "invalid-lens-count");
+        return LD_ERR_ARG;
+    }
+    return run_guarded(ctx, st, [&]() {
+        for (int32_t i = 0; i < count; ++i) validate_params(params[i]);
+        fill_sizes(st, params[0]);
+        int rebuilt = 0;
+        const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        join_bank(ctx, s);
+        build_lens_set(ctx, params, static_cast<size_t>(count), s, &rebuilt);
         fence_bank(ctx, s);
         if (st) st->bank_rebuilt = rebuilt;
     });

@@ -9,13 +9,14 @@ anti-aliased line segments).
 from __future__ import annotations
 
 import math
-from typing import Optional
+from typing import List, Optional
 
 import numpy as np
 
 from .types import (
     LensDiffApertureMode,
     LensDiffEnergyMode,
+    LensDiffFftForm,
     LensDiffLookMode,
     LensDiffParams,
     LensDiffPhaseMode,
@@ -169,6 +170,44 @@ def workload_zones8(seed: int = 1004):
     p.phaseFieldAstigTangential = astig_t
     p.fieldGrid = 8
     return p, frame
+
+
+def lens_instances(count: int = 256, seed: int = 1005, pupil=(128, 1024), pad=(2.0, 4.0), bins=(8, 64),
+                   noll_max: int = 22) -> List[LensDiffParams]:
+    """`count` unrelated lenses for batched bank builds: pupil N_p uniform in
+    `pupil`, PSF size S = pad * N_p with pad uniform in `pad` (through the
+    kernel radius R = pad * N_p / 4, since S = max(2 N_p, 512, 4 R)), B
+    wavelengths uniform in `bins` spread over 400-700 nm with Gaussian RGB
+    responses, 5-9 blade polygons with random rounding, obstruction and vanes,
+    Noll 2..noll_max ~ N(0, 0.1) waves and chromatic focus 0.2 waves; the
+    tensor-core (chosen) form."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        np_ = int(rng.integers(pupil[0], pupil[1] + 1))
+        radius = max(4, int(round(float(rng.uniform(*pad)) * np_ / 4.0)))
+        b = int(rng.integers(bins[0], bins[1] + 1))
+        p = base_params(2160)
+        p.apertureMode = LensDiffApertureMode.Polygon
+        p.bladeCount = int(rng.integers(5, 10))
+        p.roundness = float(rng.uniform(0.0, 1.0))
+        p.centralObstruction = float(rng.choice([0.0, rng.uniform(0.1, 0.4)]))
+        p.vaneCount = int(rng.integers(0, 5))
+        p.vaneThickness = float(rng.uniform(0.005, 0.03))
+        p.rotationDeg = float(rng.uniform(0.0, 60.0))
+        p.pupilResolution = np_
+        p.maxKernelRadiusPx = radius_percent(radius, 2160)
+        noll = [0.0] * 23
+        for j in range(2, noll_max + 1):
+            noll[j] = float(rng.normal(0.0, 0.1))
+        p.noll = noll
+        p.chromaticFocus = 0.2
+        p.spectralMode = LensDiffSpectralMode.Spectral9
+        p.wavelengthsNm = [float(v) for v in np.linspace(400.0, 700.0, b)]
+        p.rgbMode = LensDiffRgbMode.Gaussian
+        p.fftForm = LensDiffFftForm.OwnChosen
+        out.append(p)
+    return out
 
 
 def scaled_down(p: LensDiffParams, short_side: int, pupil: Optional[int] = None,
