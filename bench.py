@@ -2,6 +2,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl own|reference]
                     [--workload uhd31|hd16|small3|zones8] [--bank cold|warm]
+    python bench.py --lens-set [--lenses 256]     (PSF banks of unrelated lenses)
+    python bench.py --serving                     (Poisson frame serving)
 
 A step renders one frame of the workload through the path: with --bank cold
 (the default, the headline) every frame changes the defocus coefficient by
@@ -62,6 +64,9 @@ def parse():
                     help="transform chain of the headline line (own: hand-written FP32)")
     ap.add_argument("--serving", action="store_true",
                     help="Poisson stream of mixed-size frames through the continuous-batching server")
+    ap.add_argument("--lens-set", action="store_true",
+                    help="lens-set workload: the PSF banks of --lenses unrelated lenses per step")
+    ap.add_argument("--lenses", type=int, default=256, help="lenses per step of --lens-set")
     ap.add_argument("--rates", default="5,20,50,100,200", help="arrival rates (frames/s) of --serving")
     ap.add_argument("--requests", type=int, default=48, help="requests per rate of --serving")
     ap.add_argument("--slots", type=int, default=4, help="server slots of --serving")
@@ -98,6 +103,21 @@ def _ref_unit(args):
     pupil = np.ones((np_, np_), np.float32)
     t = time.perf_counter()
     R.convolve_scalar(d, ker)
+    R.raw_psf_from(pupil, None, s)
+    return time.perf_counter() - t
+
+
+def _ref_psf_unit(args):
+    """One raw PSF of the reference (buildShiftedRawPsf,
+    LensDiffCpuReference.cpp:831-859): pupil np_ -> PSF size s.  Seconds."""
+    np_, s = args
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    from oracle import ref_lib as R
+
+    pupil = np.ones((np_, np_), np.float32)
+    t = time.perf_counter()
     R.raw_psf_from(pupil, None, s)
     return time.perf_counter() - t
 
@@ -349,6 +369,114 @@ def run_serving(args):
         "sweep": sweep}))
 
 
+def run_lens_set(args):
+    """Lens-set workload: each step builds the PSF banks of `--lenses`
+    unrelated lenses (synthetic.lens_instances: pupil 128-1024, PSF 2-4x the
+    pupil, 8-64 wavelengths, 5-9 blade polygons, Noll 2..22, chromatic focus)
+    through ld_build_psf_banks, whose tensor-core windows for every (lens,
+    wavelength) pair come from one persistent GEMM launch per transform pass
+    and scratch chunk.  Every step changes every lens's defocus by 1e-6 waves,
+    so all banks are rebuilt.  Metric: lens banks/s, device time."""
+    import numpy as np
+    import torch
+
+    from lensdiff_b200 import synthetic as S
+    from lensdiff_b200.backend import LensDiffPsfBankCache, resolve_sizes
+
+    lenses = S.lens_instances(args.lenses)
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cache = LensDiffPsfBankCache(0)
+    stream = torch.cuda.Stream(device=dev)
+    k = [0]
+
+    def step():
+        k[0] += 1
+        st = cache.build_psf_banks([q.copy(phaseDefocus=q.phaseDefocus + 1e-6 * k[0]) for q in lenses], stream)
+        if not st.ok or st.banks_rebuilt != len(lenses):
+            raise RuntimeError(f"lens-set build failed: {st}")
+        return st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(0)
+    clocks.start()
+    time.sleep(0.3)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    launches = 0
+    evs[0].record(stream)
+    for i in range(args.steps):
+        launches += step().kernel_launches
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    per_step = sorted(evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps))
+    total_ms = evs[0].elapsed_time(evs[-1])
+    # stages and tensor-core work of one profiled step
+    cache.set_profiling(True)
+    cache.profile_collect()
+    cache.tensor_flops()
+    step()
+    torch.cuda.synchronize(dev)
+    stage = cache.profile_collect()
+    flops = cache.tensor_flops()
+    cache.set_profiling(False)
+    if cache.check_device_errors():
+        raise RuntimeError("device error word set by the lens-set builds")
+    cache.close()
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 1400.0, "fallback (sustained bf16)"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            pk = json.load(f)
+        peak = float(pk.get("bf16_tflops_sustained", pk.get("bf16_tflops")))
+        peak_src = "measured (sustained bf16)"
+    g_ms, g_n = stage.get("dft_gemm", (0.0, 0))
+    roofline = None
+    if g_n:
+        achieved = flops / g_n / (g_ms / g_n / 1000.0) / 1e12
+        roofline = {"bound": "tensor", "kernel": "dft_gemm", "achieved": achieved, "peak": peak,
+                    "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_src, "traffic": None,
+                    "flops_per_launch": flops / g_n, "launch_ms": g_ms / g_n, "launches": g_n,
+                    "note": "bf16 MMA flops issued, the BF16x3 split's three products counted"}
+    sizes = [resolve_sizes(q) for q in lenses]
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref_lib as R
+
+        if R.available():
+            rng = np.random.default_rng(9)
+            small = [i for i, z in enumerate(sizes) if z[1] <= 2048]
+            workers = min(16, os.cpu_count() or 1)
+            pick = [int(i) for i in rng.choice(small, size=min(workers, len(small)), replace=False)]
+            ctx = mp.get_context("spawn")
+            with ctx.Pool(len(pick)) as pool:
+                ts = pool.map(_ref_psf_unit, [(sizes[i][0], sizes[i][1]) for i in pick])
+            cost = lambda z: z[1] * z[1] * math.log2(z[1])  # noqa: E731
+            c = float(np.mean([t / cost(sizes[i]) for t, i in zip(ts, pick)]))
+            est = sum(z[3] * c * cost(z) for z in sizes) / len(pick)
+            cpu = {"value": len(lenses) / est, "unit": "lens banks/s", "cores": len(pick), "kind": "reference",
+                   "sample": (f"{len(pick)} processes, each one reference buildShiftedRawPsf of a sampled lens "
+                              f"(PSF <= 2048); seconds per raw PSF fitted as c*S^2*log2(S), summed over every "
+                              f"(lens, wavelength) of the set and divided by the processes (raw PSFs only: the "
+                              f"reference's resampling and shaping are not counted)")}
+    print(json.dumps({
+        "metric": "lens PSF banks/s (uneven pupils, PSF sizes, wavelength counts)",
+        "value": args.steps * len(lenses) / (total_ms / 1000.0), "unit": "lens banks/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "p50_ms": per_step[len(per_step) // 2], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16x3 (tensor-core DFT), f32 elsewhere", "data": "synthetic",
+        "config": {"workload": f"lens_set{len(lenses)}", "lenses": len(lenses),
+                   "pupil": [min(z[0] for z in sizes), max(z[0] for z in sizes)],
+                   "psf": [min(z[1] for z in sizes), max(z[1] for z in sizes)],
+                   "wavelengths_total": sum(z[3] for z in sizes), "bank": "cold",
+                   "l2": "inputs larger than L2 (tens of GB of windows and canvases per step)"},
+        "gpu_launches": launches,
+        "stage_ms_per_step": {k: round(v[0], 3) for k, v in stage.items() if v[1]},
+        "roofline": roofline, "clocks": clk, "cpu_baseline": cpu}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -356,6 +484,9 @@ def main():
         return
     if args.serving:
         run_serving(args)
+        return
+    if args.lens_set:
+        run_lens_set(args)
         return
     ws, rank, local = dist_env()
     import numpy as np

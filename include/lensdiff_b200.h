@@ -237,7 +237,8 @@ enum {
     LD_STAGE_PSF_ROWS = 0, LD_STAGE_PSF_COLS, LD_STAGE_RESAMPLE, LD_STAGE_SHAPE_STATS,
     LD_STAGE_SUPPORT, LD_STAGE_CROP_SUM, LD_STAGE_COMBINE, LD_STAGE_KSPEC_ROWS,
     LD_STAGE_KSPEC_COLS, LD_STAGE_FRAME_ROWS, LD_STAGE_FRAME_COLS, LD_STAGE_FRAME_INVERSE,
-    LD_STAGE_PUPIL, LD_STAGE_COMPOSITE, LD_STAGE_SCATTER, LD_STAGE_WORKING_SOURCE, LD_STAGE_COUNT
+    LD_STAGE_PUPIL, LD_STAGE_COMPOSITE, LD_STAGE_SCATTER, LD_STAGE_WORKING_SOURCE,
+    LD_STAGE_DFT_GEMM, LD_STAGE_COUNT
 };
 /* Per-frame chains are captured into CUDA graphs on first use and replayed
  * when a later frame issues identical launches (same buffers, geometry and
@@ -252,6 +253,9 @@ int ld_set_profiling(ld_ctx* ctx, int enable);
 /* Synchronises the recorded events and writes, per stage id, the summed
  * device milliseconds and the launch count since the last collect; resets. */
 int ld_profile_collect(ld_ctx* ctx, double* ms_per_stage, int32_t* launches_per_stage, int32_t count);
+/* Tensor-core MMA flops issued by the DFT-as-GEMM launches (LD_STAGE_DFT_GEMM)
+ * since the last call, the BF16x3 split's three products counted; resets. */
+int ld_profile_tensor_flops(ld_ctx* ctx, double* flops);
 
 /* ---- the drop-in render (replaces RunLensDiffCuda, LensDiffCuda.h:7-10) -- */
 /* Enqueues the whole frame on request->cuda_stream; no host synchronisation

@@ -299,6 +299,7 @@ EXPORTED_SYMBOLS = [
     "ld_render",
     "ld_build_psf_bank",
     "ld_build_psf_banks",
+    "ld_profile_tensor_flops",
     "ld_export_psf_bank",
     "ld_raw_psf",
     "ld_raw_psf_noalloc",
@@ -327,7 +328,7 @@ class ld_server_stats(ctypes.Structure):
 
 STAGE_NAMES = ["psf_rows", "psf_cols", "resample", "shape_stats", "support", "crop_sum", "combine",
                "kspec_rows", "kspec_cols", "frame_rows", "frame_cols", "frame_inverse", "pupil", "composite",
-               "scatter", "working_source"]
+               "scatter", "working_source", "dft_gemm"]
 
 
 def lib() -> ctypes.CDLL:
@@ -358,6 +359,8 @@ def lib() -> ctypes.CDLL:
     L.ld_build_psf_bank.restype = ctypes.c_int
     L.ld_build_psf_banks.argtypes = [vp, ctypes.POINTER(ld_params), ctypes.c_int32, vp, ctypes.POINTER(ld_status)]
     L.ld_build_psf_banks.restype = ctypes.c_int
+    L.ld_profile_tensor_flops.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.ld_profile_tensor_flops.restype = ctypes.c_int
     L.ld_export_psf_bank.argtypes = [vp, ctypes.POINTER(ld_params), vp,
                                      ctypes.POINTER(c_f32), ctypes.POINTER(c_i32),
                                      ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(c_f32),

@@ -163,6 +163,12 @@ class LensDiffPsfBankCache:
         self._lib.ld_profile_collect(self._h, ms, cnt, n)
         return {abi.STAGE_NAMES[i]: (float(ms[i]), int(cnt[i])) for i in range(n)}
 
+    def tensor_flops(self) -> float:
+        """Tensor-core MMA flops issued by DFT-GEMM launches since the last call."""
+        f = ctypes.c_double(0.0)
+        self._lib.ld_profile_tensor_flops(self._h, ctypes.byref(f))
+        return float(f.value)
+
     # -- entry points -------------------------------------------------------
     def render(self, request: LensDiffRenderRequest, params: LensDiffParams) -> LensDiffStatus:
         rq = to_abi_request(request)

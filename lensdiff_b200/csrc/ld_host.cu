@@ -120,6 +120,16 @@ struct ld_ctx {
     std::vector<cudaEvent_t> stage_ev;
     std::vector<bool> stage_pending;
     int stage_next = 0;
+    // pinned buffers for uploads larger than a staging slot (the problem
+    // tables of a lens set's batched transform), reused round-robin
+    struct BigStage {
+        void* host = nullptr;
+        size_t bytes = 0;
+        cudaEvent_t ev = nullptr;
+        bool pending = false;
+    };
+    std::vector<BigStage> big_stage;
+    int big_next = 0;
     std::string scatter_key;
     // comparator form (cuFFT): plans and its own work buffers
     CufftPlanCache cufft;
@@ -132,6 +142,7 @@ struct ld_ctx {
     std::vector<cudaEvent_t> event_pool;
     size_t events_used = 0;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+    double tensor_flops = 0.0;  // MMA flops issued by DFT-GEMM launches (ld_profile_tensor_flops)
 };
 
 namespace {
@@ -199,6 +210,7 @@ void* ensure(ld_ctx* c, DevBuf& b, size_t bytes) {
 // ---------------------------------------------------------------------------
 constexpr size_t kStageSlot = 16384;
 constexpr int kStageSlots = 64;  // 16 cold frames of uploads in flight
+constexpr int kBigStages = 8;
 
 // One CTA copies `words` 4-byte words from mapped pinned host memory.
 __global__ void __launch_bounds__(256) host_words_kernel(uint32_t* dst, const uint32_t* src, int words) {
@@ -213,8 +225,28 @@ __global__ void __launch_bounds__(256) host_words_kernel(uint32_t* dst, const ui
 // refilled only after the kernel that last read it has finished.  Arrays
 // above one slot take a plain copy.
 void upload_async(ld_ctx* c, void* dst, const void* src, size_t bytes, cudaStream_t s, const char* what) {
-    if (bytes > kStageSlot || (bytes & 3) != 0 || (reinterpret_cast<uintptr_t>(dst) & 3) != 0) {
+    if ((bytes & 3) != 0 || (reinterpret_cast<uintptr_t>(dst) & 3) != 0) {
         check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), what);
+        return;
+    }
+    if (bytes > kStageSlot) {  // a pinned copy: no wait for the stream, as a pageable one would
+        if (c->big_stage.empty()) c->big_stage.resize(kBigStages);
+        ld_ctx::BigStage& b = c->big_stage[static_cast<size_t>(c->big_next)];
+        c->big_next = (c->big_next + 1) % kBigStages;
+        if (b.pending) check_cuda(cudaEventSynchronize(b.ev), what);
+        b.pending = false;
+        if (!b.ev) check_cuda(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming), what);
+        if (b.bytes < bytes) {
+            if (b.host) cudaFreeHost(b.host);
+            b.host = nullptr;
+            b.bytes = 0;
+            check_cuda(cudaHostAlloc(&b.host, bytes, cudaHostAllocDefault), what);
+            b.bytes = bytes;
+        }
+        std::memcpy(b.host, src, bytes);
+        check_cuda(cudaMemcpyAsync(dst, b.host, bytes, cudaMemcpyHostToDevice, s), what);
+        check_cuda(cudaEventRecord(b.ev, s), what);
+        b.pending = true;
         return;
     }
     if (!c->stage_host) {
@@ -234,6 +266,7 @@ void upload_async(ld_ctx* c, void* dst, const void* src, size_t bytes, cudaStrea
     host_words_kernel<<<1, 256, 0, s>>>(static_cast<uint32_t*>(dst), static_cast<const uint32_t*>(hd),
                                          static_cast<int>(bytes / 4));
     check_launch(what);
+    ++c->launches;
     check_cuda(cudaEventRecord(c->stage_ev[static_cast<size_t>(i)], s), what);
     c->stage_pending[static_cast<size_t>(i)] = true;
 }
@@ -1052,13 +1085,21 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
             launch_pupil_field(*banks[z], plan[z], s);
             if (group[z] == z) launch_dft_basis(basis(*banks[z], plan[z], true), s);
         }
-        launch_dft_gemm(gr, s);
     });
+    staged(c, LD_STAGE_DFT_GEMM, s, [&] { launch_dft_gemm(gr, s); });
     staged(c, LD_STAGE_PSF_COLS, s, [&] {
         for (size_t z = 0; z < Z; ++z)
             if (group[z] == z) launch_dft_basis(basis(*banks[z], plan[z], false), s);
-        launch_dft_gemm(gc, s);
     });
+    staged(c, LD_STAGE_DFT_GEMM, s, [&] { launch_dft_gemm(gc, s); });
+    size_t groups = 0;  // the two preparation stages launched Z + groups and groups kernels
+    for (size_t z = 0; z < Z; ++z) groups += group[z] == z;
+    c->launches += static_cast<int>(Z + 2 * groups) - 2;
+    // a tile is a 128 x 256 x 64 real product per K-chunk, three times (hi.hi, hi.lo, lo.hi)
+    double kt = 0.0;
+    for (size_t k = 0; k < P; ++k)
+        kt += static_cast<double>(rows[k].kc) * rows[k].mt * rows[k].nt + static_cast<double>(cols[k].kc) * cols[k].mt * cols[k].nt;
+    c->tensor_flops += kt * 3.0 * 2.0 * 128.0 * 256.0 * 64.0;
 }
 
 void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthInfo>& infos, cudaStream_t s) {
@@ -1778,6 +1819,11 @@ void ld_destroy(ld_ctx* c) {
         for (auto& e : *v)
             if (e.free_ev) cudaEventDestroy(e.free_ev);
     if (c->stage_host) cudaFreeHost(c->stage_host);
+    for (auto& b : c->big_stage) {
+        if (b.pending) cudaEventSynchronize(b.ev);
+        if (b.host) cudaFreeHost(b.host);
+        if (b.ev) cudaEventDestroy(b.ev);
+    }
     DevBuf* bb[] = {&c->bank.canvas, &c->bank.ring_round, &c->bank.ring_ceil, &c->bank.ring_peak, &c->bank.ring_mean,
                     &c->bank.scalars, &c->bank.wl,        &c->spectra.spectra};
     for (DevBuf* b : bb) free_buf(c, *b);
@@ -1798,6 +1844,14 @@ int ld_set_profiling(ld_ctx* c, int enable) {
     if (!c) return LD_ERR_ARG;
     std::lock_guard<std::mutex> lock(c->mu);
     c->profiling = enable != 0;
+    return LD_OK;
+}
+
+int ld_profile_tensor_flops(ld_ctx* c, double* flops) {
+    if (!c || !flops) return LD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    *flops = c->tensor_flops;
+    c->tensor_flops = 0.0;
     return LD_OK;
 }
 
@@ -2435,10 +2489,14 @@ int ld_build_psf_bank(ld_ctx* ctx, const ld_params* params, void* stream, ld_sta
         fill_sizes(st, *params);
         bool rebuilt = false;
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        ctx->launches = 0;
         join_bank(ctx, s);
         ensure_bank(ctx, *params, s, &rebuilt);
         fence_bank(ctx, s);
-        if (st) st->bank_rebuilt = rebuilt;
+        if (st) {
+            st->bank_rebuilt = rebuilt;
+            st->kernel_launches = ctx->launches;
+        }
     });
 }
 
@@ -2457,10 +2515,14 @@ int ld_build_psf_banks(ld_ctx* ctx, const ld_params* params, int32_t count, void
         fill_sizes(st, params[0]);
         int rebuilt = 0;
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        ctx->launches = 0;
         join_bank(ctx, s);
         build_lens_set(ctx, params, static_cast<size_t>(count), s, &rebuilt);
         fence_bank(ctx, s);
-        if (st) st->bank_rebuilt = rebuilt;
+        if (st) {
+            st->bank_rebuilt = rebuilt;
+            st->kernel_launches = ctx->launches;
+        }
     });
 }
 
