@@ -84,6 +84,34 @@ def test_lens_set_matches_single_builds_and_oracle(cache):
             assert rel_err(k, b.full, b.full.max()) < PSF_TOL
 
 
+def test_lens_set_large_pupils(cache):
+    """Pupils of 1000 and 1024 (28 K-chunks per GEMM tile): PSF 4000 against
+    the FP32 FFT bank of the same lens, PSF 4124 (4 x 1031) against the FP64
+    oracle."""
+    ps = S.lens_instances(2, seed=78, pupil=(1000, 1000), bins=(8, 8))
+    ps[1] = S.lens_instances(1, seed=79, pupil=(1024, 1024), bins=(4, 4))[0]
+    ps[0].maxKernelRadiusPx = S.radius_percent(1000, 2160)
+    ps[1].maxKernelRadiusPx = S.radius_percent(1031, 2160)
+    assert [O.resolve_sizes(p)[1] for p in ps] == [4000, 4124]
+    st = cache.build_psf_banks(ps, torch.cuda.current_stream())
+    assert st.ok, st
+    assert cache.check_device_errors() == 0
+    k0, _ = _export(cache, ps[0])
+    k1, _ = _export(cache, ps[1])
+    single = LensDiffPsfBankCache(0)
+    try:
+        kf, _ = _export(single, ps[0].copy(fftForm=LensDiffFftForm.OwnFp32))
+    finally:
+        single.close()
+    for a, b in zip(k0, kf):
+        assert a.shape == b.shape
+        assert rel_err(a, b, b.max()) < PSF_TOL
+    ob = O.build_psf_bank(ps[1])
+    for a, b in zip(k1, ob.bins):
+        assert a.shape == b.full.shape
+        assert rel_err(a, b.full, b.full.max()) < PSF_TOL
+
+
 def test_lens_set_keeps_unchanged_banks_and_mixes_forms(cache):
     ps = _lenses()
     st = cache.build_psf_banks(ps, torch.cuda.current_stream())
