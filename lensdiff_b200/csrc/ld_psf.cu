@@ -296,7 +296,8 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
 #pragma unroll 4
     for (int i = 0; i < kTallH / 8; ++i) {
         const int y = ty0 + threadIdx.y + 8 * i;
-        const bool in = x < K && y < K;
+        if (y >= K) break;  // uniform: a warp is one canvas row (the last tile row is mostly past K)
+        const bool in = x < K;
         float v = 0.0f;
         int slot = -1;
         if (in) {
@@ -522,29 +523,29 @@ __global__ void __launch_bounds__(256) crop_sum_kernel(PsfBankArgs a) {
     if (y0 > R + rho) return;  // uniform
     const float inv_s3 = static_cast<float>(1.0 / sc.s3);
     const float extent = sc.extent, fade = sc.fade, start = sc.start;
-    const float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
     const int side = 2 * rho + 1;
-    const int rows = min(kCropRows, R + rho + 1 - y0);
-    const int items = rows * side;
-    constexpr int kU = 8;
+    const int lane = threadIdx.x & 31;
+    const int y = y0 + static_cast<int>(threadIdx.x >> 5);  // one warp per crop row
     float lsum = 0.0f;
-    for (int i0 = threadIdx.x; i0 < items; i0 += kU * 256) {
-        float v[kU];
+    if (y <= R + rho) {
+        const float* row = a.canvas + static_cast<size_t>(b) * K * K + static_cast<size_t>(y) * K + (R - rho);
+        const float dy = static_cast<float>(y - R);
+        const float dy2 = dy * dy;
+        constexpr int kU = 8;
+        for (int c0 = lane; c0 < side; c0 += kU * 32) {
+            float v[kU];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int i = i0 + u * 256;
-            const int r = i / side;
-            const int c = i - r * side;
-            v[u] = i < items ? __ldg(canvas + static_cast<size_t>(y0 + r) * K + (R - rho + c)) : 0.0f;
-        }
+            for (int u = 0; u < kU; ++u) {
+                const int c = c0 + u * 32;
+                v[u] = c < side ? __ldg(row + c) : 0.0f;
+            }
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int i = i0 + u * 256;
-            if (i >= items) break;
-            const int r = i / side;
-            const float dy = static_cast<float>(y0 + r - R);
-            const float dx = static_cast<float>(i - r * side - rho);
-            lsum += (v[u] * inv_s3) * taper_weight(sqrtf(dx * dx + dy * dy), extent, fade, start);
+            for (int u = 0; u < kU; ++u) {
+                const int c = c0 + u * 32;
+                if (c >= side) break;
+                const float dx = static_cast<float>(c - rho);
+                lsum += (v[u] * inv_s3) * taper_weight(sqrtf(dx * dx + dy2), extent, fade, start);
+            }
         }
     }
     const double tot = block_sum(static_cast<double>(lsum));
