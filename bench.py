@@ -17,6 +17,9 @@ e2e    the same metric through the public entry point with host buffers:
        each step copies the frame from pinned host memory, renders, and
        copies the result back (both copies inside the timed region).
 
+The Python garbage collector is paused inside timed regions, as timeit does:
+a collection pause of this driver script would idle the GPU between frames.
+
 Multi-GPU: the path does not shard inside a frame; each rank renders its own
 frames (replicas), timing is the max over ranks.
 
@@ -26,6 +29,7 @@ sources into oracle/_ref/libldref.so) on this machine's host cores.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import math
 import multiprocessing as mp
@@ -405,11 +409,14 @@ def run_lens_set(args):
     time.sleep(0.3)
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     launches = 0
+    gc.collect()
+    gc.disable()
     evs[0].record(stream)
     for i in range(args.steps):
         launches += step().kernel_launches
         evs[i + 1].record(stream)
     torch.cuda.synchronize(dev)
+    gc.enable()
     clk = clocks.stop()
     per_step = sorted(evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps))
     total_ms = evs[0].elapsed_time(evs[-1])
@@ -543,12 +550,15 @@ def main():
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
+    gc.collect()
+    gc.disable()  # a collection pause of the Python driver would idle the GPU between frames
     with torch.cuda.stream(stream):
         evs[0].record(stream)
         for i in range(args.steps):
             step()
             evs[i + 1].record(stream)
     torch.cuda.synchronize(dev)
+    gc.enable()
     if ws > 1:
         torch.distributed.barrier()
     # per-stage device times from a separate profiled pass (stage events
@@ -568,6 +578,7 @@ def main():
         raise RuntimeError(f"device error word {dev_err} after the timed frames")
     clk = clocks.stop()
     per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    sys.stderr.write("step ms: " + " ".join(f"{v:.3f}" for v in per_step) + "\n")
     total_ms = evs[0].elapsed_time(evs[-1])
     t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
     if ws > 1:
@@ -622,10 +633,13 @@ def main():
         if ws > 1:
             torch.distributed.barrier()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        gc.collect()
+        gc.disable()
         ev0.record(s_in)
         run_frames(args.steps)
         ev1.record(s_out)
         torch.cuda.synchronize(dev)
+        gc.enable()
         e_ms = torch.tensor([ev0.elapsed_time(ev1)], device=dev, dtype=torch.float64)
         if ws > 1:
             torch.distributed.all_reduce(e_ms, op=torch.distributed.ReduceOp.MAX)
@@ -686,12 +700,15 @@ def main():
                     cmp_step()
             torch.cuda.synchronize(dev)
             cev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+            gc.collect()
+            gc.disable()
             with torch.cuda.stream(stream):
                 cev[0].record(stream)
                 for i in range(args.steps):
                     cmp_step()
                     cev[i + 1].record(stream)
             torch.cuda.synchronize(dev)
+            gc.enable()
             cps = sorted(cev[i].elapsed_time(cev[i + 1]) for i in range(args.steps))
             ctot = torch.tensor([cev[0].elapsed_time(cev[-1])], device=dev, dtype=torch.float64)
             if ws > 1:

@@ -1431,7 +1431,10 @@ SpectraEntry& ensure_spectra_in(ld_ctx* c, SpectraEntry& e, BankEntry& b, const 
     return e;
 }
 
-constexpr size_t kSpectraCache = 4;
+// Three slots: one in use by the frame on the GPU, one being built on the bank
+// stream, one for a recent lens; a stream of new lenses rotates through them,
+// so its per-frame chains settle on three cached graphs.
+constexpr size_t kSpectraCache = 3;
 
 // Kernel spectra for (lens p, geometry g) from the context's LRU cache; the
 // bank is built (or reused) only on a miss.
