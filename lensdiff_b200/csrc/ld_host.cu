@@ -44,6 +44,7 @@ struct BankEntry {
     bool cufft = false;  // built with the comparator form (its spectra follow)
     bool h16 = false;    // chosen form: kernel spectra in FP16 with per-column scales
     bool split_sums = false;  // s_core / s_struct computed (first Split render of the bank)
+    bool ring_means = false;  // ring means computed (built unfused, or on first Split use)
     DevBuf canvas, ring_round, ring_ceil, ring_peak, ring_mean, scalars, wl;
     PsfBankArgs args{};
 };
@@ -1190,7 +1191,8 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
         staged(c, LD_STAGE_PSF_COLS, s, [&] { launch_psf_cols(a, s); });
     }
     staged(c, LD_STAGE_RESAMPLE, s, [&] { launch_resample(a, s); });
-    staged(c, LD_STAGE_SHAPE_STATS, s, [&] { launch_shape_stats(a, s); });
+    const bool fused = fused_shaping(a);
+    if (!fused) staged(c, LD_STAGE_SHAPE_STATS, s, [&] { launch_shape_stats(a, s); });
     staged(c, LD_STAGE_SUPPORT, s, [&] { launch_support(a, s); });
     staged(c, LD_STAGE_CROP_SUM, s, [&] { launch_crop_sum(a, s); });
     check_launch("psf-bank");
@@ -1204,6 +1206,7 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
     b.cufft = p.fft_form == LD_FFT_CUFFT;
     b.h16 = chosen_h16(p);
     b.split_sums = false;
+    b.ring_means = !fused;
     b.key = key;
     b.valid = true;
     if (!into) c->spectra.valid = false;
@@ -1382,6 +1385,10 @@ SpectraEntry& ensure_spectra_in(ld_ctx* c, SpectraEntry& e, BankEntry& b, const 
     *rebuilt = false;
     if (e.valid && e.key == key) return e;
     e.valid = false;
+    if (cb.parts == 2 && !b.ring_means) {
+        staged(c, LD_STAGE_SHAPE_STATS, s, [&] { launch_ring_means(b.args, s); });
+        b.ring_means = true;
+    }
     if (cb.parts == 2 && !b.split_sums) {
         staged(c, LD_STAGE_CROP_SUM, s, [&] { launch_split_sums(b.args, s); });
         b.split_sums = true;

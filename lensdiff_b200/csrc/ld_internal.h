@@ -73,6 +73,11 @@ void launch_psf_rows(const PsfBankArgs& a, cudaStream_t s);
 void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s);
 void launch_resample(const PsfBankArgs& a, cudaStream_t s);
 void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s);
+// Anisotropy gain 1: shaping is the identity; launch_resample then takes the
+// shaped kernel's statistics and launch_shape_stats is not needed.  The ring
+// means (Split look) then come from launch_ring_means when first needed.
+bool fused_shaping(const PsfBankArgs& a);
+void launch_ring_means(const PsfBankArgs& a, cudaStream_t s);
 void launch_support(const PsfBankArgs& a, cudaStream_t s);
 void launch_crop_sum(const PsfBankArgs& a, cudaStream_t s);
 void launch_split_sums(const PsfBankArgs& a, cudaStream_t s);  // s_core, s_struct (Split look)

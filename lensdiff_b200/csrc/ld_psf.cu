@@ -85,36 +85,6 @@ __device__ __forceinline__ void warp_runs_accumulate(int slot, float v, float* r
     }
 }
 
-// warp_runs_accumulate for two ring systems at once: runs are lanes with the
-// same (round ring, ceil ring) pair (key); each run's sum goes to ring[sr]
-// and ring_e[sc], its maximum to peak[sc].  Lanes with key < 0 add nothing.
-__device__ __forceinline__ void warp_runs_accumulate2(int key, int sr, int sc, float v, float* ring, float* ring_e,
-                                                      unsigned int* peak) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int prev = __shfl_up_sync(full, key, 1);
-    const unsigned heads = __ballot_sync(full, lane == 0 || prev != key);
-    const int head = 31 - __clz(heads & (full >> (31 - lane)));
-    float sum = v, m = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const float t = __shfl_up_sync(full, sum, o);
-        const float u = __shfl_up_sync(full, m, o);
-        if (lane - o >= head) {
-            sum += t;
-            m = fmaxf(m, u);
-        }
-    }
-    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u) != 0u;
-    if (tail && key >= 0) {
-        if (sum != 0.0f) {
-            atomicAdd(&ring[sr], sum);
-            atomicAdd(&ring_e[sc], sum);
-        }
-        if (m != 0.0f) atomicMax(&peak[sc], __float_as_uint(m));
-    }
-}
-
 // ---- pupil, once per bank --------------------------------------------------------
 __global__ void __launch_bounds__(256) pupil_pre_kernel(PsfBankArgs a) {
     const int n = a.pupil.size;
@@ -304,12 +274,13 @@ __device__ __forceinline__ float sample_row(const Window& w, const ColTap& c, fl
 // FUSED (anisotropy gain 1): reshapeAnisotropy (LensDiffCpuReference.cpp:1122-1134)
 // then gives mean + (base - mean) * 1, the base kernel itself up to one
 // rounding, so the canvas keeps the resampled values unnormalised and this
-// pass also takes the shaped kernel's statistics that shape_stats_kernel
-// takes otherwise: s3 = s1, the ceil(r) ring energies and peaks, the peak.
+// pass takes the shaped kernel's statistics that shape_stats_kernel takes
+// otherwise (s3 = s1, the ceil(r) ring energies and peaks, the peak) in
+// place of the round(r) ring sums, which only the Split look's ring means
+// need (ring_sums_kernel, run when a Split render first uses the bank).
 template <bool FUSED>
 __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
-    __shared__ float ring[kRingSpanTall];
-    __shared__ float ring_e[FUSED ? kRingSpanTall : 1];
+    __shared__ float ring[kRingSpanTall];  // FUSED: the ceil(r) ring energies
     __shared__ unsigned int ring_p[FUSED ? kRingSpanTall : 1];
     const int b = blockIdx.z;
     const WavelengthInfo* wi = a.wl + b;
@@ -319,10 +290,7 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
     const int rbase = tile_ring_base<kTallH>(tx0, ty0, R, R);
     for (int i = tid; i < kRingSpanTall; i += 256) {
         ring[i] = 0.0f;
-        if constexpr (FUSED) {
-            ring_e[i] = 0.0f;
-            ring_p[i] = 0u;
-        }
+        if constexpr (FUSED) ring_p[i] = 0u;
     }
     __syncthreads();
     const Window w{a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride, a.win_stride, wi->win_x0,
@@ -344,34 +312,28 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
         if (y >= K) break;  // uniform: a warp is one canvas row (the last tile row is mostly past K)
         const bool in = x < K;
         float v = 0.0f;
-        int slot = -1, slot_c = 0;
+        int slot = -1;
         if (in) {
             const float dy = static_cast<float>(y) - kc;
             v = taps == 0 ? sample_row(w, ct, rc + dy * inv)
                           : sample_filtered(w, rc + dx * inv, rc + dy * inv, inv, taps, step);
             canvas[static_cast<size_t>(y) * K + x] = v;
             lsum += v;
-            const float rad = sqrtf(dx * dx + dy * dy);
-            slot = min(R, static_cast<int>(roundf(rad))) - rbase;
             if constexpr (FUSED) {
                 lpeak = max(lpeak, __float_as_uint(v));
-                slot_c = min(R, static_cast<int>(ceilf(rad))) - rbase;
+                slot = min(R, static_cast<int>(ceilf(sqrtf(dx * dx + dy * dy)))) - rbase;
+            } else {
+                slot = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy)))) - rbase;
             }
         }
-        if constexpr (FUSED) {
-            // ceil(r) - round(r) is 0 or 1: one key orders both ring systems
-            warp_runs_accumulate2(slot < 0 ? -1 : 2 * slot + (slot_c - slot), slot, slot_c, v, ring, ring_e, ring_p);
-        } else {
-            warp_runs_accumulate<false>(slot, v, ring, nullptr);
-        }
+        warp_runs_accumulate<FUSED>(slot, v, ring, ring_p);
     }
     __syncthreads();
     const size_t ro = static_cast<size_t>(b) * (R + 1);
     for (int i = tid; i < kRingSpanTall; i += 256) {
         if (rbase + i > R) continue;
-        if (ring[i] != 0.0f) atomicAdd(&a.ring_round[ro + rbase + i], static_cast<double>(ring[i]));
+        if (ring[i] != 0.0f) atomicAdd(&(FUSED ? a.ring_ceil : a.ring_round)[ro + rbase + i], static_cast<double>(ring[i]));
         if constexpr (FUSED) {
-            if (ring_e[i] != 0.0f) atomicAdd(&a.ring_ceil[ro + rbase + i], static_cast<double>(ring_e[i]));
             if (ring_p[i] != 0u) atomicMax(&a.ring_peak[ro + rbase + i], ring_p[i]);
         }
     }
@@ -416,6 +378,40 @@ __global__ void __launch_bounds__(256) ring_mean_kernel(PsfBankArgs a) {
     float* out = a.ring_mean + static_cast<size_t>(b) * (R + 1);
     for (int r = threadIdx.x; r <= R; r += blockDim.x)
         out[r] = static_cast<float>(((rr[r] / s1) / max(1, a.count_round[r])) / s2);
+}
+
+// grid (ceil(K/32), ceil(K/128), B), block (32, 8): the round(r) ring sums
+// of a canvas that resample_kernel<true> filled (the unnormalised resampled
+// kernel), for the ring means of the Split look.
+__global__ void __launch_bounds__(256) ring_sums_kernel(PsfBankArgs a) {
+    __shared__ float ring[kRingSpanTall];
+    const int b = blockIdx.z;
+    const int K = a.K, R = a.R;
+    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTallH;
+    const int tid = threadIdx.x + threadIdx.y * 32;
+    const int rbase = tile_ring_base<kTallH>(tx0, ty0, R, R);
+    for (int i = tid; i < kRingSpanTall; i += 256) ring[i] = 0.0f;
+    __syncthreads();
+    const float kc = static_cast<float>(K - 1) * 0.5f;
+    const float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
+    const int x = tx0 + threadIdx.x;
+    const float dx = static_cast<float>(x) - kc;
+    for (int i = 0; i < kTallH / 8; ++i) {
+        const int y = ty0 + threadIdx.y + 8 * i;
+        if (y >= K) break;  // uniform: a warp is one canvas row
+        float v = 0.0f;
+        int slot = -1;
+        if (x < K) {
+            const float dy = static_cast<float>(y) - kc;
+            v = __ldg(canvas + static_cast<size_t>(y) * K + x);
+            slot = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy)))) - rbase;
+        }
+        warp_runs_accumulate<false>(slot, v, ring, nullptr);
+    }
+    __syncthreads();
+    const size_t ro = static_cast<size_t>(b) * (R + 1);
+    for (int i = tid; i < kRingSpanTall; i += 256)
+        if (ring[i] != 0.0f && rbase + i <= R) atomicAdd(&a.ring_round[ro + rbase + i], static_cast<double>(ring[i]));
 }
 
 // grid (ceil(K/32), ceil(K/128), B): shaped kernel (reshapeAnisotropy of the
@@ -958,8 +954,6 @@ void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s) {
     else cols_launch<kE16, 1>(a, s);
 }
 
-// Anisotropy gain 1: the shaping is the identity and resample_kernel takes
-// the shaped kernel's statistics itself.
 bool fused_shaping(const PsfBankArgs& a) { return a.gain == 1.0f; }
 
 void launch_resample(const PsfBankArgs& a, cudaStream_t s) {
@@ -968,8 +962,13 @@ void launch_resample(const PsfBankArgs& a, cudaStream_t s) {
 }
 
 void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s) {
-    ring_mean_kernel<<<a.B, 256, 0, s>>>(a);  // the ring means serve the Split look and its views
-    if (!fused_shaping(a)) shape_stats_kernel<<<tall_grid(a), dim3(32, 8), 0, s>>>(a);
+    ring_mean_kernel<<<a.B, 256, 0, s>>>(a);
+    shape_stats_kernel<<<tall_grid(a), dim3(32, 8), 0, s>>>(a);
+}
+
+void launch_ring_means(const PsfBankArgs& a, cudaStream_t s) {
+    ring_sums_kernel<<<tall_grid(a), dim3(32, 8), 0, s>>>(a);
+    ring_mean_kernel<<<a.B, 256, 0, s>>>(a);
 }
 
 void launch_support(const PsfBankArgs& a, cudaStream_t s) { support_kernel<<<a.B, 256, 0, s>>>(a); }
