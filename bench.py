@@ -254,8 +254,8 @@ class Clocks:
 # cold workload (profiles/), by transform form
 MEASURED_TRAFFIC_UHD31 = {
     "own": {"frame_rows": 156.4e6, "frame_cols": 322.9e6, "frame_inverse": 352.6e6},
-    "chosen": {"shape_stats": 209.3e6, "frame_rows": 155.6e6, "frame_cols": 169.5e6, "frame_inverse": 285.3e6,
-               "resample": 81.5e6, "crop_sum": 130.8e6, "combine": 136.4e6},
+    "chosen": {"frame_rows": 155.6e6, "frame_cols": 169.5e6, "frame_inverse": 285.3e6,
+               "resample": 86.4e6, "crop_sum": 130.8e6, "combine": 136.4e6},
 }
 
 
@@ -277,7 +277,9 @@ def algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, out_pixels, B=0, K=0, h16
     canvas = 4 * B * K * K
     Kp = K + (K & 1)
     return {
-        # bank passes over the B canvases of K x K floats (read + write)
+        # bank passes over the B canvases of K x K floats (written once by the
+        # lambda-rescale, which also takes the shaping statistics; read by the
+        # crop sums and the combination)
         "resample": canvas, "shape_stats": 2 * canvas, "crop_sum": canvas,
         "combine": canvas + 4 * n_ker * K * K,
         "kspec_rows": 4 * n_ker * K * K + 8 * n_ker * Kp * bins,
