@@ -664,7 +664,8 @@ struct CombineBin {
     int rho;                   // crop radius
 };
 
-template <bool SPLIT>
+// NK: kernel sets of the Physical look (1 Mono, 3 spectral; 4 covers any n_ker <= 4).
+template <bool SPLIT, int NK>
 __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
     __shared__ float inv[kMaxBins], inv_s3[kMaxBins], inv_core[kMaxBins], inv_struct[kMaxBins];
     __shared__ float ext[kMaxBins], fade[kMaxBins], start[kMaxBins];
@@ -704,7 +705,9 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
         const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
         const float rad = sqrtf(dx * dx + dy * dy);
         if constexpr (!SPLIT) {
-            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            float acc[NK];
+#pragma unroll
+            for (int k = 0; k < NK; ++k) acc[k] = 0.0f;
             for (int b0 = 0; b0 < B; b0 += kU) {
                 float v[kU];
 #pragma unroll
@@ -718,12 +721,12 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
                         const CombineBin& cb = bin[b0 + u];
                         const float f = v[u] * taper_weight(rad, cb.ext, cb.fade, cb.start);
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) acc[k] += cb.w[k] * f;
+                        for (int k = 0; k < NK; ++k) acc[k] += cb.w[k] * f;
                     }
                 }
             }
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
+            for (int k = 0; k < NK; ++k)
                 if (k < a.n_ker) a.out[k * plane + idx] = acc[k];
         } else {
         // Split: core = mean * taper / s_core, structure = max(0, shaped *
@@ -982,8 +985,11 @@ void launch_split_sums(const PsfBankArgs& a, cudaStream_t s) {
 }
 
 void launch_combine(const CombineArgs& a, cudaStream_t s) {
-    if (a.split) combine_kernel<true><<<canvas_grid(a.bank, 1), dim3(32, 8), 0, s>>>(a);
-    else combine_kernel<false><<<canvas_grid(a.bank, 1), dim3(32, 8), 0, s>>>(a);
+    const dim3 grid = canvas_grid(a.bank, 1), block(32, 8);
+    if (a.split) combine_kernel<true, 4><<<grid, block, 0, s>>>(a);
+    else if (a.n_ker == 1) combine_kernel<false, 1><<<grid, block, 0, s>>>(a);
+    else if (a.n_ker == 3) combine_kernel<false, 3><<<grid, block, 0, s>>>(a);
+    else combine_kernel<false, 4><<<grid, block, 0, s>>>(a);
 }
 
 void launch_export(const PsfBankArgs& a, const int64_t* offsets_dev, float* out, cudaStream_t s) {
