@@ -173,19 +173,16 @@ __global__ void __launch_bounds__(256) dft_basis_kernel(DftBasisArgs a) {
     *reinterpret_cast<uint32_t*>(a.lo + off) = lo;
 }
 
-// Pupil field images of wavelength blockIdx.y: row m (pupil row row_lo + m)
+// Pupil field images of wavelength blockIdx.z: row m (pupil row row_lo + m)
 // over K-chunk c (pupil column col_lo + 32 c + q), the field
 // amplitude * exp(i 2 pi phase) as the row transform embeds it
 // (psf_rows_kernel; LensDiffCpuReference.cpp:831-845).
+// grid (mt_rows * 128 / 8, kc_rows, B), block (32, 8): lane q of warp row m
+// of K-chunk c (one 128-byte image row per warp).
 __global__ void __launch_bounds__(256) pupil_field_kernel(PsfBankArgs a, DftPlan d) {
-    const int b = blockIdx.y;
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int rows = d.mt_rows * kTileM;
-    const int64_t per_chunk = static_cast<int64_t>(rows) * 32;
-    if (i >= per_chunk * d.kc_rows) return;
-    const int c = static_cast<int>(i / per_chunk);
-    const int rem = static_cast<int>(i - static_cast<int64_t>(c) * per_chunk);
-    const int m = rem >> 5, q = rem & 31;
+    const int b = blockIdx.z;
+    const int c = blockIdx.y;
+    const int m = blockIdx.x * 8 + threadIdx.y, q = threadIdx.x;
     const int np = a.pupil.size;
     const int y = a.row_lo + m, x = d.col_lo + c * 32 + q;
     float fr = 0.0f, fi = 0.0f;
@@ -397,9 +394,9 @@ void launch_dft_basis(const DftBasisArgs& a, cudaStream_t s) {
 }
 
 void launch_pupil_field(const PsfBankArgs& a, const DftPlan& d, cudaStream_t s) {
-    const int64_t total = static_cast<int64_t>(d.mt_rows) * kTileM * 32 * d.kc_rows;
-    if (total <= 0) return;
-    pupil_field_kernel<<<dim3(static_cast<unsigned>((total + 255) / 256), a.B), 256, 0, s>>>(a, d);
+    if (d.mt_rows <= 0 || d.kc_rows <= 0) return;
+    pupil_field_kernel<<<dim3(static_cast<unsigned>(d.mt_rows * kTileM / 8), static_cast<unsigned>(d.kc_rows), a.B),
+                         dim3(32, 8), 0, s>>>(a, d);
 }
 
 void launch_dft_gemm(const DftBatchArgs& g, cudaStream_t s) {
