@@ -326,14 +326,20 @@ def run_serving(args):
     srv = LensDiffServer(0, slots=args.slots, hbm_budget_bytes=150 * 10 ** 9)
     sweep = []
     lens = new_lens()
-    # warm-up: every size once with the starting lens
-    outs = {sz: torch.empty_like(frames[sz]).pin_memory() for sz in sizes}
-    for sz in sizes:
-        p = lens.copy(maxKernelRadiusPx=S.radius_percent(radius[sz], sz[1]))
-        t, _ = srv.submit(frames[sz].numpy(), p, outs[sz].numpy())
-        st, _ = srv.wait(t, 300.0)
-        if not st.ok:
-            raise RuntimeError(f"serving warm-up failed: {st}")
+    # warm-up, as a server would start: every slot renders every size once,
+    # largest first (each slot's buffers reach their final size before the
+    # sweep); one lens per slot, submitted together so they spread over the slots
+    outs = [{sz: torch.empty_like(frames[sz]).pin_memory() for sz in sizes} for _ in range(args.slots)]
+    for sz in sorted(sizes, key=lambda z: -z[0] * z[1]):
+        ts = []
+        for k in range(args.slots):
+            p = lens.copy(maxKernelRadiusPx=S.radius_percent(radius[sz], sz[1]),
+                          phaseDefocus=lens.phaseDefocus + 1e-3 * k)
+            ts.append(srv.submit(frames[sz].numpy(), p, outs[k][sz].numpy())[0])
+        for t in ts:
+            st, _ = srv.wait(t, 300.0)
+            if not st.ok:
+                raise RuntimeError(f"serving warm-up failed: {st}")
     pool = [{sz: torch.empty_like(frames[sz]).pin_memory() for sz in sizes} for _ in range(2 * args.slots)]
     for rate in [float(r) for r in args.rates.split(",")]:
         srv.reset_stats()

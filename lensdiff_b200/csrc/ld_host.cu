@@ -755,10 +755,24 @@ void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthI
 // ---------------------------------------------------------------------------
 // first-zero calibration of the clear circle (one host sync per (N_p, S))
 // ---------------------------------------------------------------------------
+// The first-zero radius is a function of (N_p, S) alone: every context of the
+// process (a server's slots among them) shares it, so each pair is calibrated
+// (and the host synchronised for it) once per process.
+std::mutex g_r0_mu;
+std::map<std::pair<int, int>, float> g_r0;
+
 float first_zero(ld_ctx* c, int np, int S, cudaStream_t s) {
     auto key = std::make_pair(np, S);
     auto it = c->r0_cache.find(key);
     if (it != c->r0_cache.end()) return it->second;
+    {
+        std::lock_guard<std::mutex> lock(g_r0_mu);
+        auto g = g_r0.find(key);
+        if (g != g_r0.end()) {
+            c->r0_cache[key] = g->second;
+            return g->second;
+        }
+    }
     ld_params cp{};
     cp.pupil_resolution = np;
     PsfBankArgs a{};
@@ -835,6 +849,10 @@ float first_zero(ld_ctx* c, int np, int S, cudaStream_t s) {
     }
     c->launches += 5;
     c->r0_cache[key] = r0;
+    {
+        std::lock_guard<std::mutex> lock(g_r0_mu);
+        g_r0[key] = r0;
+    }
     return r0;
 }
 
