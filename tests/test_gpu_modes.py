@@ -315,6 +315,44 @@ def test_split_look_matches_reference(cache, kw):
     assert rel_err(phys, ref, ref[..., :3].max()) > 20 * OUT_TOL  # the look matters here
 
 
+def test_split_render_after_physical_render_of_the_same_lens(cache):
+    """A Physical render builds the bank with the shaping statistics taken in
+    the lambda-rescale (anisotropy gain 1), without the ring means; a Split
+    render of the same lens then reuses that bank and computes its ring means
+    from the canvas."""
+    from lensdiff_b200.types import LensDiffFftForm, LensDiffLookMode
+    _reference_available()
+    src = S.make_frame(224, 144, 20, 1.0, 80.0, seed=53)
+    for form in (LensDiffFftForm.OwnFp32, LensDiffFftForm.OwnChosen):
+        p = _lens(phaseDefocus=0.23, coreGain=0.8, structureGain=1.4, coreShoulder=2.0, structureShoulder=0.5,
+                  fftForm=form)
+        phys = _render(cache, with_matrices(p), src)
+        ref_phys = R.render(p, src)
+        assert rel_err(phys, ref_phys, ref_phys[..., :3].max()) < OUT_TOL, form
+        q = p.copy(lookMode=LensDiffLookMode.Split)
+        out = _render(cache, with_matrices(q), src)
+        ref = R.render(q, src)
+        assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL, form
+
+
+@pytest.mark.parametrize("emphasis", [0.0, 0.3, 1.0])
+def test_bank_with_anisotropy_emphasis_matches_reference(cache, emphasis):
+    """Gain 1 (emphasis 0) takes the fused path; gains 2.2 and 5 the separate
+    shaping pass (reshapeAnisotropy, LensDiffCpuReference.cpp:1122-1134)."""
+    from lensdiff_b200.types import LensDiffFftForm
+    from tests.helpers import PSF_TOL
+    _reference_available()
+    p = _lens(anisotropyEmphasis=emphasis, spectralMode=LensDiffSpectralMode.Spectral5)
+    _, ref, _, _, _ = R.bank(p)
+    for form in (LensDiffFftForm.OwnFp32, LensDiffFftForm.OwnChosen):
+        wls, kernels, st = cache.export_psf_bank(p.copy(fftForm=form), torch.cuda.current_stream())
+        assert st.ok, st
+        assert len(kernels) == len(ref)
+        for k, r in zip(kernels, ref):
+            assert k.shape == r.shape, (form, k.shape, r.shape)
+            assert rel_err(k, r, r.max()) < PSF_TOL, form
+
+
 def test_split_look_with_field_zones_and_chosen_form(cache):
     from lensdiff_b200.types import LensDiffFftForm, LensDiffLookMode
     _reference_available()
