@@ -36,6 +36,7 @@ import multiprocessing as mp
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -203,7 +204,9 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        # LD_CLOCKS_DIR keeps the raw samples; by default they go to the temp directory
+        self.path = os.path.join(os.environ.get("LD_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"clocks_bench_{os.getpid()}.csv")
 
     def start(self):
         try:
