@@ -17,6 +17,8 @@
 // overwritten stage by stage: resampled value -> shaped value (shape_stats) ->
 // shaped * taper inside the crop box, 0 outside (crop_sum); the final,
 // normalised kernel is that value / (s3 * s4).
+#include <climits>
+
 #include "ld_internal.h"
 
 namespace ld {
@@ -694,9 +696,57 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
     const int x = blockIdx.x * kTile + threadIdx.x;
     const int K = a.bank.K, R = a.bank.R;
     const size_t plane = static_cast<size_t>(K) * K;
-    constexpr int kU = 8;
+    if constexpr (!SPLIT) {
+        // four pixels per thread (rows 8 apart) share each wavelength's bin
+        // constants; per pixel the wavelengths are summed in order, as below
+        constexpr int kP = kTile / 8;
+        float acc[kP][NK], rad[kP];
+        int aix[kP];
+        size_t idx[kP];
+#pragma unroll
+        for (int p = 0; p < kP; ++p) {
+            const int y = blockIdx.y * kTile + threadIdx.y + 8 * p;
+            const bool in = x < K && y < K;
+            const int ix = x - R, iy = y - R;
+            aix[p] = in ? max(abs(ix), abs(iy)) : INT_MAX;  // inside the crop box of b iff aix <= rho[b]
+            const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
+            rad[p] = sqrtf(dx * dx + dy * dy);
+            idx[p] = in ? static_cast<size_t>(y) * K + x : 0;
+#pragma unroll
+            for (int k = 0; k < NK; ++k) acc[p][k] = 0.0f;
+        }
+#pragma unroll 2
+        for (int b = 0; b < B; ++b) {
+            const CombineBin& cb = bin[b];
+            const int rho_b = cb.rho;
+            const float* cv = a.bank.canvas + b * plane;
+            float v[kP];
+#pragma unroll
+            for (int p = 0; p < kP; ++p) v[p] = aix[p] <= rho_b ? __ldg(cv + idx[p]) : 0.0f;
+            const float ext_b = cb.ext, fade_b = cb.fade, start_b = cb.start;
+            float w[NK];
+#pragma unroll
+            for (int k = 0; k < NK; ++k) w[k] = cb.w[k];
+#pragma unroll
+            for (int p = 0; p < kP; ++p) {
+                if (v[p] != 0.0f) {  // else outside the crop box, or a zero kernel value
+                    const float f = v[p] * taper_weight(rad[p], ext_b, fade_b, start_b);
+#pragma unroll
+                    for (int k = 0; k < NK; ++k) acc[p][k] += w[k] * f;
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < kP; ++p) {
+            if (aix[p] == INT_MAX) continue;
+#pragma unroll
+            for (int k = 0; k < NK; ++k)
+                if (k < a.n_ker) a.out[k * plane + idx[p]] = acc[p][k];
+        }
+        return;
+    }
 #pragma unroll 1
-    for (int i = 0; i < kTile / 8; ++i) {
+    for (int i = 0; i < kTile / 8; ++i) {  // Split look
         const int y = blockIdx.y * kTile + threadIdx.y + 8 * i;
         if (x >= K || y >= K) continue;
         const size_t idx = static_cast<size_t>(y) * K + x;
@@ -704,31 +754,7 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
         const int aix = max(abs(ix), abs(iy));  // inside the crop box of b iff aix <= rho[b]
         const float dx = static_cast<float>(ix), dy = static_cast<float>(iy);
         const float rad = sqrtf(dx * dx + dy * dy);
-        if constexpr (!SPLIT) {
-            float acc[NK];
-#pragma unroll
-            for (int k = 0; k < NK; ++k) acc[k] = 0.0f;
-            for (int b0 = 0; b0 < B; b0 += kU) {
-                float v[kU];
-#pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    const int b = b0 + u;
-                    v[u] = (b < B && aix <= bin[b].rho) ? __ldg(a.bank.canvas + b * plane + idx) : 0.0f;
-                }
-#pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    if (v[u] != 0.0f) {  // else outside the crop box, or a zero kernel value
-                        const CombineBin& cb = bin[b0 + u];
-                        const float f = v[u] * taper_weight(rad, cb.ext, cb.fade, cb.start);
-#pragma unroll
-                        for (int k = 0; k < NK; ++k) acc[k] += cb.w[k] * f;
-                    }
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < NK; ++k)
-                if (k < a.n_ker) a.out[k * plane + idx] = acc[k];
-        } else {
+        {
         // Split: core = mean * taper / s_core, structure = max(0, shaped *
         // taper / s3 - mean * taper) / s_struct
         const int ring = min(R, static_cast<int>(roundf(rad)));
