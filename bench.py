@@ -53,6 +53,9 @@ METRIC = "UHD frames/s (31-wavelength PSF bank, FFT convolution, composite)"
 
 FFT_FORMS = {"own": 0, "chosen": 1, "cufft": 2}
 FORM_NAMES = {"own": "own_fp32", "chosen": "own_chosen", "cufft": "cufft"}
+# the arithmetic each form computes in
+FORM_DTYPES = {"own": "f32", "cufft": "f32",
+               "chosen": "f32 frame math; bf16x3-split psf windows (f32 accumulate); fp16 frame spectra"}
 
 
 def parse():
@@ -77,6 +80,8 @@ def parse():
     ap.add_argument("--slots", type=int, default=4, help="server slots of --serving")
     ap.add_argument("--no-comparators", action="store_true",
                     help="skip timing the other transform chains on the same workload")
+    ap.add_argument("--no-error-check", action="store_true",
+                    help="skip stating each form's error against the FP64 oracle (outside the timed regions)")
     return ap.parse_args()
 
 
@@ -249,17 +254,26 @@ class Clocks:
                 "samples": len(sms)}
 
 
-# DRAM bytes per launch (read + write) of the frame kernels on the UHD
-# 31-wavelength workload, from the one-pass ncu capture summarised in
-# profiles/frame_*_hd16.md (writes still resident in L2 at kernel end are not
-# counted by DRAM counters).
-# DRAM read + write per launch, one-pass ncu captures of the UHD 31-wavelength
-# cold workload (profiles/), by transform form
-MEASURED_TRAFFIC_UHD31 = {
-    "own": {"frame_rows": 156.4e6, "frame_cols": 322.9e6, "frame_inverse": 352.6e6},
-    "chosen": {"frame_rows": 155.6e6, "frame_cols": 169.5e6, "frame_inverse": 285.3e6,
-               "resample": 86.4e6, "crop_sum": 130.8e6, "combine": 136.4e6},
-}
+# DRAM read + write per launch of the UHD 31-wavelength cold workload's
+# kernels, by transform form, from one ncu capture of the kernel sources whose
+# digest is KERNEL_SOURCES_SHA (sources_digest()).  Any other revision of the
+# kernels reports traffic null: a figure measured on other code says nothing
+# about this code.
+TRAFFIC_SOURCES_SHA = "unmeasured"
+MEASURED_TRAFFIC_UHD31 = {}
+
+
+def sources_digest() -> str:
+    """sha256 (first 16 hex digits) of the CUDA sources of the library."""
+    import hashlib
+
+    csrc = os.path.join(ROOT, "lensdiff_b200", "csrc")
+    h = hashlib.sha256()
+    for name in sorted(os.listdir(csrc)):
+        if name.endswith((".cu", ".cuh", ".h")):
+            with open(os.path.join(csrc, name), "rb") as f:
+                h.update(name.encode() + b"\0" + f.read())
+    return h.hexdigest()[:16]
 
 
 # ---------------------------------------------------------------------------
@@ -295,6 +309,35 @@ def algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, out_pixels, B=0, K=0, h16
 
 SERVING_SIZES = [((1920, 1080), 0.4, 256), ((2048, 1080), 0.2, 256), ((3840, 2160), 0.3, 512),
                  ((6144, 3160), 0.1, 750)]  # (frame, share, kernel radius px; 4R keeps the PSF grid 5-smooth)
+
+
+def error_check(args, p, frame, cache, stream, dev, forms):
+    """Error of one frame rendered in each of `forms` (FORM_NAMES values)
+    against the FP64 oracle (oracle/check.py), with the workload's own
+    parameters.  The checker runs on the host after the timed regions."""
+    import torch
+    from lensdiff_b200.backend import image_request
+    from oracle import check as C
+
+    ref = C.OracleResult(p, frame)
+    src = torch.from_numpy(frame).to(dev)
+    dst = torch.empty_like(src)
+    req = image_request(src, dst, stream, frame_short_side=p.frameShortSidePx)
+    by_name = {v: k for k, v in FORM_NAMES.items()}
+    out = {}
+    for name in forms:
+        pp = p.copy(fftForm=FFT_FORMS[by_name[name]])
+        with torch.cuda.stream(stream):
+            st = cache.render(req, pp)
+        if not st.ok:
+            raise RuntimeError(f"error-check render failed: {st}")
+        _, kernels, st2 = cache.export_psf_bank(pp, stream)
+        if not st2.ok:
+            raise RuntimeError(f"error-check bank export failed: {st2}")
+        torch.cuda.synchronize(dev)
+        rep = C.error_report(kernels, dst.cpu().numpy(), ref)
+        out[name] = {k: (float(f"{v:.3e}") if isinstance(v, float) else v) for k, v in rep.items()}
+    return out
 
 
 def run_serving(args):
@@ -677,10 +720,17 @@ def main():
     dominant = max(stage, key=lambda k: stage[k][0])
     dom_ms, dom_n = stage[dominant]
     roofline = None
+    traffic_ok = args.workload == "uhd31" and args.bank == "cold" and sources_digest() == TRAFFIC_SOURCES_SHA
+    # every HBM-bound kernel's fraction of the measured peak (the frame chain's
+    # fused FFT kernels first among them)
+    kernel_frac = {}
+    for name, (ms, n) in stage.items():
+        if name in alg and n and ms > 0:
+            kernel_frac[name] = round(alg[name] / (ms / n / 1000.0) / 1e9 / peak, 4)
     if dominant in alg and dom_n:
         per_launch_ms = dom_ms / dom_n
         achieved = alg[dominant] / (per_launch_ms / 1000.0) / 1e9
-        traffic = MEASURED_TRAFFIC_UHD31.get(args.fft_form, {}).get(dominant) if args.workload == "uhd31" else None
+        traffic = MEASURED_TRAFFIC_UHD31.get(args.fft_form, {}).get(dominant) if traffic_ok else None
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                     "algorithmic_bytes_per_launch": alg[dominant], "launch_ms": per_launch_ms}
@@ -731,6 +781,12 @@ def main():
         if cache.check_device_errors():
             raise RuntimeError("device error word set by a comparator chain")
 
+    # ---- error against the FP64 oracle (checker only; outside every timed
+    # region): one frame of the workload's own parameters in each timed form
+    errors = None
+    if rank == 0 and not args.no_error_check:
+        errors = error_check(args, p, frame, cache, stream, dev, list(comparators) + [FORM_NAMES[args.fft_form]])
+
     # ---- CPU baseline (rank 0, N=1) ----------------------------------------
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -747,7 +803,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "p50_ms": p50, "p99_ms": p99,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": FORM_DTYPES[args.fft_form],
             "data": "synthetic (seeded generator; no public dataset exists)",
             "config": {"workload": args.workload, "frame": [W, H], "wavelengths": st0.wavelength_count,
                        "pupil": st0.pupil_size, "psf": st0.raw_psf_size,
@@ -758,11 +814,16 @@ def main():
             "gpu_launches": launches_per_frame[0] * args.steps,
             "stage_ms_per_frame": stage_ms,
             "roofline": roofline,
+            "kernel_hbm_frac": kernel_frac,
+            "error": errors.get(FORM_NAMES[args.fft_form]) if errors else None,
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "comparators": comparators,
         }
+        if errors:
+            for name, c in comparators.items():
+                c["error"] = errors.get(name)
         print(json.dumps(line))
     cache.close()
     if ws > 1:

@@ -337,9 +337,13 @@ void ld_server_reset_stats(ld_server* server);
  * reservation).  No context and no allocation: the scratch is a 12 MiB
  * file-scope device array that every GPU loading the library holds until
  * exit.  Limit: pupil <= 512 and PSF grid <= 1024 (maximum kernel radius
- * <= 256 px); larger requests return LD_ERR_ARG.  All calls on a device share
- * the array, so calls that overlap on the GPU race; the first call on a
- * device resolves the array's address and should precede any stream capture.
+ * <= 256 px); larger requests return LD_ERR_ARG.  A PSF grid whose size has
+ * a prime factor above 5 (e.g. 4R with R = 131) returns LD_ERR_UNSUPPORTED
+ * "fft-length-not-5-smooth"; the aperture checks and their codes are those of
+ * ld_raw_psf.  All calls on a device share the array, so calls that overlap
+ * on the GPU race.  The array's address is looked up in the calling thread's
+ * current CUDA context on every call outside a stream capture; the first call
+ * in a context must precede any stream capture in it.
  * This entry point has no counterpart in the reference. */
 int ld_raw_psf_noalloc(const ld_params* params, int wavelength_index, float* psf_out_device, void* stream,
                        ld_status* status);

@@ -20,10 +20,19 @@
 // One library context per CUDA device serves every effect instance; the
 // device-resident PSF-bank cache lives in that context (the plugin's
 // LensDiffPsfBankCache is left untouched unless a caller needs host kernels).
+//
+// Environment switches, read once per process in the style of the reference
+// backend's LENSDIFF_CUDA_* variables (LensDiffCuda.cu:462-517):
+//   LENSDIFF_B200_FFT_FORM       chosen (default): tensor-core PSF windows and
+//                                FP16 frame spectra; fp32: the hand-written FP32
+//                                chain; cufft: the cuFFT comparator chain.
+//   LENSDIFF_B200_HBM_BUDGET_MB  device memory the library context may hold
+//                                (0 or unset: no budget).
 #include "LensDiffSpectrum.h"
 #include "LensDiffTypes.h"
 #include "lensdiff_b200.h"
 
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -33,6 +42,24 @@
 #include <cuda_runtime.h>
 
 namespace {
+
+// LENSDIFF_B200_FFT_FORM; an unknown value selects the default form.
+int32_t fftFormFromEnvironment() {
+    static const int32_t form = [] {
+        const char* v = std::getenv("LENSDIFF_B200_FFT_FORM");
+        if (v != nullptr && std::strcmp(v, "fp32") == 0) return static_cast<int32_t>(LD_FFT_OWN_FP32);
+        if (v != nullptr && std::strcmp(v, "cufft") == 0) return static_cast<int32_t>(LD_FFT_CUFFT);
+        return static_cast<int32_t>(LD_FFT_OWN_CHOSEN);
+    }();
+    return form;
+}
+
+std::size_t hbmBudgetFromEnvironment() {
+    const char* v = std::getenv("LENSDIFF_B200_HBM_BUDGET_MB");
+    if (v == nullptr) return 0;
+    const long long mb = std::atoll(v);
+    return mb > 0 ? static_cast<std::size_t>(mb) << 20 : 0;
+}
 
 std::mutex& contextMutex() {
     static std::mutex m;
@@ -50,7 +77,7 @@ ld_ctx* contextForCurrentDevice(std::string* error) {
     auto it = contexts.find(device);
     if (it != contexts.end()) return it->second;
     ld_ctx* ctx = nullptr;
-    if (ld_create(&ctx, device, 0) != LD_OK) {
+    if (ld_create(&ctx, device, hbmBudgetFromEnvironment()) != LD_OK) {
         if (error) *error = "lensdiff-b200-context-create-failed";
         return nullptr;
     }
@@ -149,7 +176,7 @@ ld_params toParams(const LensDiffParams& p) {
     o.core_shoulder = p.coreShoulder;
     o.structure_shoulder = p.structureShoulder;
     o.rgb_mode = LD_RGB_FROM_CALLER;
-    o.fft_form = LD_FFT_OWN_FP32;
+    o.fft_form = fftFormFromEnvironment();
     return o;
 }
 

@@ -2688,6 +2688,7 @@ int run_guarded(ld_ctx* ctx, ld_status* st, const std::function<void()>& fn) {
 namespace ld {
 bool host_factor_plan(int n, bool allow25, FftPlan* plan) { return factor_plan(n, allow25, plan); }
 PupilParams host_pupil_params(const ld_params& p) { return pupil_params(p, false); }
+void host_pupil_geometry(PsfBankArgs& a, const ld_params& p) { pupil_geometry(a, p, false); }
 PhaseCoeffs host_phase_for_wavelength(const ld_params& p, float wavelength) {
     return phase_for_wavelength(p, wavelength);
 }

@@ -19,21 +19,28 @@
 //     Calls whose work overlaps on the GPU (different streams, or different
 //     host threads without ordering) race on the array and must be serialised
 //     by the caller;
-//   * the first call on a device resolves the array's device address with
-//     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture.
+//   * the array's device address belongs to the CUDA context that is current
+//     when the call is made (the device's primary context for runtime-API
+//     callers, or a context the host pushed itself).  Every call made outside
+//     a stream capture looks the address up again with cudaGetSymbolAddress
+//     and remembers it for that context; a call whose stream is being captured
+//     uses the remembered address, so the first call in a context must come
+//     before any stream capture in it.  After cudaDeviceReset the next call
+//     outside a capture looks the address up afresh.
 #include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "../../include/lensdiff_b200.h"
 #include "ld_internal.h"
 
 namespace ld {
 bool host_factor_plan(int n, bool allow25, FftPlan* plan);
-PupilParams host_pupil_params(const ld_params& p);
+void host_pupil_geometry(PsfBankArgs& a, const ld_params& p);
 PhaseCoeffs host_phase_for_wavelength(const ld_params& p, float wavelength);
 std::vector<float> host_wavelengths(const ld_params& p);
 void host_sizes(const ld_params& p, int* np, int* S, int* R);
@@ -46,35 +53,86 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = 12u << 20;  // 12 MiB
 constexpr int kNoAllocMaxPsf = 1024;                // PSF grid S
 constexpr int kNoAllocMaxPupil = 512;               // pupil raster N_p
-constexpr int kMaxDevices = 64;
+constexpr int kMaxContexts = 64;
 
 // The scratch.  In host code this name is only a host-side stand-in: the
 // device address comes from cudaGetSymbolAddress (scratch_address below).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+// Remembered scratch addresses, one per CUDA context.
+struct ContextAddress {
+    CUcontext ctx;
+    unsigned char* addr;
+};
 std::mutex g_addr_mu;
-unsigned char* g_addr[kMaxDevices] = {};
+ContextAddress g_addr[kMaxContexts] = {};
+int g_addr_n = 0;
 
-// Device address of the scratch on the current device (set-up on first use).
-int scratch_address(unsigned char** out, std::string* stage) {
+// cuCtxGetCurrent through the runtime's driver entry-point lookup, so the
+// library needs no link-time dependency on the driver library.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<CtxGetCurrentFn>(nullptr);
+        }
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    return fn;
+}
+
+// Device address of the scratch in the current context, for work on stream s.
+int scratch_address(cudaStream_t s, unsigned char** out, std::string* stage) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         *stage = "no-alloc-no-current-device";
         return LD_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lock(g_addr_mu);
-    if (g_addr[dev] == nullptr) {
-        void* p = nullptr;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        cap = cudaStreamCaptureStatusActive;  // unknown: do not call set-up APIs
+    }
+    void* p = nullptr;
+    if (cap == cudaStreamCaptureStatusNone) {
+        // also makes the device's primary context current when none is
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || p == nullptr) {
             cudaGetLastError();
             *stage = std::string("no-alloc-symbol-address: ") + cudaGetErrorString(e);
             return LD_ERR_CUDA;
         }
-        g_addr[dev] = static_cast<unsigned char*>(p);
     }
-    *out = g_addr[dev];
+    CtxGetCurrentFn get = ctx_get_current();
+    CUcontext ctx = nullptr;
+    if (get == nullptr || get(&ctx) != CUDA_SUCCESS || ctx == nullptr) {
+        *stage = "no-alloc-no-current-context";
+        return LD_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lock(g_addr_mu);
+    int slot = -1;
+    for (int i = 0; i < g_addr_n; ++i)
+        if (g_addr[i].ctx == ctx) slot = i;
+    if (cap == cudaStreamCaptureStatusNone) {
+        if (slot < 0) {
+            if (g_addr_n == kMaxContexts) {
+                *stage = "no-alloc-too-many-contexts";
+                return LD_ERR_CUDA;
+            }
+            slot = g_addr_n++;
+            g_addr[slot].ctx = ctx;
+        }
+        g_addr[slot].addr = static_cast<unsigned char*>(p);
+    } else if (slot < 0) {
+        *stage = "no-alloc-first-call-inside-stream-capture";
+        return LD_ERR_ARG;
+    }
+    *out = g_addr[slot].addr;
     return LD_OK;
 }
 
@@ -114,10 +172,13 @@ extern "C" int ld_raw_psf_noalloc(const ld_params* params, int wavelength_index,
         return LD_ERR_ARG;
     }
     const ld_params& p = *params;
-    if (p.aperture_mode == LD_APERTURE_CUSTOM || p.aperture_mode < LD_APERTURE_CIRCLE ||
-        p.aperture_mode > LD_APERTURE_SNOWFLAKE) {
-        set_stage(st, LD_ERR_UNSUPPORTED, "unsupported-aperture-mode");
+    if (p.aperture_mode == LD_APERTURE_CUSTOM) {
+        set_stage(st, LD_ERR_UNSUPPORTED, "unsupported-custom-aperture");
         return LD_ERR_UNSUPPORTED;
+    }
+    if (p.aperture_mode < LD_APERTURE_CIRCLE || p.aperture_mode > LD_APERTURE_SNOWFLAKE) {
+        set_stage(st, LD_ERR_ARG, "invalid-aperture-mode");
+        return LD_ERR_ARG;
     }
     int np = 0, S = 0, R = 0;
     host_sizes(p, &np, &S, &R);
@@ -141,23 +202,7 @@ extern "C" int ld_raw_psf_noalloc(const ld_params* params, int wavelength_index,
         return LD_ERR_UNSUPPORTED;
     }
     PsfBankArgs a{};
-    a.pupil = host_pupil_params(p);
-    a.base_phase = host_phase_for_wavelength(p, 550.0f);
-    a.base_phase.c[4] = 0.0f;  // defocus is carried per wavelength
-    int lo = np, hi = 0;       // pupil rows that can be non-zero
-    for (int y = 0; y < np; ++y) {
-        const float ny = ((static_cast<float>(y) + 0.5f) / static_cast<float>(np) - 0.5f) * 2.0f;
-        if (std::abs(ny - a.pupil.decy) <= 0.8601f) {
-            lo = std::min(lo, y);
-            hi = std::max(hi, y + 1);
-        }
-    }
-    if (hi <= lo) {
-        lo = 0;
-        hi = 1;
-    }
-    a.row_lo = lo;
-    a.row_n = hi - lo;
+    host_pupil_geometry(a, p);  // pupil parameters, base phase, rows that can be non-zero
     // scratch layout: twiddles | pupil pre-pass | row-pass output | info | sums
     const size_t o_pre = align256(static_cast<size_t>(S) * sizeof(float2));
     const size_t o_rows = o_pre + align256(static_cast<size_t>(np) * np * sizeof(float4));
@@ -168,14 +213,21 @@ extern "C" int ld_raw_psf_noalloc(const ld_params* params, int wavelength_index,
         set_stage(st, LD_ERR_ARG, "exceeds-no-alloc-scratch");
         return LD_ERR_ARG;
     }
+    // an error left pending by earlier work on this thread is reported as
+    // such, not as a failure of these launches
+    const cudaError_t pending = cudaGetLastError();
+    if (pending != cudaSuccess) {
+        set_stage(st, LD_ERR_CUDA, std::string("no-alloc-pending-error-before-call: ") + cudaGetErrorString(pending));
+        return LD_ERR_CUDA;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned char* base = nullptr;
     std::string stage;
-    const int rc = scratch_address(&base, &stage);
+    const int rc = scratch_address(s, &base, &stage);
     if (rc != LD_OK) {
         set_stage(st, rc, stage);
         return rc;
     }
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     float2* tw = reinterpret_cast<float2*>(base);
     plan.tw = tw;
     a.pupil_pre = reinterpret_cast<float4*>(base + o_pre);

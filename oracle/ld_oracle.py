@@ -26,6 +26,31 @@ from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
+try:  # the same FP64 transforms, spread over the host's cores
+    import os as _os
+
+    import scipy.fft as _sfft
+
+    _WORKERS = max(1, _os.cpu_count() or 1)
+
+    def _fft2(x):
+        return _sfft.fft2(x, workers=_WORKERS)
+
+    def _rfft2(x, s=None):
+        return _sfft.rfft2(x, s, workers=_WORKERS)
+
+    def _irfft2(x, s):
+        return _sfft.irfft2(x, s, workers=_WORKERS)
+except ImportError:  # numpy's pocketfft, one core
+    def _fft2(x):
+        return np.fft.fft2(x)
+
+    def _rfft2(x, s=None):
+        return np.fft.rfft2(x, s)
+
+    def _irfft2(x, s):
+        return np.fft.irfft2(x, s)
+
 F = np.float32
 K_PI_F = F(3.14159265358979323846)  # kPi, LensDiffCpuReference.cpp:25
 GRAY18 = F(0.18)
@@ -307,7 +332,7 @@ def raw_psf(amplitude: np.ndarray, phase: Optional[np.ndarray], size: int,
         field = a * np.exp(1j * ang)
     grid = np.zeros((size, size), dtype=np.complex128)
     grid[off:off + n, off:off + n] = field[: size - off, : size - off]
-    spec = np.fft.fft2(grid)
+    spec = _fft2(grid)
     inten = spec.real ** 2 + spec.imag ** 2
     inten = fft_shift_square(inten)
     if normalize:
@@ -684,7 +709,7 @@ def convolve(plane: np.ndarray, kernel: np.ndarray) -> np.ndarray:
     ys = (np.arange(k) - c) % ph
     xs = (np.arange(k) - c) % pw
     kg[np.ix_(ys, xs)] = kernel
-    out = np.fft.irfft2(np.fft.rfft2(plane, (ph, pw)) * np.fft.rfft2(kg), (ph, pw))[:h, :w]
+    out = _irfft2(_rfft2(plane, (ph, pw)) * _rfft2(kg), (ph, pw))[:h, :w]
     return np.maximum(0.0, out)
 
 

@@ -11,7 +11,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libldref.so")
-REF_ROOT = "/root/reference"
+# The reference project's source tree, named by the environment (the build
+# script sets it where the sources are present; nothing here needs it at run time).
+REF_ROOT = os.environ.get("LENSDIFF_REFERENCE_ROOT", "")
 
 _lib: Optional[ctypes.CDLL] = None
 
@@ -20,7 +22,7 @@ def build(force: bool = False) -> bool:
     """Compiles the reference shim when the reference sources are present."""
     if os.path.exists(REF_LIB) and not force:
         return True
-    if not os.path.isdir(REF_ROOT):
+    if not REF_ROOT or not os.path.isdir(REF_ROOT):
         return False
     subprocess.run(["make", "-C", HERE, f"REF={REF_ROOT}"], check=True,
                    stdout=subprocess.DEVNULL)

@@ -32,6 +32,10 @@ def adapter():
         pytest.skip("no CUDA device")
     if not (os.path.exists(ADAPTER) and R.available()):
         pytest.skip("adapter harness / compiled reference not built")
+    return _adapter_lib()
+
+
+def _adapter_lib():
     abi.lib()  # the adapter resolves the library's symbols
     L = ctypes.CDLL(ADAPTER)
     i, ll, vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p
@@ -95,3 +99,40 @@ def test_run_lensdiff_cuda_error_strings(adapter):
     assert ok == 0 and err == "cuda-render-not-enabled-by-host"
     ok, err, _ = _run(adapter, p, src, torch.cuda.Stream(), null_src=True)
     assert ok == 0 and err == "missing-source-or-destination-cuda-buffer"  # :4652-4657
+
+
+_CHILD = r"""
+import sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+from tests.test_gpu_adapter import _adapter_lib, _lens, _run
+from lensdiff_b200 import synthetic as S
+L = _adapter_lib()
+p = _lens()
+src = S.make_frame(200, 120, 14, 1.0, 60.0, seed=41)
+ok, err, out = _run(L, p, src, torch.cuda.Stream())
+assert ok == 1, err
+np.save(sys.argv[2], out)
+"""
+
+
+@pytest.mark.parametrize("form", ["chosen", "fp32", "cufft"])
+def test_run_lensdiff_cuda_form_switch(adapter, form):
+    """LENSDIFF_B200_FFT_FORM selects the transform chain behind the plugin's
+    call (read once per process, so each form runs in its own process)."""
+    import subprocess
+    import sys
+    import tempfile
+
+    root = os.path.dirname(HERE)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "out.npy")
+        env = dict(os.environ, LENSDIFF_B200_FFT_FORM=form, LENSDIFF_B200_HBM_BUDGET_MB="4096")
+        res = subprocess.run([sys.executable, "-c", _CHILD, root, path], capture_output=True, text=True,
+                             timeout=600, env=env)
+        assert res.returncode == 0, res.stderr[-2000:]
+        out = np.load(path)
+    p = _lens()
+    ref = R.render(p, S.make_frame(200, 120, 14, 1.0, 60.0, seed=41))
+    assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL

@@ -7,9 +7,16 @@ checks that two calls in a row both reproduce the allocating entry point
 limit is refused with an error instead of running.
 
 This file sorts last so that a run stopping at the first failure has already
-run every other test; it also passes alone in a fresh process.
+run every other test; it also passes alone in a fresh process.  The no-alloc
+calls run before this test creates any library context, and one test runs
+them in a fresh child process that never creates one, so the context-free
+path (the first call's address lookup included) is exercised on its own.
 """
 import ctypes
+import os
+import subprocess
+import sys
+import tempfile
 
 import numpy as np
 import pytest
@@ -50,13 +57,9 @@ def _noalloc(p, wl_index, out, stream):
     return rc, st
 
 
-@pytest.mark.parametrize("pupil,radius,wl_index", [(256, 40, 0), (512, 200, 2)])
-def test_noalloc_matches_allocating_entry_point_twice(pupil, radius, wl_index):
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
-    p = _lens(pupil, radius)
-    np_, S_, _, _ = resolve_sizes(p)
-    stream = torch.cuda.Stream()
+def _reference_psf(p, wl_index, stream):
+    """ld_raw_psf through a library context (the allocating entry point)."""
+    _, S_, _, _ = resolve_sizes(p)
     cache = LensDiffPsfBankCache(0)
     ref = torch.zeros(S_, S_, device="cuda")
     st = cache.raw_psf(p, wl_index, ref, stream)
@@ -64,14 +67,65 @@ def test_noalloc_matches_allocating_entry_point_twice(pupil, radius, wl_index):
     stream.synchronize()
     ref_h = ref.cpu().numpy()
     cache.close()
-    for _ in range(2):
+    return ref_h
+
+
+@pytest.mark.parametrize("pupil,radius,wl_index", [(256, 40, 0), (512, 200, 2)])
+def test_noalloc_matches_allocating_entry_point_twice(pupil, radius, wl_index):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    p = _lens(pupil, radius)
+    _, S_, _, _ = resolve_sizes(p)
+    stream = torch.cuda.Stream()
+    got = []
+    for _ in range(2):  # before any library context exists in this test
         out = torch.full((S_, S_), -1.0, device="cuda")
         rc, st = _noalloc(p, wl_index, out, stream)
         assert rc == abi.LD_OK, st.stage
         stream.synchronize()
-        got = out.cpu().numpy()
-        assert rel_err(got, ref_h, ref_h.max()) < PSF_TOL
-        assert abs(float(got.sum()) - 1.0) < 1e-5
+        got.append(out.cpu().numpy())
+    ref_h = _reference_psf(p, wl_index, stream)
+    for g in got:
+        assert rel_err(g, ref_h, ref_h.max()) < PSF_TOL
+        assert abs(float(g.sum()) - 1.0) < 1e-5
+
+
+_CHILD = r"""
+import ctypes, sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+from lensdiff_b200 import abi
+from tests.test_zz_no_alloc import _lens, _noalloc
+from lensdiff_b200.backend import resolve_sizes
+p = _lens(256, 40)
+_, S_, _, _ = resolve_sizes(p)
+stream = torch.cuda.Stream()
+outs = []
+for _ in range(2):
+    out = torch.full((S_, S_), -1.0, device="cuda")
+    rc, st = _noalloc(p, 1, out, stream)
+    assert rc == abi.LD_OK, st.stage
+    stream.synchronize()
+    outs.append(out.cpu().numpy())
+np.save(sys.argv[2], np.stack(outs))
+"""
+
+
+def test_noalloc_in_a_fresh_process_without_any_context():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "psf.npy")
+        res = subprocess.run([sys.executable, "-c", _CHILD, root, path], capture_output=True, text=True,
+                             timeout=300)
+        assert res.returncode == 0, res.stderr[-2000:]
+        got = np.load(path)
+    p = _lens(256, 40)
+    ref_h = _reference_psf(p, 1, torch.cuda.Stream())
+    for g in got:
+        assert rel_err(g, ref_h, ref_h.max()) < PSF_TOL
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
