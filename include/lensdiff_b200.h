@@ -247,6 +247,24 @@ enum {
  * stream is being captured.  No counterpart in the reference. */
 int ld_set_graphs(ld_ctx* ctx, int enable);
 
+/* Autotuner of the frame chain's transforms.  The row length M and column
+ * length Py of a frame grid can each run on one of several compiled radix
+ * orders (ld_fxplans.h).  With autotuning on (the default), the first frame
+ * rendered at a grid, when it composites directly (no field zones, Preserve
+ * energy or scatter) and the caller's stream is not being captured, times
+ * every order of both lengths on that frame's own buffers with CUDA events
+ * (the timed kernels rewrite the same results) and keeps the fastest for
+ * later frames of the context: that first frame synchronises its stream a
+ * few times.  mode 1: tune (the default); 0: the first compiled order of each
+ * length; -1: the runtime-planned transforms only, no compiled orders.  No
+ * counterpart in the reference. */
+int ld_set_autotune(ld_ctx* ctx, int mode);
+/* The radix order chosen for transform length n: writes up to 4 radices
+ * (first stage first) and returns how many, 0 when n has no compiled order
+ * or has not been tuned yet; *ms_out (may be null) gets the winner's time per
+ * tuned launch group. */
+int ld_autotune_choice(ld_ctx* ctx, int32_t n, int32_t* radices_out, double* ms_out);
+
 /* When enabled, every kernel launch of ld_render / ld_build_psf_bank is
  * bracketed by a pair of CUDA events on its stream. */
 int ld_set_profiling(ld_ctx* ctx, int enable);

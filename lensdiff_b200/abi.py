@@ -309,6 +309,8 @@ EXPORTED_SYMBOLS = [
     "ld_profile_collect",
     "ld_estimate_device_bytes",
     "ld_set_graphs",
+    "ld_set_autotune",
+    "ld_autotune_choice",
     "ld_server_create",
     "ld_server_destroy",
     "ld_server_submit",
@@ -386,6 +388,10 @@ def lib() -> ctypes.CDLL:
     L.ld_profile_collect.restype = ctypes.c_int
     L.ld_set_graphs.argtypes = [vp, ctypes.c_int]
     L.ld_set_graphs.restype = ctypes.c_int
+    L.ld_set_autotune.argtypes = [vp, ctypes.c_int]
+    L.ld_set_autotune.restype = ctypes.c_int
+    L.ld_autotune_choice.argtypes = [vp, c_i32, ctypes.POINTER(c_i32), ctypes.POINTER(ctypes.c_double)]
+    L.ld_autotune_choice.restype = ctypes.c_int
     L.ld_estimate_device_bytes.argtypes = [ctypes.POINTER(ld_params), c_i32, c_i32]
     L.ld_estimate_device_bytes.restype = ctypes.c_size_t
     L.ld_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_size_t]

@@ -152,6 +152,21 @@ class LensDiffPsfBankCache:
         """Replay per-frame chains as CUDA graphs (default on)."""
         self._lib.ld_set_graphs(self._h, 1 if enable else 0)
 
+    def set_autotune(self, mode: int) -> None:
+        """1: time the compiled radix orders of a new grid's transform lengths
+        on its first composite frame and keep the fastest (the default); 0: the
+        first compiled order; -1: runtime-planned transforms only."""
+        rc = self._lib.ld_set_autotune(self._h, int(mode))
+        if rc != abi.LD_OK:
+            raise ValueError(f"autotune mode {mode!r} rejected ({rc})")
+
+    def autotune_choice(self, n: int):
+        """(radix order, ms) the autotuner chose for transform length n, or None."""
+        r = (abi.c_i32 * 4)()
+        ms = ctypes.c_double(0.0)
+        k = self._lib.ld_autotune_choice(self._h, int(n), r, ctypes.byref(ms))
+        return (tuple(int(r[i]) for i in range(k)), float(ms.value)) if k else None
+
     def set_profiling(self, enable: bool) -> None:
         self._lib.ld_set_profiling(self._h, 1 if enable else 0)
 

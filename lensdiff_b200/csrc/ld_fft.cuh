@@ -48,6 +48,10 @@ struct FftPlan {
     int nstages;
     unsigned long long codes;  // stage count of kPlanRadices[i] at bits 4i..4i+3
     const float2* tw;          // n entries, exp(-2 pi i k / n)
+    // Compile-time plan (ld_fxplans.h) the launchers use for this length, 0
+    // for none, and its per-stage twiddle tables (ld_fftx.cuh)
+    int fixed;
+    const float2* stw;
 };
 
 __host__ __device__ inline int plan_count(const FftPlan& p, int i) {

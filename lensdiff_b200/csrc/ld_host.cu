@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/lensdiff_b200.h"
+#include "ld_fxplans.h"
 #include "ld_internal.h"
 
 using namespace ld;
@@ -71,6 +72,10 @@ struct ld_ctx {
     bool configured = false;
     std::mutex mu;
     std::map<int, DevBuf> twiddles;
+    std::map<int, DevBuf> stage_twiddles;  // by fixed plan id
+    std::map<int, int> fixed_choice;       // transform length -> fixed plan id (autotuner)
+    std::map<int, double> fixed_ms;        // transform length -> the winner's timed ms
+    int autotune = 1;  // 1: tune, 0: first compiled order, -1: runtime-planned transforms only
     std::map<std::pair<int, int>, float> r0_cache;
     std::map<int, DevBuf> ring_counts;  // by R
     BankEntry bank;
@@ -419,10 +424,35 @@ const float2* twiddles(ld_ctx* c, int n) {
     return static_cast<const float2*>(b.p);
 }
 
+// Per-stage twiddle tables of a fixed plan (ld_fxplans.h), uploaded once.
+const float2* stage_twiddles(ld_ctx* c, int id) {
+    auto it = c->stage_twiddles.find(id);
+    if (it != c->stage_twiddles.end()) return static_cast<const float2*>(it->second.p);
+    const std::vector<float2> h = fx_stage_table(id);
+    DevBuf b;
+    ensure(c, b, std::max<size_t>(16, h.size() * sizeof(float2)));
+    if (!h.empty())
+        check_cuda(cudaMemcpy(b.p, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice), "stage-twiddle-upload");
+    c->stage_twiddles[id] = b;
+    return static_cast<const float2*>(b.p);
+}
+
+// The fixed plan a length runs on: the autotuner's choice when it has made
+// one, else the first compiled radix order of that length (0: none).
+int fixed_plan_for(ld_ctx* c, int n, bool allow25) {
+    if (!allow25 || c->autotune < 0) return 0;  // fixed plans are compiled in the 25-element family
+    auto it = c->fixed_choice.find(n);
+    if (it != c->fixed_choice.end()) return it->second;
+    int ids[8];
+    return fx_candidates(n, ids, 8) > 0 ? ids[0] : 0;
+}
+
 FftPlan make_plan(ld_ctx* c, int n, bool allow25) {
     FftPlan p{};
     if (!factor_plan(n, allow25, &p)) throw Fail{LD_ERR_UNSUPPORTED, "fft-length-not-5-smooth"};
     p.tw = twiddles(c, n);
+    p.fixed = fixed_plan_for(c, n, allow25);
+    p.stw = p.fixed ? stage_twiddles(c, p.fixed) : nullptr;
     return p;
 }
 
@@ -1827,6 +1857,7 @@ void ld_destroy(ld_ctx* c) {
     if (!c) return;
     DeviceGuard g(c->device);
     for (auto& kv : c->twiddles) free_buf(c, kv.second);
+    for (auto& kv : c->stage_twiddles) free_buf(c, kv.second);
     for (auto& kv : c->ring_counts) free_buf(c, kv.second);
     DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,    &c->frameB,
                       &c->calib,  &c->calib_psf, &c->err_word,  &c->pupil_pre,  &c->effect,    &c->cf_grid,
@@ -1939,6 +1970,77 @@ namespace {
 
 constexpr size_t kGraphCache = 4;
 
+// ---------------------------------------------------------------------------
+// Autotuner of the fixed transform plans (ld_fxplans.h)
+// ---------------------------------------------------------------------------
+// Times launch(id) for every compiled radix order of length n on stream s
+// (one untimed launch, then kTuneReps between two events), records the
+// fastest in c->fixed_choice[n].  Lengths with one order record it untimed.
+void tune_length(ld_ctx* c, int n, cudaStream_t s, const std::function<void(int)>& launch) {
+    int ids[8];
+    const int k = fx_candidates(n, ids, 8);
+    if (k == 0 || c->fixed_choice.count(n)) return;
+    if (k == 1) {
+        c->fixed_choice[n] = ids[0];
+        return;
+    }
+    constexpr int kTuneReps = 3;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    check_cuda(cudaEventCreate(&e0), "tune-event");
+    check_cuda(cudaEventCreate(&e1), "tune-event");
+    int best = ids[0];
+    float best_ms = 0.0f;
+    for (int i = 0; i < k; ++i) {
+        launch(ids[i]);
+        check_cuda(cudaEventRecord(e0, s), "tune-record");
+        for (int r = 0; r < kTuneReps; ++r) launch(ids[i]);
+        check_cuda(cudaEventRecord(e1, s), "tune-record");
+        check_cuda(cudaEventSynchronize(e1), "tune-sync");
+        float ms = 0.0f;
+        check_cuda(cudaEventElapsedTime(&ms, e0, e1), "tune-elapsed");
+        ms /= kTuneReps;
+        if (i == 0 || ms < best_ms) {
+            best = ids[i];
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_launch("autotune");
+    c->fixed_choice[n] = best;
+    c->fixed_ms[n] = best_ms;
+}
+
+// Tunes the row length (frame_rows + frame_inverse, which share its plan) and
+// the column length (frame_cols) of a composite frame's grid, re-running the
+// frame's own launches: each rewrites the results it wrote before.
+void autotune_frame(ld_ctx* c, const FrameArgs& fa, cudaStream_t s) {
+    if (c->autotune != 1 || fa.effect_mode != kEffectComposite) return;
+    if (c->fixed_choice.count(fa.g.M) && c->fixed_choice.count(fa.g.Py)) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return;
+    }
+    if (fa.g.fam_m == kE25) {
+        tune_length(c, fa.g.M, s, [&](int id) {
+            FrameArgs a = fa;
+            a.g.plan_m.fixed = id;
+            a.g.plan_m.stw = stage_twiddles(c, id);
+            launch_frame_rows(a, s);
+            launch_frame_inverse(a, s);
+        });
+    }
+    if (fa.g.fam_py == kE25) {
+        tune_length(c, fa.g.Py, s, [&](int id) {
+            FrameArgs a = fa;
+            a.g.plan_py.fixed = id;
+            a.g.plan_py.stw = stage_twiddles(c, id);
+            launch_frame_cols(a, s);
+        });
+    }
+}
+
 // Issues a frame chain through a cached CUDA graph: on the first call with a
 // given key the chain is captured (thread-local capture mode) and
 // instantiated, later calls with the same key launch the graph.  The key is
@@ -2012,6 +2114,29 @@ int ld_set_graphs(ld_ctx* c, int enable) {
     std::lock_guard<std::mutex> lock(c->mu);
     c->graphs_enabled = enable != 0;
     return LD_OK;
+}
+
+int ld_set_autotune(ld_ctx* c, int enable) {
+    if (!c) return LD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (enable < -1 || enable > 1) return LD_ERR_ARG;
+    c->autotune = enable;
+    return LD_OK;
+}
+
+int ld_autotune_choice(ld_ctx* c, int32_t n, int32_t* radices_out, double* ms_out) {
+    if (!c || !radices_out) return 0;
+    std::lock_guard<std::mutex> lock(c->mu);
+    auto it = c->fixed_choice.find(n);
+    if (it == c->fixed_choice.end()) return 0;
+    const FxPlanDesc* d = fx_plan(it->second);
+    if (d == nullptr) return 0;
+    for (int i = 0; i < d->count; ++i) radices_out[i] = d->radix[i];
+    if (ms_out) {
+        auto m = c->fixed_ms.find(n);
+        *ms_out = m != c->fixed_ms.end() ? m->second : 0.0;
+    }
+    return d->count;
 }
 
 size_t ld_estimate_device_bytes(const ld_params* params, int32_t width, int32_t height) {
@@ -2492,6 +2617,9 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             if (fa.effect_mode != kEffectComposite) staged(ctx, LD_STAGE_COMPOSITE, s, [&] { launch_composite(fin, s); });
         };
         run_chain(ctx, s, gkey, chain);
+        // the first composite frame at this grid picks the transforms' radix orders
+        if (!run_scatter && !zones && fa.effect_mode == kEffectComposite && dv == LD_DEBUG_FINAL)
+            autotune_frame(ctx, fw, s);
         for (const SpectraEntry* e : spectra) mark_used(const_cast<SpectraEntry&>(*e), s);
         check_launch("frame-chain");
         if (st) {

@@ -7,6 +7,7 @@
 
 #include <map>
 #include <tuple>
+#include <vector>
 
 #include "ld_fft.cuh"
 #include "ld_optics.cuh"
@@ -150,6 +151,16 @@ struct KernelSpectraArgs {
 };
 void launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s);
 void launch_kspec_cols(const KernelSpectraArgs& a, cudaStream_t s);
+// Fixed-plan launches (ld_frame_fx.cu): false when no compiled fixed plan
+// covers the launch, which then takes the runtime-planned kernel.
+struct FrameArgs;
+bool fx_launch_frame_rows(const FrameArgs& a, cudaStream_t s);
+bool fx_launch_frame_cols(const FrameArgs& a, cudaStream_t s);
+bool fx_launch_frame_inverse(const FrameArgs& a, int rows, cudaStream_t s);
+bool fx_launch_kspec_cols(const KernelSpectraArgs& a, cudaStream_t s);
+void fx_configure();
+// FP64 stage twiddle tables of fixed plan `id` (ld_fxplans.h).
+std::vector<float2> fx_stage_table(int id);
 size_t kspec_cols_smem(int Py, int Kp, int n_ker);
 
 struct SelectionParams {
