@@ -265,6 +265,26 @@ int ld_set_autotune(ld_ctx* ctx, int mode);
  * tuned launch group. */
 int ld_autotune_choice(ld_ctx* ctx, int32_t n, int32_t* radices_out, double* ms_out);
 
+/* ---- failure detection without a fault (no counterpart in the reference) --
+ * ld_selftest_wait runs one CTA that exercises the device-side failure paths
+ * every bulk-copy wait of the library relies on, and returns what the
+ * context's device error word recorded (cleared afterwards):
+ *   LD_SELFTEST_WAIT_TIMEOUT   waits on a barrier nothing will complete; the
+ *                              wait gives up after budget_cycles SM cycles
+ *                              (1e3 .. 2e9) and records 1: LD_ERR_TIMEOUT;
+ *   LD_SELFTEST_BAD_COPY_ARGS  asks for a bulk copy of 20 bytes, which the
+ *                              argument check refuses without issuing it,
+ *                              recording 2: LD_ERR_TIMEOUT;
+ *   LD_SELFTEST_VALID_COPY     one valid copy: nothing recorded, LD_OK.
+ * Synchronises `stream`.  The error word must be clear when it is called. */
+enum { LD_SELFTEST_WAIT_TIMEOUT = 0, LD_SELFTEST_BAD_COPY_ARGS = 1, LD_SELFTEST_VALID_COPY = 2 };
+int ld_selftest_wait(ld_ctx* ctx, int32_t mode, int64_t budget_cycles, void* stream, int32_t* error_word);
+/* Host-side fault injection: the allocation after `after` more successful
+ * ones fails as a refused cudaMalloc would (LD_ERR_OOM, stage
+ * "device-allocation-failed (injected)"); -1 turns it off.  The failing call
+ * returns the error and the context stays usable. */
+int ld_inject_alloc_failure(ld_ctx* ctx, int32_t after);
+
 /* When enabled, every kernel launch of ld_render / ld_build_psf_bank is
  * bracketed by a pair of CUDA events on its stream. */
 int ld_set_profiling(ld_ctx* ctx, int enable);

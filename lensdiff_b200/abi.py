@@ -310,6 +310,8 @@ EXPORTED_SYMBOLS = [
     "ld_estimate_device_bytes",
     "ld_set_graphs",
     "ld_set_autotune",
+    "ld_selftest_wait",
+    "ld_inject_alloc_failure",
     "ld_autotune_choice",
     "ld_server_create",
     "ld_server_destroy",
@@ -388,6 +390,10 @@ def lib() -> ctypes.CDLL:
     L.ld_profile_collect.restype = ctypes.c_int
     L.ld_set_graphs.argtypes = [vp, ctypes.c_int]
     L.ld_set_graphs.restype = ctypes.c_int
+    L.ld_selftest_wait.argtypes = [vp, c_i32, ctypes.c_int64, vp, ctypes.POINTER(c_i32)]
+    L.ld_selftest_wait.restype = ctypes.c_int
+    L.ld_inject_alloc_failure.argtypes = [vp, c_i32]
+    L.ld_inject_alloc_failure.restype = ctypes.c_int
     L.ld_set_autotune.argtypes = [vp, ctypes.c_int]
     L.ld_set_autotune.restype = ctypes.c_int
     L.ld_autotune_choice.argtypes = [vp, c_i32, ctypes.POINTER(c_i32), ctypes.POINTER(ctypes.c_double)]

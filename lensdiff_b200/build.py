@@ -20,7 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "liblensdiff_b200.so")
 ROOT = os.path.dirname(HERE)
 SOURCES = ["ld_host.cu", "ld_psf.cu", "ld_frame.cu", "ld_frame_fx.cu", "ld_noalloc.cu", "ld_cufft.cu",
-           "ld_server.cu", "ld_dftgemm.cu", "ld_debug.cu"]
+           "ld_server.cu", "ld_dftgemm.cu", "ld_debug.cu", "ld_selftest.cu"]
 # cuFFT backs only the comparator form (fft_form LD_FFT_CUFFT)
 LIBS = ["-L/usr/local/cuda/lib64", "-lcufft", "-Xlinker", "-rpath", "-Xlinker", "/usr/local/cuda/lib64"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -120,11 +120,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait for phase `parity` of `bar`.  Returns false (and sets *err) if
-// the budget ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+// the budget (SM clock cycles) ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err,
+                                          long long budget = kWaitBudgetCycles) {
     const long long start = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - start > kWaitBudgetCycles) {
+        if (clock64() - start > budget) {
             if (err) atomicExch(err, kErrWaitTimeout);
             return false;
         }

@@ -76,6 +76,7 @@ struct ld_ctx {
     std::map<int, int> fixed_choice;       // transform length -> fixed plan id (autotuner)
     std::map<int, double> fixed_ms;        // transform length -> the winner's timed ms
     int autotune = 1;  // 1: tune, 0: first compiled order, -1: runtime-planned transforms only
+    int fail_alloc_after = -1;  // fault injection: allocations until one fails (-1: off)
     std::map<std::pair<int, int>, float> r0_cache;
     std::map<int, DevBuf> ring_counts;  // by R
     BankEntry bank;
@@ -142,6 +143,7 @@ struct ld_ctx {
     DevBuf cf_grid, cf_planes, cf_sd, cf_prod;
     DevBuf err_word;    // device int: nonzero after a bounded wait gave up
     int* err = nullptr;
+    DevBuf selftest;    // ld_selftest_wait's source and destination
     int launches = 0;
     // stage timing
     bool profiling = false;
@@ -199,6 +201,10 @@ void* ensure(ld_ctx* c, DevBuf& b, size_t bytes) {
     const size_t old = b.bytes;
     if (c->budget && c->held - old + bytes > c->budget)
         throw Fail{LD_ERR_BUDGET, "hbm-budget-exceeded"};
+    // host-side fault injection (ld_inject_alloc_failure): this allocation
+    // fails as a refused cudaMalloc would, before anything is freed
+    if (c->fail_alloc_after >= 0 && c->fail_alloc_after-- == 0)
+        throw Fail{LD_ERR_OOM, "device-allocation-failed (injected)"};
     free_buf(c, b);
     void* p = nullptr;
     if (cudaMalloc(&p, bytes) != cudaSuccess) {
@@ -1862,7 +1868,7 @@ void ld_destroy(ld_ctx* c) {
     DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,    &c->frameB,
                       &c->calib,  &c->calib_psf, &c->err_word,  &c->pupil_pre,  &c->effect,    &c->cf_grid,
                       &c->cf_planes, &c->cf_sd,  &c->cf_prod,   &c->work,       &c->scatter_canvas,
-                      &c->scatter_ks, &c->dft,  &c->debug};
+                      &c->scatter_ks, &c->dft,  &c->debug,      &c->selftest};
     c->cufft.release();
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
@@ -2114,6 +2120,35 @@ int ld_set_graphs(ld_ctx* c, int enable) {
     std::lock_guard<std::mutex> lock(c->mu);
     c->graphs_enabled = enable != 0;
     return LD_OK;
+}
+
+int ld_inject_alloc_failure(ld_ctx* c, int32_t after) {
+    if (!c) return LD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->fail_alloc_after = after < 0 ? -1 : after;
+    return LD_OK;
+}
+
+int ld_selftest_wait(ld_ctx* c, int32_t mode, int64_t budget_cycles, void* stream, int32_t* error_word) {
+    if (!c || !error_word) return LD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    DeviceGuard g(c->device);
+    try {
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        int v = 0;
+        check_cuda(cudaMemcpy(&v, c->err, sizeof(int), cudaMemcpyDeviceToHost), "selftest-read");
+        if (v != 0) throw Fail{LD_ERR_ARG, "selftest-error-word-not-clear"};
+        float4* scratch = static_cast<float4*>(ensure(c, c->selftest, 2 * 64 * sizeof(float4)));
+        const int rc = launch_wait_selftest(mode, budget_cycles, scratch, c->err, s);
+        if (rc != LD_OK) return rc;
+        check_cuda(cudaStreamSynchronize(s), "selftest-sync");
+        check_cuda(cudaMemcpy(&v, c->err, sizeof(int), cudaMemcpyDeviceToHost), "selftest-read");
+        check_cuda(cudaMemset(c->err, 0, sizeof(int)), "selftest-clear");
+        *error_word = v;
+        return v == 0 ? LD_OK : LD_ERR_TIMEOUT;
+    } catch (const Fail& f) {
+        return f.code;
+    }
 }
 
 int ld_set_autotune(ld_ctx* c, int enable) {

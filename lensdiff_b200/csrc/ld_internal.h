@@ -159,6 +159,8 @@ bool fx_launch_frame_cols(const FrameArgs& a, cudaStream_t s);
 bool fx_launch_frame_inverse(const FrameArgs& a, int rows, cudaStream_t s);
 bool fx_launch_kspec_cols(const KernelSpectraArgs& a, cudaStream_t s);
 void fx_configure();
+// ld_selftest.cu: one bounded-wait self-test (LD_SELFTEST_*) on `err`.
+int launch_wait_selftest(int mode, long long budget, float4* scratch, int* err, cudaStream_t s);
 // FP64 stage twiddle tables of fixed plan `id` (ld_fxplans.h).
 std::vector<float2> fx_stage_table(int id);
 size_t kspec_cols_smem(int Py, int Kp, int n_ker);
