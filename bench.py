@@ -738,6 +738,12 @@ def main():
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": None, "peak": peak, "unit": "GB/s",
                     "frac": None, "peak_source": peak_src, "traffic": None}
     stage_ms = {k: round(v[0] / n_prof, 4) for k, v in stage.items() if v[1]}
+    # the radix orders and launch shapes the autotuner picked for the grid
+    autotune = {}
+    for n in (grid[0] // 2, grid[1]):
+        ch = cache.autotune_choice(n)
+        if ch:
+            autotune[str(n)] = {"radices": list(ch[0]), "shape": ch[1], "ms": round(ch[2], 4)}
 
     # ---- the other transform chains on the same workload (device time) ------
     comparators = {}
@@ -815,6 +821,7 @@ def main():
             "stage_ms_per_frame": stage_ms,
             "roofline": roofline,
             "kernel_hbm_frac": kernel_frac,
+            "autotune": autotune,
             "error": errors.get(FORM_NAMES[args.fft_form]) if errors else None,
             "clocks": clk,
             "e2e": e2e,

@@ -261,9 +261,10 @@ int ld_set_graphs(ld_ctx* ctx, int enable);
 int ld_set_autotune(ld_ctx* ctx, int mode);
 /* The radix order chosen for transform length n: writes up to 4 radices
  * (first stage first) and returns how many, 0 when n has no compiled order
- * or has not been tuned yet; *ms_out (may be null) gets the winner's time per
- * tuned launch group. */
-int ld_autotune_choice(ld_ctx* ctx, int32_t n, int32_t* radices_out, double* ms_out);
+ * or has not been tuned yet.  *shape_out (may be null): the launch shape
+ * (1: the inverse row pass at one more CTA per SM); *ms_out (may be null):
+ * the winner's time per tuned launch group. */
+int ld_autotune_choice(ld_ctx* ctx, int32_t n, int32_t* radices_out, int32_t* shape_out, double* ms_out);
 
 /* ---- failure detection without a fault (no counterpart in the reference) --
  * ld_selftest_wait runs one CTA that exercises the device-side failure paths

@@ -396,7 +396,8 @@ def lib() -> ctypes.CDLL:
     L.ld_inject_alloc_failure.restype = ctypes.c_int
     L.ld_set_autotune.argtypes = [vp, ctypes.c_int]
     L.ld_set_autotune.restype = ctypes.c_int
-    L.ld_autotune_choice.argtypes = [vp, c_i32, ctypes.POINTER(c_i32), ctypes.POINTER(ctypes.c_double)]
+    L.ld_autotune_choice.argtypes = [vp, c_i32, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32),
+                                     ctypes.POINTER(ctypes.c_double)]
     L.ld_autotune_choice.restype = ctypes.c_int
     L.ld_estimate_device_bytes.argtypes = [ctypes.POINTER(ld_params), c_i32, c_i32]
     L.ld_estimate_device_bytes.restype = ctypes.c_size_t

@@ -161,11 +161,13 @@ class LensDiffPsfBankCache:
             raise ValueError(f"autotune mode {mode!r} rejected ({rc})")
 
     def autotune_choice(self, n: int):
-        """(radix order, ms) the autotuner chose for transform length n, or None."""
+        """(radix order, launch shape, ms) the autotuner chose for transform
+        length n, or None."""
         r = (abi.c_i32 * 4)()
+        shape = abi.c_i32(0)
         ms = ctypes.c_double(0.0)
-        k = self._lib.ld_autotune_choice(self._h, int(n), r, ctypes.byref(ms))
-        return (tuple(int(r[i]) for i in range(k)), float(ms.value)) if k else None
+        k = self._lib.ld_autotune_choice(self._h, int(n), r, ctypes.byref(shape), ctypes.byref(ms))
+        return (tuple(int(r[i]) for i in range(k)), int(shape.value), float(ms.value)) if k else None
 
     def set_profiling(self, enable: bool) -> None:
         self._lib.ld_set_profiling(self._h, 1 if enable else 0)

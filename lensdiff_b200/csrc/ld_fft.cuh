@@ -52,6 +52,9 @@ struct FftPlan {
     // for none, and its per-stage twiddle tables (ld_fftx.cuh)
     int fixed;
     const float2* stw;
+    // launch shape of the fixed plan's kernels (0: default; 1: one more CTA
+    // per SM for the inverse row pass, under a tighter register cap)
+    int shape;
 };
 
 __host__ __device__ inline int plan_count(const FftPlan& p, int i) {

@@ -29,6 +29,13 @@ namespace {
 
 
 // ---- launch helpers -------------------------------------------------------------------
+// Launch with a.ahead = the CTAs of f resident at once (the L2 prefetch distance).
+template <class Kern>
+void launch_ahead(Kern f, FrameArgs a, int grid, int T, size_t sm, cudaStream_t s) {
+    a.ahead = resident_ctas(f, T, sm);
+    f<<<grid, T, sm, s>>>(a);
+}
+
 template <int E>
 void rows_e(const FrameArgs& a, cudaStream_t s) {
     const int M = a.g.M;
@@ -37,17 +44,17 @@ void rows_e(const FrameArgs& a, cudaStream_t s) {
         // transform fits 224 threads; else four rows per CTA
         if (fft_threads(M, 2, E) <= 224) {
             const size_t sm = static_cast<size_t>(M) * 2 * sizeof(float2);
-            frame_rows_kernel<E, 2, 1, 224, 3><<<a.Hp / 2, fft_threads(M, 2, E), sm, s>>>(a);
+            launch_ahead(frame_rows_kernel<E, 2, 1, 224, 3>, a, a.Hp / 2, fft_threads(M, 2, E), sm, s);
         } else {
             const size_t sm = static_cast<size_t>(M) * 4 * sizeof(float2);
-            frame_rows_kernel<E, 4, 1><<<a.Hp / 4, fft_threads(M, 4, E), sm, s>>>(a);
+            launch_ahead(frame_rows_kernel<E, 4, 1>, a, a.Hp / 4, fft_threads(M, 4, E), sm, s);
         }
     } else {
         const size_t sm = static_cast<size_t>(M) * 3 * sizeof(float2);
         if (a.drv_effect)
             frame_rows_kernel<E, 3, 3, Fam<E>::max_threads, 1, true><<<a.Hp, fft_threads(M, 3, E), sm, s>>>(a);
         else
-            frame_rows_kernel<E, 3, 3><<<a.Hp, fft_threads(M, 3, E), sm, s>>>(a);
+            launch_ahead(frame_rows_kernel<E, 3, 3>, a, a.Hp, fft_threads(M, 3, E), sm, s);
     }
 }
 
@@ -92,8 +99,8 @@ void inverse_c(const FrameArgs& a, int rows, cudaStream_t s) {
     const int T = fft_threads(M, C, E);
     const size_t sm = static_cast<size_t>(M) * C * sizeof(float2);
     // two CTAs per SM when the transform fits 320 threads (register cap 102)
-    if (T <= 320) frame_inverse_kernel<E, C, 320, 2, H16><<<rows, T, sm, s>>>(a);
-    else frame_inverse_kernel<E, C, Fam<E>::max_threads, 1, H16><<<rows, T, sm, s>>>(a);
+    if (T <= 320) launch_ahead(frame_inverse_kernel<E, C, 320, 2, H16>, a, rows, T, sm, s);
+    else launch_ahead(frame_inverse_kernel<E, C, Fam<E>::max_threads, 1, H16>, a, rows, T, sm, s);
 }
 
 template <int E>

@@ -61,7 +61,10 @@ void rows_fixed(const FrameArgs& a, cudaStream_t s) {
     constexpr int C = rows_c(N);
     constexpr int T = fft_threads(N, C, kE25);
     const size_t sm = static_cast<size_t>(N) * C * sizeof(float2);
-    frame_rows_kernel<kE25, C, 1, T, minb_for(T), false, FFT><<<a.Hp / C, T, sm, s>>>(a);
+    FrameArgs b = a;
+    auto f = frame_rows_kernel<kE25, C, 1, T, minb_for(T), false, FFT>;
+    b.ahead = resident_ctas(f, T, sm);
+    f<<<a.Hp / C, T, sm, s>>>(b);
 }
 
 template <class FFT, bool H16>
@@ -74,12 +77,23 @@ void cols_fixed(FrameArgs a, cudaStream_t s) {
     f<<<a.g.cols, T, sm, s>>>(a);
 }
 
-template <class FFT, bool H16>
-void inverse_fixed(const FrameArgs& a, int rows, cudaStream_t s) {
+template <class FFT, bool H16, int MINB>
+void inverse_fixed_m(const FrameArgs& a, int rows, cudaStream_t s) {
     constexpr int N = FFT::n;
     constexpr int T = fft_threads(N, 3, kE25);
     const size_t sm = static_cast<size_t>(N) * 3 * sizeof(float2);
-    frame_inverse_kernel<kE25, 3, T, minb_for(T), H16, FFT><<<rows, T, sm, s>>>(a);
+    FrameArgs b = a;
+    auto f = frame_inverse_kernel<kE25, 3, T, MINB, H16, FFT>;
+    b.ahead = resident_ctas(f, T, sm);
+    f<<<rows, T, sm, s>>>(b);
+}
+
+// shape 0: minb_for(T) CTAs per SM; shape 1: one more (tighter register cap)
+template <class FFT, bool H16>
+void inverse_fixed(const FrameArgs& a, int rows, cudaStream_t s) {
+    constexpr int T = fft_threads(FFT::n, 3, kE25);
+    if (a.g.plan_m.shape == 1) inverse_fixed_m<FFT, H16, minb_for(T) + 1>(a, rows, s);
+    else inverse_fixed_m<FFT, H16, minb_for(T)>(a, rows, s);
 }
 
 template <class FFT, bool H16>
@@ -103,6 +117,8 @@ void configure_fixed() {
         set_smem(frame_rows_kernel<kE25, C, 1, TR, minb_for(TR), false, FFT>);
         set_smem(frame_inverse_kernel<kE25, 3, T3, minb_for(T3), false, FFT>);
         set_smem(frame_inverse_kernel<kE25, 3, T3, minb_for(T3), true, FFT>);
+        set_smem(frame_inverse_kernel<kE25, 3, T3, minb_for(T3) + 1, false, FFT>);
+        set_smem(frame_inverse_kernel<kE25, 3, T3, minb_for(T3) + 1, true, FFT>);
     } else {
         constexpr int T3 = fft_threads(N, 3, kE25);
         set_smem(frame_cols_kernel<kE25, 3, T3, cols_minb(T3), false, FFT>);

@@ -159,6 +159,16 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
     const int64_t pitch = a.src_pitch;
     const bool aligned = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(pitch)) & 15) == 0;
     const int W = a.W, H = a.H, M = a.g.M;
+    // the source rows of this CTA and of the CTA one resident generation
+    // later go to L2 through the bulk-copy engine while this CTA loads
+    if (!FROM_EFFECT && aligned && threadIdx.x == 0) {
+        const uint32_t row_bytes = static_cast<uint32_t>(W) * 16u;
+        const int later = y0 + a.ahead * RPC;
+        for (int r = 0; r < RPC; ++r) {
+            if (y0 + r < H) bulk_prefetch_l2(a.src + static_cast<int64_t>(y0 + r) * pitch, row_bytes);
+            if (a.ahead > 0 && later + r < H) bulk_prefetch_l2(a.src + static_cast<int64_t>(later + r) * pitch, row_bytes);
+        }
+    }
     const SelectionParams sel = a.sel;
     // one thread per (row, pixel pair): the selection mask is evaluated once
     // per pixel and feeds every driver plane.  kU pairs per thread are loaded
@@ -371,6 +381,16 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
     const int sy = yo - a.src_y1;
     const bool have = sy >= 0 && sy < a.H;
     const int M = a.g.M;
+    // composite: this row's source pixels, and those of the row one resident
+    // generation later, go to L2 while the row's spectrum loads and transforms
+    if (a.effect_mode == kEffectComposite && threadIdx.x == 0 &&
+        ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(a.src_pitch)) & 15) == 0) {
+        const uint32_t row_bytes = static_cast<uint32_t>(a.W) * 16u;
+        if (have) bulk_prefetch_l2(a.src + static_cast<int64_t>(sy) * a.src_pitch, row_bytes);
+        const int sl = sy + a.ahead;
+        if (a.ahead > 0 && sl >= 0 && sl < a.H && bid + a.ahead < static_cast<int>(gridDim.x))
+            bulk_prefetch_l2(a.src + static_cast<int64_t>(sl) * a.src_pitch, row_bytes);
+    }
     if (have) {
         const float2* tw_px = a.g.tw_px;
         // Hermitian pairs: one load of X[p] and X[M-p] per channel gives both

@@ -73,7 +73,7 @@ struct ld_ctx {
     std::mutex mu;
     std::map<int, DevBuf> twiddles;
     std::map<int, DevBuf> stage_twiddles;  // by fixed plan id
-    std::map<int, int> fixed_choice;       // transform length -> fixed plan id (autotuner)
+    std::map<int, int> fixed_choice;       // transform length -> fixed plan id | shape << 8 (autotuner)
     std::map<int, double> fixed_ms;        // transform length -> the winner's timed ms
     int autotune = 1;  // 1: tune, 0: first compiled order, -1: runtime-planned transforms only
     int fail_alloc_after = -1;  // fault injection: allocations until one fails (-1: off)
@@ -457,7 +457,9 @@ FftPlan make_plan(ld_ctx* c, int n, bool allow25) {
     FftPlan p{};
     if (!factor_plan(n, allow25, &p)) throw Fail{LD_ERR_UNSUPPORTED, "fft-length-not-5-smooth"};
     p.tw = twiddles(c, n);
-    p.fixed = fixed_plan_for(c, n, allow25);
+    const int choice = fixed_plan_for(c, n, allow25);
+    p.fixed = choice & 255;
+    p.shape = choice >> 8;
     p.stw = p.fixed ? stage_twiddles(c, p.fixed) : nullptr;
     return p;
 }
@@ -1801,6 +1803,7 @@ SelectionParams selection_params(const ld_params& p) {  // CpuReference.cpp:1221
     s.thr_linear = 0.18f * std::pow(2.0f, thr);
     s.point_emphasis = static_cast<float>(p.point_emphasis);
     s.rscale = 1.0f - static_cast<float>(std::min(std::max(p.core_preserve, 0.0), 1.0));
+    s.sig_zero = static_cast<float>(0.18 * std::exp2(static_cast<double>(s.edge0)) * 0.999);
     return s;
 }
 
@@ -1979,14 +1982,15 @@ constexpr size_t kGraphCache = 4;
 // ---------------------------------------------------------------------------
 // Autotuner of the fixed transform plans (ld_fxplans.h)
 // ---------------------------------------------------------------------------
-// Times launch(id) for every compiled radix order of length n on stream s
-// (one untimed launch, then kTuneReps between two events), records the
-// fastest in c->fixed_choice[n].  Lengths with one order record it untimed.
-void tune_length(ld_ctx* c, int n, cudaStream_t s, const std::function<void(int)>& launch) {
+// Times launch(id, shape) for every compiled radix order of length n and
+// every launch shape in [0, shapes) on stream s (one untimed launch, then
+// kTuneReps between two events) and records the fastest as
+// c->fixed_choice[n] = id | shape << 8.  A single candidate is recorded untimed.
+void tune_length(ld_ctx* c, int n, int shapes, cudaStream_t s, const std::function<void(int, int)>& launch) {
     int ids[8];
     const int k = fx_candidates(n, ids, 8);
     if (k == 0 || c->fixed_choice.count(n)) return;
-    if (k == 1) {
+    if (k == 1 && shapes == 1) {
         c->fixed_choice[n] = ids[0];
         return;
     }
@@ -1996,18 +2000,22 @@ void tune_length(ld_ctx* c, int n, cudaStream_t s, const std::function<void(int)
     check_cuda(cudaEventCreate(&e1), "tune-event");
     int best = ids[0];
     float best_ms = 0.0f;
+    bool first = true;
     for (int i = 0; i < k; ++i) {
-        launch(ids[i]);
-        check_cuda(cudaEventRecord(e0, s), "tune-record");
-        for (int r = 0; r < kTuneReps; ++r) launch(ids[i]);
-        check_cuda(cudaEventRecord(e1, s), "tune-record");
-        check_cuda(cudaEventSynchronize(e1), "tune-sync");
-        float ms = 0.0f;
-        check_cuda(cudaEventElapsedTime(&ms, e0, e1), "tune-elapsed");
-        ms /= kTuneReps;
-        if (i == 0 || ms < best_ms) {
-            best = ids[i];
-            best_ms = ms;
+        for (int sh = 0; sh < shapes; ++sh) {
+            launch(ids[i], sh);
+            check_cuda(cudaEventRecord(e0, s), "tune-record");
+            for (int r = 0; r < kTuneReps; ++r) launch(ids[i], sh);
+            check_cuda(cudaEventRecord(e1, s), "tune-record");
+            check_cuda(cudaEventSynchronize(e1), "tune-sync");
+            float ms = 0.0f;
+            check_cuda(cudaEventElapsedTime(&ms, e0, e1), "tune-elapsed");
+            ms /= kTuneReps;
+            if (first || ms < best_ms) {
+                best = ids[i] | (sh << 8);
+                best_ms = ms;
+                first = false;
+            }
         }
     }
     cudaEventDestroy(e0);
@@ -2017,9 +2025,10 @@ void tune_length(ld_ctx* c, int n, cudaStream_t s, const std::function<void(int)
     c->fixed_ms[n] = best_ms;
 }
 
-// Tunes the row length (frame_rows + frame_inverse, which share its plan) and
-// the column length (frame_cols) of a composite frame's grid, re-running the
-// frame's own launches: each rewrites the results it wrote before.
+// Tunes the row length (frame_rows + frame_inverse, which share its plan; the
+// inverse pass at two launch shapes) and the column length (frame_cols) of a
+// composite frame's grid, re-running the frame's own launches: each rewrites
+// the results it wrote before.
 void autotune_frame(ld_ctx* c, const FrameArgs& fa, cudaStream_t s) {
     if (c->autotune != 1 || fa.effect_mode != kEffectComposite) return;
     if (c->fixed_choice.count(fa.g.M) && c->fixed_choice.count(fa.g.Py)) return;
@@ -2029,18 +2038,20 @@ void autotune_frame(ld_ctx* c, const FrameArgs& fa, cudaStream_t s) {
         return;
     }
     if (fa.g.fam_m == kE25) {
-        tune_length(c, fa.g.M, s, [&](int id) {
+        tune_length(c, fa.g.M, 2, s, [&](int id, int shape) {
             FrameArgs a = fa;
             a.g.plan_m.fixed = id;
+            a.g.plan_m.shape = shape;
             a.g.plan_m.stw = stage_twiddles(c, id);
             launch_frame_rows(a, s);
             launch_frame_inverse(a, s);
         });
     }
     if (fa.g.fam_py == kE25) {
-        tune_length(c, fa.g.Py, s, [&](int id) {
+        tune_length(c, fa.g.Py, 1, s, [&](int id, int) {
             FrameArgs a = fa;
             a.g.plan_py.fixed = id;
+            a.g.plan_py.shape = 0;
             a.g.plan_py.stw = stage_twiddles(c, id);
             launch_frame_cols(a, s);
         });
@@ -2159,14 +2170,15 @@ int ld_set_autotune(ld_ctx* c, int enable) {
     return LD_OK;
 }
 
-int ld_autotune_choice(ld_ctx* c, int32_t n, int32_t* radices_out, double* ms_out) {
+int ld_autotune_choice(ld_ctx* c, int32_t n, int32_t* radices_out, int32_t* shape_out, double* ms_out) {
     if (!c || !radices_out) return 0;
     std::lock_guard<std::mutex> lock(c->mu);
     auto it = c->fixed_choice.find(n);
     if (it == c->fixed_choice.end()) return 0;
-    const FxPlanDesc* d = fx_plan(it->second);
+    const FxPlanDesc* d = fx_plan(it->second & 255);
     if (d == nullptr) return 0;
     for (int i = 0; i < d->count; ++i) radices_out[i] = d->radix[i];
+    if (shape_out) *shape_out = it->second >> 8;
     if (ms_out) {
         auto m = c->fixed_ms.find(n);
         *ms_out = m != c->fixed_ms.end() ? m->second : 0.0;

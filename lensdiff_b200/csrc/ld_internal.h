@@ -172,6 +172,9 @@ struct SelectionParams {
     float thr_linear;      // 0.18 * 2^threshold
     float point_emphasis;
     float rscale;          // 1 - corePreserve
+    // signals at or below this give a zero mask: their stops lie below edge0
+    // by more than log2f's rounding (0.18 * 2^edge0 * 0.999)
+    float sig_zero;
 };
 
 // FrameArgs::transfer values (the public LD_TRANSFER_* enum)
@@ -202,7 +205,7 @@ struct FrameArgs {
     int h16;                   // chosen form: KS and B in FP16 with per-column scales
     const float* kscale;       // [cols] (h16)
     float* bscale;             // [cols] (h16)
-    int ahead;                 // column-pass CTAs resident at once (set by the launcher)
+    int ahead;                 // CTAs of the launch resident at once: the L2 prefetch distance (set by each launcher)
     int* err;                  // device error word
     // What the inverse pass does with the mapped effect of a row:
     //   kEffectComposite: composite the render window directly (Augment);

@@ -12,11 +12,15 @@ namespace ld {
 
 __device__ __forceinline__ float saturate(float v) { return fminf(fmaxf(v, 0.0f), 1.0f); }
 
-// buildSelectionMask per pixel (LensDiffCpuReference.cpp:1225-1245).
+// buildSelectionMask per pixel (LensDiffCpuReference.cpp:1225-1245).  A
+// non-positive signal gives a zero gate; so does one whose clamped value
+// max(sig, 1e-6) is at or below s.sig_zero (its stops lie below edge0, t = 0)
+// whatever the boost: such pixels (most of a frame) return at once.
 __device__ __forceinline__ float selection_mask(const SelectionParams& s, float r, float g, float b, float* signal) {
     const float maxrgb = fmaxf(fmaxf(r, g), b);
     const float sig = s.luma ? 0.2126f * r + 0.7152f * g + 0.0722f * b : maxrgb;
     *signal = sig;
+    if (sig <= 0.0f || fmaxf(sig, 1e-6f) <= s.sig_zero) return 0.0f;
     float gate = 0.0f;
     if (sig > 0.0f) {
         const float stops = log2f(fmaxf(sig, 1e-6f) / 0.18f);

@@ -22,6 +22,7 @@ from lensdiff_b200 import abi  # noqa: E402
 from lensdiff_b200 import synthetic as S  # noqa: E402
 from lensdiff_b200.backend import LensDiffPsfBankCache, image_request  # noqa: E402
 from lensdiff_b200.types import LensDiffApertureMode, LensDiffSpectralMode  # noqa: E402
+from tests.helpers import with_matrices  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -44,7 +45,7 @@ def _lens():
     p.maxKernelRadiusPx = S.radius_percent(14, 96)
     p.diffractionScalePx = 3.0
     p.spectralMode = LensDiffSpectralMode.Tristimulus
-    return p
+    return with_matrices(p)
 
 
 def _render(c, p, frame):
