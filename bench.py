@@ -565,7 +565,9 @@ def main():
     from lensdiff_b200 import synthetic as S
     from lensdiff_b200.backend import LensDiffPsfBankCache, image_request
 
-    p, frame = getattr(S, WORKLOADS[args.workload])(seed=1003 + rank)
+    from lensdiff_b200 import replicas as RP
+
+    p, frame = getattr(S, WORKLOADS[args.workload])(seed=RP.replica_seed(1003, rank))
     p = p.copy(fftForm=FFT_FORMS[args.fft_form])
     H, W = frame.shape[:2]
     dev = torch.device("cuda", local)
@@ -633,12 +635,8 @@ def main():
     clk = clocks.stop()
     per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     sys.stderr.write("step ms: " + " ".join(f"{v:.3f}" for v in per_step) + "\n")
-    total_ms = evs[0].elapsed_time(evs[-1])
-    t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-    if ws > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = ws * args.steps / (total_ms / 1000.0)
+    total_ms = RP.max_over_ranks(evs[0].elapsed_time(evs[-1]), torch.distributed if ws > 1 else None, device=dev)
+    value = RP.job_throughput(ws, args.steps, total_ms)
     ps = sorted(per_step)
     p50 = ps[len(ps) // 2]
     p99 = ps[min(len(ps) - 1, int(math.ceil(0.99 * len(ps))) - 1)]

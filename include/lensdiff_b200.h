@@ -266,6 +266,22 @@ int ld_set_autotune(ld_ctx* ctx, int mode);
  * the winner's time per tuned launch group. */
 int ld_autotune_choice(ld_ctx* ctx, int32_t n, int32_t* radices_out, int32_t* shape_out, double* ms_out);
 
+/* ---- kernel spectra between contexts (no counterpart in the reference) ---
+ * The kernel spectra of a lens for a width x height source frame (the FFT of
+ * the RGB kernels on the frame's grid, what a cold frame builds before its
+ * convolution) as one opaque device block, so that one GPU can build them and
+ * others take them over NVLink instead of rebuilding: ld_export_kernel_spectra
+ * builds them if the context does not hold them yet and copies them to
+ * device_dst on `stream` (device_dst null: only *bytes_out is written);
+ * ld_import_kernel_spectra installs a block exported for the same parameters
+ * and frame size into the context's spectra cache, so the next ld_render of
+ * that lens and size starts from them.  Not with field zones or the cuFFT
+ * form (LD_ERR_UNSUPPORTED). */
+int ld_export_kernel_spectra(ld_ctx* ctx, const ld_params* params, int32_t width, int32_t height, void* device_dst,
+                             size_t capacity, size_t* bytes_out, void* stream, ld_status* status);
+int ld_import_kernel_spectra(ld_ctx* ctx, const ld_params* params, int32_t width, int32_t height,
+                             const void* device_src, size_t bytes, void* stream, ld_status* status);
+
 /* ---- failure detection without a fault (no counterpart in the reference) --
  * ld_selftest_wait runs one CTA that exercises the device-side failure paths
  * every bulk-copy wait of the library relies on, and returns what the

@@ -311,6 +311,8 @@ EXPORTED_SYMBOLS = [
     "ld_set_graphs",
     "ld_set_autotune",
     "ld_selftest_wait",
+    "ld_export_kernel_spectra",
+    "ld_import_kernel_spectra",
     "ld_inject_alloc_failure",
     "ld_autotune_choice",
     "ld_server_create",
@@ -390,6 +392,12 @@ def lib() -> ctypes.CDLL:
     L.ld_profile_collect.restype = ctypes.c_int
     L.ld_set_graphs.argtypes = [vp, ctypes.c_int]
     L.ld_set_graphs.restype = ctypes.c_int
+    L.ld_export_kernel_spectra.argtypes = [vp, ctypes.POINTER(ld_params), c_i32, c_i32, vp, ctypes.c_size_t,
+                                           ctypes.POINTER(ctypes.c_size_t), vp, ctypes.POINTER(ld_status)]
+    L.ld_export_kernel_spectra.restype = ctypes.c_int
+    L.ld_import_kernel_spectra.argtypes = [vp, ctypes.POINTER(ld_params), c_i32, c_i32, vp, ctypes.c_size_t, vp,
+                                           ctypes.POINTER(ld_status)]
+    L.ld_import_kernel_spectra.restype = ctypes.c_int
     L.ld_selftest_wait.argtypes = [vp, c_i32, ctypes.c_int64, vp, ctypes.POINTER(c_i32)]
     L.ld_selftest_wait.restype = ctypes.c_int
     L.ld_inject_alloc_failure.argtypes = [vp, c_i32]

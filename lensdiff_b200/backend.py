@@ -200,6 +200,34 @@ class LensDiffPsfBankCache:
         self._lib.ld_build_psf_bank(self._h, ctypes.byref(pp), _stream(stream), ctypes.byref(st))
         return LensDiffStatus(st)
 
+    def kernel_spectra_bytes(self, params: LensDiffParams, width: int, height: int) -> Tuple[int, LensDiffStatus]:
+        """Size of the kernel-spectra block of a lens for a width x height frame."""
+        pp = abi.to_abi_params(params)
+        st = abi.ld_status()
+        n = ctypes.c_size_t(0)
+        self._lib.ld_export_kernel_spectra(self._h, ctypes.byref(pp), int(width), int(height), None, 0,
+                                           ctypes.byref(n), None, ctypes.byref(st))
+        return int(n.value), LensDiffStatus(st)
+
+    def export_kernel_spectra(self, params: LensDiffParams, width: int, height: int, out, stream=None) -> LensDiffStatus:
+        """Builds (if needed) and copies the kernel spectra into the device buffer `out`."""
+        pp = abi.to_abi_params(params)
+        st = abi.ld_status()
+        n = ctypes.c_size_t(0)
+        cap = int(out.numel() * out.element_size()) if hasattr(out, "numel") else 0
+        self._lib.ld_export_kernel_spectra(self._h, ctypes.byref(pp), int(width), int(height), _ptr(out), cap,
+                                           ctypes.byref(n), _stream(stream), ctypes.byref(st))
+        return LensDiffStatus(st)
+
+    def import_kernel_spectra(self, params: LensDiffParams, width: int, height: int, src, nbytes: int,
+                              stream=None) -> LensDiffStatus:
+        """Installs kernel spectra exported by another context for the same lens and frame size."""
+        pp = abi.to_abi_params(params)
+        st = abi.ld_status()
+        self._lib.ld_import_kernel_spectra(self._h, ctypes.byref(pp), int(width), int(height), _ptr(src), int(nbytes),
+                                           _stream(stream), ctypes.byref(st))
+        return LensDiffStatus(st)
+
     def build_psf_banks(self, params_list: Sequence[LensDiffParams], stream=None) -> LensDiffStatus:
         """Builds the banks of several unrelated lenses together (their
         tensor-core windows in one launch per transform pass); they stay

@@ -278,6 +278,7 @@ void launch_resample_source(const FrameArgs& a, cudaStream_t s) {
 }
 
 void launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s) {
+    if (fx_launch_kspec_rows(a, s)) return;
     if (a.g.fam_m == kE25) kspec_rows_e<kE25>(a, s);
     else kspec_rows_e<kE16>(a, s);
 }

@@ -106,6 +106,13 @@ void kspec_cols_fixed(KernelSpectraArgs a, cudaStream_t s) {
     f<<<a.g.cols, T, sm, s>>>(a);
 }
 
+template <class FFT>
+void kspec_rows_fixed(const KernelSpectraArgs& a, cudaStream_t s) {
+    constexpr int T = fft_threads(FFT::n, 3, kE25);
+    const size_t sm = static_cast<size_t>(FFT::n) * 3 * sizeof(float2);
+    kspec_rows_kernel<kE25, 3, T, minb_for(T) + 1, FFT><<<a.Kp, T, sm, s>>>(a);
+}
+
 template <class D>
 void configure_fixed() {
     using FFT = typename D::type;
@@ -119,6 +126,7 @@ void configure_fixed() {
         set_smem(frame_inverse_kernel<kE25, 3, T3, minb_for(T3), true, FFT>);
         set_smem(frame_inverse_kernel<kE25, 3, T3, minb_for(T3) + 1, false, FFT>);
         set_smem(frame_inverse_kernel<kE25, 3, T3, minb_for(T3) + 1, true, FFT>);
+        set_smem(kspec_rows_kernel<kE25, 3, T3, minb_for(T3) + 1, FFT>);
     } else {
         constexpr int T3 = fft_threads(N, 3, kE25);
         set_smem(frame_cols_kernel<kE25, 3, T3, cols_minb(T3), false, FFT>);
@@ -165,6 +173,19 @@ bool fx_launch_frame_inverse(const FrameArgs& a, int rows, cudaStream_t s) {
         if constexpr (D::role == kRowPlan) {
             if (a.h16) inverse_fixed<typename D::type, true>(a, rows, s);
             else inverse_fixed<typename D::type, false>(a, rows, s);
+            done = true;
+        }
+    });
+    return done;
+}
+
+bool fx_launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s) {
+    if (a.n_ker != 3 || a.g.fam_m != kE25) return false;
+    bool done = false;
+    fx_visit(a.g.plan_m.fixed, [&](auto d) {
+        using D = decltype(d);
+        if constexpr (D::role == kRowPlan) {
+            kspec_rows_fixed<typename D::type>(a, s);
             done = true;
         }
     });

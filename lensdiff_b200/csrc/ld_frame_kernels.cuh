@@ -768,8 +768,8 @@ __device__ __forceinline__ int canvas_index(int g, int P, int R) {
 
 // One canvas row i = blockIdx.x of all C kernels per CTA (rows >= K are zero):
 // KR[k][i][c], k < M + 1.
-template <int E, int C>
-__global__ void __launch_bounds__(Fam<E>::max_threads, 1) kspec_rows_kernel(KernelSpectraArgs a) {
+template <int E, int C, int MAXT = Fam<E>::max_threads, int MINB = 1, class FFT = GenericFft<E>>
+__global__ void __launch_bounds__(MAXT, MINB) kspec_rows_kernel(KernelSpectraArgs a) {
     extern __shared__ float2 smem[];
     const int i = blockIdx.x;
     const int Px = a.g.Px, R = a.R, K = a.K;
@@ -782,7 +782,7 @@ __global__ void __launch_bounds__(Fam<E>::max_threads, 1) kspec_rows_kernel(Kern
         const int j1 = canvas_index(2 * idx + 1, Px, R);
         return make_float2(j0 >= 0 ? p[j0] : 0.0f, j1 >= 0 ? p[j1] : 0.0f);
     });
-    fft_run<E, C, false>(a.g.plan_m, smem);
+    FFT::template run<C, false, MAXT>(a.g.plan_m, smem);
     store_bins(a.g.M, C, static_cast<int64_t>(a.Kp) * C, static_cast<int64_t>(i) * C, a.g.tw_px, smem, a.rows);
 }
 

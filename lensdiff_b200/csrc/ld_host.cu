@@ -1809,6 +1809,33 @@ SelectionParams selection_params(const ld_params& p) {  // CpuReference.cpp:1221
 
 int run_guarded(ld_ctx* ctx, ld_status* st, const std::function<void()>& fn);
 
+// The combination and frame grid of the kernel spectra that ld_render uses
+// for a width x height source frame (the same resolution as the render's).
+struct SpectraGeometry {
+    Combination cb;
+    GridGeom g;
+    std::string key;
+    size_t bytes;
+};
+SpectraGeometry spectra_geometry(ld_ctx* c, const ld_params& p, int W, int H) {
+    validate_params(p);
+    if (W <= 0 || H <= 0) throw Fail{LD_ERR_ARG, "invalid-frame-size"};
+    if (has_field_phase(p)) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-spectra-transfer-with-field-zones"};
+    if (p.fft_form == LD_FFT_CUFFT) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-spectra-transfer-with-cufft-form"};
+    const std::vector<float> wl = wavelengths_of(p);
+    SpectraGeometry sg{make_combination(p, wl), GridGeom{}, std::string(), 0};
+    int Ww = W, Hw = H;
+    working_size(post_effects(p), W, H, &Ww, &Hw);
+    const int c_rows = std::max(std::max(sg.cb.n_drv == 1 ? 4 : 3, sg.cb.n_out), sg.cb.n_ker);
+    const int c_cols = std::max(std::max(sg.cb.n_out, sg.cb.n_ker), sg.cb.n_drv);
+    int rw = 0, rh = 0;
+    sg.g = make_geometry(c, Ww, Hw, 2 * max_kernel_radius(p) + 1, c_rows, c_cols, &rw, &rh);
+    sg.key = spectra_key_for(bank_key(p, wl), sg.cb, sg.g);
+    const bool h16 = chosen_h16(p);
+    sg.bytes = sg.cb.parts * (ks_part_bytes(sg.cb.n_ker, sg.g, h16) + static_cast<size_t>(sg.g.cols) * sizeof(float));
+    return sg;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -2131,6 +2158,80 @@ int ld_set_graphs(ld_ctx* c, int enable) {
     std::lock_guard<std::mutex> lock(c->mu);
     c->graphs_enabled = enable != 0;
     return LD_OK;
+}
+
+int ld_export_kernel_spectra(ld_ctx* ctx, const ld_params* params, int32_t width, int32_t height, void* device_dst,
+                             size_t capacity, size_t* bytes_out, void* stream, ld_status* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (!ctx || !params || !bytes_out) {
+        set_status(st, LD_ERR_ARG, "null-argument");
+        return LD_ERR_ARG;
+    }
+    return run_guarded(ctx, st, [&]() {
+        const ld_params& p = *params;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const SpectraGeometry sg = spectra_geometry(ctx, p, width, height);
+        *bytes_out = sg.bytes;
+        if (device_dst == nullptr) return;  // size query
+        if (capacity < sg.bytes) throw Fail{LD_ERR_ARG, "spectra-buffer-too-small"};
+        join_bank(ctx, s);
+        bool bank_rebuilt = false, spectra_rebuilt = false;
+        SpectraEntry& e = cached_spectra(ctx, p, sg.cb, sg.g, s, &bank_rebuilt, &spectra_rebuilt);
+        check_cuda(cudaMemcpyAsync(device_dst, e.spectra.p, sg.bytes, cudaMemcpyDeviceToDevice, s), "spectra-export");
+        mark_used(e, s);
+        fence_bank(ctx, s);
+        if (st) {
+            st->bank_rebuilt = bank_rebuilt;
+            st->spectra_rebuilt = spectra_rebuilt;
+            st->grid_used_w = sg.g.Px;
+            st->grid_used_h = sg.g.Py;
+        }
+    });
+}
+
+int ld_import_kernel_spectra(ld_ctx* ctx, const ld_params* params, int32_t width, int32_t height,
+                             const void* device_src, size_t bytes, void* stream, ld_status* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (!ctx || !params || !device_src) {
+        set_status(st, LD_ERR_ARG, "null-argument");
+        return LD_ERR_ARG;
+    }
+    return run_guarded(ctx, st, [&]() {
+        const ld_params& p = *params;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const SpectraGeometry sg = spectra_geometry(ctx, p, width, height);
+        if (bytes != sg.bytes) throw Fail{LD_ERR_ARG, "spectra-size-mismatch"};
+        join_bank(ctx, s);
+        SpectraEntry* slot = nullptr;
+        for (auto& e : ctx->spectra_lru)
+            if (e.valid && e.key == sg.key) slot = &e;
+        if (slot == nullptr) {
+            if (ctx->spectra_lru.size() < kSpectraCache) ctx->spectra_lru.emplace_back();
+            slot = &ctx->spectra_lru.front();
+            for (auto& e : ctx->spectra_lru) {
+                if (!e.valid) {
+                    slot = &e;
+                    break;
+                }
+                if (e.last_use < slot->last_use) slot = &e;
+            }
+        }
+        wait_free(*slot, s);
+        slot->valid = false;
+        ensure(ctx, slot->spectra, sg.bytes);
+        check_cuda(cudaMemcpyAsync(slot->spectra.p, device_src, sg.bytes, cudaMemcpyDeviceToDevice, s),
+                   "spectra-import");
+        slot->g = sg.g;
+        slot->n_ker = sg.cb.n_ker;
+        slot->key = sg.key;
+        slot->valid = true;
+        slot->last_use = ++ctx->spectra_clock;
+        fence_bank(ctx, s);
+        if (st) {
+            st->grid_used_w = sg.g.Px;
+            st->grid_used_h = sg.g.Py;
+        }
+    });
 }
 
 int ld_inject_alloc_failure(ld_ctx* c, int32_t after) {

@@ -157,6 +157,7 @@ struct FrameArgs;
 bool fx_launch_frame_rows(const FrameArgs& a, cudaStream_t s);
 bool fx_launch_frame_cols(const FrameArgs& a, cudaStream_t s);
 bool fx_launch_frame_inverse(const FrameArgs& a, int rows, cudaStream_t s);
+bool fx_launch_kspec_rows(const KernelSpectraArgs& a, cudaStream_t s);
 bool fx_launch_kspec_cols(const KernelSpectraArgs& a, cudaStream_t s);
 void fx_configure();
 // ld_selftest.cu: one bounded-wait self-test (LD_SELFTEST_*) on `err`.

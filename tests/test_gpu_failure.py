@@ -114,7 +114,7 @@ def test_injected_allocation_failure_is_reported_and_recoverable():
 def test_hbm_budget_refusal_then_a_fitting_frame():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    c = LensDiffPsfBankCache(0, hbm_budget_bytes=4 << 20)  # 4 MiB: far below one bank
+    c = LensDiffPsfBankCache(0, hbm_budget_bytes=64 << 10)  # 64 KiB: below one 128-pixel pupil's buffers
     st, _ = _render(c, _lens(), S.make_frame(160, 96, 8, 1.0, 50.0, seed=5))
     assert st.code == abi.LD_ERR_BUDGET and "hbm-budget-exceeded" in st.stage
     c.close()
