@@ -311,6 +311,89 @@ SERVING_SIZES = [((1920, 1080), 0.4, 256), ((2048, 1080), 0.2, 256), ((3840, 216
                  ((6144, 3160), 0.1, 750)]  # (frame, share, kernel radius px; 4R keeps the PSF grid 5-smooth)
 
 
+def _reference_matrices(p):
+    """The reference's spectral matrices of p's mode (BuildLensDiffSpectrumConfig
+    output committed with the golden fixtures)."""
+    from lensdiff_b200.types import LensDiffSpectralMode, LensDiffSpectrumStyle
+
+    with open(os.path.join(ROOT, "tests", "golden", "spectrum_matrices.json")) as f:
+        mats = json.load(f)
+    m = mats[f"{LensDiffSpectralMode(int(p.spectralMode)).name}/{LensDiffSpectrumStyle(int(p.spectrumStyle)).name}"]
+    return p.copy(naturalMatrix=m["natural"], styleMatrix=m["style"])
+
+
+def reference_cuda_comparator(args, cache, dev):
+    """The reference's RunLensDiffCuda (source/src/cuda/LensDiffCuda.cu,
+    compiled unchanged with its cuFFT transforms, oracle/_ref/libldrefcuda.so)
+    and the library's chosen form, both cold (bank rebuilt every frame), on
+    the UHD frame at the reference-expressible setting (Spectral9, pupil 512,
+    kernel radius 512 px); device time by CUDA events around each frame, plus
+    the two outputs' difference.  The reference synchronises the host inside
+    each call, so its event time equals its wall time."""
+    import numpy as np
+    import torch
+    from lensdiff_b200 import synthetic as S
+    from lensdiff_b200.backend import image_request
+    from oracle import ref_lib as R
+
+    if not R.cuda_available():
+        return {"reference_cuda": {"unavailable": "oracle/_ref/libldrefcuda.so not built"}}
+    p, frame = S.workload_reference_uhd()
+    ours = _reference_matrices(p.copy(fftForm=FFT_FORMS["chosen"]))
+    H, W = frame.shape[:2]
+    stream = torch.cuda.Stream(device=dev)
+    src = torch.from_numpy(frame).to(dev)
+    dst_ref = torch.empty_like(src)
+    dst_own = torch.empty_like(src)
+    req = image_request(src, dst_own, stream, frame_short_side=p.frameShortSidePx)
+    n = max(3, min(args.steps, 10))
+
+    def time_frames(fn, count):
+        ms = []
+        for i in range(count):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn(i)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms
+
+    def ref_frame(i):
+        R.cuda_render(p.copy(phaseDefocus=p.phaseDefocus + 1e-6 * (i + 1)), src.data_ptr(), dst_ref.data_ptr(), W, H,
+                      stream.cuda_stream, instance=0)
+
+    def own_frame(i):
+        with torch.cuda.stream(stream):
+            st = cache.render(req, ours.copy(phaseDefocus=ours.phaseDefocus + 1e-6 * (i + 1)))
+        if not st.ok:
+            raise RuntimeError(f"render failed: {st}")
+
+    torch.cuda.synchronize(dev)
+    time_frames(ref_frame, 2)
+    ref_ms = time_frames(ref_frame, n)
+    time_frames(own_frame, 3)
+    own_ms = time_frames(own_frame, n)
+    # one frame of each at the unperturbed setting: how far apart they are
+    R.cuda_render(p, src.data_ptr(), dst_ref.data_ptr(), W, H, stream.cuda_stream, instance=1)
+    with torch.cuda.stream(stream):
+        cache.render(req, ours)
+    stream.synchronize()
+    a, b = dst_own.cpu().numpy(), dst_ref.cpu().numpy()
+    diff = float(np.abs(a.astype(np.float64) - b).max() / max(float(b[..., :3].max()), 1e-30))
+
+    def summary(ms):
+        ms = sorted(ms)
+        return {"value": 1000.0 / (sum(ms) / len(ms)), "unit": "frames/s", "ms_per_step": sum(ms) / len(ms),
+                "p50_ms": ms[len(ms) // 2], "frames": len(ms)}
+
+    setting = "3840x2160 Spectral9 (reference spectral matrices), pupil 512 -> PSF 2048, kernel radius 512 px, cold"
+    return {"reference_cuda": dict(summary(ref_ms), config=setting,
+                                   what="reference RunLensDiffCuda (LensDiffCuda.cu unchanged, cuFFT transforms)"),
+            "own_chosen_at_reference_setting": dict(summary(own_ms), config=setting,
+                                                    out_diff_vs_reference_cuda=float(f"{diff:.3e}"))}
+
+
 def error_check(args, p, frame, cache, stream, dev, forms):
     """Error of one frame rendered in each of `forms` (FORM_NAMES values)
     against the FP64 oracle (oracle/check.py), with the workload's own
@@ -785,11 +868,18 @@ def main():
         if cache.check_device_errors():
             raise RuntimeError("device error word set by a comparator chain")
 
+    # ---- the reference's own CUDA chain on this GPU (1 GPU runs only) -------
+    if ws == 1 and not args.no_comparators and args.workload == "uhd31":
+        ref_cuda = reference_cuda_comparator(args, cache, dev)
+        if ref_cuda is not None:
+            comparators.update(ref_cuda)
+
     # ---- error against the FP64 oracle (checker only; outside every timed
     # region): one frame of the workload's own parameters in each timed form
     errors = None
     if rank == 0 and not args.no_error_check:
-        errors = error_check(args, p, frame, cache, stream, dev, list(comparators) + [FORM_NAMES[args.fft_form]])
+        forms = [n for n in comparators if n in FORM_NAMES.values()] + [FORM_NAMES[args.fft_form]]
+        errors = error_check(args, p, frame, cache, stream, dev, forms)
 
     # ---- CPU baseline (rank 0, N=1) ----------------------------------------
     cpu = None

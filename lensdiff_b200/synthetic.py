@@ -154,6 +154,18 @@ def workload_uhd31(seed: int = 1003, chromatic_focus: float = 0.2):
     return p, frame
 
 
+def workload_reference_uhd(seed: int = 1003):
+    """The UHD frame and lens of workload_uhd31 at a setting the reference's
+    own CUDA chain can express: its Spectral9 mode (9 wavelengths, its own
+    spectral matrices), no chromatic focus, pupil 512 -> PSF 2048, kernel
+    radius up to 512 px.  The same-GPU comparison with that chain runs here."""
+    p, frame = workload_uhd31(seed, chromatic_focus=0.0)
+    p.spectralMode = LensDiffSpectralMode.Spectral9
+    p.wavelengthsNm = []
+    p.rgbMode = LensDiffRgbMode.FromCaller
+    return p, frame
+
+
 def workload_zones8(seed: int = 1004):
     """The UHD 31-wavelength frame with field-varying aberrations on an 8 x 8
     zone grid, each zone its own PSF bank: coma and astigmatism grow with the

@@ -197,3 +197,42 @@ def convolve_scalar(plane: np.ndarray, kernel: np.ndarray) -> np.ndarray:
     k = np.ascontiguousarray(kernel, np.float32)
     lib().ldref_convolve_scalar(_f(p), w, h, _f(k), k.shape[0], _f(out))
     return out
+
+
+# ---------------------------------------------------------------------------
+# The reference's own CUDA chain (oracle/_ref/libldrefcuda.so): the GPU
+# comparator, RunLensDiffCuda of source/src/cuda/LensDiffCuda.cu on cuFFT.
+# ---------------------------------------------------------------------------
+REF_CUDA_LIB = os.path.join(HERE, "_ref", "libldrefcuda.so")
+_cuda_lib: Optional[ctypes.CDLL] = None
+
+
+def cuda_available() -> bool:
+    return os.path.exists(REF_CUDA_LIB)
+
+
+def cuda_lib() -> ctypes.CDLL:
+    global _cuda_lib
+    if _cuda_lib is None:
+        if not cuda_available():
+            raise RuntimeError("oracle/_ref/libldrefcuda.so is not built")
+        L = ctypes.CDLL(REF_CUDA_LIB)
+        vp = ctypes.c_void_p
+        L.ldrefcuda_render.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, vp, vp,
+                                       ctypes.c_char_p, ctypes.c_int]
+        L.ldrefcuda_render.restype = ctypes.c_int
+        _cuda_lib = L
+    return _cuda_lib
+
+
+def cuda_render(params, src_ptr: int, dst_ptr: int, width: int, height: int, stream_ptr: int,
+                instance: int = 0) -> None:
+    """RunLensDiffCuda on device RGBA float buffers (rows of width * 16 bytes),
+    enqueued on stream_ptr; `instance` picks one of four persistent
+    LensDiffPsfBankCache objects, as the plugin keeps one per effect instance."""
+    err = ctypes.create_string_buffer(256)
+    s, ref = _abi(params)
+    ok = cuda_lib().ldrefcuda_render(ref, int(instance), ctypes.c_void_p(src_ptr), int(width), int(height),
+                                     int(width) * 16, ctypes.c_void_p(dst_ptr), ctypes.c_void_p(stream_ptr), err, 256)
+    if not ok:
+        raise RuntimeError("reference RunLensDiffCuda: " + err.value.decode())
