@@ -266,6 +266,21 @@ int ld_set_autotune(ld_ctx* ctx, int mode);
  * the winner's time per tuned launch group. */
 int ld_autotune_choice(ld_ctx* ctx, int32_t n, int32_t* radices_out, int32_t* shape_out, double* ms_out);
 
+/* The Custom aperture mode's image (LD_APERTURE_CUSTOM).  The reference
+ * loads it from LensDiffParams::customAperturePath with WIC or ImageIO
+ * (LensDiffApertureImage.cpp:301-365), decoding each pixel to an amplitude,
+ * then normalises and inverts it as customApertureNormalize /
+ * customApertureInvert ask (:367-399) and samples it into the pupil
+ * (LensDiffCpuReference.cpp:707-756).  Here the host decodes the file and
+ * passes the amplitudes (height rows of width floats, host memory); the
+ * library normalises and inverts them the same way, keeps them on the
+ * context's device and samples them as the reference does.  Renders in the
+ * Custom mode without an image return LD_ERR_ARG
+ * "custom-aperture-image-not-set"; values = null clears the image.  A new
+ * image invalidates the cached banks of Custom lenses. */
+int ld_set_custom_aperture(ld_ctx* ctx, const float* values, int32_t width, int32_t height, int32_t normalize,
+                           int32_t invert);
+
 /* ---- kernel spectra between contexts (no counterpart in the reference) ---
  * The kernel spectra of a lens for a width x height source frame (the FFT of
  * the RGB kernels on the frame's grid, what a cold frame builds before its

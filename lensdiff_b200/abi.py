@@ -311,6 +311,7 @@ EXPORTED_SYMBOLS = [
     "ld_set_graphs",
     "ld_set_autotune",
     "ld_selftest_wait",
+    "ld_set_custom_aperture",
     "ld_export_kernel_spectra",
     "ld_import_kernel_spectra",
     "ld_inject_alloc_failure",
@@ -398,6 +399,8 @@ def lib() -> ctypes.CDLL:
     L.ld_import_kernel_spectra.argtypes = [vp, ctypes.POINTER(ld_params), c_i32, c_i32, vp, ctypes.c_size_t, vp,
                                            ctypes.POINTER(ld_status)]
     L.ld_import_kernel_spectra.restype = ctypes.c_int
+    L.ld_set_custom_aperture.argtypes = [vp, ctypes.POINTER(c_f32), c_i32, c_i32, c_i32, c_i32]
+    L.ld_set_custom_aperture.restype = ctypes.c_int
     L.ld_selftest_wait.argtypes = [vp, c_i32, ctypes.c_int64, vp, ctypes.POINTER(c_i32)]
     L.ld_selftest_wait.restype = ctypes.c_int
     L.ld_inject_alloc_failure.argtypes = [vp, c_i32]

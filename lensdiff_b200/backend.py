@@ -187,7 +187,31 @@ class LensDiffPsfBankCache:
         return float(f.value)
 
     # -- entry points -------------------------------------------------------
+    def set_custom_aperture(self, image, normalize: bool = True, invert: bool = False) -> int:
+        """Hands the Custom aperture's decoded amplitude image (2-D, rows
+        first) to the context (ld_set_custom_aperture); None clears it."""
+        if image is None:
+            self._custom_key = None
+            return self._lib.ld_set_custom_aperture(self._h, None, 0, 0, 0, 0)
+        a = np.ascontiguousarray(image, dtype=np.float32)
+        if a.ndim != 2:
+            raise ValueError("the custom aperture image must be 2-D")
+        rc = self._lib.ld_set_custom_aperture(self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                              a.shape[1], a.shape[0], 1 if normalize else 0, 1 if invert else 0)
+        self._custom_key = (a.shape, a.tobytes(), bool(normalize), bool(invert)) if rc == abi.LD_OK else None
+        return rc
+
+    def _sync_custom(self, params: LensDiffParams) -> None:
+        img = getattr(params, "customApertureImage", None)
+        if int(params.apertureMode) != 4 or img is None:
+            return
+        a = np.ascontiguousarray(img, dtype=np.float32)
+        key = (a.shape, a.tobytes(), bool(params.customApertureNormalize), bool(params.customApertureInvert))
+        if getattr(self, "_custom_key", None) != key:
+            self.set_custom_aperture(a, params.customApertureNormalize, params.customApertureInvert)
+
     def render(self, request: LensDiffRenderRequest, params: LensDiffParams) -> LensDiffStatus:
+        self._sync_custom(params)
         rq = to_abi_request(request)
         pp = abi.to_abi_params(params)
         st = abi.ld_status()
@@ -195,6 +219,7 @@ class LensDiffPsfBankCache:
         return LensDiffStatus(st)
 
     def build_psf_bank(self, params: LensDiffParams, stream=None) -> LensDiffStatus:
+        self._sync_custom(params)
         pp = abi.to_abi_params(params)
         st = abi.ld_status()
         self._lib.ld_build_psf_bank(self._h, ctypes.byref(pp), _stream(stream), ctypes.byref(st))
@@ -241,6 +266,7 @@ class LensDiffPsfBankCache:
 
     def export_psf_bank(self, params: LensDiffParams, stream=None) -> Tuple[List[float], List[np.ndarray], LensDiffStatus]:
         """Host copies of the bank's `full` kernels (one per wavelength)."""
+        self._sync_custom(params)
         pp = abi.to_abi_params(params)
         np_, S, R, B = resolve_sizes(params)
         k = 2 * R + 1
@@ -266,6 +292,7 @@ class LensDiffPsfBankCache:
 
     def raw_psf(self, params: LensDiffParams, wavelength_index: int, out, stream=None) -> LensDiffStatus:
         """Writes the normalised shifted raw PSF (S x S float32) to device `out`."""
+        self._sync_custom(params)
         pp = abi.to_abi_params(params)
         st = abi.ld_status()
         self._lib.ld_raw_psf(self._h, ctypes.byref(pp), int(wavelength_index), _ptr(out), _stream(stream),

@@ -36,6 +36,23 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// A custom aperture image (ld_set_custom_aperture): the prepared amplitude
+// values on the device and a digest of them for the bank key.
+struct CustomAperture {
+    DevBuf img;
+    int w = 0, h = 0;
+    uint64_t digest = 0;
+};
+
+// The context whose entry point is running on this thread: pupil set-up and
+// the bank key read its custom aperture image through it.
+thread_local const CustomAperture* t_custom = nullptr;
+struct CustomScope {
+    const CustomAperture* prev;
+    explicit CustomScope(const CustomAperture* c) : prev(t_custom) { t_custom = c; }
+    ~CustomScope() { t_custom = prev; }
+};
+
 struct BankEntry {
     bool valid = false;
     std::string key;
@@ -77,6 +94,7 @@ struct ld_ctx {
     std::map<int, double> fixed_ms;        // transform length -> the winner's timed ms
     int autotune = 1;  // 1: tune, 0: first compiled order, -1: runtime-planned transforms only
     int fail_alloc_after = -1;  // fault injection: allocations until one fails (-1: off)
+    CustomAperture custom;      // the Custom aperture mode's image
     std::map<std::pair<int, int>, float> r0_cache;
     std::map<int, DevBuf> ring_counts;  // by R
     BankEntry bank;
@@ -619,6 +637,18 @@ PupilParams pupil_params(const ld_params& p, bool circle_reference) {
     pp.decy = static_cast<float>(p.pupil_decenter_y);
     pp.phase_cs = std::cos(-pp.rotation);  // LensDiffPhase.cpp:225-226
     pp.phase_sn = std::sin(-pp.rotation);
+    if (p.aperture_mode == LD_APERTURE_CUSTOM) {  // buildCustomPupilAmplitude, CpuReference.cpp:715-721
+        const CustomAperture* ca = t_custom;
+        if (ca == nullptr || ca->img.p == nullptr) throw Fail{LD_ERR_ARG, "custom-aperture-image-not-set"};
+        pp.custom = static_cast<const float*>(ca->img.p);
+        pp.cw = ca->w;
+        pp.ch = ca->h;
+        const float aspect = static_cast<float>(ca->w) / static_cast<float>(std::max(1, ca->h));
+        pp.fit_hw = aspect >= 1.0f ? 1.0f : aspect;
+        pp.fit_hh = aspect >= 1.0f ? 1.0f / aspect : 1.0f;
+        pp.vanes = 0;
+        pp.obstruction = 0.0f;
+    }
     // per-mode constants with the reference's float expressions
     const float outer = 0.86f;
     const float rnd = pp.roundness;
@@ -674,6 +704,10 @@ std::string bank_key(const ld_params& p, const std::vector<float>& wl) {
     k = append_bytes(k, p.noll, sizeof(p.noll));
     k = append_bytes(k, wl.data(), wl.size() * sizeof(float));
     k = append_bytes(k, &p.fft_form, sizeof(p.fft_form));
+    if (p.aperture_mode == LD_APERTURE_CUSTOM && t_custom != nullptr) {  // the image, as the reference keys its path
+        const uint64_t img[3] = {t_custom->digest, static_cast<uint64_t>(t_custom->w), static_cast<uint64_t>(t_custom->h)};
+        k = append_bytes(k, img, sizeof(img));
+    }
     return k;
 }
 
@@ -731,8 +765,10 @@ void validate_params(const ld_params& p) {
         throw Fail{LD_ERR_UNSUPPORTED, "unsupported-split-look-with-cufft-form"};
     if (p.input_transfer != LD_TRANSFER_LINEAR && p.input_transfer != LD_TRANSFER_DAVINCI_INTERMEDIATE)
         throw Fail{LD_ERR_ARG, "invalid-input-transfer"};
-    if (p.aperture_mode == LD_APERTURE_CUSTOM)  // image loader: WIC / ImageIO only (LensDiffApertureImage.cpp)
-        throw Fail{LD_ERR_UNSUPPORTED, "unsupported-custom-aperture"};
+    // Custom: the image the host decoded and handed over with ld_set_custom_aperture
+    // (the reference's own loader is WIC / ImageIO only, LensDiffApertureImage.cpp)
+    if (p.aperture_mode == LD_APERTURE_CUSTOM && (t_custom == nullptr || t_custom->img.p == nullptr))
+        throw Fail{LD_ERR_ARG, "custom-aperture-image-not-set"};
     if (p.aperture_mode < LD_APERTURE_CIRCLE || p.aperture_mode > LD_APERTURE_SNOWFLAKE)
         throw Fail{LD_ERR_ARG, "invalid-aperture-mode"};
     if (p.apodization_mode < 0 || p.apodization_mode > 2) throw Fail{LD_ERR_ARG, "invalid-apodization-mode"};
@@ -1898,7 +1934,7 @@ void ld_destroy(ld_ctx* c) {
     DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,    &c->frameB,
                       &c->calib,  &c->calib_psf, &c->err_word,  &c->pupil_pre,  &c->effect,    &c->cf_grid,
                       &c->cf_planes, &c->cf_sd,  &c->cf_prod,   &c->work,       &c->scatter_canvas,
-                      &c->scatter_ks, &c->dft,  &c->debug,      &c->selftest};
+                      &c->scatter_ks, &c->dft,  &c->debug,      &c->selftest, &c->custom.img};
     c->cufft.release();
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
@@ -2232,6 +2268,46 @@ int ld_import_kernel_spectra(ld_ctx* ctx, const ld_params* params, int32_t width
             st->grid_used_h = sg.g.Py;
         }
     });
+}
+
+int ld_set_custom_aperture(ld_ctx* c, const float* values, int32_t width, int32_t height, int32_t normalize,
+                           int32_t invert) {
+    if (!c) return LD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    DeviceGuard g(c->device);
+    if (values == nullptr) {  // clear
+        free_buf(c, c->custom.img);
+        c->custom = CustomAperture{};
+        return LD_OK;
+    }
+    if (width <= 0 || height <= 0 || static_cast<int64_t>(width) * height > (int64_t(1) << 26)) return LD_ERR_ARG;
+    // LoadLensDiffPreparedApertureImage (LensDiffApertureImage.cpp:367-399):
+    // optional min/max normalisation clamped to [0, 1], then optional inversion
+    std::vector<float> v(values, values + static_cast<size_t>(width) * height);
+    float lo = v.front(), hi = v.front();
+    for (float x : v) {
+        lo = std::min(lo, x);
+        hi = std::max(hi, x);
+    }
+    if (normalize && hi > lo) {
+        const float scale = 1.0f / (hi - lo);
+        for (float& x : v) x = std::min(std::max((x - lo) * scale, 0.0f), 1.0f);
+    }
+    if (invert)
+        for (float& x : v) x = 1.0f - x;
+    uint64_t h = 1469598103934665603ull;  // FNV-1a of the prepared values
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(v.data());
+    for (size_t i = 0; i < v.size() * sizeof(float); ++i) h = (h ^ b[i]) * 1099511628211ull;
+    try {
+        float* d = static_cast<float*>(ensure(c, c->custom.img, v.size() * sizeof(float)));
+        check_cuda(cudaMemcpy(d, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice), "custom-aperture-upload");
+    } catch (const Fail& f) {
+        return f.code;
+    }
+    c->custom.w = width;
+    c->custom.h = height;
+    c->custom.digest = h;
+    return LD_OK;
 }
 
 int ld_inject_alloc_failure(ld_ctx* c, int32_t after) {
@@ -2890,7 +2966,8 @@ int ld_raw_psf(ld_ctx* ctx, const ld_params* params, int wavelength_index, float
     return run_guarded(ctx, st, [&]() {
         const ld_params& p = *params;
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        if (p.aperture_mode == LD_APERTURE_CUSTOM) throw Fail{LD_ERR_UNSUPPORTED, "unsupported-custom-aperture"};
+        if (p.aperture_mode == LD_APERTURE_CUSTOM && (t_custom == nullptr || t_custom->img.p == nullptr))
+            throw Fail{LD_ERR_ARG, "custom-aperture-image-not-set"};
         if (p.aperture_mode < LD_APERTURE_CIRCLE || p.aperture_mode > LD_APERTURE_SNOWFLAKE)
             throw Fail{LD_ERR_ARG, "invalid-aperture-mode"};
         fill_sizes(st, p);
@@ -2941,6 +3018,7 @@ namespace {
 int run_guarded(ld_ctx* ctx, ld_status* st, const std::function<void()>& fn) {
     std::lock_guard<std::mutex> lock(ctx->mu);
     DeviceGuard g(ctx->device);
+    CustomScope custom(&ctx->custom);
     try {
         fn();
     } catch (const Fail& f) {

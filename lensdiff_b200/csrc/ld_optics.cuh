@@ -43,6 +43,12 @@ struct PupilParams {
     float snow_arm_cs[6], snow_arm_sn[6];
     float snow_br_cs[6][2], snow_br_sn[6][2];
     float snow_t[5], snow_len[5];
+    // Custom: the prepared amplitude image (device, ch rows of cw) and its
+    // fit inside the unit square (buildCustomPupilAmplitude's fitHalfWidth /
+    // fitHalfHeight); null for the other modes
+    const float* custom;
+    int cw, ch;
+    float fit_hw, fit_hh;
 };
 
 struct PhaseCoeffs {
@@ -158,11 +164,47 @@ __device__ __forceinline__ bool spiral_open(const PupilParams& p, float nx, floa
 }
 
 // buildPupilAmplitude per pixel (LensDiffCpuReference.cpp:778-818)
+// sampleImageBilinear (LensDiffCpuReference.cpp:682-705) on the custom image.
+__device__ __forceinline__ float custom_sample(const PupilParams& p, float x, float y) {
+    if (x < 0.0f || y < 0.0f || x > static_cast<float>(p.cw - 1) || y > static_cast<float>(p.ch - 1)) return 0.0f;
+    const int x0 = static_cast<int>(floorf(x));
+    const int y0 = static_cast<int>(floorf(y));
+    const int x1 = min(x0 + 1, p.cw - 1);
+    const int y1 = min(y0 + 1, p.ch - 1);
+    const float tx = __fsub_rn(x, static_cast<float>(x0));
+    const float ty = __fsub_rn(y, static_cast<float>(y0));
+    const float v00 = __ldg(p.custom + static_cast<size_t>(y0) * p.cw + x0);
+    const float v10 = __ldg(p.custom + static_cast<size_t>(y0) * p.cw + x1);
+    const float v01 = __ldg(p.custom + static_cast<size_t>(y1) * p.cw + x0);
+    const float v11 = __ldg(p.custom + static_cast<size_t>(y1) * p.cw + x1);
+    const float vx0 = __fadd_rn(v00, __fmul_rn(__fsub_rn(v10, v00), tx));
+    const float vx1 = __fadd_rn(v01, __fmul_rn(__fsub_rn(v11, v01), tx));
+    return __fadd_rn(vx0, __fmul_rn(__fsub_rn(vx1, vx0), ty));
+}
+
+// buildCustomPupilAmplitude per pixel (LensDiffCpuReference.cpp:707-756): the
+// image, rotated with the aperture and fitted into the outer circle, times
+// the apodisation; no obstruction or vanes.  Unfused float operations, as the
+// reference evaluates them, so the fit and range decisions agree.
+__device__ __forceinline__ float custom_amplitude(const PupilParams& p, float dx, float dy) {
+    const float radius = sqrtf(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+    if (radius > kOuterRadius || p.custom == nullptr) return 0.0f;
+    const float rx = __fsub_rn(__fmul_rn(dx, p.phase_cs), __fmul_rn(dy, p.phase_sn));
+    const float ry = __fadd_rn(__fmul_rn(dx, p.phase_sn), __fmul_rn(dy, p.phase_cs));
+    const float ux = __fdiv_rn(rx, kOuterRadius);
+    const float uy = __fdiv_rn(ry, kOuterRadius);
+    if (fabsf(ux) > p.fit_hw || fabsf(uy) > p.fit_hh) return 0.0f;
+    const float sx = __fmul_rn(__fadd_rn(__fmul_rn(__fdiv_rn(ux, p.fit_hw), 0.5f), 0.5f), static_cast<float>(p.cw - 1));
+    const float sy = __fmul_rn(__fadd_rn(__fmul_rn(__fdiv_rn(uy, p.fit_hh), 0.5f), 0.5f), static_cast<float>(p.ch - 1));
+    return __fmul_rn(custom_sample(p, sx, sy), apodization(p.apod, __fdiv_rn(radius, kOuterRadius)));
+}
+
 __device__ __forceinline__ float pupil_amplitude(const PupilParams& p, int x, int y) {
     const float nx = pupil_coord(x, p.size);
     const float ny = pupil_coord(y, p.size);
     const float dx = nx - p.decx;
     const float dy = ny - p.decy;
+    if (p.mode == 4) return custom_amplitude(p, dx, dy);
     const float radius = sqrtf(dx * dx + dy * dy);
     bool inside;
     switch (p.mode) {

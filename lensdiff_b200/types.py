@@ -12,7 +12,7 @@ from __future__ import annotations
 import dataclasses
 import enum
 from dataclasses import dataclass, field
-from typing import List, Optional
+from typing import Any, List, Optional
 
 K_MAX_SPECTRAL_BINS = 9  # LensDiffTypes.h:12
 MAX_WAVELENGTHS = 64
@@ -172,6 +172,10 @@ class LensDiffParams:
     customAperturePath: str = ""
     customApertureNormalize: bool = True
     customApertureInvert: bool = False
+    # Extension: the Custom aperture's image as the host decoded it (a 2-D
+    # float array of amplitudes, rows first); the reference decodes
+    # customAperturePath with WIC / ImageIO, which this machine has not.
+    customApertureImage: Optional[Any] = None
     phaseMode: LensDiffPhaseMode = LensDiffPhaseMode.Off
     phaseDefocus: float = 0.0
     phaseAstigmatism0: float = 0.0

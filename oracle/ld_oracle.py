@@ -171,10 +171,69 @@ def apodization(mode: int, radial_norm):
     return np.ones_like(radial_norm, dtype=F)
 
 
+def prepared_aperture_image(values: np.ndarray, normalize: bool, invert: bool) -> np.ndarray:
+    """LoadLensDiffPreparedApertureImage, LensDiffApertureImage.cpp:367-399, on
+    an already decoded amplitude image (float32)."""
+    v = np.asarray(values, dtype=F).copy()
+    lo, hi = F(v.min()), F(v.max())
+    if normalize and hi > lo:
+        scale = F(F(1.0) / F(hi - lo))
+        v = np.clip(((v - lo).astype(F) * scale).astype(F), F(0.0), F(1.0)).astype(F)
+    if invert:
+        v = (F(1.0) - v).astype(F)
+    return v
+
+
+def custom_pupil_amplitude(p, image: np.ndarray) -> np.ndarray:
+    """buildCustomPupilAmplitude, LensDiffCpuReference.cpp:707-756, with the
+    bilinear sampleImageBilinear of :682-705 (float32 expressions)."""
+    size = pupil_size(p)
+    h, w = image.shape
+    nx, ny = _pixel_coords(size)
+    dx = (nx - F(p.pupilDecenterX)).astype(F)
+    dy = (ny - F(p.pupilDecenterY)).astype(F)
+    radius = np.sqrt((dx * dx + dy * dy).astype(F)).astype(F)
+    rot = _rotation_rad(p)
+    cs, sn = F(np.cos(-rot)), F(np.sin(-rot))
+    aspect = F(F(w) / F(max(1, h)))
+    fw = F(1.0) if aspect >= F(1.0) else aspect
+    fh = F(F(1.0) / aspect) if aspect >= F(1.0) else F(1.0)
+    rx = (dx * cs - dy * sn).astype(F)
+    ry = (dx * sn + dy * cs).astype(F)
+    ux = (rx / OUTER_RADIUS).astype(F)
+    uy = (ry / OUTER_RADIUS).astype(F)
+    keep = (radius <= OUTER_RADIUS) & (np.abs(ux) <= fw) & (np.abs(uy) <= fh)
+    sx = (((ux / fw).astype(F) * F(0.5) + F(0.5)).astype(F) * F(w - 1)).astype(F)
+    sy = (((uy / fh).astype(F) * F(0.5) + F(0.5)).astype(F) * F(h - 1)).astype(F)
+    inside = (sx >= 0) & (sy >= 0) & (sx <= F(w - 1)) & (sy <= F(h - 1))
+    xs = np.where(inside, sx, F(0)).astype(F)
+    ys = np.where(inside, sy, F(0)).astype(F)
+    x0 = np.floor(xs).astype(np.int64)
+    y0 = np.floor(ys).astype(np.int64)
+    x1 = np.minimum(x0 + 1, w - 1)
+    y1 = np.minimum(y0 + 1, h - 1)
+    tx = (xs - x0.astype(F)).astype(F)
+    ty = (ys - y0.astype(F)).astype(F)
+    img = image.astype(F)
+    vx0 = (img[y0, x0] + (img[y0, x1] - img[y0, x0]) * tx).astype(F)
+    vx1 = (img[y1, x0] + (img[y1, x1] - img[y1, x0]) * tx).astype(F)
+    sample = np.where(inside, (vx0 + (vx1 - vx0) * ty).astype(F), F(0))
+    amp = (sample * apodization(int(p.apodizationMode), (radius / OUTER_RADIUS).astype(F))).astype(F)
+    return np.where(keep, amp, F(0)).astype(F)
+
+
 def pupil_amplitude(p) -> np.ndarray:
-    """buildPupilAmplitude, LensDiffCpuReference.cpp:758-822 (Circle/Polygon/Hexagon)."""
+    """buildPupilAmplitude, LensDiffCpuReference.cpp:758-822 (Circle/Polygon/Hexagon;
+    Custom through custom_pupil_amplitude with the decoded image of
+    p.customApertureImage)."""
     size = pupil_size(p)
     mode = int(p.apertureMode)
+    if mode == 4:
+        img = getattr(p, "customApertureImage", None)
+        if img is None:
+            raise ValueError("Custom aperture without a decoded image")
+        prepared = prepared_aperture_image(img, bool(p.customApertureNormalize), bool(p.customApertureInvert))
+        return custom_pupil_amplitude(p, prepared)
     if mode not in (0, 1, 5):
         raise NotImplementedError(f"aperture mode {mode} is not restated")
     nx, ny = _pixel_coords(size)

@@ -236,3 +236,13 @@ def cuda_render(params, src_ptr: int, dst_ptr: int, width: int, height: int, str
                                      int(width) * 16, ctypes.c_void_p(dst_ptr), ctypes.c_void_p(stream_ptr), err, 256)
     if not ok:
         raise RuntimeError("reference RunLensDiffCuda: " + err.value.decode())
+
+
+def set_custom_aperture(values: np.ndarray, normalize: bool = True, invert: bool = False) -> None:
+    """Hands a decoded amplitude image to the reference's own aperture loader
+    (its cache), for the Custom aperture mode of later calls."""
+    v = np.ascontiguousarray(values, np.float32)
+    L = lib()
+    L.ldref_set_custom_aperture.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int]
+    L.ldref_set_custom_aperture(_f(v), v.shape[1], v.shape[0], 1 if normalize else 0, 1 if invert else 0)

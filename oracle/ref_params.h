@@ -5,8 +5,28 @@
 #include "LensDiffTypes.h"
 #include "lensdiff_b200.h"
 
+#include <string>
+
+// The Custom aperture's image as the checker handed it to the reference: the
+// path it sits under in the reference's own aperture-image cache and the
+// flags (set by ldref_set_custom_aperture in ref_shim.cpp).
+struct RefCustomAperture {
+    std::string path;
+    bool normalize = true;
+    bool invert = false;
+};
+inline RefCustomAperture& refCustomAperture() {
+    static RefCustomAperture c;
+    return c;
+}
+
 inline LensDiffParams toReference(const ld_params& p) {
     LensDiffParams r {};
+    if (p.aperture_mode == LD_APERTURE_CUSTOM) {
+        r.customAperturePath = refCustomAperture().path;
+        r.customApertureNormalize = refCustomAperture().normalize;
+        r.customApertureInvert = refCustomAperture().invert;
+    }
     r.extractionMode = static_cast<LensDiffExtractionMode>(p.extraction_mode);
     r.apertureMode = static_cast<LensDiffApertureMode>(p.aperture_mode);
     r.apodizationMode = static_cast<LensDiffApodizationMode>(p.apodization_mode);

@@ -12,6 +12,10 @@
 // the resulting oracle/_ref/libldref.so.
 
 #include "LensDiffCpuReference.cpp"  // reference TU, compiled in place
+// and its aperture-image loader, in place too, so the checker can seed the
+// loader's own cache with an image decoded here (the loader's decoders are
+// WIC / ImageIO only)
+#include "LensDiffApertureImage.cpp"
 
 #include "lensdiff_b200.h"
 #include "ref_params.h"
@@ -29,6 +33,27 @@ void copyStage(const std::string& s, char* out, int cap) {
 }  // namespace
 
 extern "C" {
+
+// Puts a decoded amplitude image (h rows of w floats) into the reference's
+// aperture-image cache (LensDiffApertureImage.cpp:301-365) under a path that
+// names no file, so LoadLensDiffPreparedApertureImage finds it there and
+// applies its own normalise / invert; Custom-mode calls then use it.
+void ldref_set_custom_aperture(const float* values, int w, int h, int normalize, int invert) {
+    const std::string path = "lensdiff-b200-checker-decoded-aperture";
+    LensDiffApertureImage img;
+    img.width = w;
+    img.height = h;
+    img.values.assign(values, values + static_cast<std::size_t>(w) * h);
+    {
+        std::lock_guard<std::mutex> lock(apertureImageCacheMutex());
+        CachedApertureImage& cached = apertureImageCache()[path];
+        cached.hasTimestamp = false;
+        cached.image = img;
+    }
+    refCustomAperture().path = path;
+    refCustomAperture().normalize = normalize != 0;
+    refCustomAperture().invert = invert != 0;
+}
 
 // Path sizes: N_p, S, R_max (LensDiffCpuReference.cpp:1709-1711).
 void ldref_sizes(const ld_params* p, int* pupil, int* raw, int* rmax) {
