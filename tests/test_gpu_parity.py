@@ -233,7 +233,7 @@ def test_error_behaviour_mirrors_reference(cache):
     req = image_request(src, dst, stream, frame_short_side=144)
     st = cache.render(req, p.copy(debugView=99))
     assert not st.ok and st.stage == "invalid-debug-view"
-    st = cache.render(req, p.copy(apertureMode=4))  # not built: refused, never silently wrong
-    assert st.code == 6 and "custom-aperture" in st.stage
+    st = cache.render(req, p.copy(apertureMode=4))  # Custom without a decoded image: refused, never silently wrong
+    assert st.code == 1 and st.stage == "custom-aperture-image-not-set"
     st = cache.render(req, p)
     assert st.ok
