@@ -173,39 +173,44 @@ __global__ void __launch_bounds__(256) dft_basis_kernel(DftBasisArgs a) {
     *reinterpret_cast<uint32_t*>(a.lo + off) = lo;
 }
 
-// Pupil field images of wavelength blockIdx.z: row m (pupil row row_lo + m)
+// Pupil field images of every wavelength: row m (pupil row row_lo + m)
 // over K-chunk c (pupil column col_lo + 32 c + q), the field
 // amplitude * exp(i 2 pi phase) as the row transform embeds it
 // (psf_rows_kernel; LensDiffCpuReference.cpp:831-845).
-// grid (mt_rows * 128 / 8, kc_rows, B), block (32, 8): lane q of warp row m
-// of K-chunk c (one 128-byte image row per warp).
+// grid (mt_rows * 128 / 8, kc_rows), block (32, 8): lane q of warp row m
+// of K-chunk c (one 128-byte image row per warp), looping over the
+// wavelengths.
 __global__ void __launch_bounds__(256) pupil_field_kernel(PsfBankArgs a, DftPlan d) {
-    const int b = blockIdx.z;
     const int c = blockIdx.y;
     const int m = blockIdx.x * 8 + threadIdx.y, q = threadIdx.x;
     const int np = a.pupil.size;
     const int y = a.row_lo + m, x = d.col_lo + c * 32 + q;
-    float fr = 0.0f, fi = 0.0f;
-    if (m < a.row_n && c * 32 + q < d.col_n && x < np && y < np) {
-        const WavelengthInfo* w = a.wl + b;
-        const float4 p = a.pupil_pre[static_cast<size_t>(y) * np + x];
+    // the pupil pre-pass of this pixel is read once and serves every
+    // wavelength (their fields differ only in the defocus term)
+    float4 p = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (m < a.row_n && c * 32 + q < d.col_n && x < np && y < np) p = a.pupil_pre[static_cast<size_t>(y) * np + x];
+    const size_t off0 = static_cast<size_t>(c) * d.pf_slab + img_byte(m, 2 * q);
+#pragma unroll 2
+    for (int b = 0; b < a.B; ++b) {
+        float fr = 0.0f, fi = 0.0f;
         if (p.x > 0.0f) {
+            const WavelengthInfo* w = a.wl + b;
             const float ph = (w->phase.enabled && p.w != 0.0f) ? p.y + w->phase.c[4] * p.z : 0.0f;
             if (ph == 0.0f) {
                 fr = p.x;
             } else {
                 float sn, cs;
-                sincosf(ph * 2.0f * kPiF, &sn, &cs);
+                sincospif(2.0f * ph, &sn, &cs);  // exp(i 2 pi phase), phase in waves
                 fr = p.x * cs;
                 fi = p.x * sn;
             }
         }
+        uint32_t hi, lo;
+        split_pair(fr, fi, &hi, &lo);
+        const size_t off = static_cast<size_t>(b) * d.pf_lambda + off0;
+        *reinterpret_cast<uint32_t*>(d.pf_hi + off) = hi;
+        *reinterpret_cast<uint32_t*>(d.pf_lo + off) = lo;
     }
-    uint32_t hi, lo;
-    split_pair(fr, fi, &hi, &lo);
-    const size_t off = static_cast<size_t>(b) * d.pf_lambda + static_cast<size_t>(c) * d.pf_slab + img_byte(m, 2 * q);
-    *reinterpret_cast<uint32_t*>(d.pf_hi + off) = hi;
-    *reinterpret_cast<uint32_t*>(d.pf_lo + off) = lo;
 }
 
 // ---- the GEMM --------------------------------------------------------------------------
@@ -395,7 +400,7 @@ void launch_dft_basis(const DftBasisArgs& a, cudaStream_t s) {
 
 void launch_pupil_field(const PsfBankArgs& a, const DftPlan& d, cudaStream_t s) {
     if (d.mt_rows <= 0 || d.kc_rows <= 0) return;
-    pupil_field_kernel<<<dim3(static_cast<unsigned>(d.mt_rows * kTileM / 8), static_cast<unsigned>(d.kc_rows), a.B),
+    pupil_field_kernel<<<dim3(static_cast<unsigned>(d.mt_rows * kTileM / 8), static_cast<unsigned>(d.kc_rows), 1),
                          dim3(32, 8), 0, s>>>(a, d);
 }
 

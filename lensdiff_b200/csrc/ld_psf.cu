@@ -280,10 +280,32 @@ __device__ __forceinline__ float sample_row(const Window& w, const ColTap& c, fl
 // otherwise (s3 = s1, the ceil(r) ring energies and peaks, the peak) in
 // place of the round(r) ring sums, which only the Split look's ring means
 // need (ring_sums_kernel, run when a Split render first uses the bank).
+// The bilinear path (no box filter: the canvas samples the |F|^2 window at
+// most one window pixel apart, scaleFactor >= 1) stages the window pixels a
+// 32 x 128 tile reads in shared memory first: at most 33 x 129 of them, with
+// one more on each side so that the span holds whatever the rounding of the
+// sample positions.
+constexpr int kStageW = kTile + 4, kStageH = kTallH + 4;
+
+// Rows / columns of the window that canvas coordinates c0 .. c1 sample
+// (sample_bilinear's x0 .. x1 of the first and last sample, clamped to the
+// window as it clamps them): [lo, hi] in window indices.
+__device__ __forceinline__ void stage_span(const Window& w, float rc, float kc, float inv, int c0, int c1, int* lo,
+                                           int* hi) {
+    const float p0 = rc + (static_cast<float>(c0) - kc) * inv;
+    const float p1 = rc + (static_cast<float>(c1) - kc) * inv;
+    const int whi = w.n - 1;
+    const int a0 = static_cast<int>(floorf(fmaxf(p0, 0.0f)));
+    const int a1 = min(static_cast<int>(floorf(fminf(fmaxf(p1, 0.0f), static_cast<float>(w.S - 1)))) + 1, w.S - 1);
+    *lo = min(max(a0 - 1 - w.x0, 0), whi);
+    *hi = min(max(a1 + 1 - w.x0, 0), whi);
+}
+
 template <bool FUSED>
 __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
     __shared__ float ring[kRingSpanTall];  // FUSED: the ceil(r) ring energies
     __shared__ unsigned int ring_p[FUSED ? kRingSpanTall : 1];
+    __shared__ float stage[kStageH][kStageW];
     const int b = blockIdx.z;
     const WavelengthInfo* wi = a.wl + b;
     const int K = a.K, R = a.R;
@@ -294,7 +316,6 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
         ring[i] = 0.0f;
         if constexpr (FUSED) ring_p[i] = 0u;
     }
-    __syncthreads();
     const Window w{a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride, a.win_stride, wi->win_x0,
                    wi->win_n, a.S};
     const float kc = static_cast<float>(K - 1) * 0.5f;
@@ -307,28 +328,83 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
     unsigned int lpeak = 0u;
     const int x = tx0 + threadIdx.x;
     const float dx = static_cast<float>(x) - kc;
-    const ColTap ct = col_tap(w, rc + dx * inv);
+    int cx0 = 0, cx1 = -1, cy0 = 0, cy1 = -1;
+    if (taps == 0) {
+        stage_span(w, rc, kc, inv, tx0, min(tx0 + kTile, K) - 1, &cx0, &cx1);
+        stage_span(w, rc, kc, inv, ty0, min(ty0 + kTallH, K) - 1, &cy0, &cy1);
+    }
+    const int sw = cx1 - cx0 + 1, sh = cy1 - cy0 + 1;
+    if (taps == 0 && sw <= kStageW && sh <= kStageH) {  // uniform per CTA (one wavelength, one tile)
+        for (int i = tid; i < sw * sh; i += 256) {
+            const int r = i / sw, c = i - r * sw;
+            stage[r][c] = __ldg(w.p + static_cast<size_t>(cy0 + r) * w.stride + cx0 + c);
+        }
+        __syncthreads();
+        // the column half of each sample, in staged coordinates
+        const ColTap ct = col_tap(w, rc + dx * inv);
+        const int sx0 = ct.ax0 - cx0, sx1 = ct.ax1 - cx0;
+        const float lim = static_cast<float>(w.S - 1);
+        const int hi = w.n - 1;
 #pragma unroll 4
-    for (int i = 0; i < kTallH / 8; ++i) {
-        const int y = ty0 + threadIdx.y + 8 * i;
-        if (y >= K) break;  // uniform: a warp is one canvas row (the last tile row is mostly past K)
-        const bool in = x < K;
-        float v = 0.0f;
-        int slot = -1;
-        if (in) {
+        for (int i = 0; i < kTallH / 8; ++i) {
+            const int y = ty0 + threadIdx.y + 8 * i;
+            if (y >= K) break;  // uniform: a warp is one canvas row
+            if (x >= K) continue;
             const float dy = static_cast<float>(y) - kc;
-            v = taps == 0 ? sample_row(w, ct, rc + dy * inv)
-                          : sample_filtered(w, rc + dx * inv, rc + dy * inv, inv, taps, step);
+            const float yy = rc + dy * inv;
+            float v = 0.0f;
+            if (ct.in && !(yy < 0.0f || yy > lim)) {  // sample_row's arithmetic on staged pixels
+                const int y0 = static_cast<int>(floorf(yy));
+                const int y1 = min(y0 + 1, w.S - 1);
+                const float ty = yy - static_cast<float>(y0);
+                const int sy0 = min(max(y0 - w.x0, 0), hi) - cy0;
+                const int sy1 = min(max(y1 - w.x0, 0), hi) - cy0;
+                const float v00 = stage[sy0][sx0], v10 = stage[sy0][sx1];
+                const float v01 = stage[sy1][sx0], v11 = stage[sy1][sx1];
+                const float vx0 = v00 + (v10 - v00) * ct.tx;
+                const float vx1 = v01 + (v11 - v01) * ct.tx;
+                v = vx0 + (vx1 - vx0) * ty;
+            }
             canvas[static_cast<size_t>(y) * K + x] = v;
             lsum += v;
+            const float rr = sqrtf(dx * dx + dy * dy);
             if constexpr (FUSED) {
                 lpeak = max(lpeak, __float_as_uint(v));
-                slot = min(R, static_cast<int>(ceilf(sqrtf(dx * dx + dy * dy)))) - rbase;
+                const int slot = min(R, static_cast<int>(ceilf(rr))) - rbase;
+                if (v != 0.0f) {
+                    atomicAdd(&ring[slot], v);
+                    atomicMax(&ring_p[slot], __float_as_uint(v));
+                }
             } else {
-                slot = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy)))) - rbase;
+                const int slot = min(R, static_cast<int>(roundf(rr))) - rbase;
+                if (v != 0.0f) atomicAdd(&ring[slot], v);
             }
         }
-        warp_runs_accumulate<FUSED>(slot, v, ring, ring_p);
+    } else {  // box-filtered samples (and any span too wide to stage) read the window directly
+        __syncthreads();
+        const ColTap ct = col_tap(w, rc + dx * inv);
+#pragma unroll 4
+        for (int i = 0; i < kTallH / 8; ++i) {
+            const int y = ty0 + threadIdx.y + 8 * i;
+            if (y >= K) break;  // uniform: a warp is one canvas row (the last tile row is mostly past K)
+            const bool in = x < K;
+            float v = 0.0f;
+            int slot = -1;
+            if (in) {
+                const float dy = static_cast<float>(y) - kc;
+                v = taps == 0 ? sample_row(w, ct, rc + dy * inv)
+                              : sample_filtered(w, rc + dx * inv, rc + dy * inv, inv, taps, step);
+                canvas[static_cast<size_t>(y) * K + x] = v;
+                lsum += v;
+                if constexpr (FUSED) {
+                    lpeak = max(lpeak, __float_as_uint(v));
+                    slot = min(R, static_cast<int>(ceilf(sqrtf(dx * dx + dy * dy)))) - rbase;
+                } else {
+                    slot = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy)))) - rbase;
+                }
+            }
+            warp_runs_accumulate<FUSED>(slot, v, ring, ring_p);
+        }
     }
     __syncthreads();
     const size_t ro = static_cast<size_t>(b) * (R + 1);
@@ -577,8 +653,22 @@ __global__ void __launch_bounds__(256) support_kernel(PsfBankArgs a) {
 // applySupportBoundaryTaper (LensDiffCpuReference.cpp:1038-1058, :957-982).
 // The canvas keeps the shaped kernel; the crop and the taper are applied
 // where the kernel is read (combine_kernel, split_sums_kernel, export_kernel).
-// One CTA sums 8 rows of the crop box, eight reads in flight per thread.
+// The taper is 1 up to radius `start` and 0 from `extent` on, and every pixel
+// with r < extent lies in the crop box, so s4 = (the ceil(r) ring energies of
+// rings 0 .. S0 = floor(start)) / s3 + the annulus S0 < r < extent pixel by
+// pixel.  A pixel's ring is ceil(sqrtf(dx^2 + dy^2)) <= S0 exactly when
+// dx^2 + dy^2 <= S0^2 (integers; exact below 2^24), so each crop row reads
+// only its |dx| > isqrt(S0^2 - dy^2) part.  One warp per crop row, eight
+// reads in flight per thread.
 constexpr int kCropRows = 8;
+
+__device__ __forceinline__ int isqrt_floor(int v) {  // floor(sqrt(v)), v >= 0
+    int r = static_cast<int>(sqrtf(static_cast<float>(v)));
+    while (r > 0 && r * r > v) --r;
+    while ((r + 1) * (r + 1) <= v) ++r;
+    return r;
+}
+
 __global__ void __launch_bounds__(256) crop_sum_kernel(PsfBankArgs a) {
     const int b = blockIdx.y;
     const PsfScalars& sc = a.scalars[b];
@@ -588,32 +678,43 @@ __global__ void __launch_bounds__(256) crop_sum_kernel(PsfBankArgs a) {
     if (y0 > R + rho) return;  // uniform
     const float inv_s3 = static_cast<float>(1.0 / sc.s3);
     const float extent = sc.extent, fade = sc.fade, start = sc.start;
-    const int side = 2 * rho + 1;
+    const int s0 = static_cast<int>(floorf(start));
     const int lane = threadIdx.x & 31;
     const int y = y0 + static_cast<int>(threadIdx.x >> 5);  // one warp per crop row
     float lsum = 0.0f;
     if (y <= R + rho) {
-        const float* row = a.canvas + static_cast<size_t>(b) * K * K + static_cast<size_t>(y) * K + (R - rho);
-        const float dy = static_cast<float>(y - R);
-        const float dy2 = dy * dy;
+        const float* row = a.canvas + static_cast<size_t>(b) * K * K + static_cast<size_t>(y) * K + R;  // dx = 0
+        const int dyi = y - R;
+        const int in2 = s0 * s0 - dyi * dyi;
+        const int xin = in2 >= 0 ? isqrt_floor(in2) : -1;  // |dx| <= xin: inside ring s0
+        const int len = rho - xin;                          // pixels per side
+        const float dy2 = static_cast<float>(dyi) * static_cast<float>(dyi);
         constexpr int kU = 8;
-        for (int c0 = lane; c0 < side; c0 += kU * 32) {
+        for (int t0 = lane; t0 < 2 * len; t0 += kU * 32) {
             float v[kU];
+            int dxs[kU];
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                const int c = c0 + u * 32;
-                v[u] = c < side ? __ldg(row + c) : 0.0f;
+                const int t = t0 + u * 32;
+                dxs[u] = t < len ? t - rho : xin + 1 + (t - len);
+                v[u] = t < 2 * len ? __ldg(row + dxs[u]) : 0.0f;
             }
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                const int c = c0 + u * 32;
-                if (c >= side) break;
-                const float dx = static_cast<float>(c - rho);
+                if (t0 + u * 32 >= 2 * len) break;
+                const float dx = static_cast<float>(dxs[u]);
                 lsum += (v[u] * inv_s3) * taper_weight(sqrtf(dx * dx + dy2), extent, fade, start);
             }
         }
     }
-    const double tot = block_sum(static_cast<double>(lsum));
+    double tot = block_sum(static_cast<double>(lsum));
+    if (blockIdx.x == 0) {  // the rings inside the taper's flat part
+        const double* e = a.ring_ceil + static_cast<size_t>(b) * (R + 1);
+        double ring = 0.0;
+        for (int r = threadIdx.x; r <= s0; r += blockDim.x) ring += e[r];
+        ring = block_sum(ring);
+        if (threadIdx.x == 0) tot += ring / sc.s3;
+    }
     if (threadIdx.x == 0) atomicAdd(&a.scalars[b].s4, tot);
 }
 
