@@ -349,11 +349,10 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
         for (int i = 0; i < kTallH / 8; ++i) {
             const int y = ty0 + threadIdx.y + 8 * i;
             if (y >= K) break;  // uniform: a warp is one canvas row
-            if (x >= K) continue;
             const float dy = static_cast<float>(y) - kc;
             const float yy = rc + dy * inv;
             float v = 0.0f;
-            if (ct.in && !(yy < 0.0f || yy > lim)) {  // sample_row's arithmetic on staged pixels
+            if (x < K && ct.in && !(yy < 0.0f || yy > lim)) {  // sample_row's arithmetic on staged pixels
                 const int y0 = static_cast<int>(floorf(yy));
                 const int y1 = min(y0 + 1, w.S - 1);
                 const float ty = yy - static_cast<float>(y0);
@@ -365,20 +364,17 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
                 const float vx1 = v01 + (v11 - v01) * ct.tx;
                 v = vx0 + (vx1 - vx0) * ty;
             }
-            canvas[static_cast<size_t>(y) * K + x] = v;
+            if (x < K) canvas[static_cast<size_t>(y) * K + x] = v;
             lsum += v;
             const float rr = sqrtf(dx * dx + dy * dy);
+            int slot;
             if constexpr (FUSED) {
                 lpeak = max(lpeak, __float_as_uint(v));
-                const int slot = min(R, static_cast<int>(ceilf(rr))) - rbase;
-                if (v != 0.0f) {
-                    atomicAdd(&ring[slot], v);
-                    atomicMax(&ring_p[slot], __float_as_uint(v));
-                }
+                slot = min(R, static_cast<int>(ceilf(rr))) - rbase;
             } else {
-                const int slot = min(R, static_cast<int>(roundf(rr))) - rbase;
-                if (v != 0.0f) atomicAdd(&ring[slot], v);
+                slot = min(R, static_cast<int>(roundf(rr))) - rbase;
             }
+            warp_runs_accumulate<FUSED>(x < K ? slot : -1, v, ring, ring_p);
         }
     } else {  // box-filtered samples (and any span too wide to stage) read the window directly
         __syncthreads();
@@ -686,22 +682,26 @@ __global__ void __launch_bounds__(256) crop_sum_kernel(PsfBankArgs a) {
         const float* row = a.canvas + static_cast<size_t>(b) * K * K + static_cast<size_t>(y) * K + R;  // dx = 0
         const int dyi = y - R;
         const int in2 = s0 * s0 - dyi * dyi;
-        const int xin = in2 >= 0 ? isqrt_floor(in2) : -1;  // |dx| <= xin: inside ring s0
-        const int len = rho - xin;                          // pixels per side
+        // |dx| <= xin lies inside ring s0; a row that misses that disc reads
+        // all of [-rho, rho] (left part [-rho, 0], right part [1, rho])
+        const int xin = in2 >= 0 ? isqrt_floor(in2) : -1;
+        const int nl = xin >= 0 ? rho - xin : rho + 1;  // left part: dx = -rho .. -rho + nl - 1
+        const int r0 = xin >= 0 ? xin + 1 : 1;          // right part: dx = r0 .. rho
+        const int n = nl + (rho - r0 + 1);
         const float dy2 = static_cast<float>(dyi) * static_cast<float>(dyi);
         constexpr int kU = 8;
-        for (int t0 = lane; t0 < 2 * len; t0 += kU * 32) {
+        for (int t0 = lane; t0 < n; t0 += kU * 32) {
             float v[kU];
             int dxs[kU];
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 const int t = t0 + u * 32;
-                dxs[u] = t < len ? t - rho : xin + 1 + (t - len);
-                v[u] = t < 2 * len ? __ldg(row + dxs[u]) : 0.0f;
+                dxs[u] = t < nl ? t - rho : r0 + (t - nl);
+                v[u] = t < n ? __ldg(row + dxs[u]) : 0.0f;
             }
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                if (t0 + u * 32 >= 2 * len) break;
+                if (t0 + u * 32 >= n) break;
                 const float dx = static_cast<float>(dxs[u]);
                 lsum += (v[u] * inv_s3) * taper_weight(sqrtf(dx * dx + dy2), extent, fade, start);
             }

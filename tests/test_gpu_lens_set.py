@@ -161,6 +161,6 @@ def test_lens_set_rejects_bad_arguments(cache):
     st = cache.build_psf_banks([], torch.cuda.current_stream())
     assert not st.ok and st.stage == "invalid-lens-count"
     bad = _lenses()[:2]
-    bad[1] = bad[1].copy(apertureMode=4)  # custom image aperture: not built
+    bad[1] = bad[1].copy(apertureMode=4)  # Custom aperture with no decoded image handed over
     st = cache.build_psf_banks(bad, torch.cuda.current_stream())
-    assert not st.ok and st.stage == "unsupported-custom-aperture"
+    assert not st.ok and st.stage == "custom-aperture-image-not-set"
