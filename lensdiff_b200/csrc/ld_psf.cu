@@ -816,24 +816,35 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineArgs a) {
 #pragma unroll
             for (int k = 0; k < NK; ++k) acc[p][k] = 0.0f;
         }
-#pragma unroll 2
-        for (int b = 0; b < B; ++b) {
-            const CombineBin& cb = bin[b];
-            const int rho_b = cb.rho;
-            const float* cv = a.bank.canvas + b * plane;
-            float v[kP];
+        // kL wavelengths' reads are issued before any of them is used, so
+        // kL * kP reads per thread are in flight over the canvases
+        constexpr int kL = 4;
+        for (int b0 = 0; b0 < B; b0 += kL) {
+            float v[kL][kP];
 #pragma unroll
-            for (int p = 0; p < kP; ++p) v[p] = aix[p] <= rho_b ? __ldg(cv + idx[p]) : 0.0f;
-            const float ext_b = cb.ext, fade_b = cb.fade, start_b = cb.start;
-            float w[NK];
+            for (int l = 0; l < kL; ++l) {
+                const int b = b0 + l;
+                const int rho_b = b < B ? bin[b].rho : -1;
+                const float* cv = a.bank.canvas + static_cast<size_t>(b < B ? b : 0) * plane;
 #pragma unroll
-            for (int k = 0; k < NK; ++k) w[k] = cb.w[k];
+                for (int p = 0; p < kP; ++p) v[l][p] = aix[p] <= rho_b ? __ldg(cv + idx[p]) : 0.0f;
+            }
 #pragma unroll
-            for (int p = 0; p < kP; ++p) {
-                if (v[p] != 0.0f) {  // else outside the crop box, or a zero kernel value
-                    const float f = v[p] * taper_weight(rad[p], ext_b, fade_b, start_b);
+            for (int l = 0; l < kL; ++l) {  // per pixel the wavelengths are summed in order
+                const int b = b0 + l;
+                if (b >= B) break;
+                const CombineBin& cb = bin[b];
+                const float ext_b = cb.ext, fade_b = cb.fade, start_b = cb.start;
+                float w[NK];
 #pragma unroll
-                    for (int k = 0; k < NK; ++k) acc[p][k] += w[k] * f;
+                for (int k = 0; k < NK; ++k) w[k] = cb.w[k];
+#pragma unroll
+                for (int p = 0; p < kP; ++p) {
+                    if (v[l][p] != 0.0f) {  // else outside the crop box, or a zero kernel value
+                        const float f = v[l][p] * taper_weight(rad[p], ext_b, fade_b, start_b);
+#pragma unroll
+                        for (int k = 0; k < NK; ++k) acc[p][k] += w[k] * f;
+                    }
                 }
             }
         }
