@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--slots", type=int, default=4, help="server slots of --serving")
     ap.add_argument("--no-comparators", action="store_true",
                     help="skip timing the other transform chains on the same workload")
+    ap.add_argument("--no-other-workloads", action="store_true",
+                    help="skip the short runs of the 8x8-zone and lens-set workloads added to the line")
     ap.add_argument("--no-error-check", action="store_true",
                     help="skip stating each form's error against the FP64 oracle (outside the timed regions)")
     return ap.parse_args()
@@ -406,6 +408,65 @@ def reference_cuda_comparator(args, cache, dev):
             "own_chosen_at_reference_setting": dict(summary(own_ms), config=setting + ", cold",
                                                     warm=summary(own_warm_ms),
                                                     out_diff_vs_reference_cuda=float(f"{diff:.3e}"))}
+
+
+def other_workloads(dev):
+    """Short device-timed runs of the other measured workloads, so one default
+    run reports them too (full runs: --workload zones8, --lens-set):
+      zones8    the UHD 31-wavelength frame with an 8x8 grid of field zones
+                (64 banks, 64 convolutions per frame), cold, 3 frames;
+      lens_set  the banks of 256 unrelated lenses per step (pupil 128-1024,
+                PSF 2-4x, 8-64 wavelengths), cold, 2 steps."""
+    import torch
+    from lensdiff_b200 import synthetic as S
+    from lensdiff_b200.backend import LensDiffPsfBankCache, image_request
+
+    out = {}
+    stream = torch.cuda.Stream(device=dev)
+
+    def timed(fn, warm, n):
+        for i in range(warm):
+            fn(i)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(n):
+            fn(warm + i)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / n
+
+    p, frame = S.workload_zones8()
+    cache = LensDiffPsfBankCache(dev.index or 0)
+    src = torch.from_numpy(frame).to(dev)
+    dst = torch.empty_like(src)
+    req = image_request(src, dst, stream, frame_short_side=p.frameShortSidePx)
+
+    def zone_frame(i):
+        with torch.cuda.stream(stream):
+            st = cache.render(req, p.copy(phaseDefocus=p.phaseDefocus + 1e-6 * (i + 1)))
+        if not st.ok:
+            raise RuntimeError(f"zones8 render failed: {st}")
+
+    ms = timed(zone_frame, 1, 3)
+    out["zones8"] = {"value": 1000.0 / ms, "unit": "frames/s", "ms_per_step": ms, "bank": "cold",
+                     "config": "3840x2160, 8x8 field zones (64 banks x 31 wavelengths), pupil 512 -> PSF 2048"}
+    cache.close()
+    lenses = S.lens_instances(256)
+    cache = LensDiffPsfBankCache(dev.index or 0)
+
+    def lens_step(i):
+        st = cache.build_psf_banks([q.copy(phaseDefocus=q.phaseDefocus + 1e-6 * (i + 1)) for q in lenses], stream)
+        if not st.ok or st.banks_rebuilt != len(lenses):
+            raise RuntimeError(f"lens-set build failed: {st}")
+
+    ms = timed(lens_step, 1, 2)
+    out["lens_set"] = {"value": 256 * 1000.0 / ms, "unit": "lens banks/s", "ms_per_step": ms, "bank": "cold",
+                       "config": "256 unrelated lenses per step: pupil 128-1024, PSF 2-4x, 8-64 wavelengths"}
+    if cache.check_device_errors():
+        raise RuntimeError("device error word set by the other workloads")
+    cache.close()
+    return out
 
 
 def error_check(args, p, frame, cache, stream, dev, forms):
@@ -895,6 +956,10 @@ def main():
         forms = [n for n in comparators if n in FORM_NAMES.values()] + [FORM_NAMES[args.fft_form]]
         errors = error_check(args, p, frame, cache, stream, dev, forms)
 
+    workloads = None
+    if rank == 0 and ws == 1 and args.workload == "uhd31" and not args.no_other_workloads:
+        workloads = other_workloads(dev)
+
     # ---- CPU baseline (rank 0, N=1) ----------------------------------------
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -929,6 +994,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "comparators": comparators,
+            "workloads": workloads,
         }
         if errors:
             for name, c in comparators.items():
