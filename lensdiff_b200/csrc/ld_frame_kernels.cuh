@@ -159,14 +159,18 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
     const int64_t pitch = a.src_pitch;
     const bool aligned = ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(pitch)) & 15) == 0;
     const int W = a.W, H = a.H, M = a.g.M;
+    const int tx0 = a.tile_x0, ty0 = a.tile_y0;  // grid origin in frame pixels (tiles)
     // the source rows of this CTA and of the CTA one resident generation
-    // later go to L2 through the bulk-copy engine while this CTA loads
+    // later (their part under the grid) go to L2 through the bulk-copy
+    // engine while this CTA loads
     if (!FROM_EFFECT && aligned && threadIdx.x == 0) {
-        const uint32_t row_bytes = static_cast<uint32_t>(W) * 16u;
+        const int px0 = max(0, tx0), px1 = min(W, tx0 + 2 * M);
+        const uint32_t span = px1 > px0 ? static_cast<uint32_t>(px1 - px0) * 16u : 0u;
         const int later = y0 + a.ahead * RPC;
-        for (int r = 0; r < RPC; ++r) {
-            if (y0 + r < H) bulk_prefetch_l2(a.src + static_cast<int64_t>(y0 + r) * pitch, row_bytes);
-            if (a.ahead > 0 && later + r < H) bulk_prefetch_l2(a.src + static_cast<int64_t>(later + r) * pitch, row_bytes);
+        for (int r = 0; r < RPC && span > 0; ++r) {
+            const int fy = y0 + r + ty0, fl = later + r + ty0;
+            if (fy >= 0 && fy < H) bulk_prefetch_l2(a.src + static_cast<int64_t>(fy) * pitch + px0 * 16, span);
+            if (a.ahead > 0 && fl >= 0 && fl < H) bulk_prefetch_l2(a.src + static_cast<int64_t>(fl) * pitch + px0 * 16, span);
         }
     }
     const SelectionParams sel = a.sel;
@@ -183,12 +187,12 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
             const int i = i0 + u * T;
             const int r = i / M;
             const int idx = i - r * M;
-            const int y = y0 + r;
-            const int x0 = 2 * idx;
+            const int y = y0 + r + ty0;   // frame row
+            const int x0 = 2 * idx + tx0;  // frame column of the pair's first pixel
             const unsigned char* row = a.src + static_cast<int64_t>(y) * pitch;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                const bool in = i < RPC * M && y < H && x0 + h < W;
+                const bool in = i < RPC * M && y >= 0 && y < H && x0 + h >= 0 && x0 + h < W;
                 if constexpr (FROM_EFFECT)
                     px[u][h] = in ? a.effect[static_cast<int64_t>(y) * W + x0 + h] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 else
@@ -379,7 +383,8 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
     const int yo = a.effect_mode == kEffectComposite ? a.out_y1 + bid
                                                      : a.src_y1 + (a.effect_mode == kEffectAccumulate ? a.row0 + bid : bid);
     const int sy = yo - a.src_y1;
-    const bool have = sy >= 0 && sy < a.H;
+    const int by = sy - a.tile_y0;  // the grid row of frame row sy
+    const bool have = sy >= 0 && sy < a.H && by >= 0 && by < a.Hp;
     const int M = a.g.M;
     // composite: this row's source pixels, and those of the row one resident
     // generation later, go to L2 while the row's spectrum loads and transforms
@@ -412,11 +417,11 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
                     const int c = i - pk * C;
                     if constexpr (H16) {
                         const __half2* Bh = reinterpret_cast<const __half2*>(a.Bout);
-                        xp[u] = from_half2(__ldcs(&Bh[b_index(pk, sy, c, Hp, C)]), __ldg(&a.bscale[pk]));
-                        xq[u] = from_half2(__ldcs(&Bh[b_index(M - pk, sy, c, Hp, C)]), __ldg(&a.bscale[M - pk]));
+                        xp[u] = from_half2(__ldcs(&Bh[b_index(pk, by, c, Hp, C)]), __ldg(&a.bscale[pk]));
+                        xq[u] = from_half2(__ldcs(&Bh[b_index(M - pk, by, c, Hp, C)]), __ldg(&a.bscale[M - pk]));
                     } else {
-                        xp[u] = __ldcs(&a.Bout[b_index(pk, sy, c, Hp, C)]);
-                        xq[u] = __ldcs(&a.Bout[b_index(M - pk, sy, c, Hp, C)]);
+                        xp[u] = __ldcs(&a.Bout[b_index(pk, by, c, Hp, C)]);
+                        xq[u] = __ldcs(&a.Bout[b_index(M - pk, by, c, Hp, C)]);
                     }
                     wp[u] = __ldg(&tw_px[pk]);
                     wq[u] = __ldg(&tw_px[M - pk]);
@@ -444,10 +449,10 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
         if (wy <= 0.0f) return;
         const float gain = a.acc_gain, sh = a.acc_shoulder;
         float4* erow = a.effect + static_cast<int64_t>(sy) * a.W;
-        for (int sx = threadIdx.x; sx < a.W; sx += blockDim.x) {
+        for (int sx = a.acc_x0 + threadIdx.x; sx < a.acc_x1; sx += blockDim.x) {
             const float wgt = (a.zone_n > 0 ? zone_weight(sx, a.W, a.zone_x, a.zone_n) : 1.0f) * wy;
             if (wgt <= 0.0f) continue;
-            float3 e = mapped_effect<C>(a, smem, sx);
+            float3 e = mapped_effect<C>(a, smem, sx - a.tile_x0);
             if (sh > 0.0f) e = make_float3(soft_shoulder(e.x, sh), soft_shoulder(e.y, sh), soft_shoulder(e.z, sh));
             float4 acc = erow[sx];
             acc.x += e.x * gain * wgt;

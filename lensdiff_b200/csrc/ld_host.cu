@@ -716,6 +716,36 @@ static_assert(LD_TRANSFER_LINEAR == kTransferLinear && LD_TRANSFER_DAVINCI_INTER
 
 // The steps after the effect (CpuReference.cpp:2089-2094, :2180-2198): the
 // resolution-aware working frame, scatter and creative fringe.
+// Field zone z (of n per side) over `extent` working pixels: the pixels its
+// tent weight can reach, [lo, hi) (accumulateWeightedImage's weight
+// max(0, 1 - |x (n - 1) / (extent - 1) - z|), LensDiffCpuReference.cpp:
+// 1458-1466, is zero outside ((z - 1) step, (z + 1) step); one pixel of margin
+// each side, the inverse pass evaluates the weight itself).
+void zone_span(int extent, int n, int z, int* lo, int* hi) {
+    const double step = static_cast<double>(std::max(1, extent - 1)) / static_cast<double>(n - 1);
+    *lo = std::max(0, static_cast<int>(std::floor((z - 1) * step)) - 1);
+    *hi = std::min(extent, static_cast<int>(std::ceil((z + 1) * step)) + 2);
+}
+
+// The largest zone window of an n x n zone grid: the output size every
+// zone's overlap-add tile must hold.
+struct ZoneTiles {
+    int n = 0;
+    int wo = 0, ho = 0;
+};
+ZoneTiles zone_tiles(int W, int H, int n) {
+    ZoneTiles t;
+    t.n = n;
+    for (int z = 0; z < n; ++z) {
+        int lo = 0, hi = 0;
+        zone_span(W, n, z, &lo, &hi);
+        t.wo = std::max(t.wo, hi - lo);
+        zone_span(H, n, z, &lo, &hi);
+        t.ho = std::max(t.ho, hi - lo);
+    }
+    return t;
+}
+
 struct PostEffects {
     bool resample = false;
     double scale = 1.0;   // working / source (ResolveLensDiffEffectWorkingScale)
@@ -2542,11 +2572,23 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         int rw = 0, rh = 0;
         const int c_rows = std::max(std::max(cb.n_drv == 1 ? 4 : 3, cb.n_out), cb.n_ker);
         const int c_cols = std::max(std::max(cb.n_out, cb.n_ker), cb.n_drv);
-        const GridGeom g = make_geometry(ctx, Ww, Hw, 2 * max_kernel_radius(p) + 1, c_rows, c_cols, &rw, &rh);
+        const int Kmax = 2 * max_kernel_radius(p) + 1;
+        // Field zones: each zone's tent weight is non-zero only over its
+        // neighbours' centres, so its convolution is needed only there.  With
+        // overlap-add tiles every zone convolves just that window plus the
+        // kernel's reach on a grid of its own size (one grid shared by every
+        // zone) instead of the whole frame, when that grid is at most half
+        // the frame's.
+        const ZoneTiles zt = zones && p.fft_form != LD_FFT_CUFFT ? zone_tiles(Ww, Hw, zn) : ZoneTiles{};
+        const bool tiled = zt.n > 0 && static_cast<double>(zt.wo + Kmax - 1) * (zt.ho + Kmax - 1) <=
+                                           0.5 * static_cast<double>(Ww + Kmax - 1) * (Hw + Kmax - 1);
+        const GridGeom g = tiled ? make_geometry(ctx, zt.wo, zt.ho, Kmax, c_rows, c_cols, &rw, &rh)
+                                 : make_geometry(ctx, Ww, Hw, Kmax, c_rows, c_cols, &rw, &rh);
         // Spectra already cached (a warm frame)?  If not, the bank and kernel
         // spectra are built on s while the source's row transforms run on a
-        // side stream: they do not depend on the lens.
-        const bool overlap_rows = p.fft_form != LD_FFT_CUFFT && p.debug_view != LD_DEBUG_SELECTION &&
+        // side stream: they do not depend on the lens.  (Tiles transform
+        // their rows per zone, inside the chain.)
+        const bool overlap_rows = p.fft_form != LD_FFT_CUFFT && p.debug_view != LD_DEBUG_SELECTION && !tiled &&
                                   !spectra_cached(ctx, p, zones, zn, cb, g);
 
         FrameArgs fa;
@@ -2623,7 +2665,8 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             int srw = 0, srh = 0;
             gs = make_geometry(ctx, Ww, Hw, Ks, 3, 3, &srw, &srh);
         }
-        const int Hp = (Hw + 3) & ~3;
+        // rows of the row spectra: the frame's, or a tile's input rows
+        const int Hp = tiled ? ((zt.ho + Kmax - 1 + 3) & ~3) : ((Hw + 3) & ~3);
         const size_t a_bytes = std::max(static_cast<size_t>(cb.n_drv) * g.cols,
                                         post.scatter ? static_cast<size_t>(3) * gs.cols : size_t(0)) *
                                Hp * sizeof(float2);
@@ -2646,6 +2689,8 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         }
         for (FrameArgs* f : {&fa, &fw}) {
             f->Hp = Hp;
+            f->acc_x0 = 0;
+            f->acc_x1 = f->W;
             f->A = abuf;
             f->Bout = reinterpret_cast<float2*>(bbuf);
             f->bscale = reinterpret_cast<float*>(bbuf + b_bytes_of(cb.n_out, g, fa.h16));
@@ -2801,7 +2846,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             clear_effect();
             if (!overlap_rows) {  // else already on the side stream
                 if (post.resample) staged(ctx, LD_STAGE_WORKING_SOURCE, s, [&] { launch_resample_source(fin, s); });
-                staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
+                if (!tiled) staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
             }
             if (fa.effect_mode != kEffectAccumulate) {
                 staged(ctx, LD_STAGE_FRAME_COLS, s, [&] { launch_frame_cols(fa, s); });
@@ -2817,11 +2862,18 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
                         fa.zone_y = z / zn;
                         // working rows whose tent weight can be non-zero (the kernel
                         // evaluates the weight itself; one row of margin each side)
-                        const double step = static_cast<double>(std::max(1, Hw - 1)) / static_cast<double>(zn - 1);
-                        r0 = std::max(0, static_cast<int>(std::floor((fa.zone_y - 1) * step)) - 1);
-                        r1 = std::min(Hw, static_cast<int>(std::ceil((fa.zone_y + 1) * step)) + 2);
+                        zone_span(Hw, zn, fa.zone_y, &r0, &r1);
                     }
                     fa.row0 = r0;
+                    if (tiled) {  // this zone's tile: its own row transforms, its columns only
+                        int c0 = 0, c1 = Ww;
+                        zone_span(Ww, zn, fa.zone_x, &c0, &c1);
+                        fa.tile_x0 = c0 - Kmax / 2;
+                        fa.tile_y0 = r0 - Kmax / 2;
+                        fa.acc_x0 = c0;
+                        fa.acc_x1 = c1;
+                        staged(ctx, LD_STAGE_FRAME_ROWS, s, [&] { launch_frame_rows(fa, s); });
+                    }
                     for (int part = part_lo; part < part_hi; ++part) {
                         fa.spectra = ks_part(base, part, cb.n_ker, g, fa.h16);
                         fa.kscale = ks_scale(base, part, cb.parts, cb.n_ker, g, fa.h16);

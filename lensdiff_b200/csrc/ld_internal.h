@@ -224,6 +224,13 @@ struct FrameArgs {
     int effect_mode;
     int preserve;
     int zone_x, zone_y, zone_n, row0;  // zone_n = 0: no field zones (weight 1)
+    // Overlap-add tiles (field zones): the FFT grid's origin in working-frame
+    // pixels (0, 0 for the whole frame; may be negative, pixels outside the
+    // frame read as zero).  Grid row / column g is frame row / column
+    // g + tile_y0 / g + tile_x0; A and B hold grid rows [0, Hp).  The inverse
+    // pass's accumulate mode writes the frame columns [acc_x0, acc_x1).
+    int tile_x0, tile_y0;
+    int acc_x0, acc_x1;
     // kEffectAccumulate adds weight * gain * shoulder(effect): Split look
     // (core / structure gains and soft shoulders, LensDiffCpuReference.cpp:
     // 2123-2146, :1340-1352); 1 and 0 otherwise
