@@ -55,7 +55,8 @@ FFT_FORMS = {"own": 0, "chosen": 1, "cufft": 2}
 FORM_NAMES = {"own": "own_fp32", "chosen": "own_chosen", "cufft": "cufft"}
 # the arithmetic each form computes in
 FORM_DTYPES = {"own": "f32", "cufft": "f32",
-               "chosen": "f32 frame math; bf16x3-split psf windows (f32 accumulate); fp16 frame spectra"}
+               "chosen": ("f32 frame math; bf16x3-split psf windows (f32 accumulate); fp16 frame spectra "
+                          "(row spectra scaled per row tile, kernel spectra and column outputs per column)")}
 
 
 def parse():
@@ -283,14 +284,15 @@ def sources_digest() -> str:
 # ---------------------------------------------------------------------------
 def algorithmic_bytes(W, H, grid, n_drv, n_ker, n_out, out_pixels, B=0, K=0, h16=False):
     """Bytes each frame kernel must move with this algorithm (complex = 8 B,
-    4 B for the kernel spectra and column outputs of the chosen form, h16):
-    frame_rows reads the RGBA source and writes the H x (Px/2+1) row spectra;
+    4 B for the kernel spectra, column outputs and one-driver row spectra of
+    the chosen form, h16, whose row spectra also carry one exponent byte per
+    row): frame_rows reads the RGBA source and writes the H x (Px/2+1) row spectra;
     frame_cols reads them and the kernel spectra (Py x (Px/2+1) each) and writes
     H x (Px/2+1) per output; frame_inverse reads those, re-reads the source for
     the composite and writes the RGBA output."""
     Px, Py = grid
     bins = Px // 2 + 1
-    row_spec = 8 * H * bins
+    row_spec = (4 * H * bins + H) if (h16 and n_drv == 1) else 8 * H * bins
     cplx = 4 if h16 else 8
     out_spec = cplx * H * bins
     canvas = 4 * B * K * K

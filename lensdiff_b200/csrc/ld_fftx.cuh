@@ -10,11 +10,13 @@
 //   * its output addresses are one base and immediate offsets r * NS * C;
 //   * (b / C) % NS divides by constants;
 //   * the twiddles w^r (r < R) of butterfly k come from a per-stage table
-//     laid out [k][RP] (RP = R rounded up to even), read as R/2 16-byte loads,
-//     instead of a serial chain of R - 2 complex products.
-// The stage tables are generated in FP64 on the host (fx_stage_table_len and
-// the host generator in ld_host.cu) and stored after one another for the
-// stages after the first (the first stage's twiddles are all 1).
+//     of pairs (w^2q, w^(2q+1)) laid out [q][k] (q < RP / 2, RP = R rounded
+//     up to even), read as R/2 16-byte loads that the threads of a warp
+//     (consecutive k) make to consecutive addresses, instead of a serial
+//     chain of R - 2 complex products.
+// The stage tables are generated in FP64 on the host (fx_stage_table in
+// ld_frame_fx.cu) and stored after one another for the stages after the
+// first (the first stage's twiddles are all 1).
 #pragma once
 
 #include "ld_fft.cuh"
@@ -49,10 +51,10 @@ __device__ __forceinline__ void fx_stage(float2* s, const float2* __restrict__ s
         if ((it + 1) * T <= NB || b < NB) {
             if constexpr (NS > 1) {
                 const int k = (b / C) % NS;
-                const float4* t = reinterpret_cast<const float4*>(stw + k * RP);
+                const float4* t = reinterpret_cast<const float4*>(stw) + k;
 #pragma unroll
                 for (int q = 0; q < RP / 2; ++q) {
-                    const float4 w = __ldg(t + q);
+                    const float4 w = __ldg(t + q * NS);
                     if (2 * q >= 1 && 2 * q < R) {
                         const float2 w0 = make_float2(w.x, w.y);
                         v[it][2 * q] = INV ? cmulc(v[it][2 * q], w0) : cmul(v[it][2 * q], w0);

@@ -43,14 +43,14 @@ void rows_e(const FrameArgs& a, cudaStream_t s) {
         // two rows per CTA and three CTAs per SM (register cap 80) when the
         // transform fits 224 threads; else four rows per CTA
         if (fft_threads(M, 2, E) <= 224) {
-            const size_t sm = static_cast<size_t>(M) * 2 * sizeof(float2);
+            const size_t sm = rows_smem(M, 2);
             launch_ahead(frame_rows_kernel<E, 2, 1, 224, 3>, a, a.Hp / 2, fft_threads(M, 2, E), sm, s);
         } else {
-            const size_t sm = static_cast<size_t>(M) * 4 * sizeof(float2);
+            const size_t sm = rows_smem(M, 4);
             launch_ahead(frame_rows_kernel<E, 4, 1>, a, a.Hp / 4, fft_threads(M, 4, E), sm, s);
         }
     } else {
-        const size_t sm = static_cast<size_t>(M) * 3 * sizeof(float2);
+        const size_t sm = rows_smem(M, 3);
         if (a.drv_effect)
             frame_rows_kernel<E, 3, 3, Fam<E>::max_threads, 1, true><<<a.Hp, fft_threads(M, 3, E), sm, s>>>(a);
         else
@@ -199,7 +199,7 @@ void configure_e() {
 size_t frame_cols_smem(int Py, int n_out) {
     const size_t n = static_cast<size_t>(Py);
     const size_t bufs = n_out == 0 ? 4 * n : (1 + static_cast<size_t>(n_out)) * n;
-    return bufs * sizeof(float2) + 2 * sizeof(uint64_t);
+    return bufs * sizeof(float2) + 4 * sizeof(uint64_t);
 }
 
 size_t kspec_cols_smem(int Py, int Kp, int n_ker) {

@@ -60,7 +60,7 @@ void rows_fixed(const FrameArgs& a, cudaStream_t s) {
     constexpr int N = FFT::n;
     constexpr int C = rows_c(N);
     constexpr int T = fft_threads(N, C, kE25);
-    const size_t sm = static_cast<size_t>(N) * C * sizeof(float2);
+    const size_t sm = rows_smem(N, C);
     FrameArgs b = a;
     auto f = frame_rows_kernel<kE25, C, 1, T, minb_for(T), false, FFT>;
     b.ahead = resident_ctas(f, T, sm);
@@ -212,7 +212,10 @@ void fx_configure() {
 
 // Stage twiddle tables of fixed plan `id`: for every stage after the first,
 // NS x RP entries w^(k r), w = exp(-2 pi i / (NS R)), k < NS, r < R (zero for
-// r >= R), RP = R rounded up to even; evaluated in FP64.
+// r >= R), RP = R rounded up to even, as RP / 2 rows of NS pairs
+// (w^(k 2q), w^(k (2q+1))): pair q of butterfly span k at q * NS + k, so
+// the threads of a warp (consecutive k) read consecutive 16-byte pairs;
+// evaluated in FP64.
 std::vector<float2> fx_stage_table(int id) {
     std::vector<float2> out;
     const FxPlanDesc* d = fx_plan(id);
@@ -222,14 +225,16 @@ std::vector<float2> fx_stage_table(int id) {
         const int R = d->radix[st];
         const int RP = (R + 1) & ~1;
         if (ns > 1) {
-            for (int k = 0; k < ns; ++k) {
-                for (int r = 0; r < RP; ++r) {
-                    if (r < R) {
+            for (int q = 0; q < RP / 2; ++q) {
+                for (int k = 0; k < ns; ++k) {
+                    for (int r = 2 * q; r < 2 * q + 2; ++r) {
+                        if (r >= R) {
+                            out.push_back(make_float2(0.0f, 0.0f));
+                            continue;
+                        }
                         const long long e = static_cast<long long>(k) * r;
                         const double ang = -2.0 * M_PI * static_cast<double>(e) / static_cast<double>(ns * R);
                         out.push_back(make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(std::sin(ang))));
-                    } else {
-                        out.push_back(make_float2(0.0f, 0.0f));
                     }
                 }
             }

@@ -95,11 +95,9 @@ __device__ __forceinline__ void store_b_column(const float2* s, float2* B, int k
 // 4e-9 m, and nothing overflows.
 constexpr float kHalfTop = 16384.0f;
 
-// Largest |real| / |imag| of s[0, n) over the CTA (all threads get it).
-__device__ float block_absmax(const float2* s, int n) {
+// Largest m over the CTA's threads (all threads get it; a barrier for all).
+__device__ float block_max(float m) {
     __shared__ float part[32];
-    float m = 0.0f;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, fmaxf(fabsf(s[i].x), fabsf(s[i].y)));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -110,6 +108,13 @@ __device__ float block_absmax(const float2* s, int n) {
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     __syncthreads();  // part[] may be reused
     return m;
+}
+
+// Largest |real| / |imag| of s[0, n) over the CTA (all threads get it).
+__device__ float block_absmax(const float2* s, int n) {
+    float m = 0.0f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, fmaxf(fabsf(s[i].x), fabsf(s[i].y)));
+    return block_max(m);
 }
 
 __device__ __forceinline__ __half2 to_half2(float2 v, float s) { return __floats2half2_rn(v.x * s, v.y * s); }
@@ -144,7 +149,55 @@ __device__ __forceinline__ void store_bins(int M, int C, int64_t col_elems, int6
     }
 }
 
+// 2^e as a float, e in [-126, 127] (exact; built from the exponent field).
+__device__ __forceinline__ float exp2_int(int e) { return __int_as_float((127 + e) << 23); }
+
+// Row-spectrum exponent of a tile whose largest component is m: every value
+// times 2^-e lies below 2^14 in magnitude (FP16 keeps its 11-bit mantissa
+// down to 2^-14 of that, and has room to 65504).
+__device__ __forceinline__ int row_tile_exp(float m) {
+    if (!(m > 0.0f)) return 0;
+    int e;
+    frexpf(m, &e);  // m < 2^e
+    return min(110, max(-110, e - 14));
+}
+
+// FP16 row spectra (the chosen form, one driver per row): the bins of the C
+// rows in smem are formed in place (bin M of row col goes to s[M * C + col],
+// so smem holds (M + 1) * C values), the tile's largest component sets its
+// exponent e (row_tile_exp), and bin k of row y0 + col is stored as half2
+// values times 2^-e at out[k * Hp + y0 + col], with e in aexp[y0 + col].
+__device__ __forceinline__ void store_bins_h16(int M, int C, int Hp, int y0, const float2* __restrict__ tw_px,
+                                               float2* s, __half2* out, signed char* aexp) {
+    // pairs (k, M - k): one thread forms both bins from Z[k], Z[M - k]
+    // (k = 0: bins 0 and M from Z[0]; k = M / 2 of an even M pairs with itself)
+    float m = 0.0f;
+    for (int i = threadIdx.x; i < (M / 2 + 1) * C; i += blockDim.x) {
+        const int k = i / C;
+        const int col = i - k * C;
+        const float2 zk = s[k * C + col];
+        const float2 zm = s[(k == 0 ? 0 : M - k) * C + col];
+        const float2 xk = r2c_post(zk, zm, __ldg(&tw_px[k]));
+        const float2 xm = r2c_post(zm, zk, __ldg(&tw_px[M - k]));
+        s[k * C + col] = xk;
+        s[(M - k) * C + col] = xm;
+        m = fmaxf(m, fmaxf(fmaxf(fabsf(xk.x), fabsf(xk.y)), fmaxf(fabsf(xm.x), fabsf(xm.y))));
+    }
+    const int e = row_tile_exp(block_max(m));  // its barrier publishes the bins
+    const float sc = exp2_int(-e);
+    if (static_cast<int>(threadIdx.x) < C) aexp[y0 + threadIdx.x] = static_cast<signed char>(e);
+    for (int i = threadIdx.x; i < (M + 1) * C; i += blockDim.x) {
+        const int k = i / C;
+        const int col = i - k * C;
+        out[static_cast<int64_t>(k) * Hp + y0 + col] = to_half2(s[i], sc);
+    }
+}
+
 // ---- forward rows --------------------------------------------------------------------
+// Shared memory of a forward row pass over C sequences of length M (one
+// spare bin per sequence for the in-place bins of store_bins_h16).
+constexpr size_t rows_smem(int M, int C) { return (static_cast<size_t>(M) + 1) * C * sizeof(float2); }
+
 // Spectral (NDRV = 1): C = 4 frame rows per CTA, the scalar driver of each.
 // Mono (NDRV = 3): C = 3, one frame row per CTA, its three colour drivers.
 // Column col of the transform is row y0 + col / NDRV, driver col % NDRV; its
@@ -231,7 +284,10 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
     }
     __syncthreads();
     FFT::template run<C, false, MAXT>(a.g.plan_m, smem);
-    store_bins(M, C, static_cast<int64_t>(a.Hp) * NDRV, static_cast<int64_t>(y0) * NDRV, a.g.tw_px, smem, a.A);
+    if (NDRV == 1 && !FROM_EFFECT && a.h16)
+        store_bins_h16(M, C, a.Hp, y0, a.g.tw_px, smem, reinterpret_cast<__half2*>(a.A), a.aexp);
+    else
+        store_bins(M, C, static_cast<int64_t>(a.Hp) * NDRV, static_cast<int64_t>(y0) * NDRV, a.g.tw_px, smem, a.A);
 }
 
 // ---- column pass, spectral: forward, multiply by NOUT kernel spectra, inverse ----------
@@ -240,6 +296,9 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
 // Wk [Py][NOUT] (the column's NOUT kernel spectra land here, are multiplied by
 // F in place and inverse-transformed together as NOUT interleaved sequences),
 // two mbarriers.  The first Hp rows of Wk go to B with one bulk store.
+// H16: the half2 row spectra land at the start of Wk and the rows' exponents
+// right after them (a third mbarrier), and are widened into F; the half2
+// kernel spectra land in the upper half of Wk and are widened in the multiply.
 template <int E, int NOUT, int MAXT = Fam<E>::max_threads, int MINB = 1, bool H16 = false, class FFT = GenericFft<E>>
 __global__ void __launch_bounds__(MAXT, MINB) frame_cols_kernel(FrameArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -248,31 +307,43 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_cols_kernel(FrameArgs a) {
     float2* F = reinterpret_cast<float2*>(smraw);
     float2* Wk = F + Py;
     uint64_t* bars = reinterpret_cast<uint64_t*>(Wk + static_cast<size_t>(Py) * NOUT);
-    const uint32_t a_bytes = static_cast<uint32_t>(Hp * sizeof(float2));
-    // FP16 kernel spectra land in the upper half of Wk and are widened in the multiply
+    const uint32_t a_bytes = static_cast<uint32_t>(Hp * (H16 ? sizeof(__half2) : sizeof(float2)));
+    void* adst = H16 ? static_cast<void*>(Wk) : static_cast<void*>(F);
+    const char* asrc = reinterpret_cast<const char*>(a.A) + static_cast<size_t>(k) * a_bytes;
     const size_t kn = static_cast<size_t>(Py) * NOUT;
     const uint32_t k_bytes = static_cast<uint32_t>(kn * (H16 ? sizeof(__half2) : sizeof(float2)));
     void* kdst = H16 ? static_cast<void*>(reinterpret_cast<__half2*>(Wk) + kn) : static_cast<void*>(Wk);
     const void* ksrc = H16 ? static_cast<const void*>(reinterpret_cast<const __half2*>(a.spectra) + k * kn)
                            : static_cast<const void*>(a.spectra + k * kn);
     const bool lead = threadIdx.x == 0;
+    signed char* aex = reinterpret_cast<signed char*>(Wk) + static_cast<size_t>(Hp) * sizeof(__half2);
     if (lead) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
+        if (H16) mbar_init(&bars[2], 1);
         mbar_init_fence();
     }
     __syncthreads();  // barriers initialised before anyone waits on them
     if (lead) {
-        bulk_load_checked(F, a.A + static_cast<size_t>(k) * Hp, a_bytes, &bars[0], smraw, a.err);
+        bulk_load_checked(adst, asrc, a_bytes, &bars[0], smraw, a.err);
+        if (H16) bulk_load_checked(aex, a.aexp, static_cast<uint32_t>((Hp + 15) & ~15), &bars[2], smraw, a.err);
         bulk_load_checked(kdst, ksrc, k_bytes, &bars[1], smraw, a.err);
         const int later = k + a.ahead;
         if (later < cols) {
-            bulk_prefetch_l2(a.A + static_cast<size_t>(later) * Hp, a_bytes);
+            bulk_prefetch_l2(asrc + (later - k) * static_cast<size_t>(a_bytes), a_bytes);
             bulk_prefetch_l2(static_cast<const char*>(ksrc) + (later - k) * static_cast<size_t>(k_bytes), k_bytes);
         }
     }
-    for (int i = Hp + threadIdx.x; i < Py; i += blockDim.x) F[i] = make_float2(0.0f, 0.0f);
-    if (__syncthreads_or(!mbar_wait(&bars[0], 0, a.err))) return;
+    if constexpr (H16) {
+        if (__syncthreads_or(!mbar_wait(&bars[0], 0, a.err) || !mbar_wait(&bars[2], 0, a.err))) return;
+        const __half2* ah = reinterpret_cast<const __half2*>(Wk);
+        for (int i = threadIdx.x; i < Py; i += blockDim.x)
+            F[i] = i < Hp ? from_half2(ah[i], exp2_int(aex[i])) : make_float2(0.0f, 0.0f);
+        __syncthreads();
+    } else {
+        for (int i = Hp + threadIdx.x; i < Py; i += blockDim.x) F[i] = make_float2(0.0f, 0.0f);
+        if (__syncthreads_or(!mbar_wait(&bars[0], 0, a.err))) return;
+    }
     FFT::template run<1, false, MAXT>(a.g.plan_py, F);
     if (__syncthreads_or(!mbar_wait(&bars[1], 0, a.err))) return;
     if constexpr (H16) {

@@ -2667,10 +2667,13 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
         }
         // rows of the row spectra: the frame's, or a tile's input rows
         const int Hp = tiled ? ((zt.ho + Kmax - 1 + 3) & ~3) : ((Hw + 3) & ~3);
-        const size_t a_bytes = std::max(static_cast<size_t>(cb.n_drv) * g.cols,
-                                        post.scatter ? static_cast<size_t>(3) * gs.cols : size_t(0)) *
-                               Hp * sizeof(float2);
-        float2* abuf = static_cast<float2*>(ensure(ctx, ctx->frameA, a_bytes));
+        // (the chosen form's half2 row spectra take half; their row exponents follow)
+        const size_t a_bytes = align256(std::max(static_cast<size_t>(cb.n_drv) * g.cols,
+                                                 post.scatter ? static_cast<size_t>(3) * gs.cols : size_t(0)) *
+                                        Hp * sizeof(float2));
+        // (the exponents go to shared memory in 16-byte units)
+        float2* abuf = static_cast<float2*>(ensure(ctx, ctx->frameA, a_bytes + ((static_cast<size_t>(Hp) + 15) & ~size_t(15))));
+        signed char* aexp = reinterpret_cast<signed char*>(abuf) + a_bytes;
         // column outputs in groups of four columns (ld_frame.cu b_index)
         auto b_bytes_of = [&](int n_out, const GridGeom& gg, bool h16) {
             const size_t bcols = (static_cast<size_t>(gg.cols) + 3) / 4 * 4;
@@ -2692,6 +2695,7 @@ int ld_render(ld_ctx* ctx, const ld_render_request* rq, const ld_params* params,
             f->acc_x0 = 0;
             f->acc_x1 = f->W;
             f->A = abuf;
+            f->aexp = aexp;
             f->Bout = reinterpret_cast<float2*>(bbuf);
             f->bscale = reinterpret_cast<float*>(bbuf + b_bytes_of(cb.n_out, g, fa.h16));
             f->effect = effect;

@@ -203,10 +203,14 @@ struct FrameArgs {
     float2* A;
     float2* Bout;
     const float2* spectra;     // KS; half2 when h16
-    int h16;                   // chosen form: KS and B in FP16 with per-column scales
+    int h16;                   // chosen form: KS and B in FP16 with per-column scales, A per row tile
     const float* kscale;       // [cols] (h16)
     float* bscale;             // [cols] (h16)
-    int ahead;                 // CTAs of the launch resident at once: the L2 prefetch distance (set by each launcher)
+    // h16 row spectra (n_drv = 1): A holds half2 values, column-major
+    // [bin][Hp]; row r's values are its spectrum times 2^-aexp[r] (one
+    // exponent per row tile of the forward row pass, stored for each row)
+    signed char* aexp;         // [Hp] (h16)
+    int ahead;                // CTAs of the launch resident at once: the L2 prefetch distance (set by each launcher)
     int* err;                  // device error word
     // What the inverse pass does with the mapped effect of a row:
     //   kEffectComposite: composite the render window directly (Augment);

@@ -8,8 +8,8 @@ The context must stay usable afterwards.
 
 Host side: an injected allocation failure (ld_inject_alloc_failure) and an
 HBM budget too small for the frame come back as status codes with stage
-strings, and a later call on the same context succeeds with the same result
-as a clean context.
+strings, and a later call on the same context succeeds with the result of a
+clean context (to the last float step of the frame maximum).
 """
 import ctypes
 
@@ -106,7 +106,11 @@ def test_injected_allocation_failure_is_reported_and_recoverable():
         assert c._lib.ld_inject_alloc_failure(c.handle, -1) == abi.LD_OK
         st, out = _render(c, _lens(), frame)
         assert st.ok, st
-        assert np.array_equal(out, ref)
+        # each context builds its own bank, whose ring and energy sums are
+        # double-precision atomic adds in no fixed order: a sum that rounds
+        # to float on the other side of a tie moves the output by one float
+        # step of the frame maximum, so the bound is a few such steps
+        assert np.abs(out - ref).max() <= 1e-6 * np.abs(ref[..., :3]).max()
         assert c.check_device_errors() == 0
         c.close()
 
