@@ -216,77 +216,112 @@ __global__ void __launch_bounds__(256) pupil_field_kernel(PsfBankArgs a, DftPlan
 // ---- the GEMM --------------------------------------------------------------------------
 // Persistent work queue over a table of transform problems (each one pass of
 // one wavelength of one lens, with its own operands, sizes and window): one
-// CTA per SM, four warps, tensor memory allocated once.  A CTA takes the next
-// 128 x 128-complex output tile from a global counter until none are left.
-// Per tile, thread 0 streams the K-chunks' hi and lo tiles of A and B into a
-// two-stage ring with bulk copies; thread 32 issues the tensor-core MMAs
-// (three per 16-wide K step: hi*hi, hi*lo, lo*hi) and commits each stage
-// back to the producer; then all four warps read the accumulators out of
-// TMEM (warp w owns lanes 32w..32w+31) for the epilogue:
-//   kDftRows: Y as the column pass's A images (row n, K pair m);
-//   kDftCols: |Z|^2 into the PSF window (and its sum when asked).
-// The ring position and the barrier phases carry over from tile to tile.
-// Every wait is bounded; a wait that gives up records the error, and the CTA
-// stops taking tiles, releases its tensor memory and returns.
-__global__ void __launch_bounds__(128, 1) dft_gemm_kernel(DftBatchArgs g) {
+// CTA per SM, tensor memory allocated once, three warp roles that run ahead
+// of one another as far as their buffers allow:
+//   warp 0 (one thread), producer: takes the next 128 x 128-complex output
+//     tile from a global counter, publishes it in a four-entry tile ring,
+//     and streams the tile's K-chunks (hi and lo tiles of A and B) into a
+//     two-stage shared-memory ring with bulk copies;
+//   warp 1 (one thread), MMA issuer: per tile, waits for one of the two
+//     256-column accumulators in tensor memory to be drained, issues the
+//     tensor-core MMAs of every K-chunk into it (three per 16-wide K step:
+//     hi*hi, hi*lo, lo*hi), commits each stage back to the producer and the
+//     finished accumulator to the epilogue;
+//   warps 2-5, epilogue: read the accumulator out of tensor memory (warp w
+//     owns lanes 32 (w % 4) .. + 31) while the next tile's MMAs run in the
+//     other accumulator:
+//       kDftRows: Y as the column pass's A images (row n, K pair m);
+//       kDftCols: |Z|^2 into the PSF window (and its sum when asked).
+// A tile index past the last tile ends every role.  Every wait is bounded; a
+// wait that gives up records the error, its role stops, and the other roles'
+// waits on it give up in turn; the CTA then releases its tensor memory.
+constexpr int kTileRing = 4;
+constexpr uint32_t kAccCols = 2 * kTmemCols;  // two accumulators
+constexpr int kGemmThreads = 192;
+
+struct TileSlot {
+    int prob;    // problem of the tile; -1: no more tiles
+    int tm, tn;  // its M and N tile within the problem
+};
+
+__device__ __forceinline__ TileSlot next_tile(const DftBatchArgs& g) {
+    TileSlot ts{-1, 0, 0};
+    const int t = atomicAdd(g.counter, 1);
+    if (t >= g.tiles) return ts;
+    // the problem of tile t: the last p with tile_start[p] <= t
+    int lo = 0, hi = g.problems - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&g.tile_start[mid]) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const int local = t - __ldg(&g.tile_start[lo]);
+    const int mt = g.probs[lo].mt;
+    ts.prob = lo;
+    ts.tm = local % mt;
+    ts.tn = local / mt;
+    return ts;
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1) dft_gemm_kernel(DftBatchArgs g) {
     extern __shared__ __align__(1024) unsigned char smraw[];
-    __shared__ uint64_t bars[2 * kStages + 1];
+    __shared__ uint64_t full[kStages], empty[kStages];
+    __shared__ uint64_t acc_full[2], acc_empty[2];
+    __shared__ uint64_t tq_full[kTileRing], tq_empty[kTileRing];
+    __shared__ uint64_t drained;
+    __shared__ TileSlot tq[kTileRing];
     __shared__ uint32_t tmem_slot;
-    __shared__ int tile_sh, fail_sh;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* base =
         smraw + ((1024u - (smem_addr(smraw) & 1023u)) & 1023u);  // 1024-byte aligned stages
-    uint64_t* full = bars;
-    uint64_t* empty = bars + kStages;
-    uint64_t* done = bars + 2 * kStages;
-    if (warp == 0) {
-        tmem_alloc(&tmem_slot, kTmemCols);
+    if (warp == 1) {
+        tmem_alloc(&tmem_slot, kAccCols);
         tmem_relinquish();
     }
-    if (threadIdx.x == 32) {
+    if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
-            mbar_init(&full[s], 4);
-            mbar_init(&empty[s], 1);
+            mbar_init(&full[s], 4);   // the four bulk copies of a stage
+            mbar_init(&empty[s], 1);  // the MMA issuer's commit
         }
-        mbar_init(done, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);   // the MMA issuer's commit
+            mbar_init(&acc_empty[b], 4);  // one arrive per epilogue warp
+        }
+        for (int d = 0; d < kTileRing; ++d) {
+            mbar_init(&tq_full[d], 1);   // the producer
+            mbar_init(&tq_empty[d], 5);  // the MMA issuer and the four epilogue warps
+        }
+        mbar_init(&drained, 1);
         mbar_init_fence();
     }
-    if (threadIdx.x == 0) fail_sh = 0;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    uint32_t gc = 0;     // K-chunks this CTA has streamed: ring stage and barrier phases
-    uint32_t ntile = 0;  // tiles this CTA has finished: phase of `done`
-    for (;;) {
-        if (threadIdx.x == 0) tile_sh = atomicAdd(g.counter, 1);
-        __syncthreads();
-        const int t = tile_sh;
-        if (t >= g.tiles || fail_sh) break;  // uniform
-        // the problem of tile t: the last p with tile_start[p] <= t
-        int lo = 0, hi = g.problems - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(&g.tile_start[mid]) <= t) lo = mid;
-            else hi = mid - 1;
-        }
-        const DftProblem pr = g.probs[lo];
-        const int local = t - __ldg(&g.tile_start[lo]);
-        const int tm = local % pr.mt, tn = local / pr.mt;
-        const int kc = pr.kc;
-        const unsigned char* a_hi = pr.a_hi + static_cast<size_t>(tm) * kImgA;
-        const unsigned char* a_lo = pr.a_lo + static_cast<size_t>(tm) * kImgA;
-        const size_t b_row0 = static_cast<size_t>(2) * (pr.n0 + tn * (kTileN / 2));  // multiple of 8
-        const unsigned char* b_hi = pr.b_hi + (b_row0 >> 3) * 1024;
-        const unsigned char* b_lo = pr.b_lo + (b_row0 >> 3) * 1024;
-        if (warp == 0) {
-            if (lane == 0) {  // producer
-                for (int c = 0; c < kc; ++c) {
-                    const uint32_t k = gc + static_cast<uint32_t>(c);
-                    const int s = static_cast<int>(k % kStages);
-                    const uint32_t use = k / kStages;
-                    if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, g.err)) {
-                        fail_sh = 1;
+    if (warp == 0) {
+        if (lane == 0) {  // producer
+            uint32_t gc = 0;  // K-chunks streamed: ring stage and barrier phases
+            for (uint32_t i = 0;; ++i) {
+                const int d = static_cast<int>(i % kTileRing);
+                const uint32_t use = i / kTileRing;
+                if (use > 0 && !mbar_wait(&tq_empty[d], (use - 1) & 1, g.err)) break;
+                const TileSlot ts = next_tile(g);
+                tq[d] = ts;
+                mbar_arrive(&tq_full[d]);  // release: the slot is visible to its waiters
+                if (ts.prob < 0) break;
+                const DftProblem& pr = g.probs[ts.prob];
+                const int kc = pr.kc;
+                const unsigned char* a_hi = pr.a_hi + static_cast<size_t>(ts.tm) * kImgA;
+                const unsigned char* a_lo = pr.a_lo + static_cast<size_t>(ts.tm) * kImgA;
+                const size_t b_row0 = static_cast<size_t>(2) * (pr.n0 + ts.tn * (kTileN / 2));  // multiple of 8
+                const unsigned char* b_hi = pr.b_hi + (b_row0 >> 3) * 1024;
+                const unsigned char* b_lo = pr.b_lo + (b_row0 >> 3) * 1024;
+                bool ok = true;
+                for (int c = 0; c < kc; ++c, ++gc) {
+                    const int s = static_cast<int>(gc % kStages);
+                    const uint32_t su = gc / kStages;
+                    if (su > 0 && !mbar_wait(&empty[s], (su - 1) & 1, g.err)) {
+                        ok = false;
                         break;
                     }
                     unsigned char* st = base + s * kStageBytes;
@@ -298,15 +333,35 @@ __global__ void __launch_bounds__(128, 1) dft_gemm_kernel(DftBatchArgs g) {
                     bulk_load_checked(st + 2 * kImgA + kImgB, b_lo + static_cast<size_t>(c) * pr.b_slab, kImgB,
                                       &full[s], smraw, g.err);
                 }
+                if (!ok) break;
             }
-            __syncwarp();
-        } else if (warp == 1) {
-            if (lane == 0) {  // MMA issuer
+            // the copies still in flight land before the CTA exits: wait
+            // (bounded) for the last use of each stage (gc: chunks issued)
+            for (int s = 0; s < kStages; ++s) {
+                const uint32_t issued = (gc + kStages - 1 - s) / kStages;  // uses of stage s
+                if (issued > 0) mbar_wait(&full[s], (issued - 1) & 1, g.err);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer
+            uint32_t gc = 0;
+            for (uint32_t i = 0;; ++i) {
+                const int d = static_cast<int>(i % kTileRing);
+                if (!mbar_wait(&tq_full[d], (i / kTileRing) & 1, g.err)) break;
+                const TileSlot ts = tq[d];
+                mbar_arrive(&tq_empty[d]);
+                if (ts.prob < 0) break;
+                const int kc = g.probs[ts.prob].kc;
+                const int buf = static_cast<int>(i & 1);
+                const uint32_t au = i >> 1;  // earlier uses of this accumulator
+                if (au > 0 && !mbar_wait(&acc_empty[buf], (au - 1) & 1, g.err)) break;
+                tc_fence_after();
+                const uint32_t acc = tmem + static_cast<uint32_t>(buf) * kTmemCols;
                 bool ok = true;
-                for (int c = 0; c < kc; ++c) {
-                    const uint32_t k = gc + static_cast<uint32_t>(c);
-                    const int s = static_cast<int>(k % kStages);
-                    if (!mbar_wait(&full[s], (k / kStages) & 1, g.err)) {
+                for (int c = 0; c < kc; ++c, ++gc) {
+                    const int s = static_cast<int>(gc % kStages);
+                    if (!mbar_wait(&full[s], (gc / kStages) & 1, g.err)) {
                         ok = false;
                         break;
                     }
@@ -317,29 +372,43 @@ __global__ void __launch_bounds__(128, 1) dft_gemm_kernel(DftBatchArgs g) {
 #pragma unroll
                     for (int kk = 0; kk < kChunkK / 16; ++kk) {
                         const uint64_t dk = static_cast<uint64_t>(kk * 2);  // 32 bytes, in 16-byte units
-                        mma_bf16(tmem, ah + dk, bh + dk, kIdesc, (c | kk) != 0 ? 1u : 0u);
-                        mma_bf16(tmem, ah + dk, bl + dk, kIdesc, 1u);
-                        mma_bf16(tmem, al + dk, bh + dk, kIdesc, 1u);
+                        mma_bf16(acc, ah + dk, bh + dk, kIdesc, (c | kk) != 0 ? 1u : 0u);
+                        mma_bf16(acc, ah + dk, bl + dk, kIdesc, 1u);
+                        mma_bf16(acc, al + dk, bh + dk, kIdesc, 1u);
                     }
                     mma_commit(&empty[s]);
                 }
-                if (ok) mma_commit(done);
-                else fail_sh = 1;
+                if (!ok) break;
+                mma_commit(&acc_full[buf]);
             }
-            __syncwarp();
+            // every MMA this thread issued has completed before tensor
+            // memory is released (the commit arrives at once if none is left)
+            mma_commit(&drained);
+            mbar_wait(&drained, 0, g.err);
         }
-
-        // ---- epilogue: all four warps ----
-        const bool ready = __all_sync(0xffffffffu, mbar_wait(done, ntile & 1, g.err));  // warp-uniform
-        tc_fence_after();
-        float esum = 0.0f;  // kDftCols: this thread's window pixels
-        if (ready) {
-            const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
-            const int row = tm * kTileM + warp * 32 + lane;  // M index of this thread
+        __syncwarp();
+    } else {  // epilogue, warps 2-5
+        const int quarter = warp & 3;  // the TMEM lanes this warp may read
+        const uint32_t lane_base = static_cast<uint32_t>(quarter * 32) << 16;
+        for (uint32_t i = 0;; ++i) {
+            const int d = static_cast<int>(i % kTileRing);
+            if (!__all_sync(0xffffffffu, mbar_wait(&tq_full[d], (i / kTileRing) & 1, g.err))) break;
+            const TileSlot ts = tq[d];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tq_empty[d]);
+            if (ts.prob < 0) break;
+            const int buf = static_cast<int>(i & 1);
+            const bool ready = __all_sync(0xffffffffu, mbar_wait(&acc_full[buf], (i >> 1) & 1, g.err));
+            tc_fence_after();
+            if (!ready) break;
+            const DftProblem& pr = g.probs[ts.prob];
+            float esum = 0.0f;  // kDftCols: this thread's window pixels
+            const uint32_t lane_addr = tmem + static_cast<uint32_t>(buf) * kTmemCols + lane_base;
+            const int row = ts.tm * kTileM + quarter * 32 + lane;  // M index of this thread
             for (int q = 0; q < static_cast<int>(kTmemCols) / 32; ++q) {
                 uint32_t v[32];
                 tmem_ld32(lane_addr + static_cast<uint32_t>(q * 32), v);
-                const int n_first = tn * (kTileN / 2) + q * 16;  // complex column of v[0], v[1]
+                const int n_first = ts.tn * (kTileN / 2) + q * 16;  // complex column of v[0], v[1]
                 if (g.mode == kDftRows) {
                     // Y[m = row][n]: the column pass's A image row n, K pair m
                     const size_t chunk_off = static_cast<size_t>(row >> 5) * pr.y_slab;
@@ -370,22 +439,22 @@ __global__ void __launch_bounds__(128, 1) dft_gemm_kernel(DftBatchArgs g) {
                     }
                 }
             }
-        } else if (threadIdx.x == 0) {
-            fail_sh = 1;
-        }
-        if (pr.energy) {  // uniform
+            // this warp's reads of the accumulator are complete: hand it back
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[buf]);
+            if (pr.energy) {  // uniform
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
-            if (lane == 0 && esum != 0.0f) atomicAdd(pr.energy, static_cast<double>(esum));
+                for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+                if (lane == 0 && esum != 0.0f) atomicAdd(pr.energy, static_cast<double>(esum));
+            }
         }
-        gc += static_cast<uint32_t>(kc);
-        ++ntile;
-        // every thread's TMEM reads are complete before the next tile's MMAs
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
     }
-    if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+    // every role is done with tensor memory before it is released
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, kAccCols);
 }
 
 }  // namespace
@@ -409,7 +478,7 @@ void launch_dft_gemm(const DftBatchArgs& g, cudaStream_t s) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    dft_gemm_kernel<<<static_cast<unsigned>(std::min(g.tiles, sms)), 128, dft_gemm_smem(), s>>>(g);
+    dft_gemm_kernel<<<static_cast<unsigned>(std::min(g.tiles, sms)), kGemmThreads, dft_gemm_smem(), s>>>(g);
 }
 
 void configure_dft_kernels() {
