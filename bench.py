@@ -412,9 +412,10 @@ def reference_cuda_comparator(args, cache, dev):
                                                     out_diff_vs_reference_cuda=float(f"{diff:.3e}"))}
 
 
-def other_workloads(dev):
-    """Short device-timed runs of the other measured workloads, so one default
-    run reports them too (full runs: --workload zones8, --lens-set):
+def other_workloads(dev, form):
+    """Short device-timed runs of the other measured workloads in transform
+    form `form` (a FFT_FORMS key), so one default run reports them too (full
+    runs: --workload zones8, --lens-set):
       zones8    the UHD 31-wavelength frame with an 8x8 grid of field zones
                 (64 banks, 64 convolutions per frame), cold, 3 frames after
                 2 untimed ones (the first calibrates, the second captures
@@ -441,6 +442,7 @@ def other_workloads(dev):
         return e0.elapsed_time(e1) / n
 
     p, frame = S.workload_zones8()
+    p = p.copy(fftForm=FFT_FORMS[form])
     cache = LensDiffPsfBankCache(dev.index or 0)
     src = torch.from_numpy(frame).to(dev)
     dst = torch.empty_like(src)
@@ -454,9 +456,10 @@ def other_workloads(dev):
 
     ms = timed(zone_frame, 2, 3)
     out["zones8"] = {"value": 1000.0 / ms, "unit": "frames/s", "ms_per_step": ms, "bank": "cold",
+                     "fft_form": FORM_NAMES[form],
                      "config": "3840x2160, 8x8 field zones (64 banks x 31 wavelengths), pupil 512 -> PSF 2048"}
     cache.close()
-    lenses = S.lens_instances(256)
+    lenses = [q.copy(fftForm=FFT_FORMS[form]) for q in S.lens_instances(256)]
     cache = LensDiffPsfBankCache(dev.index or 0)
 
     def lens_step(i):
@@ -466,6 +469,7 @@ def other_workloads(dev):
 
     ms = timed(lens_step, 1, 2)
     out["lens_set"] = {"value": 256 * 1000.0 / ms, "unit": "lens banks/s", "ms_per_step": ms, "bank": "cold",
+                       "fft_form": FORM_NAMES[form],
                        "config": "256 unrelated lenses per step: pupil 128-1024, PSF 2-4x, 8-64 wavelengths"}
     if cache.check_device_errors():
         raise RuntimeError("device error word set by the other workloads")
@@ -992,7 +996,7 @@ def main():
 
     workloads = None
     if rank == 0 and ws == 1 and args.workload == "uhd31" and not args.no_other_workloads:
-        workloads = other_workloads(dev)
+        workloads = other_workloads(dev, args.fft_form)
 
     # ---- CPU baseline (rank 0, N=1) ----------------------------------------
     cpu = None
