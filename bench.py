@@ -88,6 +88,30 @@ def parse():
     return ap.parse_args()
 
 
+def gpu_local_cpus(dev):
+    """The host CPUs NVML reports as local to GPU `dev` (its NUMA node), among
+    those this process may run on; None when NVML cannot say.  The end-to-end
+    leg runs there, so its pinned frame buffers are placed in that node's
+    memory and the copies do not cross the socket interconnect."""
+    try:
+        import pynvml
+        import torch
+
+        pr = torch.cuda.get_device_properties(dev)
+        bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            words = pynvml.nvmlDeviceGetCpuAffinity(h, ((os.cpu_count() or 1) + 63) // 64)
+        finally:
+            pynvml.nvmlShutdown()
+        cpus = {64 * w + b for w, m in enumerate(words) for b in range(64) if (int(m) >> b) & 1}
+        cpus &= os.sched_getaffinity(0)
+        return cpus or None
+    except Exception:
+        return None
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -257,13 +281,27 @@ class Clocks:
                 "samples": len(sms)}
 
 
-# DRAM read + write per launch of the UHD 31-wavelength cold workload's
-# kernels, by transform form, from one ncu capture of the kernel sources whose
-# digest is KERNEL_SOURCES_SHA (sources_digest()).  Any other revision of the
-# kernels reports traffic null: a figure measured on other code says nothing
-# about this code.
-TRAFFIC_SOURCES_SHA = "unmeasured"
-MEASURED_TRAFFIC_UHD31 = {}
+# DRAM read + write per launch (bytes, median over the run's launches) of the
+# UHD 31-wavelength cold workload's kernels, by transform form, from one
+# one-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# kernel sources whose digest is TRAFFIC_SOURCES_SHA (sources_digest()).  Any
+# other revision of the kernels reports traffic null: a figure measured on
+# other code says nothing about this code.  Writes still resident in L2 when a
+# kernel ends are not counted.
+TRAFFIC_SOURCES_SHA = "485228694f8faa8a"
+MEASURED_TRAFFIC_UHD31 = {
+    "chosen": {
+        "resample": 82761984,
+        "crop_sum": 40303872,
+        "combine": 132654080,
+        "kspec_rows": 17591296,
+        "kspec_cols": 106215680,
+        "frame_rows": 172225536,
+        "frame_cols": 146559488,
+        "frame_inverse": 300989952,
+        "dft_gemm": 55958656,
+    },
+}
 
 
 def sources_digest() -> str:
@@ -814,6 +852,10 @@ def main():
     # events), so the copies overlap the device work as a video host would.
     e2e = None
     if not args.no_e2e:
+        all_cpus = os.sched_getaffinity(0)
+        local_cpus = gpu_local_cpus(dev)
+        if local_cpus:
+            os.sched_setaffinity(0, local_cpus)
         host_in = torch.from_numpy(frame).pin_memory()
         host_out = [torch.empty_like(host_in).pin_memory() for _ in range(2)]
         srcs = [src, torch.empty_like(src)]
@@ -862,9 +904,12 @@ def main():
         if ws > 1:
             torch.distributed.all_reduce(e_ms, op=torch.distributed.ReduceOp.MAX)
         nbytes = frame.nbytes
+        os.sched_setaffinity(0, all_cpus)
         e2e = {"value": ws * args.steps / (float(e_ms.item()) / 1000.0), "unit": "frames/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "pipelining": "copy-in / render / copy-out streams, two frame slots"}
+               "pipelining": "copy-in / render / copy-out streams, two frame slots",
+               "host_cpus": (f"{len(local_cpus)} local to the GPU (NVML affinity)" if local_cpus
+                             else "all (no NVML affinity)")}
 
     # ---- roofline of the dominant kernel ----------------------------------
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -1026,6 +1071,11 @@ def main():
             "stage_ms_per_frame": stage_ms,
             "roofline": roofline,
             "kernel_hbm_frac": kernel_frac,
+            # DRAM bytes per launch measured on these kernel sources, beside
+            # the algorithmic bytes (null on any other revision)
+            "kernel_traffic": ({k: {"dram_bytes": v, "algorithmic_bytes": alg.get(k)}
+                                for k, v in MEASURED_TRAFFIC_UHD31.get(args.fft_form, {}).items()}
+                               if traffic_ok else None),
             "autotune": autotune,
             "error": errors.get(FORM_NAMES[args.fft_form]) if errors else None,
             "clocks": clk,
