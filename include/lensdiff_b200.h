@@ -256,8 +256,10 @@ int ld_set_graphs(ld_ctx* ctx, int enable);
  * (the timed kernels rewrite the same results) and keeps the fastest for
  * later frames of the context: that first frame synchronises its stream a
  * few times.  mode 1: tune (the default); 0: the first compiled order of each
- * length; -1: the runtime-planned transforms only, no compiled orders.  No
- * counterpart in the reference. */
+ * length; 2 + k (k <= 7): the k-th compiled order of each length (its last
+ * when it has fewer), for tests and offline tuning; -1: the
+ * runtime-planned transforms only, no compiled orders.  No counterpart in
+ * the reference. */
 int ld_set_autotune(ld_ctx* ctx, int mode);
 /* The radix order chosen for transform length n: writes up to 4 radices
  * (first stage first) and returns how many, 0 when n has no compiled order

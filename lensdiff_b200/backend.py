@@ -155,7 +155,8 @@ class LensDiffPsfBankCache:
     def set_autotune(self, mode: int) -> None:
         """1: time the compiled radix orders of a new grid's transform lengths
         on its first composite frame and keep the fastest (the default); 0: the
-        first compiled order; -1: runtime-planned transforms only."""
+        first compiled order; 2 + k: the k-th compiled order of each length
+        (its last when it has fewer); -1: runtime-planned transforms only."""
         rc = self._lib.ld_set_autotune(self._h, int(mode))
         if rc != abi.LD_OK:
             raise ValueError(f"autotune mode {mode!r} rejected ({rc})")

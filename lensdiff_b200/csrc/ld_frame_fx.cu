@@ -15,21 +15,30 @@
 namespace ld {
 namespace {
 
-// Fixed plan ID: its transform type and the passes it serves (kRowPlan: the
-// frame's row transforms, length M; kColPlan: its column transforms, length Py).
+// Fixed plan ID: its transform type, the passes it serves (kRowPlan: the
+// frame's row transforms, length M; kColPlan: its column transforms, length
+// Py) and the elements per thread E its kernels are compiled for (ld_fxplans.h).
 constexpr int kRowPlan = 1, kColPlan = 2;
 template <int ID>
 struct FxType;
-template <> struct FxType<1> { using type = FixedFft<2500, 25, 25, 4>; static constexpr int role = kRowPlan; };
-template <> struct FxType<2> { using type = FixedFft<2500, 25, 4, 25>; static constexpr int role = kRowPlan; };
-template <> struct FxType<3> { using type = FixedFft<3200, 25, 16, 8>; static constexpr int role = kColPlan; };
-template <> struct FxType<4> { using type = FixedFft<3200, 25, 8, 16>; static constexpr int role = kColPlan; };
-template <> struct FxType<5> { using type = FixedFft<1250, 25, 25, 2>; static constexpr int role = kRowPlan; };
-template <> struct FxType<6> { using type = FixedFft<1250, 25, 2, 25>; static constexpr int role = kRowPlan; };
-template <> struct FxType<7> { using type = FixedFft<1600, 25, 16, 4>; static constexpr int role = kColPlan; };
-template <> struct FxType<8> { using type = FixedFft<1600, 25, 4, 16>; static constexpr int role = kColPlan; };
-template <> struct FxType<9> { using type = FixedFft<1280, 5, 16, 16>; static constexpr int role = kRowPlan; };
-template <> struct FxType<10> { using type = FixedFft<1280, 16, 5, 16>; static constexpr int role = kRowPlan; };
+template <class F, int ROLE, int FAM>
+struct FxTypeOf {
+    using type = F;
+    static constexpr int role = ROLE;
+    static constexpr int E = FAM;
+};
+template <> struct FxType<1> : FxTypeOf<FixedFft<2500, 25, 25, 4>, kRowPlan, kE25> {};
+template <> struct FxType<2> : FxTypeOf<FixedFft<2500, 25, 4, 25>, kRowPlan, kE25> {};
+template <> struct FxType<3> : FxTypeOf<FixedFft<3200, 25, 16, 8>, kColPlan, kE25> {};
+template <> struct FxType<4> : FxTypeOf<FixedFft<3200, 25, 8, 16>, kColPlan, kE25> {};
+template <> struct FxType<5> : FxTypeOf<FixedFft<1250, 25, 25, 2>, kRowPlan, kE25> {};
+template <> struct FxType<6> : FxTypeOf<FixedFft<1250, 25, 2, 25>, kRowPlan, kE25> {};
+template <> struct FxType<7> : FxTypeOf<FixedFft<1600, 25, 16, 4>, kColPlan, kE25> {};
+template <> struct FxType<8> : FxTypeOf<FixedFft<1600, 25, 4, 16>, kColPlan, kE25> {};
+template <> struct FxType<9> : FxTypeOf<FixedFft<1280, 5, 16, 16>, kRowPlan, kE25> {};
+template <> struct FxType<10> : FxTypeOf<FixedFft<1280, 16, 5, 16>, kRowPlan, kE25> {};
+template <> struct FxType<11> : FxTypeOf<FixedFft<3200, 5, 5, 16, 8>, kColPlan, kE16> {};
+template <> struct FxType<12> : FxTypeOf<FixedFft<1600, 5, 5, 16, 4>, kColPlan, kE16> {};
 
 // Calls f(FxType<id>{}); false when there is no fixed plan `id`.
 template <class F>
@@ -45,6 +54,8 @@ bool fx_visit(int id, F&& f) {
         case 8: f(FxType<8>{}); return true;
         case 9: f(FxType<9>{}); return true;
         case 10: f(FxType<10>{}); return true;
+        case 11: f(FxType<11>{}); return true;
+        case 12: f(FxType<12>{}); return true;
         default: return false;
     }
 }
@@ -53,7 +64,11 @@ bool fx_visit(int id, F&& f) {
 // from __launch_bounds__(T, MINB)).
 constexpr int rows_c(int n) { return fft_threads(n, 2, kE25) <= 224 ? 2 : 4; }
 constexpr int minb_for(int t) { return t <= 128 ? 4 : (t <= 224 ? 3 : 2); }
-constexpr int cols_minb(int t) { return t <= 192 ? 4 : 2; }
+// column passes: as many CTAs per SM as the column's working set (four
+// sequences of n complex values) fits in shared memory, at most four
+constexpr int cols_minb(int n) {
+    return kMaxSmem / (32 * n + 1024) >= 4 ? 4 : (kMaxSmem / (32 * n + 1024) >= 3 ? 3 : 2);
+}
 
 template <class FFT>
 void rows_fixed(const FrameArgs& a, cudaStream_t s) {
@@ -67,12 +82,13 @@ void rows_fixed(const FrameArgs& a, cudaStream_t s) {
     f<<<a.Hp / C, T, sm, s>>>(b);
 }
 
-template <class FFT, bool H16>
+template <class D, bool H16>
 void cols_fixed(FrameArgs a, cudaStream_t s) {
+    using FFT = typename D::type;
     constexpr int N = FFT::n;
-    constexpr int T = fft_threads(N, 3, kE25);
+    constexpr int T = fft_threads(N, 3, D::E);
     const size_t sm = frame_cols_smem(N, 3);
-    auto f = frame_cols_kernel<kE25, 3, T, cols_minb(T), H16, FFT>;
+    auto f = frame_cols_kernel<D::E, 3, T, cols_minb(N), H16, FFT>;
     a.ahead = resident_ctas(f, T, sm);
     f<<<a.g.cols, T, sm, s>>>(a);
 }
@@ -96,12 +112,13 @@ void inverse_fixed(const FrameArgs& a, int rows, cudaStream_t s) {
     else inverse_fixed_m<FFT, H16, minb_for(T)>(a, rows, s);
 }
 
-template <class FFT, bool H16>
+template <class D, bool H16>
 void kspec_cols_fixed(KernelSpectraArgs a, cudaStream_t s) {
+    using FFT = typename D::type;
     constexpr int N = FFT::n;
-    constexpr int T = fft_threads(N, 3, kE25);
+    constexpr int T = fft_threads(N, 3, D::E);
     const size_t sm = kspec_cols_smem(N, a.Kp, 3);
-    auto f = kspec_cols_kernel<kE25, 3, T, cols_minb(T), H16, FFT>;
+    auto f = kspec_cols_kernel<D::E, 3, T, cols_minb(N), H16, FFT>;
     a.ahead = resident_ctas(f, T, sm);
     f<<<a.g.cols, T, sm, s>>>(a);
 }
@@ -128,11 +145,11 @@ void configure_fixed() {
         set_smem(frame_inverse_kernel<kE25, 3, T3, minb_for(T3) + 1, true, FFT>);
         set_smem(kspec_rows_kernel<kE25, 3, T3, minb_for(T3) + 1, FFT>);
     } else {
-        constexpr int T3 = fft_threads(N, 3, kE25);
-        set_smem(frame_cols_kernel<kE25, 3, T3, cols_minb(T3), false, FFT>);
-        set_smem(frame_cols_kernel<kE25, 3, T3, cols_minb(T3), true, FFT>);
-        set_smem(kspec_cols_kernel<kE25, 3, T3, cols_minb(T3), false, FFT>);
-        set_smem(kspec_cols_kernel<kE25, 3, T3, cols_minb(T3), true, FFT>);
+        constexpr int T3 = fft_threads(N, 3, D::E);
+        set_smem(frame_cols_kernel<D::E, 3, T3, cols_minb(N), false, FFT>);
+        set_smem(frame_cols_kernel<D::E, 3, T3, cols_minb(N), true, FFT>);
+        set_smem(kspec_cols_kernel<D::E, 3, T3, cols_minb(N), false, FFT>);
+        set_smem(kspec_cols_kernel<D::E, 3, T3, cols_minb(N), true, FFT>);
     }
 }
 
@@ -157,8 +174,8 @@ bool fx_launch_frame_cols(const FrameArgs& a, cudaStream_t s) {
     fx_visit(a.g.plan_py.fixed, [&](auto d) {
         using D = decltype(d);
         if constexpr (D::role == kColPlan) {
-            if (a.h16) cols_fixed<typename D::type, true>(a, s);
-            else cols_fixed<typename D::type, false>(a, s);
+            if (a.h16) cols_fixed<D, true>(a, s);
+            else cols_fixed<D, false>(a, s);
             done = true;
         }
     });
@@ -198,8 +215,8 @@ bool fx_launch_kspec_cols(const KernelSpectraArgs& a, cudaStream_t s) {
     fx_visit(a.g.plan_py.fixed, [&](auto d) {
         using D = decltype(d);
         if constexpr (D::role == kColPlan) {
-            if (a.h16) kspec_cols_fixed<typename D::type, true>(a, s);
-            else kspec_cols_fixed<typename D::type, false>(a, s);
+            if (a.h16) kspec_cols_fixed<D, true>(a, s);
+            else kspec_cols_fixed<D, false>(a, s);
             done = true;
         }
     });

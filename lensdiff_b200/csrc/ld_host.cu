@@ -463,12 +463,16 @@ const float2* stage_twiddles(ld_ctx* c, int id) {
 
 // The fixed plan a length runs on: the autotuner's choice when it has made
 // one, else the first compiled radix order of that length (0: none).
+// Mode 2 + k pins the k-th compiled order of every length (its last when it
+// has fewer).
 int fixed_plan_for(ld_ctx* c, int n, bool allow25) {
-    if (!allow25 || c->autotune < 0) return 0;  // fixed plans are compiled in the 25-element family
+    if (!allow25 || c->autotune < 0) return 0;  // the fixed launchers serve grids of the 25-element family
+    int ids[8];
+    const int count = fx_candidates(n, ids, 8);
+    if (c->autotune >= 2) return count > 0 ? ids[std::min(c->autotune - 2, count - 1)] : 0;
     auto it = c->fixed_choice.find(n);
     if (it != c->fixed_choice.end()) return it->second;
-    int ids[8];
-    return fx_candidates(n, ids, 8) > 0 ? ids[0] : 0;
+    return count > 0 ? ids[0] : 0;
 }
 
 FftPlan make_plan(ld_ctx* c, int n, bool allow25) {
@@ -2372,7 +2376,7 @@ int ld_selftest_wait(ld_ctx* c, int32_t mode, int64_t budget_cycles, void* strea
 int ld_set_autotune(ld_ctx* c, int enable) {
     if (!c) return LD_ERR_ARG;
     std::lock_guard<std::mutex> lock(c->mu);
-    if (enable < -1 || enable > 1) return LD_ERR_ARG;
+    if (enable < -1 || enable > 9) return LD_ERR_ARG;
     c->autotune = enable;
     return LD_OK;
 }

@@ -78,3 +78,27 @@ def test_uhd_grid_tunes_both_lengths():
     assert choice[2500] is not None and choice[3200] is not None
     generic, _, _ = _render(-1, p, frame, frames=1)
     assert np.abs(out - generic).max() / float(generic[..., :3].max()) < 1e-5
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_every_compiled_order_agrees_and_matches_oracle(k):
+    """Mode 2 + k pins the k-th compiled order of each length (the 1600-point
+    columns have three: 25·16·4, 25·4·16 and the 16-element family's
+    5·5·16·4; the 1250-point rows two, the second standing in for k = 2)."""
+    p, frame = _hd_lens()
+    p = p.copy(fftForm=LensDiffFftForm.OwnChosen)
+    generic, grid, _ = _render(-1, p, frame)
+    pinned, _, _ = _render(2 + k, p, frame)
+    assert tuple(grid) == (2500, 1600)
+    assert np.abs(pinned - generic).max() / float(generic[..., :3].max()) < 1e-5
+    assert C.output_error(pinned, C.OracleResult(p, frame)) < OUT_TOL
+
+
+def test_uhd_sixteen_element_column_order_agrees():
+    """The UHD grid's 3200-point columns on the 16-element family's 5·5·16·8
+    (608 threads, two CTAs per SM) against the runtime-planned transforms."""
+    p, frame = S.workload_uhd31()
+    pinned, grid, _ = _render(4, p, frame, frames=1)
+    assert tuple(grid) == (5000, 3200)
+    generic, _, _ = _render(-1, p, frame, frames=1)
+    assert np.abs(pinned - generic).max() / float(generic[..., :3].max()) < 1e-5
