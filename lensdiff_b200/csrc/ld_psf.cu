@@ -301,114 +301,81 @@ __device__ __forceinline__ void stage_span(const Window& w, float rc, float kc, 
     *hi = min(max(a1 + 1 - w.x0, 0), whi);
 }
 
+// Shared memory of one λ-rescale tile.
 template <bool FUSED>
-__global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
-    __shared__ float ring[kRingSpanTall];  // FUSED: the ceil(r) ring energies
-    __shared__ unsigned int ring_p[FUSED ? kRingSpanTall : 1];
-    __shared__ float stage[kStageH][kStageW];
-    const int b = blockIdx.z;
-    const WavelengthInfo* wi = a.wl + b;
-    const int K = a.K, R = a.R;
-    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTallH;
-    const int tid = threadIdx.x + threadIdx.y * 32;
-    const int rbase = tile_ring_base<kTallH>(tx0, ty0, R, R);
-    for (int i = tid; i < kRingSpanTall; i += 256) {
-        ring[i] = 0.0f;
-        if constexpr (FUSED) ring_p[i] = 0u;
+struct ResampleSmem {
+    float ring[kRingSpanTall];  // FUSED: the ceil(r) ring energies, else the round(r) sums
+    unsigned int ring_p[FUSED ? kRingSpanTall : 1];
+    float stage[kStageH][kStageW];
+};
+
+// Ring slot of canvas pixel (x, y) relative to the tile's first ring `rbase`
+// (-1: no pixel): ceil(r) (FUSED) or round(r) of its distance to the centre.
+template <bool FUSED>
+__device__ __forceinline__ int ring_slot(bool in, float dx, float dy, int R, int rbase) {
+    if (!in) return -1;
+    const float rr = sqrtf(dx * dx + dy * dy);
+    return min(R, static_cast<int>(FUSED ? ceilf(rr) : roundf(rr))) - rbase;
+}
+
+// The window pixels (rows cy0.., columns cx0..) a staged tile samples.
+struct StageBox {
+    int cx0, cy0, sw, sh;
+};
+
+// The staged box of wavelength `w`'s window for the tile at (tx0, ty0);
+// ok = false when the samples are box-filtered or the span is too wide.
+__device__ __forceinline__ bool stage_box(const Window& w, float rc, float kc, float inv, int taps, int tx0, int ty0,
+                                          int K, StageBox* b) {
+    if (taps != 0) return false;
+    int cx1 = -1, cy1 = -1;
+    stage_span(w, rc, kc, inv, tx0, min(tx0 + kTile, K) - 1, &b->cx0, &cx1);
+    stage_span(w, rc, kc, inv, ty0, min(ty0 + kTallH, K) - 1, &b->cy0, &cy1);
+    b->sw = cx1 - b->cx0 + 1;
+    b->sh = cy1 - b->cy0 + 1;
+    return b->sw <= kStageW && b->sh <= kStageH;
+}
+
+__device__ __forceinline__ void stage_load(const Window& w, const StageBox& b, float (*stage)[kStageW], int tid) {
+    for (int i = tid; i < b.sw * b.sh; i += 256) {
+        const int r = i / b.sw, c = i - r * b.sw;
+        stage[r][c] = __ldg(w.p + static_cast<size_t>(b.cy0 + r) * w.stride + b.cx0 + c);
     }
-    const Window w{a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride, a.win_stride, wi->win_x0,
-                   wi->win_n, a.S};
-    const float kc = static_cast<float>(K - 1) * 0.5f;
-    const float inv = wi->inv_scale;
-    const int taps = wi->taps;
-    const float step = wi->step;
-    const float rc = a.raw_center;
-    float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
-    float lsum = 0.0f;  // this thread's pixels; one double add per thread below
-    unsigned int lpeak = 0u;
-    const int x = tx0 + threadIdx.x;
-    const float dx = static_cast<float>(x) - kc;
-    int cx0 = 0, cx1 = -1, cy0 = 0, cy1 = -1;
-    if (taps == 0) {
-        stage_span(w, rc, kc, inv, tx0, min(tx0 + kTile, K) - 1, &cx0, &cx1);
-        stage_span(w, rc, kc, inv, ty0, min(ty0 + kTallH, K) - 1, &cy0, &cy1);
-    }
-    const int sw = cx1 - cx0 + 1, sh = cy1 - cy0 + 1;
-    if (taps == 0 && sw <= kStageW && sh <= kStageH) {  // uniform per CTA (one wavelength, one tile)
-        for (int i = tid; i < sw * sh; i += 256) {
-            const int r = i / sw, c = i - r * sw;
-            stage[r][c] = __ldg(w.p + static_cast<size_t>(cy0 + r) * w.stride + cx0 + c);
-        }
-        __syncthreads();
-        // the column half of each sample, in staged coordinates
-        const ColTap ct = col_tap(w, rc + dx * inv);
-        const int sx0 = ct.ax0 - cx0, sx1 = ct.ax1 - cx0;
-        const float lim = static_cast<float>(w.S - 1);
-        const int hi = w.n - 1;
-#pragma unroll 4
-        for (int i = 0; i < kTallH / 8; ++i) {
-            const int y = ty0 + threadIdx.y + 8 * i;
-            if (y >= K) break;  // uniform: a warp is one canvas row
-            const float dy = static_cast<float>(y) - kc;
-            const float yy = rc + dy * inv;
-            float v = 0.0f;
-            if (x < K && ct.in && !(yy < 0.0f || yy > lim)) {  // sample_row's arithmetic on staged pixels
-                const int y0 = static_cast<int>(floorf(yy));
-                const int y1 = min(y0 + 1, w.S - 1);
-                const float ty = yy - static_cast<float>(y0);
-                const int sy0 = min(max(y0 - w.x0, 0), hi) - cy0;
-                const int sy1 = min(max(y1 - w.x0, 0), hi) - cy0;
-                const float v00 = stage[sy0][sx0], v10 = stage[sy0][sx1];
-                const float v01 = stage[sy1][sx0], v11 = stage[sy1][sx1];
-                const float vx0 = v00 + (v10 - v00) * ct.tx;
-                const float vx1 = v01 + (v11 - v01) * ct.tx;
-                v = vx0 + (vx1 - vx0) * ty;
-            }
-            if (x < K) canvas[static_cast<size_t>(y) * K + x] = v;
-            lsum += v;
-            const float rr = sqrtf(dx * dx + dy * dy);
-            int slot;
-            if constexpr (FUSED) {
-                lpeak = max(lpeak, __float_as_uint(v));
-                slot = min(R, static_cast<int>(ceilf(rr))) - rbase;
-            } else {
-                slot = min(R, static_cast<int>(roundf(rr))) - rbase;
-            }
-            warp_runs_accumulate<FUSED>(x < K ? slot : -1, v, ring, ring_p);
-        }
-    } else {  // box-filtered samples (and any span too wide to stage) read the window directly
-        __syncthreads();
-        const ColTap ct = col_tap(w, rc + dx * inv);
-#pragma unroll 4
-        for (int i = 0; i < kTallH / 8; ++i) {
-            const int y = ty0 + threadIdx.y + 8 * i;
-            if (y >= K) break;  // uniform: a warp is one canvas row (the last tile row is mostly past K)
-            const bool in = x < K;
-            float v = 0.0f;
-            int slot = -1;
-            if (in) {
-                const float dy = static_cast<float>(y) - kc;
-                v = taps == 0 ? sample_row(w, ct, rc + dy * inv)
-                              : sample_filtered(w, rc + dx * inv, rc + dy * inv, inv, taps, step);
-                canvas[static_cast<size_t>(y) * K + x] = v;
-                lsum += v;
-                if constexpr (FUSED) {
-                    lpeak = max(lpeak, __float_as_uint(v));
-                    slot = min(R, static_cast<int>(ceilf(sqrtf(dx * dx + dy * dy)))) - rbase;
-                } else {
-                    slot = min(R, static_cast<int>(roundf(sqrtf(dx * dx + dy * dy)))) - rbase;
-                }
-            }
-            warp_runs_accumulate<FUSED>(slot, v, ring, ring_p);
-        }
-    }
+}
+
+// sample_row's arithmetic on staged pixels: the bilinear sample at window
+// row coordinate yy of the column tap ct (sx0, sx1: its columns in the box).
+__device__ __forceinline__ float staged_sample(const Window& w, const ColTap& ct, int sx0, int sx1, int cy0,
+                                              const float (*stage)[kStageW], bool in, float yy) {
+    const float lim = static_cast<float>(w.S - 1);
+    if (!(in && ct.in && !(yy < 0.0f || yy > lim))) return 0.0f;
+    const int hi = w.n - 1;
+    const int y0 = static_cast<int>(floorf(yy));
+    const int y1 = min(y0 + 1, w.S - 1);
+    const float ty = yy - static_cast<float>(y0);
+    const int sy0 = min(max(y0 - w.x0, 0), hi) - cy0;
+    const int sy1 = min(max(y1 - w.x0, 0), hi) - cy0;
+    const float v00 = stage[sy0][sx0], v10 = stage[sy0][sx1];
+    const float v01 = stage[sy1][sx0], v11 = stage[sy1][sx1];
+    const float vx0 = v00 + (v10 - v00) * ct.tx;
+    const float vx1 = v01 + (v11 - v01) * ct.tx;
+    return vx0 + (vx1 - vx0) * ty;
+}
+
+// The end of one wavelength's tile: the CTA's ring sums and peaks, the peak
+// and the canvas sum go to the wavelength's global statistics.
+template <bool FUSED>
+__device__ __forceinline__ void resample_flush(const PsfBankArgs& a, int b, int rbase, ResampleSmem<FUSED>& sm,
+                                               float lsum, unsigned int lpeak, int tid) {
     __syncthreads();
+    const int R = a.R;
     const size_t ro = static_cast<size_t>(b) * (R + 1);
     for (int i = tid; i < kRingSpanTall; i += 256) {
         if (rbase + i > R) continue;
-        if (ring[i] != 0.0f) atomicAdd(&(FUSED ? a.ring_ceil : a.ring_round)[ro + rbase + i], static_cast<double>(ring[i]));
+        if (sm.ring[i] != 0.0f)
+            atomicAdd(&(FUSED ? a.ring_ceil : a.ring_round)[ro + rbase + i], static_cast<double>(sm.ring[i]));
         if constexpr (FUSED) {
-            if (ring_p[i] != 0u) atomicMax(&a.ring_peak[ro + rbase + i], ring_p[i]);
+            if (sm.ring_p[i] != 0u) atomicMax(&a.ring_peak[ro + rbase + i], sm.ring_p[i]);
         }
     }
     if constexpr (FUSED) {
@@ -420,6 +387,199 @@ __global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
         atomicAdd(&a.scalars[b].s1, tot);
         if constexpr (FUSED) atomicAdd(&a.scalars[b].s3, tot);
     }
+}
+
+// One wavelength's 32 x 128 canvas tile (grid (ceil(K/32), ceil(K/128), .),
+// block (32, 8); 16 rows per thread).
+// FUSED (anisotropy gain 1): reshapeAnisotropy (LensDiffCpuReference.cpp:1122-1134)
+// then gives mean + (base - mean) * 1, the base kernel itself up to one
+// rounding, so the canvas keeps the resampled values unnormalised and this
+// pass takes the shaped kernel's statistics that shape_stats_kernel takes
+// otherwise (s3 = s1, the ceil(r) ring energies and peaks, the peak) in
+// place of the round(r) ring sums, which only the Split look's ring means
+// need (ring_sums_kernel, run when a Split render first uses the bank).
+// The bilinear path (no box filter: the canvas samples the |F|^2 window at
+// most one window pixel apart, scaleFactor >= 1) stages the window pixels the
+// tile reads in shared memory first (stage_box); box-filtered samples, and
+// any span too wide to stage, read the window directly.
+template <bool FUSED>
+__device__ void resample_tile(const PsfBankArgs& a, int b, int rbase, ResampleSmem<FUSED>& sm, int tid) {
+    for (int i = tid; i < kRingSpanTall; i += 256) {
+        sm.ring[i] = 0.0f;
+        if constexpr (FUSED) sm.ring_p[i] = 0u;
+    }
+    const WavelengthInfo* wi = a.wl + b;
+    const int K = a.K, R = a.R;
+    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTallH;
+    const Window w{a.win + static_cast<size_t>(b) * a.win_stride * a.win_stride, a.win_stride, wi->win_x0,
+                   wi->win_n, a.S};
+    const float kc = static_cast<float>(K - 1) * 0.5f;
+    const float inv = wi->inv_scale;
+    const int taps = wi->taps;
+    const float step = wi->step;
+    const float rc = a.raw_center;
+    float* canvas = a.canvas + static_cast<size_t>(b) * K * K;
+    float lsum = 0.0f;  // this thread's pixels; one double add per thread at the flush
+    unsigned int lpeak = 0u;
+    const int x = tx0 + threadIdx.x;
+    const bool in = x < K;
+    const float dx = static_cast<float>(x) - kc;
+    StageBox bx;
+    if (stage_box(w, rc, kc, inv, taps, tx0, ty0, K, &bx)) {  // uniform per CTA
+        stage_load(w, bx, sm.stage, tid);
+        __syncthreads();
+        const ColTap ct = col_tap(w, rc + dx * inv);
+        const int sx0 = ct.ax0 - bx.cx0, sx1 = ct.ax1 - bx.cx0;
+#pragma unroll 4
+        for (int i = 0; i < kTallH / 8; ++i) {
+            const int y = ty0 + threadIdx.y + 8 * i;
+            if (y >= K) break;  // uniform: a warp is one canvas row
+            const float dy = static_cast<float>(y) - kc;
+            const float v = staged_sample(w, ct, sx0, sx1, bx.cy0, sm.stage, in, rc + dy * inv);
+            if (in) canvas[static_cast<size_t>(y) * K + x] = v;
+            lsum += v;
+            if constexpr (FUSED) lpeak = max(lpeak, __float_as_uint(v));
+            warp_runs_accumulate<FUSED>(ring_slot<FUSED>(in, dx, dy, R, rbase), v, sm.ring, sm.ring_p);
+        }
+    } else {
+        __syncthreads();
+        const ColTap ct = col_tap(w, rc + dx * inv);
+#pragma unroll 4
+        for (int i = 0; i < kTallH / 8; ++i) {
+            const int y = ty0 + threadIdx.y + 8 * i;
+            if (y >= K) break;  // uniform: a warp is one canvas row (the last tile row is mostly past K)
+            const float dy = static_cast<float>(y) - kc;
+            float v = 0.0f;
+            if (in) {
+                v = taps == 0 ? sample_row(w, ct, rc + dy * inv)
+                              : sample_filtered(w, rc + dx * inv, rc + dy * inv, inv, taps, step);
+                canvas[static_cast<size_t>(y) * K + x] = v;
+                lsum += v;
+                if constexpr (FUSED) lpeak = max(lpeak, __float_as_uint(v));
+            }
+            warp_runs_accumulate<FUSED>(ring_slot<FUSED>(in, dx, dy, R, rbase), v, sm.ring, sm.ring_p);
+        }
+    }
+    resample_flush<FUSED>(a, b, rbase, sm, lsum, lpeak, tid);
+}
+
+// grid (ceil(K/32), ceil(K/128), B), block (32, 8): wavelength blockIdx.z.
+template <bool FUSED>
+__global__ void __launch_bounds__(256) resample_kernel(PsfBankArgs a) {
+    __shared__ ResampleSmem<FUSED> sm;
+    const int tid = threadIdx.x + threadIdx.y * 32;
+    const int rbase = tile_ring_base<kTallH>(blockIdx.x * kTile, blockIdx.y * kTallH, a.R, a.R);
+    resample_tile<FUSED>(a, blockIdx.z, rbase, sm, tid);
+}
+
+// warp_runs_accumulate for the same pixels of two wavelengths: one ring
+// geometry (slot, run heads) for both, each wavelength's run sums and peaks
+// formed by the same scan steps in the same order as the single form.
+template <bool PEAK>
+__device__ __forceinline__ void warp_runs_accumulate2(int slot, float v0, float v1, float* ring0,
+                                                      unsigned int* peak0, float* ring1, unsigned int* peak1) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int prev = __shfl_up_sync(full, slot, 1);
+    const unsigned heads = __ballot_sync(full, lane == 0 || prev != slot);
+    const int head = 31 - __clz(heads & (full >> (31 - lane)));
+    float s0 = v0, s1 = v1, m0 = v0, m1 = v1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float t0 = __shfl_up_sync(full, s0, o);
+        const float t1 = __shfl_up_sync(full, s1, o);
+        const float u0 = PEAK ? __shfl_up_sync(full, m0, o) : 0.0f;
+        const float u1 = PEAK ? __shfl_up_sync(full, m1, o) : 0.0f;
+        if (lane - o >= head) {
+            s0 += t0;
+            s1 += t1;
+            if (PEAK) {
+                m0 = fmaxf(m0, u0);
+                m1 = fmaxf(m1, u1);
+            }
+        }
+    }
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u) != 0u;
+    if (tail && slot >= 0) {
+        if (s0 != 0.0f) atomicAdd(&ring0[slot], s0);
+        if (s1 != 0.0f) atomicAdd(&ring1[slot], s1);
+        if (PEAK && m0 != 0.0f) atomicMax(&peak0[slot], __float_as_uint(m0));
+        if (PEAK && m1 != 0.0f) atomicMax(&peak1[slot], __float_as_uint(m1));
+    }
+}
+
+// grid (ceil(K/32), ceil(K/128), B / 2), block (32, 8): wavelengths 2z and
+// 2z + 1 of the same tile.  When both are staged, one pass over the tile
+// samples both from their staged windows and takes each pixel's ring slot and
+// run boundaries once for the two; otherwise the two tiles run in turn.  The
+// canvases and every statistic equal those of resample_kernel.
+template <bool FUSED>
+__global__ void __launch_bounds__(256) resample_pair_kernel(PsfBankArgs a) {
+    __shared__ ResampleSmem<FUSED> sm[2];
+    const int tid = threadIdx.x + threadIdx.y * 32;
+    const int K = a.K, R = a.R;
+    const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTallH;
+    const int rbase = tile_ring_base<kTallH>(tx0, ty0, R, R);
+    const int b0 = 2 * blockIdx.z, b1 = b0 + 1;
+    const WavelengthInfo* wi0 = a.wl + b0;
+    const WavelengthInfo* wi1 = a.wl + b1;
+    const size_t wsz = static_cast<size_t>(a.win_stride) * a.win_stride;
+    const Window w0{a.win + b0 * wsz, a.win_stride, wi0->win_x0, wi0->win_n, a.S};
+    const Window w1{a.win + b1 * wsz, a.win_stride, wi1->win_x0, wi1->win_n, a.S};
+    const float kc = static_cast<float>(K - 1) * 0.5f;
+    const float rc = a.raw_center;
+    const float inv0 = wi0->inv_scale, inv1 = wi1->inv_scale;
+    StageBox bx0, bx1;
+    const bool joint = stage_box(w0, rc, kc, inv0, wi0->taps, tx0, ty0, K, &bx0) &&
+                       stage_box(w1, rc, kc, inv1, wi1->taps, tx0, ty0, K, &bx1);  // uniform per CTA
+    if (!joint) {
+        resample_tile<FUSED>(a, b0, rbase, sm[0], tid);
+        resample_tile<FUSED>(a, b1, rbase, sm[1], tid);
+        return;
+    }
+    for (int i = tid; i < kRingSpanTall; i += 256) {
+        sm[0].ring[i] = 0.0f;
+        sm[1].ring[i] = 0.0f;
+        if constexpr (FUSED) {
+            sm[0].ring_p[i] = 0u;
+            sm[1].ring_p[i] = 0u;
+        }
+    }
+    stage_load(w0, bx0, sm[0].stage, tid);
+    stage_load(w1, bx1, sm[1].stage, tid);
+    __syncthreads();
+    const int x = tx0 + threadIdx.x;
+    const bool in = x < K;
+    const float dx = static_cast<float>(x) - kc;
+    const ColTap ct0 = col_tap(w0, rc + dx * inv0), ct1 = col_tap(w1, rc + dx * inv1);
+    const int s00 = ct0.ax0 - bx0.cx0, s01 = ct0.ax1 - bx0.cx0;
+    const int s10 = ct1.ax0 - bx1.cx0, s11 = ct1.ax1 - bx1.cx0;
+    float* canvas0 = a.canvas + static_cast<size_t>(b0) * K * K;
+    float* canvas1 = a.canvas + static_cast<size_t>(b1) * K * K;
+    float lsum0 = 0.0f, lsum1 = 0.0f;
+    unsigned int lpeak0 = 0u, lpeak1 = 0u;
+#pragma unroll 2
+    for (int i = 0; i < kTallH / 8; ++i) {
+        const int y = ty0 + threadIdx.y + 8 * i;
+        if (y >= K) break;  // uniform: a warp is one canvas row
+        const float dy = static_cast<float>(y) - kc;
+        const float v0 = staged_sample(w0, ct0, s00, s01, bx0.cy0, sm[0].stage, in, rc + dy * inv0);
+        const float v1 = staged_sample(w1, ct1, s10, s11, bx1.cy0, sm[1].stage, in, rc + dy * inv1);
+        if (in) {
+            canvas0[static_cast<size_t>(y) * K + x] = v0;
+            canvas1[static_cast<size_t>(y) * K + x] = v1;
+        }
+        lsum0 += v0;
+        lsum1 += v1;
+        if constexpr (FUSED) {
+            lpeak0 = max(lpeak0, __float_as_uint(v0));
+            lpeak1 = max(lpeak1, __float_as_uint(v1));
+        }
+        warp_runs_accumulate2<FUSED>(ring_slot<FUSED>(in, dx, dy, R, rbase), v0, v1, sm[0].ring, sm[0].ring_p,
+                                     sm[1].ring, sm[1].ring_p);
+    }
+    resample_flush<FUSED>(a, b0, rbase, sm[0], lsum0, lpeak0, tid);
+    resample_flush<FUSED>(a, b1, rbase, sm[1], lsum1, lpeak1, tid);
 }
 
 // Sum over rings of the unnormalised azimuthal mean, i.e. the normaliser of
@@ -1097,9 +1257,38 @@ void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s) {
 
 bool fused_shaping(const PsfBankArgs& a) { return a.gain == 1.0f; }
 
+// The bank's wavelengths from b0 on, as a bank of their own (the per-wavelength
+// arrays the canvas passes index by wavelength, advanced to b0).
+PsfBankArgs bank_from(const PsfBankArgs& a, int b0) {
+    PsfBankArgs t = a;
+    const size_t rr = static_cast<size_t>(a.R) + 1;
+    t.wl = a.wl + b0;
+    t.win = a.win + static_cast<size_t>(b0) * a.win_stride * a.win_stride;
+    t.canvas = a.canvas + static_cast<size_t>(b0) * a.K * a.K;
+    t.ring_round = a.ring_round + b0 * rr;
+    t.ring_ceil = a.ring_ceil + b0 * rr;
+    t.ring_peak = a.ring_peak + b0 * rr;
+    t.ring_mean = a.ring_mean ? a.ring_mean + b0 * rr : nullptr;
+    t.scalars = a.scalars + b0;
+    t.B = a.B - b0;
+    return t;
+}
+
+// Wavelengths in pairs (resample_pair_kernel), the last one of an odd count
+// on its own.
 void launch_resample(const PsfBankArgs& a, cudaStream_t s) {
-    if (fused_shaping(a)) resample_kernel<true><<<tall_grid(a), dim3(32, 8), 0, s>>>(a);
-    else resample_kernel<false><<<tall_grid(a), dim3(32, 8), 0, s>>>(a);
+    const bool fused = fused_shaping(a);
+    if (a.B >= 2) {
+        dim3 g = tall_grid(a);
+        g.z = a.B / 2;
+        if (fused) resample_pair_kernel<true><<<g, dim3(32, 8), 0, s>>>(a);
+        else resample_pair_kernel<false><<<g, dim3(32, 8), 0, s>>>(a);
+    }
+    if (a.B & 1) {
+        const PsfBankArgs t = bank_from(a, a.B - 1);
+        if (fused) resample_kernel<true><<<tall_grid(t), dim3(32, 8), 0, s>>>(t);
+        else resample_kernel<false><<<tall_grid(t), dim3(32, 8), 0, s>>>(t);
+    }
 }
 
 void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s) {
