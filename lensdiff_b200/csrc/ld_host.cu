@@ -242,9 +242,20 @@ constexpr size_t kStageSlot = 16384;
 constexpr int kStageSlots = 64;  // 16 cold frames of uploads in flight
 constexpr int kBigStages = 8;
 
-// One CTA copies `words` 4-byte words from mapped pinned host memory.
-__global__ void __launch_bounds__(256) host_words_kernel(uint32_t* dst, const uint32_t* src, int words) {
-    for (int i = threadIdx.x; i < words; i += 256) dst[i] = src[i];
+// One CTA copies `words` 4-byte words from mapped pinned host memory (`src`
+// 16-byte aligned): 16 bytes per thread where `dst` allows, so a staging
+// slot's reads are all in flight at once and the copy costs about one PCIe
+// round trip.
+constexpr int kHostWordsThreads = 1024;
+__global__ void __launch_bounds__(kHostWordsThreads) host_words_kernel(uint32_t* dst, const uint32_t* src, int words) {
+    int i0 = 0;
+    if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+        const int q = words / 4;
+        for (int k = threadIdx.x; k < q; k += kHostWordsThreads)
+            reinterpret_cast<uint4*>(dst)[k] = reinterpret_cast<const uint4*>(src)[k];
+        i0 = 4 * q;
+    }
+    for (int k = i0 + threadIdx.x; k < words; k += kHostWordsThreads) dst[k] = src[k];
 }
 
 // Host -> device copy of a small host array that leaves the host free: the
@@ -293,8 +304,8 @@ void upload_async(ld_ctx* c, void* dst, const void* src, size_t bytes, cudaStrea
     std::memcpy(h, src, bytes);
     void* hd = nullptr;
     check_cuda(cudaHostGetDevicePointer(&hd, h, 0), what);
-    host_words_kernel<<<1, 256, 0, s>>>(static_cast<uint32_t*>(dst), static_cast<const uint32_t*>(hd),
-                                         static_cast<int>(bytes / 4));
+    host_words_kernel<<<1, kHostWordsThreads, 0, s>>>(static_cast<uint32_t*>(dst), static_cast<const uint32_t*>(hd),
+                                                       static_cast<int>(bytes / 4));
     check_launch(what);
     ++c->launches;
     check_cuda(cudaEventRecord(c->stage_ev[static_cast<size_t>(i)], s), what);
@@ -1188,17 +1199,24 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
             cstart[i + 1] = cstart[i] + q.mt * q.nt;
         }
     }
+    // one block, one upload: the row and column problems, then the tile
+    // prefixes and the two counters
     const int np = static_cast<int>(P);
-    DftProblem* drows = reinterpret_cast<DftProblem*>(take(2 * P * sizeof(DftProblem)));
-    DftProblem* dcols = drows + P;
-    int* dstart = reinterpret_cast<int*>(take((2 * P + 4) * sizeof(int)));
+    const size_t prob_bytes = (2 * P * sizeof(DftProblem) + 15) & ~static_cast<size_t>(15);
     std::vector<int> starts(rstart);
     starts.insert(starts.end(), cstart.begin(), cstart.end());
     starts.push_back(0);  // the two counters
     starts.push_back(0);
-    upload_async(c, drows, rows.data(), rows.size() * sizeof(DftProblem), s, "dft-upload");
-    upload_async(c, dcols, cols.data(), cols.size() * sizeof(DftProblem), s, "dft-upload");
-    upload_async(c, dstart, starts.data(), starts.size() * sizeof(int), s, "dft-upload");
+    const size_t table_bytes = prob_bytes + starts.size() * sizeof(int);
+    unsigned char* dtab = take(table_bytes);
+    DftProblem* drows = reinterpret_cast<DftProblem*>(dtab);
+    DftProblem* dcols = drows + P;
+    int* dstart = reinterpret_cast<int*>(dtab + prob_bytes);
+    std::vector<unsigned char> table(table_bytes, 0);
+    std::memcpy(table.data(), rows.data(), P * sizeof(DftProblem));
+    std::memcpy(table.data() + P * sizeof(DftProblem), cols.data(), P * sizeof(DftProblem));
+    std::memcpy(table.data() + prob_bytes, starts.data(), starts.size() * sizeof(int));
+    upload_async(c, dtab, table.data(), table_bytes, s, "dft-upload");
     DftBatchArgs gr{drows, dstart, np, rstart.back(), kDftRows, dstart + 2 * (np + 1), c->err};
     DftBatchArgs gc{dcols, dstart + (np + 1), np, cstart.back(), kDftCols, dstart + 2 * (np + 1) + 1, c->err};
     auto basis = [&](const PsfBankArgs& a, const DftPlan& d, bool rows_pass) {
