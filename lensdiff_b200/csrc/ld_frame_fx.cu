@@ -104,11 +104,12 @@ void inverse_fixed_m(const FrameArgs& a, int rows, cudaStream_t s) {
     f<<<rows, T, sm, s>>>(b);
 }
 
-// shape 0: minb_for(T) CTAs per SM; shape 1: one more (tighter register cap)
+// shape bit 0 clear: minb_for(T) CTAs per SM; set: one more (tighter
+// register cap).  (Bit 1 is the row pass's prefetch, frame_rows_kernel.)
 template <class FFT, bool H16>
 void inverse_fixed(const FrameArgs& a, int rows, cudaStream_t s) {
     constexpr int T = fft_threads(FFT::n, 3, kE25);
-    if (a.g.plan_m.shape == 1) inverse_fixed_m<FFT, H16, minb_for(T) + 1>(a, rows, s);
+    if (a.g.plan_m.shape & 1) inverse_fixed_m<FFT, H16, minb_for(T) + 1>(a, rows, s);
     else inverse_fixed_m<FFT, H16, minb_for(T)>(a, rows, s);
 }
 

@@ -216,14 +216,17 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_rows_kernel(FrameArgs a) {
     // the source rows of this CTA and of the CTA one resident generation
     // later (their part under the grid) go to L2 through the bulk-copy
     // engine while this CTA loads
+    // (bit 1 of the row plan's launch shape turns the later generation's
+    // prefetch off; the autotuner times both)
     if (!FROM_EFFECT && aligned && threadIdx.x == 0) {
         const int px0 = max(0, tx0), px1 = min(W, tx0 + 2 * M);
         const uint32_t span = px1 > px0 ? static_cast<uint32_t>(px1 - px0) * 16u : 0u;
         const int later = y0 + a.ahead * RPC;
+        const bool ahead = a.ahead > 0 && (a.g.plan_m.shape & 2) == 0;
         for (int r = 0; r < RPC && span > 0; ++r) {
             const int fy = y0 + r + ty0, fl = later + r + ty0;
             if (fy >= 0 && fy < H) bulk_prefetch_l2(a.src + static_cast<int64_t>(fy) * pitch + px0 * 16, span);
-            if (a.ahead > 0 && fl >= 0 && fl < H) bulk_prefetch_l2(a.src + static_cast<int64_t>(fl) * pitch + px0 * 16, span);
+            if (ahead && fl >= 0 && fl < H) bulk_prefetch_l2(a.src + static_cast<int64_t>(fl) * pitch + px0 * 16, span);
         }
     }
     const SelectionParams sel = a.sel;

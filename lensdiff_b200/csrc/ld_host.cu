@@ -128,6 +128,11 @@ struct ld_ctx {
     DevBuf work, scatter_canvas, scatter_ks;
     // chosen form's DFT-as-GEMM operand images and per-wavelength tiles
     DevBuf dft;
+    // the DFT basis images of the last single-lens bank: they depend only on
+    // the transform geometry (PSF size, pupil extent, union window), which a
+    // lens keeps from frame to frame when only its phase changes
+    DevBuf basis;
+    std::vector<int> basis_key;
     DevBuf debug;  // static debug views: maxima, square images, OTF scratch
     // side stream for the source's row transforms while a bank is built
     cudaStream_t side = nullptr;
@@ -1125,7 +1130,24 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
             }
         }
         P += static_cast<size_t>(a.B);
-        bytes += dft_lens_bytes(d, a.B) + (group[z] == z ? dft_basis_bytes(d) : 0);
+        bytes += dft_lens_bytes(d, a.B) + (group[z] == z && Z > 1 ? dft_basis_bytes(d) : 0);
+    }
+    // one lens: its basis images live in the context's basis cache, rebuilt
+    // only when the geometry changes
+    bool basis_cached = false;
+    if (Z == 1) {
+        const PsfBankArgs& a = *banks[0];
+        const DftPlan& d = plan[0];
+        const std::vector<int> key{a.S,       d.basis_rows, d.x0,     d.kc_rows,         d.col_n,
+                                   a.off + d.col_lo,        d.kc_cols, a.row_n, a.off + a.row_lo};
+        const size_t rb = align1k(d.dx_slab * d.kc_rows), cb = align1k(d.dy_slab * d.kc_cols);
+        basis_cached = c->basis_key == key && c->basis.bytes >= 2 * (rb + cb);
+        unsigned char* q = static_cast<unsigned char*>(ensure(c, c->basis, 2 * (rb + cb)));
+        if (!basis_cached) c->basis_key = key;
+        plan[0].dx_hi = q;
+        plan[0].dx_lo = q + rb;
+        plan[0].dy_hi = q + 2 * rb;
+        plan[0].dy_lo = q + 2 * rb + cb;
     }
     bytes += align1k(2 * P * sizeof(DftProblem)) + align1k((2 * P + 4) * sizeof(int));
     char* p = static_cast<char*>(ensure(c, c->dft, bytes));
@@ -1142,6 +1164,7 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
         d.yt_hi = take(B * d.yt_lambda);
         d.yt_lo = take(B * d.yt_lambda);
         if (group[z] == z) {
+            if (Z == 1) continue;  // the basis cache's images
             d.dx_hi = take(d.dx_slab * d.kc_rows);
             d.dx_lo = take(d.dx_slab * d.kc_rows);
             d.dy_hi = take(d.dy_slab * d.kc_cols);
@@ -1228,18 +1251,20 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
     staged(c, LD_STAGE_PSF_ROWS, s, [&] {
         for (size_t z = 0; z < Z; ++z) {
             launch_pupil_field(*banks[z], plan[z], s);
-            if (group[z] == z) launch_dft_basis(basis(*banks[z], plan[z], true), s);
+            if (group[z] == z && !basis_cached) launch_dft_basis(basis(*banks[z], plan[z], true), s);
         }
     });
     staged(c, LD_STAGE_DFT_GEMM, s, [&] { launch_dft_gemm(gr, s); });
-    staged(c, LD_STAGE_PSF_COLS, s, [&] {
-        for (size_t z = 0; z < Z; ++z)
-            if (group[z] == z) launch_dft_basis(basis(*banks[z], plan[z], false), s);
-    });
+    if (!basis_cached) {
+        staged(c, LD_STAGE_PSF_COLS, s, [&] {
+            for (size_t z = 0; z < Z; ++z)
+                if (group[z] == z) launch_dft_basis(basis(*banks[z], plan[z], false), s);
+        });
+    }
     staged(c, LD_STAGE_DFT_GEMM, s, [&] { launch_dft_gemm(gc, s); });
-    size_t groups = 0;  // the two preparation stages launched Z + groups and groups kernels
+    size_t groups = 0;  // the preparation stages launched Z + groups and groups kernels (Z without bases)
     for (size_t z = 0; z < Z; ++z) groups += group[z] == z;
-    c->launches += static_cast<int>(Z + 2 * groups) - 2;
+    c->launches += basis_cached ? static_cast<int>(Z) - 1 : static_cast<int>(Z + 2 * groups) - 2;
     // a tile is a 128 x 256 x 64 real product per K-chunk, three times (hi.hi, hi.lo, lo.hi)
     double kt = 0.0;
     for (size_t k = 0; k < P; ++k)
@@ -1986,7 +2011,7 @@ void ld_destroy(ld_ctx* c) {
     DevBuf* bufs[] = {&c->rows,   &c->win,     &c->combine_out, &c->kspec_rows, &c->frameA,    &c->frameB,
                       &c->calib,  &c->calib_psf, &c->err_word,  &c->pupil_pre,  &c->effect,    &c->cf_grid,
                       &c->cf_planes, &c->cf_sd,  &c->cf_prod,   &c->work,       &c->scatter_canvas,
-                      &c->scatter_ks, &c->dft,  &c->debug,      &c->selftest, &c->custom.img};
+                      &c->scatter_ks, &c->dft,  &c->basis,    &c->debug,    &c->selftest, &c->custom.img};
     c->cufft.release();
     for (DevBuf* b : bufs) free_buf(c, *b);
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
@@ -2072,6 +2097,7 @@ void ld_clear_caches(ld_ctx* c) {
     for (auto& e : c->set_banks) e.valid = false;
     for (auto& z : c->zone_spectra) z.valid = false;
     for (auto& z : c->spectra_lru) z.valid = false;
+    c->basis_key.clear();
 }
 
 int ld_resolve_sizes(const ld_params* p, int32_t* np, int32_t* S, int32_t* R, int32_t* B) {
@@ -2140,8 +2166,10 @@ void tune_length(ld_ctx* c, int n, int shapes, cudaStream_t s, const std::functi
     c->fixed_ms[n] = best_ms;
 }
 
-// Tunes the row length (frame_rows + frame_inverse, which share its plan; the
-// inverse pass at two launch shapes) and the column length (frame_cols) of a
+// Tunes the row length (frame_rows + frame_inverse, which share its plan; four
+// launch shapes: the inverse pass at two CTAs-per-SM caps, the row pass with
+// and without the L2 prefetch of the rows one resident generation later) and
+// the column length (frame_cols) of a
 // composite frame's grid, re-running the frame's own launches: each rewrites
 // the results it wrote before.
 void autotune_frame(ld_ctx* c, const FrameArgs& fa, cudaStream_t s) {
@@ -2153,7 +2181,7 @@ void autotune_frame(ld_ctx* c, const FrameArgs& fa, cudaStream_t s) {
         return;
     }
     if (fa.g.fam_m == kE25) {
-        tune_length(c, fa.g.M, 2, s, [&](int id, int shape) {
+        tune_length(c, fa.g.M, 4, s, [&](int id, int shape) {  // inverse CTAs per SM x row prefetch
             FrameArgs a = fa;
             a.g.plan_m.fixed = id;
             a.g.plan_m.shape = shape;
