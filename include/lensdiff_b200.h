@@ -264,9 +264,11 @@ int ld_set_autotune(ld_ctx* ctx, int mode);
 /* The radix order chosen for transform length n: writes up to 4 radices
  * (first stage first) and returns how many, 0 when n has no compiled order
  * or has not been tuned yet.  *shape_out (may be null): the launch shape
- * bits (1: the inverse row pass at one more CTA per SM; 2: the forward row
- * pass without the L2 prefetch of the rows one resident generation later);
- * *ms_out (may be null): the winner's time per tuned launch group. */
+ * bits: for a row length 1: the inverse row pass at one more CTA per SM;
+ * 2: the forward row pass, 4: the inverse row pass without the L2 prefetch
+ * of the rows one resident generation later; for a column length 2: the
+ * column pass without its look-ahead prefetch.  *ms_out (may be null): the
+ * winner's time per tuned launch group. */
 int ld_autotune_choice(ld_ctx* ctx, int32_t n, int32_t* radices_out, int32_t* shape_out, double* ms_out);
 
 /* The Custom aperture mode's image (LD_APERTURE_CUSTOM).  The reference

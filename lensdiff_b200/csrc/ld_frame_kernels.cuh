@@ -331,8 +331,8 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_cols_kernel(FrameArgs a) {
         bulk_load_checked(adst, asrc, a_bytes, &bars[0], smraw, a.err);
         if (H16) bulk_load_checked(aex, a.aexp, static_cast<uint32_t>((Hp + 15) & ~15), &bars[2], smraw, a.err);
         bulk_load_checked(kdst, ksrc, k_bytes, &bars[1], smraw, a.err);
-        const int later = k + a.ahead;
-        if (later < cols) {
+        const int later = k + a.ahead;  // bit 1 of the column plan's shape: no look-ahead (autotuned)
+        if (later < cols && (a.g.plan_py.shape & 2) == 0) {
             bulk_prefetch_l2(asrc + (later - k) * static_cast<size_t>(a_bytes), a_bytes);
             bulk_prefetch_l2(static_cast<const char*>(ksrc) + (later - k) * static_cast<size_t>(k_bytes), k_bytes);
         }
@@ -461,13 +461,16 @@ __global__ void __launch_bounds__(MAXT, MINB) frame_inverse_kernel(FrameArgs a) 
     const bool have = sy >= 0 && sy < a.H && by >= 0 && by < a.Hp;
     const int M = a.g.M;
     // composite: this row's source pixels, and those of the row one resident
-    // generation later, go to L2 while the row's spectrum loads and transforms
+    // generation later (unless bit 2 of the row plan's shape is set; the
+    // autotuner times both), go to L2 while the row's spectrum loads and
+    // transforms
     if (a.effect_mode == kEffectComposite && threadIdx.x == 0 &&
         ((reinterpret_cast<uintptr_t>(a.src) | static_cast<uintptr_t>(a.src_pitch)) & 15) == 0) {
         const uint32_t row_bytes = static_cast<uint32_t>(a.W) * 16u;
         if (have) bulk_prefetch_l2(a.src + static_cast<int64_t>(sy) * a.src_pitch, row_bytes);
         const int sl = sy + a.ahead;
-        if (a.ahead > 0 && sl >= 0 && sl < a.H && bid + a.ahead < static_cast<int>(gridDim.x))
+        if (a.ahead > 0 && (a.g.plan_m.shape & 4) == 0 && sl >= 0 && sl < a.H &&
+            bid + a.ahead < static_cast<int>(gridDim.x))
             bulk_prefetch_l2(a.src + static_cast<int64_t>(sl) * a.src_pitch, row_bytes);
     }
     if (have) {

@@ -1359,7 +1359,8 @@ BankEntry& ensure_bank(ld_ctx* c, const ld_params& p, cudaStream_t s, bool* rebu
         staged(c, LD_STAGE_PSF_ROWS, s, [&] { launch_psf_rows(a, s); });
         staged(c, LD_STAGE_PSF_COLS, s, [&] { launch_psf_cols(a, s); });
     }
-    staged(c, LD_STAGE_RESAMPLE, s, [&] { launch_resample(a, s); });
+    const bool pairs = std::all_of(infos.begin(), infos.end(), [](const WavelengthInfo& w) { return w.taps == 0; });
+    staged(c, LD_STAGE_RESAMPLE, s, [&] { launch_resample(a, pairs, s); });
     const bool fused = fused_shaping(a);
     if (!fused) staged(c, LD_STAGE_SHAPE_STATS, s, [&] { launch_shape_stats(a, s); });
     staged(c, LD_STAGE_SUPPORT, s, [&] { launch_support(a, s); });
@@ -2127,11 +2128,12 @@ constexpr size_t kGraphCache = 4;
 // every launch shape in [0, shapes) on stream s (one untimed launch, then
 // kTuneReps between two events) and records the fastest as
 // c->fixed_choice[n] = id | shape << 8.  A single candidate is recorded untimed.
-void tune_length(ld_ctx* c, int n, int shapes, cudaStream_t s, const std::function<void(int, int)>& launch) {
+void tune_length(ld_ctx* c, int n, const std::vector<int>& shapes, cudaStream_t s,
+                 const std::function<void(int, int)>& launch) {
     int ids[8];
     const int k = fx_candidates(n, ids, 8);
     if (k == 0 || c->fixed_choice.count(n)) return;
-    if (k == 1 && shapes == 1) {
+    if (k == 1 && shapes.size() == 1) {
         c->fixed_choice[n] = ids[0];
         return;
     }
@@ -2143,7 +2145,7 @@ void tune_length(ld_ctx* c, int n, int shapes, cudaStream_t s, const std::functi
     float best_ms = 0.0f;
     bool first = true;
     for (int i = 0; i < k; ++i) {
-        for (int sh = 0; sh < shapes; ++sh) {
+        for (const int sh : shapes) {
             launch(ids[i], sh);
             check_cuda(cudaEventRecord(e0, s), "tune-record");
             for (int r = 0; r < kTuneReps; ++r) launch(ids[i], sh);
@@ -2166,10 +2168,11 @@ void tune_length(ld_ctx* c, int n, int shapes, cudaStream_t s, const std::functi
     c->fixed_ms[n] = best_ms;
 }
 
-// Tunes the row length (frame_rows + frame_inverse, which share its plan; four
-// launch shapes: the inverse pass at two CTAs-per-SM caps, the row pass with
-// and without the L2 prefetch of the rows one resident generation later) and
-// the column length (frame_cols) of a
+// Tunes the row length (frame_rows + frame_inverse, which share its plan; eight
+// launch shapes: the inverse pass at two CTAs-per-SM caps, the row pass and
+// the inverse pass each with and without the L2 prefetch of the rows one
+// resident generation later) and the column length (frame_cols, with and
+// without its look-ahead prefetch) of a
 // composite frame's grid, re-running the frame's own launches: each rewrites
 // the results it wrote before.
 void autotune_frame(ld_ctx* c, const FrameArgs& fa, cudaStream_t s) {
@@ -2181,7 +2184,9 @@ void autotune_frame(ld_ctx* c, const FrameArgs& fa, cudaStream_t s) {
         return;
     }
     if (fa.g.fam_m == kE25) {
-        tune_length(c, fa.g.M, 4, s, [&](int id, int shape) {  // inverse CTAs per SM x row prefetch
+        // shape bits: inverse at one more CTA per SM; row pass, inverse pass
+        // without their look-ahead prefetch
+        tune_length(c, fa.g.M, {0, 1, 2, 3, 4, 5, 6, 7}, s, [&](int id, int shape) {
             FrameArgs a = fa;
             a.g.plan_m.fixed = id;
             a.g.plan_m.shape = shape;
@@ -2191,10 +2196,10 @@ void autotune_frame(ld_ctx* c, const FrameArgs& fa, cudaStream_t s) {
         });
     }
     if (fa.g.fam_py == kE25) {
-        tune_length(c, fa.g.Py, 1, s, [&](int id, int) {
+        tune_length(c, fa.g.Py, {0, 2}, s, [&](int id, int shape) {  // shape 2: no look-ahead prefetch
             FrameArgs a = fa;
             a.g.plan_py.fixed = id;
-            a.g.plan_py.shape = 0;
+            a.g.plan_py.shape = shape;
             a.g.plan_py.stw = stage_twiddles(c, id);
             launch_frame_cols(a, s);
         });

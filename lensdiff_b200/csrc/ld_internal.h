@@ -72,7 +72,9 @@ struct PsfBankArgs {
 void launch_pupil_pre(const PsfBankArgs& a, cudaStream_t s);
 void launch_psf_rows(const PsfBankArgs& a, cudaStream_t s);
 void launch_psf_cols(const PsfBankArgs& a, cudaStream_t s);
-void launch_resample(const PsfBankArgs& a, cudaStream_t s);
+// pairs: every wavelength samples without a box filter (taps 0), so a tile's
+// two wavelengths can share one staged pass (resample_pair_kernel)
+void launch_resample(const PsfBankArgs& a, bool pairs, cudaStream_t s);
 void launch_shape_stats(const PsfBankArgs& a, cudaStream_t s);
 // Anisotropy gain 1: shaping is the identity; launch_resample then takes the
 // shaped kernel's statistics and launch_shape_stats is not needed.  The ring

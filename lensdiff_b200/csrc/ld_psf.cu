@@ -1274,10 +1274,15 @@ PsfBankArgs bank_from(const PsfBankArgs& a, int b0) {
     return t;
 }
 
-// Wavelengths in pairs (resample_pair_kernel), the last one of an odd count
-// on its own.
-void launch_resample(const PsfBankArgs& a, cudaStream_t s) {
+// Wavelengths in pairs (resample_pair_kernel) when none is box-filtered, the
+// last one of an odd count on its own; else one per CTA.
+void launch_resample(const PsfBankArgs& a, bool pairs, cudaStream_t s) {
     const bool fused = fused_shaping(a);
+    if (!pairs) {
+        if (fused) resample_kernel<true><<<tall_grid(a), dim3(32, 8), 0, s>>>(a);
+        else resample_kernel<false><<<tall_grid(a), dim3(32, 8), 0, s>>>(a);
+        return;
+    }
     if (a.B >= 2) {
         dim3 g = tall_grid(a);
         g.z = a.B / 2;
