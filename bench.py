@@ -304,6 +304,15 @@ MEASURED_TRAFFIC_UHD31 = {
 }
 
 
+def measured_traffic(workload, bank, form):
+    """The measured per-kernel DRAM bytes of `form` on this workload, or None
+    when they were not measured on these kernel sources (another digest,
+    another workload or bank mode)."""
+    if workload != "uhd31" or bank != "cold" or sources_digest() != TRAFFIC_SOURCES_SHA:
+        return None
+    return MEASURED_TRAFFIC_UHD31.get(form)
+
+
 def sources_digest() -> str:
     """sha256 (first 16 hex digits) of the CUDA sources of the library."""
     import hashlib
@@ -929,7 +938,7 @@ def main():
     dominant = max(stage, key=lambda k: stage[k][0])
     dom_ms, dom_n = stage[dominant]
     roofline = None
-    traffic_ok = args.workload == "uhd31" and args.bank == "cold" and sources_digest() == TRAFFIC_SOURCES_SHA
+    traffic_map = measured_traffic(args.workload, args.bank, args.fft_form)
     # every HBM-bound kernel's fraction of the measured peak (the frame chain's
     # fused FFT kernels first among them)
     kernel_frac = {}
@@ -939,7 +948,7 @@ def main():
     if dominant in alg and dom_n:
         per_launch_ms = dom_ms / dom_n
         achieved = alg[dominant] / (per_launch_ms / 1000.0) / 1e9
-        traffic = MEASURED_TRAFFIC_UHD31.get(args.fft_form, {}).get(dominant) if traffic_ok else None
+        traffic = traffic_map.get(dominant) if traffic_map else None
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                     "algorithmic_bytes_per_launch": alg[dominant], "launch_ms": per_launch_ms}
@@ -1073,9 +1082,8 @@ def main():
             "kernel_hbm_frac": kernel_frac,
             # DRAM bytes per launch measured on these kernel sources, beside
             # the algorithmic bytes (null on any other revision)
-            "kernel_traffic": ({k: {"dram_bytes": v, "algorithmic_bytes": alg.get(k)}
-                                for k, v in MEASURED_TRAFFIC_UHD31.get(args.fft_form, {}).items()}
-                               if traffic_ok else None),
+            "kernel_traffic": ({k: {"dram_bytes": v, "algorithmic_bytes": alg.get(k)} for k, v in traffic_map.items()}
+                               if traffic_map else None),
             "autotune": autotune,
             "error": errors.get(FORM_NAMES[args.fft_form]) if errors else None,
             "clocks": clk,
