@@ -289,18 +289,18 @@ class Clocks:
 # other revision of the kernels reports traffic null: a figure measured on
 # other code says nothing about this code.  Writes still resident in L2 when a
 # kernel ends are not counted.
-TRAFFIC_SOURCES_SHA = "4c1c7ba886d98e10"
+TRAFFIC_SOURCES_SHA = "d7f4cd7799c9133d"
 MEASURED_TRAFFIC_UHD31 = {
     "chosen": {
-        "resample": 77907456,
-        "crop_sum": 40303872,
-        "combine": 132434432,
-        "kspec_rows": 19881216,
-        "kspec_cols": 105158912,
-        "frame_rows": 140358912,
-        "frame_cols": 146119424,
-        "frame_inverse": 290886912,
-        "dft_gemm": 56443648,
+        "resample": 78053376,
+        "crop_sum": 40304640,
+        "combine": 132500224,
+        "kspec_rows": 19684864,
+        "kspec_cols": 105022976,
+        "frame_rows": 140078848,
+        "frame_cols": 146548480,
+        "frame_inverse": 291208192,
+        "dft_gemm": 56408320,
     },
 }
 

@@ -133,6 +133,7 @@ struct ld_ctx {
     // lens keeps from frame to frame when only its phase changes
     DevBuf basis;
     std::vector<int> basis_key;
+    std::string pupil_key;  // what pupil_pre holds (setup_pupil)
     DevBuf debug;  // static debug views: maxima, square images, OTF scratch
     // side stream for the source's row transforms while a bank is built
     cudaStream_t side = nullptr;
@@ -865,13 +866,34 @@ void pupil_geometry(PsfBankArgs& a, const ld_params& p, bool circle) {
     a.row_n = hi - lo;
 }
 
+// The pre-pass depends on the pupil's parameters and the λ-independent phase
+// only, not on defocus, so the context's own pre-pass buffer keeps its
+// contents for the next bank with the same key (a lens whose defocus alone
+// changed skips the launch).  The key is recorded once the launch is
+// enqueued; a failure before then leaves none.
 void setup_pupil(ld_ctx* c, PsfBankArgs& a, const ld_params& p, bool circle, cudaStream_t s,
                  DevBuf* target = nullptr) {
     pupil_geometry(a, p, circle);
     const int n = a.pupil.size;
-    a.pupil_pre = static_cast<float4*>(
-        ensure(c, target ? *target : c->pupil_pre, static_cast<size_t>(n) * n * sizeof(float4)));
+    const size_t bytes = static_cast<size_t>(n) * n * sizeof(float4);
+    std::string key;
+    if (!target) {
+        const uint64_t custom = (a.pupil.custom && t_custom) ? t_custom->digest : 0;
+        key = append_bytes(key, &a.pupil, sizeof(a.pupil));
+        key = append_bytes(key, &a.base_phase, sizeof(a.base_phase));
+        key = append_bytes(key, &custom, sizeof(custom));
+        if (key == c->pupil_key && c->pupil_pre.bytes >= bytes) {
+            a.pupil_pre = static_cast<float4*>(c->pupil_pre.p);
+            return;
+        }
+        c->pupil_key.clear();
+    }
+    a.pupil_pre = static_cast<float4*>(ensure(c, target ? *target : c->pupil_pre, bytes));
     staged(c, LD_STAGE_PUPIL, s, [&] { launch_pupil_pre(a, s); });
+    if (!target) {
+        check_launch("pupil-pre");
+        c->pupil_key = key;
+    }
 }
 
 void dft_gemm_psf(ld_ctx* c, const PsfBankArgs& a, const std::vector<WavelengthInfo>& infos, cudaStream_t s);
@@ -1135,6 +1157,7 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
     // one lens: its basis images live in the context's basis cache, rebuilt
     // only when the geometry changes
     bool basis_cached = false;
+    std::vector<int> basis_key;
     if (Z == 1) {
         const PsfBankArgs& a = *banks[0];
         const DftPlan& d = plan[0];
@@ -1142,8 +1165,11 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
                                    a.off + d.col_lo,        d.kc_cols, a.row_n, a.off + a.row_lo};
         const size_t rb = align1k(d.dx_slab * d.kc_rows), cb = align1k(d.dy_slab * d.kc_cols);
         basis_cached = c->basis_key == key && c->basis.bytes >= 2 * (rb + cb);
+        // the key is recorded once both basis launches are enqueued: a build
+        // that fails before then leaves no key for stale images to match
+        if (!basis_cached) c->basis_key.clear();
         unsigned char* q = static_cast<unsigned char*>(ensure(c, c->basis, 2 * (rb + cb)));
-        if (!basis_cached) c->basis_key = key;
+        basis_key = key;
         plan[0].dx_hi = q;
         plan[0].dx_lo = q + rb;
         plan[0].dy_hi = q + 2 * rb;
@@ -1260,6 +1286,8 @@ void dft_gemm_psf_batch(ld_ctx* c, const std::vector<const PsfBankArgs*>& banks,
             for (size_t z = 0; z < Z; ++z)
                 if (group[z] == z) launch_dft_basis(basis(*banks[z], plan[z], false), s);
         });
+        check_launch("dft-basis");
+        if (Z == 1) c->basis_key = basis_key;
     }
     staged(c, LD_STAGE_DFT_GEMM, s, [&] { launch_dft_gemm(gc, s); });
     size_t groups = 0;  // the preparation stages launched Z + groups and groups kernels (Z without bases)
@@ -2099,6 +2127,7 @@ void ld_clear_caches(ld_ctx* c) {
     for (auto& z : c->zone_spectra) z.valid = false;
     for (auto& z : c->spectra_lru) z.valid = false;
     c->basis_key.clear();
+    c->pupil_key.clear();
 }
 
 int ld_resolve_sizes(const ld_params* p, int32_t* np, int32_t* S, int32_t* R, int32_t* B) {

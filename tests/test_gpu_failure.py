@@ -21,7 +21,7 @@ torch = pytest.importorskip("torch")
 from lensdiff_b200 import abi  # noqa: E402
 from lensdiff_b200 import synthetic as S  # noqa: E402
 from lensdiff_b200.backend import LensDiffPsfBankCache, image_request  # noqa: E402
-from lensdiff_b200.types import LensDiffApertureMode, LensDiffSpectralMode  # noqa: E402
+from lensdiff_b200.types import LensDiffApertureMode, LensDiffFftForm, LensDiffSpectralMode  # noqa: E402
 from tests.helpers import with_matrices  # noqa: E402
 
 pytestmark = pytest.mark.gpu
@@ -89,22 +89,32 @@ def test_selftest_rejects_bad_modes_and_budgets(cache):
     assert _selftest(cache, 0, 10 ** 12)[0] == abi.LD_ERR_ARG
 
 
-def test_injected_allocation_failure_is_reported_and_recoverable():
+@pytest.mark.parametrize("form,afters", [(LensDiffFftForm.OwnFp32, (0, 3)),
+                                         (LensDiffFftForm.OwnChosen, (0, 3, 6, 9, 12, 15))])
+def test_injected_allocation_failure_is_reported_and_recoverable(form, afters):
+    """Every allocation of a first render may fail; the context must then
+    render the lens as a clean one does.  In the chosen form the failures
+    land between the cached pre-pass, DFT basis and operand allocations, so a
+    cache key recorded before its contents were written would show here."""
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     frame = S.make_frame(160, 96, 8, 1.0, 50.0, seed=4)
+    lens = _lens().copy(fftForm=form)
     clean = LensDiffPsfBankCache(0)
-    st, ref = _render(clean, _lens(), frame)
+    st, ref = _render(clean, lens, frame)
     clean.close()
     assert st.ok, st
-    for after in (0, 3):
+    for after in afters:
         c = LensDiffPsfBankCache(0)
         assert c._lib.ld_inject_alloc_failure(c.handle, after) == abi.LD_OK
-        st, _ = _render(c, _lens(), frame)
+        st, _ = _render(c, lens, frame)
+        if st.ok:  # fewer allocations than `after`: nothing failed
+            c.close()
+            continue
         assert st.code == abi.LD_ERR_OOM, st
         assert "device-allocation-failed (injected)" in st.stage
         assert c._lib.ld_inject_alloc_failure(c.handle, -1) == abi.LD_OK
-        st, out = _render(c, _lens(), frame)
+        st, out = _render(c, lens, frame)
         assert st.ok, st
         # each context builds its own bank, whose ring and energy sums are
         # double-precision atomic adds in no fixed order: a sum that rounds
