@@ -13,6 +13,7 @@ from lensdiff_b200 import synthetic as S  # noqa: E402
 from lensdiff_b200.backend import LensDiffPsfBankCache, image_request, resolve_sizes, run_lensdiff_cuda  # noqa: E402
 from lensdiff_b200.types import (  # noqa: E402
     LensDiffApertureMode,
+    LensDiffFftForm,
     LensDiffLookMode,
     LensDiffRgbMode,
     LensDiffSpectralMode,
@@ -163,8 +164,12 @@ def test_render_tier_x_hd_lens_matches_oracle(cache):
     assert rel_err(out, ref, ref[..., :3].max()) < OUT_TOL
 
 
-def test_render_window_origin_and_odd_sizes(cache):
-    p = with_matrices(small_lens())
+@pytest.mark.parametrize("form", [LensDiffFftForm.OwnFp32, LensDiffFftForm.OwnChosen])
+def test_render_window_origin_and_odd_sizes(cache, form):
+    """Odd frame sizes and shifted origins; in the chosen form the row
+    spectra rows are padded to a multiple of 4 (117 -> 120) and their
+    exponent bytes to a multiple of 16 for the column pass's bulk copy."""
+    p = with_matrices(small_lens(fftForm=form))
     src = S.make_frame(203, 117, 20, 1.0, 60.0, seed=3)
     origin = (40, -13)
     dst_origin = (30, -20)
@@ -237,3 +242,34 @@ def test_error_behaviour_mirrors_reference(cache):
     assert st.code == 1 and st.stage == "custom-aperture-image-not-set"
     st = cache.render(req, p)
     assert st.ok
+
+
+def test_pupil_and_basis_caches_follow_the_lens(cache):
+    """The context keeps the pupil pre-pass and the DFT bases of the last
+    single-lens bank while only the defocus changes.  Alternating lenses of
+    different apertures and PSF windows must give each lens's own result:
+    the same as a fresh context's, and the same on its second turn (to a
+    float step of the frame maximum: each bank rebuild sums its statistics
+    with atomics)."""
+    src = S.make_frame(200, 120, 16, 1.0, 80.0, seed=21)
+    pa = with_matrices(small_lens(fftForm=LensDiffFftForm.OwnChosen))
+    pb = with_matrices(small_lens(fftForm=LensDiffFftForm.OwnChosen, bladeCount=9, roundness=0.6,
+                                  diffractionScalePx=4.5))
+    a1, st = render_gpu(cache, pa, src)
+    assert st.ok, st
+    b1, st = render_gpu(cache, pb, src)
+    assert st.ok and st.bank_rebuilt, st
+    a2, st = render_gpu(cache, pa.copy(phaseDefocus=pa.phaseDefocus + 1e-6), src)
+    assert st.ok and st.bank_rebuilt, st
+    a3, st = render_gpu(cache, pa, src)
+    assert st.ok, st
+    fresh = LensDiffPsfBankCache(0)
+    try:
+        b0, st = render_gpu(fresh, pb, src)
+        assert st.ok, st
+    finally:
+        fresh.close()
+    for x, y in ((a1, a3), (b1, b0)):
+        assert np.abs(x - y).max() <= 1e-6 * np.abs(y[..., :3]).max()
+    assert rel_err(a2, a1, a1[..., :3].max()) < OUT_TOL
+    assert not np.allclose(a1, b1)
