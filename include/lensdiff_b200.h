@@ -224,7 +224,7 @@ void ld_destroy(ld_ctx* ctx);
 int ld_abi_version(void);
 /* Device bytes the context holds (work buffers + caches). */
 size_t ld_device_bytes(const ld_ctx* ctx);
-/* Drops the cached PSF banks and kernel spectra. */
+/* Drops the cached PSF banks, kernel spectra, DFT bases and pupil pre-pass. */
 void ld_clear_caches(ld_ctx* ctx);
 /* Reads and clears the context's device error word (synchronising the
  * device): LD_OK if no kernel reported a problem since the last check,
