@@ -478,16 +478,18 @@ def other_workloads(dev, form):
     stream = torch.cuda.Stream(device=dev)
 
     def timed(fn, warm, n):
+        """Mean and median device ms per step of n steps after `warm`."""
         for i in range(warm):
             fn(i)
         torch.cuda.synchronize(dev)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(n + 1)]
+        ev[0].record(stream)
         for i in range(n):
             fn(warm + i)
-        e1.record(stream)
+            ev[i + 1].record(stream)
         torch.cuda.synchronize(dev)
-        return e0.elapsed_time(e1) / n
+        per = sorted(ev[i].elapsed_time(ev[i + 1]) for i in range(n))
+        return ev[0].elapsed_time(ev[-1]) / n, per[n // 2]
 
     p, frame = S.workload_zones8()
     p = p.copy(fftForm=FFT_FORMS[form])
@@ -502,8 +504,8 @@ def other_workloads(dev, form):
         if not st.ok:
             raise RuntimeError(f"zones8 render failed: {st}")
 
-    ms = timed(zone_frame, 2, 3)
-    out["zones8"] = {"value": 1000.0 / ms, "unit": "frames/s", "ms_per_step": ms, "bank": "cold",
+    ms, med = timed(zone_frame, 2, 3)
+    out["zones8"] = {"value": 1000.0 / ms, "unit": "frames/s", "ms_per_step": ms, "median_ms": med, "bank": "cold",
                      "fft_form": FORM_NAMES[form],
                      "config": "3840x2160, 8x8 field zones (64 banks x 31 wavelengths), pupil 512 -> PSF 2048"}
     cache.close()
@@ -515,8 +517,9 @@ def other_workloads(dev, form):
         if not st.ok or st.banks_rebuilt != len(lenses):
             raise RuntimeError(f"lens-set build failed: {st}")
 
-    ms = timed(lens_step, 1, 2)
-    out["lens_set"] = {"value": 256 * 1000.0 / ms, "unit": "lens banks/s", "ms_per_step": ms, "bank": "cold",
+    ms, med = timed(lens_step, 1, 2)
+    out["lens_set"] = {"value": 256 * 1000.0 / ms, "unit": "lens banks/s", "ms_per_step": ms, "median_ms": med,
+                       "bank": "cold",
                        "fft_form": FORM_NAMES[form],
                        "config": "256 unrelated lenses per step: pupil 128-1024, PSF 2-4x, 8-64 wavelengths"}
     if cache.check_device_errors():
